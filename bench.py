@@ -1,0 +1,384 @@
+#!/usr/bin/env python3
+"""SpGEMM benchmark: GFLOP/s (2 x intermediate products / s) and HBM fraction.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--workload NAME]
+  python bench.py --impl reference ...      # the reference scalar CPU backend
+
+A step is one pass of the hot path over the workload's input:
+  laplace2d   (default) C = A x A, A the 2D 5-point Laplacian on 1024^2
+              (n = 1,048,576, nnz = 5,238,784): one full product
+              (work_estimation + compute) with A resident in HBM.
+  uniform4096 C = A x B, 4096^2, exactly 16 nnz/row (A seed S, B seed S+1).
+  stencil3d   C = A x A, 27-point stencil on 128^3: one full product.
+  stencil3d_reuse  the same product, numeric-only compute (structure reused,
+              values perturbed by U[-0.01, 0.01] between repeats).
+
+Output: one JSON line (rank 0).  `value` is device-timed throughput of the
+whole job with inputs resident in HBM (CUDA events around each step, L2
+flushed by a 256 MiB write between steps, max over ranks); `e2e` is the same
+metric through the public C API in host memory space (pinned host buffers,
+host<->device copies inside the timed region); `roofline` is for the
+dominant kernel phase, timed with CUDA events on its own launch stream;
+`cpu_baseline` is the reference scalar backend on this host's cores.
+
+Multi-GPU (torchrun): every rank computes the full workload on its own GPU
+(weak scaling: rows of C are independent and no data crosses GPUs).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT / "rv-sparse_b200"))
+
+METRIC = "SpGEMM GFLOP/s + HBM % peak: learned-binned/batched vs plain GPU Gustavson"
+UNIT = "GFLOP/s"
+FALLBACK_HBM_GBS = 6650.0
+
+WORKLOADS = {
+    "laplace2d": "2D 5-point Laplacian 1024x1024 (n=1,048,576, nnz=5,238,784), C=A*A, full product",
+    "uniform4096": "4096x4096, exactly 16 nnz/row uniform columns, values U[-1,1], C=A*B, full product",
+    "stencil3d": "3D 27-point stencil 128^3 (n=2,097,152, nnz=55,742,968), C=A*A, full product",
+    "stencil3d_reuse": "3D 27-point stencil 128^3, C=A*A, numeric-only repeats (values perturbed U[-0.01,0.01])",
+}
+
+
+def build_inputs(name: str, seed: int = 2024):
+    from rvsp import gen
+    if name == "laplace2d":
+        A = gen.laplacian_2d(1024)
+        return A, A
+    if name == "uniform4096":
+        return gen.uniform_rows(4096, 4096, 16, seed), gen.uniform_rows(4096, 4096, 16, seed + 1)
+    if name in ("stencil3d", "stencil3d_reuse"):
+        A = gen.stencil_3d_27(128)
+        return A, A
+    raise ValueError(name)
+
+
+def measured_peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d.get("hbm_gbs", FALLBACK_HBM_GBS)), "measured"
+    return FALLBACK_HBM_GBS, "fallback"
+
+
+def committed_traffic(workload: str, phase: str):
+    p = ROOT / "profiles" / "traffic.json"
+    if not p.exists():
+        return None
+    d = json.loads(p.read_text())
+    return d.get(workload, {}).get(phase)
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = Path(os.environ.get("TMPDIR", "/tmp")) / f"rvsp_clocks_{os.getpid()}.csv"
+
+    def start(self):
+        try:
+            self.fh = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=self.fh, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.fh.close()
+        sm, smax, reasons = [], [], set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for line in self.path.read_text().splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax.append(float(f[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        self.path.unlink(missing_ok=True)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(smax) if smax else None,
+                "samples": len(sm), "reasons": sorted(reasons)}
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def run_reference(args, world, rank):
+    """The reference scalar CPU backend (oracle/_ref/librvsp_ref.so, built from
+    the reference sources; the C restatement if that is absent) on all host
+    threads; rank 0 only."""
+    if rank != 0:
+        return 0
+    sys.path.insert(0, str(ROOT))
+    from oracle import oracle
+    from rvsp import intermediate_products
+    A, B = build_inputs(args.workload)
+    flops = 2.0 * float(intermediate_products(A, B).sum())
+    threads = os.cpu_count() or 1
+    kind = "reference" if oracle.ref_available() else "port"
+    per_step = []
+    for i in range(args.warmup + args.steps):
+        runs, el = oracle.time_reference_oneshot(A, B, seconds=0.0, threads=threads,
+                                                 max_runs=threads)
+        if i >= args.warmup:
+            per_step.append((runs, el))
+    runs = sum(r for r, _ in per_step)
+    el = sum(e for _, e in per_step)
+    value = flops * runs / el / 1e9
+    sample = (f"{runs} full one-shot products of {args.workload} "
+              f"({args.steps} steps x {threads} threads)")
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "impl": "reference",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1e3 * el / max(args.steps, 1), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic", "config": {"workload": WORKLOADS[args.workload]},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": kind,
+                             "sample": sample},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def cpu_baseline(A, B, flops, seconds=12.0):
+    sys.path.insert(0, str(ROOT))
+    from oracle import oracle
+    threads = os.cpu_count() or 1
+    runs, el = oracle.time_reference_oneshot(A, B, seconds=seconds, threads=threads,
+                                             max_runs=400)
+    return {"value": flops * runs / el / 1e9, "unit": UNIT, "cores": threads,
+            "kind": "reference" if oracle.ref_available() else "port",
+            "sample": f"{runs} full one-shot products on {threads} threads in {el:.1f} s"}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=40)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--workload", default="laplace2d", choices=sorted(WORKLOADS))
+    ap.add_argument("--impl", default="ours", choices=("ours", "reference"))
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--e2e-steps", type=int, default=10)
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    world, rank, local = dist_setup()
+
+    if args.impl == "reference":
+        return run_reference(args, world, rank)
+
+    import torch
+    import rvsp
+    from rvsp import CSR, Descriptor, DeviceCSR, intermediate_products
+    from rvsp import _lib as L
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    pg = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=dev)
+        pg = dist
+
+    A, B = build_inputs(args.workload)
+    ops = intermediate_products(A, B)
+    flops = 2.0 * float(ops.sum())
+    dA = DeviceCSR.from_host(A, dev)
+    dB = dA if B is A else DeviceCSR.from_host(B, dev)
+    stream = torch.cuda.current_stream(dev)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    reuse = args.workload.endswith("_reuse")
+
+    d = Descriptor(memory=L.MEM_DEVICE, stream=stream, profiling=True)
+    ws_bytes, c_nnz = d.work_estimation(dA, dB)
+    dC = DeviceCSR.empty(A.rows, B.cols, c_nnz, dev)
+    ws = torch.zeros(max(ws_bytes, 1), dtype=torch.uint8, device=dev)
+    alg_bytes = rvsp.algorithmic_bytes(A, B, c_nnz)
+    rng = np.random.default_rng(1)
+    perturb = None
+    if reuse:
+        d.compute(dA, dB, dC, ws)  # fill once; repeats are numeric-only
+        base = dA.values.clone()
+        perturb = [base + torch.from_numpy(rng.uniform(-0.01, 0.01, A.nnz).astype(np.float32)).to(dev)
+                   for _ in range(2)]
+
+    def step(i):
+        if reuse:
+            dA.values.copy_(perturb[i % 2])
+            d.compute(dA, dB, dC, ws)
+        else:
+            d.work_estimation(dA, dB)
+            d.compute(dA, dB, dC, ws)
+
+    sampler = ClockSampler(local)
+    sampler.start()
+    for i in range(args.warmup):
+        flush.zero_()
+        step(i)
+    torch.cuda.synchronize(dev)
+    d.synchronize()
+    d.phase_times(reset=True)
+    if pg:
+        pg.barrier()
+    torch.cuda.synchronize(dev)
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+          for _ in range(args.steps)]
+    for i in range(args.steps):
+        flush.zero_()
+        ev[i][0].record(stream)
+        step(i)
+        ev[i][1].record(stream)
+    torch.cuda.synchronize(dev)
+    d.synchronize()
+    if pg:
+        pg.barrier()
+    step_ms = [a.elapsed_time(b) for a, b in ev]
+    total_ms = float(sum(step_ms))
+    phases = d.phase_times(reset=True)
+    clocks = sampler.stop()
+    if pg:
+        t = torch.tensor([total_ms], device=dev)
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        total_ms = float(t.item())
+    ms_per_step = total_ms / args.steps
+    value = world * flops * args.steps / (total_ms * 1e-3) / 1e9
+
+    # Dominant phase and its roofline (algorithmic bytes of one product).
+    per_step = {k: (v[0] / args.steps, v[1] / args.steps) for k, v in phases.items() if v[1]}
+    dom = max(per_step, key=lambda k: per_step[k][0])
+    peak, peak_kind = measured_peaks()
+    dom_ms = per_step[dom][0]
+    achieved = alg_bytes / (dom_ms * 1e-3) / 1e9
+    launches = int(sum(v[1] for v in phases.values()))
+    traffic = committed_traffic(args.workload, dom)
+
+    # End to end through the public API, host memory space, pinned buffers.
+    e2e = None
+    if rank == 0 or world > 1:
+        def pinned(x):
+            t = torch.from_numpy(np.ascontiguousarray(x)).pin_memory()
+            return t.numpy()
+        hA = CSR(A.rows, A.cols, pinned(A.row_ptr), pinned(A.col_idx), pinned(A.values))
+        hB = hA if B is A else CSR(B.rows, B.cols, pinned(B.row_ptr), pinned(B.col_idx),
+                                   pinned(B.values))
+        n = max(c_nnz, 1)
+        hC = CSR(A.rows, B.cols, pinned(np.zeros(A.rows + 1, np.int32)),
+                 pinned(np.zeros(n, np.int32)), pinned(np.zeros(n, np.float32)))
+        hws = np.zeros(256, np.uint8)
+        he = Descriptor(memory=L.MEM_HOST)
+        he.work_estimation(hA, hB)
+        he.compute(hA, hB, hC, hws)
+        if reuse:
+            vals = [pinned(p.cpu().numpy()) for p in perturb]
+
+        def e2e_step(i):
+            if reuse:
+                he.compute(hA.with_values(vals[i % 2]), hB, hC, hws)
+            else:
+                he.work_estimation(hA, hB)
+                he.compute(hA, hB, hC, hws)
+        for i in range(3):
+            e2e_step(i)
+        torch.cuda.synchronize(dev)
+        t0 = time.perf_counter()
+        for i in range(args.e2e_steps):
+            e2e_step(i)
+        torch.cuda.synchronize(dev)
+        el = time.perf_counter() - t0
+        if reuse:
+            h2d = A.values.nbytes + (0 if B is A else B.values.nbytes)
+            d2h = 4 * (A.rows + 1) + 4 * c_nnz
+        else:
+            h2d = A.nbytes() + (0 if B is A else B.nbytes())
+            d2h = 4 * (A.rows + 1) + 8 * c_nnz
+        e2e_val = world * flops * args.e2e_steps / el / 1e9
+        if pg:
+            t = torch.tensor([el], device=dev)
+            pg.all_reduce(t, op=pg.ReduceOp.MAX)
+            e2e_val = world * flops * args.e2e_steps / float(t.item()) / 1e9
+        e2e = {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+               "d2h_bytes_per_step": int(d2h), "steps": args.e2e_steps,
+               "api": "rvsp_spgemm_work_estimation + rvsp_spgemm_compute, host memory space"}
+        he.close()
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(A, B, flops)
+
+    d.close()
+    if rank == 0:
+        sym, num = {}, {}
+        with Descriptor(memory=L.MEM_DEVICE, stream=stream) as dd:
+            dd.work_estimation(dA, dB)
+            sym, num = dd.class_counts()
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32", "data": "synthetic",
+            "config": {"workload": args.workload, "description": WORKLOADS[args.workload],
+                       "path": "plain", "rows": A.rows, "nnz_a": A.nnz, "nnz_b": B.nnz,
+                       "nnz_c": c_nnz, "products": int(ops.sum()),
+                       "flops_per_step": flops, "algorithmic_bytes_per_step": alg_bytes,
+                       "l2": "flushed between steps (256 MiB write outside the step events)",
+                       "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+                       "step_hbm_frac": alg_bytes / (ms_per_step * 1e-3) / 1e9 / peak,
+                       "row_classes_symbolic": sym, "row_classes_numeric": num},
+            "hbm_frac": alg_bytes / (ms_per_step * 1e-3) / 1e9 / peak,
+            "phase_ms_per_step": {k: v[0] for k, v in per_step.items()},
+            "roofline": {"bound": "hbm", "kernel": f"{dom} phase", "achieved": achieved,
+                         "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                         "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)"
+                         if peak_kind == "measured" else "fallback 6.65 TB/s",
+                         "traffic": traffic,
+                         "algorithmic_bytes_per_launch": alg_bytes},
+            "clocks": clocks, "e2e": e2e, "gpu_launches": launches,
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    if pg:
+        pg.barrier()
+        pg.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

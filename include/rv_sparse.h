@@ -1,0 +1,171 @@
+/*
+ * rv-sparse-b200: public API.
+ *
+ * Drop-in for the C API of merledu/rv-sparse (include/rv_sparse.h:27-142 in
+ * that project).  Every reference function keeps its name, signature and
+ * error behaviour; the comment above each cites the reference declaration it
+ * replaces.  The additions below the reference API are marked "new".
+ *
+ * Backend.  This library computes FP32 CSR SpGEMM on one NVIDIA B200
+ * (sm_100a) with hand-written CUDA kernels.  RVSP_BACKEND_CUDA is its only
+ * backend; it has no CPU fallback.  A NULL options pointer selects it.
+ *
+ * Memory.  By default the descriptor API takes HOST arrays, exactly like the
+ * reference: work_estimation and compute copy A and B to the device and C
+ * back.  rvsp_spgemm_set_memory_space(descr, RVSP_MEM_DEVICE) switches a
+ * descriptor to DEVICE pointers for A, B, C and the workspace, with no copies.
+ *
+ * Results.  C's structure (nnz, row_ptr, col_idx, ascending within rows) is
+ * identical to the reference scalar backend's.  Each value accumulates its
+ * terms in A's nonzero order with separately rounded multiply and add,
+ * starting from +0.0f, so values are bit-identical to the scalar backend too.
+ */
+#ifndef RV_SPARSE_H
+#define RV_SPARSE_H
+
+#include <stddef.h>
+
+#include "rv_sparse_types.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define RVSP_VERSION_MAJOR 0
+#define RVSP_VERSION_MINOR 1
+#define RVSP_VERSION_PATCH 0
+
+/* rv_sparse.h:27 */
+const char *rvsp_get_version(void);
+
+/* rv_sparse.h:29; also names RVSP_ERROR_DEVICE. */
+const char *rvsp_status_to_string(rvsp_status_t status);
+
+/* rv_sparse.h:38-46.  Wraps caller arrays without taking ownership, then
+ * validates like rvsp_csr_validate.  Host arrays. */
+rvsp_status_t rvsp_csr_create(rvsp_csr_matrix_t *A, int32_t rows, int32_t cols,
+                              int32_t nnz, int32_t *row_ptr, int32_t *col_idx,
+                              void *values, rvsp_dtype_t dtype);
+
+/* rv_sparse.h:48.  Null arrays, dims, row_ptr[0] == 0, row_ptr[rows] == nnz,
+ * non-decreasing row_ptr and column range; not sortedness.  Host arrays. */
+rvsp_status_t rvsp_csr_validate(const rvsp_csr_matrix_t *A);
+
+/* rv_sparse.h:50.  Frees host arrays when owns_data == 1, device arrays when
+ * owns_data == 2, then resets the struct.  NULL is accepted. */
+void rvsp_csr_destroy(rvsp_csr_matrix_t *A);
+
+/* rv_sparse.h:63-67.  One-shot C = A * B on host arrays.  Checks canonical
+ * CSR (RVSP_ERROR_INVALID_CSR), allocates C's host arrays (owns_data = 1)
+ * and leaves C nulled on failure (spgemm.c:26-133). */
+rvsp_status_t rvsp_spgemm_csr(const rvsp_csr_matrix_t *A,
+                              const rvsp_csr_matrix_t *B,
+                              rvsp_csr_matrix_t *C,
+                              const rvsp_spgemm_options_t *options);
+
+/* rv_sparse.h:81 */
+rvsp_status_t rvsp_spgemm_descr_create(rvsp_spgemm_descr_t *descr);
+
+/* rv_sparse.h:88.  NULL is accepted. */
+void rvsp_spgemm_descr_destroy(rvsp_spgemm_descr_t descr);
+
+/* rv_sparse.h:95-96.  Refused (INVALID_ARGUMENT) after work_estimation. */
+rvsp_status_t rvsp_spgemm_set_algo(rvsp_spgemm_descr_t descr,
+                                   rvsp_spgemm_algo_t algo);
+
+/* rv_sparse.h:108-112.  Runs the symbolic analysis on the GPU; reports the
+ * exact nnz(C) and the bytes of workspace compute() needs (host bytes in
+ * host memory space, device bytes in device memory space). */
+rvsp_status_t rvsp_spgemm_work_estimation(rvsp_spgemm_descr_t descr,
+                                          const rvsp_csr_matrix_t *A,
+                                          const rvsp_csr_matrix_t *B,
+                                          size_t *workspace_bytes,
+                                          int32_t *c_nnz_out);
+
+/* rv_sparse.h:122-126.  Writes C.row_ptr, C.col_idx (only when the analysed
+ * structure has not yet been written into this C->col_idx buffer) and
+ * C.values.  Repeated calls with new values and the same pattern are
+ * numeric-only. */
+rvsp_status_t rvsp_spgemm_compute(rvsp_spgemm_descr_t descr,
+                                  const rvsp_csr_matrix_t *A,
+                                  const rvsp_csr_matrix_t *B,
+                                  rvsp_csr_matrix_t *C, void *workspace);
+
+/* rv_sparse.h:134-136.  Host int64 array of n >= rows entries. */
+rvsp_status_t rvsp_spgemm_get_op_counts(rvsp_spgemm_descr_t descr,
+                                        int64_t *op_counts_out, int32_t n);
+
+/* rv_sparse.h:143.  NULL is accepted. */
+void rvsp_spgemm_invalidate_structure(rvsp_spgemm_descr_t descr);
+
+/* The reference also exports these helpers of its kernel layer
+ * (src/kernels/spgemm/rvsp_spgemm.h:34-53); they are host functions here. */
+typedef enum {
+    RVSP_CSR_OK = 0,
+    RVSP_CSR_BAD_ROW_PTR,
+    RVSP_CSR_COL_OUT_OF_RANGE,
+    RVSP_CSR_UNSORTED,
+    RVSP_CSR_DUPLICATE
+} rvsp_csr_status_t;
+
+/* rvsp_spgemm.h:48-51.  Canonical-CSR check of host arrays, O(nnz). */
+rvsp_csr_status_t rvsp_csr_check(int32_t rows, int32_t cols,
+                                 const int32_t *row_ptr,
+                                 const int32_t *col_idx, int32_t *bad_row_out);
+
+/* rvsp_spgemm.h:53 */
+const char *rvsp_csr_status_string(rvsp_csr_status_t status);
+
+/* rvsp_spgemm.h:34.  Host workspace bytes of a descriptor compute() in host
+ * memory space for a given b_cols. */
+rvsp_status_t rvsp_spgemm_buffer_size(int32_t b_cols, size_t *bytes_out);
+
+/* ---- new: device memory, streams, profiling ---------------------------- */
+
+/* Selects host (default) or device pointers for A, B, C and the workspace.
+ * Refused (INVALID_ARGUMENT) after work_estimation. */
+rvsp_status_t rvsp_spgemm_set_memory_space(rvsp_spgemm_descr_t descr,
+                                           rvsp_memory_space_t space);
+
+/* Launches this descriptor's work on a caller-owned cudaStream_t (NULL: the
+ * descriptor's own stream).  Calls still return only when their results are
+ * complete, because estimation must report nnz(C). */
+rvsp_status_t rvsp_spgemm_set_stream(rvsp_spgemm_descr_t descr, void *stream);
+
+/* When enabled, each phase is bracketed by CUDA events on the launching
+ * stream and its device time accumulates per rvsp_phase_t. */
+rvsp_status_t rvsp_spgemm_set_profiling(rvsp_spgemm_descr_t descr, int enable);
+
+/* Copies up to n accumulated phase times (ms) and launch counts (kernels
+ * launched in that phase); either pointer may be NULL.  reset != 0 zeroes the
+ * accumulators after reading. */
+rvsp_status_t rvsp_spgemm_get_phase_times(rvsp_spgemm_descr_t descr,
+                                          double *ms_out, int64_t *launches_out,
+                                          int32_t n, int reset);
+
+/* Device memory space: compute() is asynchronous with respect to the host
+ * (stream-ordered).  This waits for the descriptor's stream and returns the
+ * first error its kernels recorded (RVSP_ERROR_DEVICE), or RVSP_SUCCESS. */
+rvsp_status_t rvsp_spgemm_synchronize(rvsp_spgemm_descr_t descr);
+
+/* Rows per row class of the last analysis: symbolic classes (sized by the
+ * op-count bound) in sym_out and numeric classes (sized by the exact row
+ * nnz) in num_out, n entries each; either pointer may be NULL.  Classes in
+ * order: empty, ESC (<= 32 products), warp hash 64 / 128 / 256 / 512 / 1024 /
+ * 2048 slots, block hash 8192 slots, dense. */
+rvsp_status_t rvsp_spgemm_get_class_counts(rvsp_spgemm_descr_t descr,
+                                           int32_t *sym_out, int32_t *num_out,
+                                           int32_t n);
+
+/* One-shot C = A * B with A, B and the resulting C in DEVICE memory.  C's
+ * arrays are allocated with cudaMalloc and owns_data = 2. */
+rvsp_status_t rvsp_spgemm_csr_device(const rvsp_csr_matrix_t *A,
+                                     const rvsp_csr_matrix_t *B,
+                                     rvsp_csr_matrix_t *C,
+                                     const rvsp_spgemm_options_t *options);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* RV_SPARSE_H */

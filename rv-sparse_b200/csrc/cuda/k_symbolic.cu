@@ -1,0 +1,246 @@
+// Symbolic pass: the exact output nnz of every row (the count half of
+// rvsp_symbolic_count, rvsp_symbolic.c:27-73).  The reference marks each
+// column in a byte array and counts first touches; here each row class uses
+// the structure that fits its upper bound ub = min(ops_i, b_cols):
+//
+//   ESC     <= 32 products: one product per lane, distinct columns counted
+//           with __match_any_sync (no memory at all)
+//   W<T>    warp per row, shared-memory hash set of T >= 2 ub slots
+//   B8192   256-thread block per row, hash set of 8192 slots
+//   DENSE   512-thread block per row, bitmap over all of B's columns (shared
+//           memory when it fits in 192 KiB, else a per-block global bitmap
+//           that every row leaves cleared)
+//
+// Counting needs no order, so products are expanded 32 at a time in
+// flattened order (all lanes busy whatever the B row lengths).
+#include <climits>
+
+#include "device_common.cuh"
+#include "kernels.cuh"
+
+namespace rvsp {
+
+namespace {
+
+// Calls f(col) for every product of A row [p0, p1) that this warp owns.  The
+// row's A nonzeros are split into 32-wide chunks; chunk c goes to warp
+// (c % nwarps == wid).  Loop bounds are warp-uniform.
+template <typename F>
+__device__ __forceinline__ void for_each_product_col(const Operands &op,
+                                                     int32_t p0, int32_t p1,
+                                                     int wid, int nwarps, F f) {
+  const int lane = lane_id();
+  for (int32_t p = p0 + wid * 32; p < p1; p += nwarps * 32) {
+    const AChunk c = load_chunk(op.a_col, op.a_val, op.b_rp, p + lane, p1, false);
+    for (int t0 = 0; t0 < c.total; t0 += 32) {
+      const int t = t0 + lane;
+      const bool v = t < c.total;
+      const int j = warp_owner_of(c.incl, v ? t : 0);
+      const int excl = __shfl_sync(kFull, c.incl - c.len, j);
+      const int bbeg = __shfl_sync(kFull, c.bbeg, j);
+      if (v) f(__ldg(op.b_col + bbeg + (t - excl)));
+    }
+  }
+}
+
+__global__ void __launch_bounds__(kWarpsPerBlock * 32)
+sym_esc_kernel(Operands op, const int32_t *__restrict__ rows, int32_t nrows,
+               int32_t *__restrict__ counts) {
+  const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (w >= nrows) return;
+  const int lane = lane_id();
+  const int32_t row = rows[w];
+  const int32_t p0 = op.a_rp[row], p1 = op.a_rp[row + 1];
+  int32_t col = -1 - lane;  // distinct negative sentinel for empty lanes
+  bool valid = false;
+  int base = 0;
+  for (int32_t p = p0; p < p1; p += 32) {
+    const AChunk c = load_chunk(op.a_col, op.a_val, op.b_rp, p + lane, p1, false);
+    const int t = lane - base;
+    const bool mine = t >= 0 && t < c.total;
+    const int j = warp_owner_of(c.incl, mine ? t : 0);
+    const int excl = __shfl_sync(kFull, c.incl - c.len, j);
+    const int bbeg = __shfl_sync(kFull, c.bbeg, j);
+    if (mine) {
+      col = __ldg(op.b_col + bbeg + (t - excl));
+      valid = true;
+    }
+    base += c.total;
+  }
+  const unsigned peers = __match_any_sync(kFull, col);
+  const bool head = valid && (peers & lanemask_lt()) == 0;
+  const int cnt = __popc(__ballot_sync(kFull, head));
+  if (lane == 0) counts[row] = cnt;
+}
+
+template <int LOG2T>
+__global__ void __launch_bounds__(kWarpsPerBlock * 32)
+sym_warp_hash_kernel(Operands op, const int32_t *__restrict__ rows,
+                     int32_t nrows, int32_t *__restrict__ counts,
+                     int32_t *__restrict__ status) {
+  constexpr int T = 1 << LOG2T;
+  extern __shared__ int32_t smem_i32[];
+  int32_t *keys = smem_i32 + (threadIdx.x >> 5) * T;
+  const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (w >= nrows) return;
+  const int lane = lane_id();
+  for (int s = lane; s < T; s += 32) keys[s] = kEmpty;
+  __syncwarp();
+  const int32_t row = rows[w];
+  int cnt = 0;
+  bool bad = false;
+  for_each_product_col(op, op.a_rp[row], op.a_rp[row + 1], 0, 1,
+                       [&](int32_t col) {
+                         bool created;
+                         if (hash_insert(keys, LOG2T, col, created) < 0) bad = true;
+                         cnt += created;
+                       });
+  cnt = warp_sum(cnt);
+  if (__any_sync(kFull, bad) && lane == 0) report(status, kDevHashFull);
+  if (lane == 0) counts[row] = cnt;
+}
+
+__global__ void __launch_bounds__(kBlockHashThreads)
+sym_block_hash_kernel(Operands op, const int32_t *__restrict__ rows,
+                      int32_t *__restrict__ counts,
+                      int32_t *__restrict__ status) {
+  constexpr int T = 1 << kBlockHashLog2;
+  extern __shared__ int32_t smem_i32[];
+  int32_t *keys = smem_i32;
+  __shared__ int32_t s_cnt;
+  __shared__ int32_t s_bad;
+  for (int s = threadIdx.x; s < T; s += blockDim.x) keys[s] = kEmpty;
+  if (threadIdx.x == 0) {
+    s_cnt = 0;
+    s_bad = 0;
+  }
+  __syncthreads();
+  const int32_t row = rows[blockIdx.x];
+  int cnt = 0;
+  bool bad = false;
+  for_each_product_col(op, op.a_rp[row], op.a_rp[row + 1], threadIdx.x >> 5,
+                       blockDim.x >> 5, [&](int32_t col) {
+                         bool created;
+                         if (hash_insert(keys, kBlockHashLog2, col, created) < 0)
+                           bad = true;
+                         cnt += created;
+                       });
+  cnt = warp_sum(cnt);
+  const bool any_bad = __any_sync(kFull, bad);
+  if (lane_id() == 0) {
+    atomicAdd(&s_cnt, cnt);
+    if (any_bad) s_bad = 1;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    counts[row] = s_cnt;
+    if (s_bad) report(status, kDevHashFull);
+  }
+}
+
+template <bool kSmemBits>
+__global__ void __launch_bounds__(kDenseThreads)
+sym_dense_kernel(Operands op, const int32_t *__restrict__ rows, int32_t nrows,
+                 int32_t *__restrict__ counts, uint32_t *__restrict__ gbits,
+                 size_t gbits_stride) {
+  extern __shared__ uint32_t smem_u32[];
+  __shared__ int32_t s_cnt, s_lo, s_hi;
+  const int32_t words = (op.b_cols + 31) >> 5;
+  uint32_t *bits = kSmemBits ? smem_u32 : gbits + gbits_stride * blockIdx.x;
+  if (kSmemBits) {
+    for (int32_t w = threadIdx.x; w < words; w += blockDim.x) bits[w] = 0u;
+  }
+  for (int32_t r = blockIdx.x; r < nrows; r += gridDim.x) {
+    if (threadIdx.x == 0) {
+      s_cnt = 0;
+      s_lo = INT_MAX;
+      s_hi = -1;
+    }
+    __syncthreads();
+    const int32_t row = rows[r];
+    int cnt = 0, lo = INT_MAX, hi = -1;
+    for_each_product_col(op, op.a_rp[row], op.a_rp[row + 1], threadIdx.x >> 5,
+                         blockDim.x >> 5, [&](int32_t col) {
+                           const uint32_t bit = 1u << (col & 31);
+                           const uint32_t old = atomicOr(&bits[col >> 5], bit);
+                           cnt += (old & bit) ? 0 : 1;
+                           lo = min(lo, col);
+                           hi = max(hi, col);
+                         });
+    cnt = warp_sum(cnt);
+    lo = warp_min(lo);
+    hi = warp_max(hi);
+    if (lane_id() == 0) {
+      atomicAdd(&s_cnt, cnt);
+      atomicMin(&s_lo, lo);
+      atomicMax(&s_hi, hi);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) counts[row] = s_cnt;
+    if (s_hi >= 0) {
+      for (int32_t w = (s_lo >> 5) + threadIdx.x; w <= (s_hi >> 5); w += blockDim.x)
+        bits[w] = 0u;
+    }
+    __syncthreads();
+  }
+}
+
+template <int LOG2T>
+void launch_warp_hash(const Operands &op, const int32_t *rows, int32_t nrows,
+                      int32_t *counts, int32_t *status, cudaStream_t s) {
+  const size_t smem = size_t(kWarpsPerBlock) * (size_t(1) << LOG2T) * sizeof(int32_t);
+  const int threads = kWarpsPerBlock * 32;
+  const int grid = (nrows + kWarpsPerBlock - 1) / kWarpsPerBlock;
+  sym_warp_hash_kernel<LOG2T><<<grid, threads, smem, s>>>(op, rows, nrows, counts,
+                                                          status);
+}
+
+}  // namespace
+
+void launch_symbolic_class(int cls, const Operands &op, const int32_t *rows,
+                           int32_t nrows, int32_t *counts, uint32_t *gbitmap,
+                           int32_t gbitmap_slots, int32_t *status, int num_sms,
+                           cudaStream_t s) {
+  if (nrows <= 0) return;
+  switch (cls) {
+    case kEsc: {
+      const int threads = kWarpsPerBlock * 32;
+      const int grid = (nrows + kWarpsPerBlock - 1) / kWarpsPerBlock;
+      sym_esc_kernel<<<grid, threads, 0, s>>>(op, rows, nrows, counts);
+      break;
+    }
+    case kW64: launch_warp_hash<6>(op, rows, nrows, counts, status, s); break;
+    case kW128: launch_warp_hash<7>(op, rows, nrows, counts, status, s); break;
+    case kW256: launch_warp_hash<8>(op, rows, nrows, counts, status, s); break;
+    case kW512: launch_warp_hash<9>(op, rows, nrows, counts, status, s); break;
+    case kW1024: launch_warp_hash<10>(op, rows, nrows, counts, status, s); break;
+    case kW2048: launch_warp_hash<11>(op, rows, nrows, counts, status, s); break;
+    case kB8192: {
+      const size_t smem = (size_t(1) << kBlockHashLog2) * sizeof(int32_t);
+      sym_block_hash_kernel<<<nrows, kBlockHashThreads, smem, s>>>(op, rows, counts,
+                                                                  status);
+      break;
+    }
+    case kDense: {
+      const int64_t words = (int64_t(op.b_cols) + 31) >> 5;
+      if (op.b_cols <= kSmemBitmapMaxCols) {
+        const size_t smem = size_t(words) * sizeof(uint32_t);
+        cudaFuncSetAttribute(sym_dense_kernel<true>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             static_cast<int>(smem));
+        const int grid = nrows < num_sms ? nrows : num_sms;
+        sym_dense_kernel<true><<<grid, kDenseThreads, smem, s>>>(op, rows, nrows,
+                                                                 counts, nullptr, 0);
+      } else {
+        const size_t stride = dense_slot_bits_bytes(op.b_cols) / sizeof(uint32_t);
+        const int grid = nrows < gbitmap_slots ? nrows : gbitmap_slots;
+        sym_dense_kernel<false><<<grid, kDenseThreads, 0, s>>>(op, rows, nrows,
+                                                               counts, gbitmap, stride);
+      }
+      break;
+    }
+    default: break;
+  }
+}
+
+}  // namespace rvsp

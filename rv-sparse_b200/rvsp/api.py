@@ -1,0 +1,201 @@
+"""Python mirror of the rv-sparse C API on the CUDA backend.
+
+Names follow the reference API (include/rv_sparse.h of merledu/rv-sparse):
+`spgemm_csr` is rvsp_spgemm_csr, `Descriptor` wraps the rvsp_spgemm_descr_*
+sequence (create -> set_algo -> work_estimation -> compute -> get_op_counts ->
+invalidate_structure -> destroy).  Errors raise RvspError carrying the
+rvsp_status_t code.  Everything calls the C-ABI library; nothing here computes.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _lib as L
+from .csr import CSR
+
+
+def spgemm_csr(A: CSR, B: CSR, backend: int | None = L.BACKEND_CUDA) -> CSR:
+    """One-shot C = A * B on host arrays (rvsp_spgemm_csr).  backend=None
+    passes NULL options."""
+    lib = L.load()
+    a, b = A.struct(), B.struct()
+    c = L.CsrMatrix()
+    opts = None
+    if backend is not None:
+        opts = L.SpgemmOptions(backend, L.DTYPE_FP32, L.DTYPE_FP32)
+    st = lib.rvsp_spgemm_csr(C.byref(a), C.byref(b), C.byref(c),
+                             C.byref(opts) if opts is not None else None)
+    L.check(st, "rvsp_spgemm_csr")
+    try:
+        n = c.nnz
+        rp = np.ctypeslib.as_array(C.cast(c.row_ptr, C.POINTER(C.c_int32)),
+                                   shape=(c.rows + 1,)).copy()
+        if n > 0:
+            ci = np.ctypeslib.as_array(C.cast(c.col_idx, C.POINTER(C.c_int32)),
+                                       shape=(n,)).copy()
+            cv = np.ctypeslib.as_array(C.cast(c.values, C.POINTER(C.c_float)),
+                                       shape=(n,)).copy()
+        else:
+            ci = np.zeros(0, np.int32)
+            cv = np.zeros(0, np.float32)
+        return CSR(c.rows, c.cols, rp, ci, cv)
+    finally:
+        lib.rvsp_csr_destroy(C.byref(c))
+
+
+class DeviceCSR:
+    """CSR arrays in device memory (torch CUDA tensors, used only as storage)."""
+
+    def __init__(self, rows, cols, row_ptr, col_idx, values):
+        self.rows, self.cols = int(rows), int(cols)
+        self.row_ptr, self.col_idx, self.values = row_ptr, col_idx, values
+
+    @property
+    def nnz(self) -> int:
+        return int(self.col_idx.numel())
+
+    # Both constructors finish their device work before returning, so the
+    # arrays are ready for a descriptor on any stream.
+    @staticmethod
+    def from_host(M: CSR, device="cuda") -> "DeviceCSR":
+        import torch
+        out = DeviceCSR(M.rows, M.cols,
+                        torch.from_numpy(M.row_ptr).to(device),
+                        torch.from_numpy(M.col_idx).to(device),
+                        torch.from_numpy(M.values).to(device))
+        torch.cuda.synchronize(device)
+        return out
+
+    @staticmethod
+    def empty(rows, cols, nnz, device="cuda") -> "DeviceCSR":
+        import torch
+        out = DeviceCSR(rows, cols,
+                        torch.zeros(rows + 1, dtype=torch.int32, device=device),
+                        torch.zeros(max(nnz, 1), dtype=torch.int32, device=device),
+                        torch.zeros(max(nnz, 1), dtype=torch.float32, device=device))
+        torch.cuda.synchronize(device)
+        return out
+
+    def struct(self, nnz: int | None = None) -> L.CsrMatrix:
+        m = L.CsrMatrix()
+        m.rows, m.cols = self.rows, self.cols
+        m.nnz = self.nnz if nnz is None else nnz
+        m.row_ptr = self.row_ptr.data_ptr()
+        m.col_idx = self.col_idx.data_ptr()
+        m.values = self.values.data_ptr()
+        m.dtype, m.format, m.owns_data = L.DTYPE_FP32, L.FORMAT_CSR, 0
+        return m
+
+    def to_host(self, nnz: int | None = None) -> CSR:
+        n = self.nnz if nnz is None else nnz
+        return CSR(self.rows, self.cols, self.row_ptr.cpu().numpy(),
+                   self.col_idx[:n].cpu().numpy(), self.values[:n].cpu().numpy())
+
+
+class Descriptor:
+    """rvsp_spgemm_descr_t with its lifecycle in one object."""
+
+    def __init__(self, algo: int = L.ALGO_DEFAULT, memory: int = L.MEM_HOST,
+                 stream=None, profiling: bool = False):
+        self.lib = L.load()
+        self.h = C.c_void_p()
+        L.check(self.lib.rvsp_spgemm_descr_create(C.byref(self.h)), "descr_create")
+        if algo != L.ALGO_DEFAULT:
+            L.check(self.lib.rvsp_spgemm_set_algo(self.h, algo), "set_algo")
+        if memory != L.MEM_HOST:
+            L.check(self.lib.rvsp_spgemm_set_memory_space(self.h, memory),
+                    "set_memory_space")
+        if stream is not None:
+            ptr = stream.cuda_stream if hasattr(stream, "cuda_stream") else stream
+            L.check(self.lib.rvsp_spgemm_set_stream(self.h, C.c_void_p(ptr)),
+                    "set_stream")
+        if profiling:
+            L.check(self.lib.rvsp_spgemm_set_profiling(self.h, 1), "set_profiling")
+        self.memory = memory
+        self.c_nnz = None
+        self.ws_bytes = None
+        self._keep = []
+
+    def close(self):
+        if self.h:
+            self.lib.rvsp_spgemm_descr_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def work_estimation(self, A, B):
+        a, b = A.struct(), B.struct()
+        ws = C.c_size_t()
+        nnz = C.c_int32()
+        L.check(self.lib.rvsp_spgemm_work_estimation(self.h, C.byref(a), C.byref(b),
+                                                     C.byref(ws), C.byref(nnz)),
+                "work_estimation")
+        self.c_nnz, self.ws_bytes = nnz.value, ws.value
+        return ws.value, nnz.value
+
+    def compute(self, A, B, Cm, workspace) -> None:
+        a, b = A.struct(), B.struct()
+        # an output C advertises its capacity, not its (not yet written) row_ptr
+        c = Cm.struct(self.c_nnz) if isinstance(Cm, DeviceCSR) else \
+            Cm.struct(nnz=int(Cm.col_idx.size))
+        if isinstance(workspace, np.ndarray):
+            wptr = workspace.ctypes.data
+        elif hasattr(workspace, "data_ptr"):
+            wptr = workspace.data_ptr()
+        else:
+            wptr = workspace
+        L.check(self.lib.rvsp_spgemm_compute(self.h, C.byref(a), C.byref(b),
+                                             C.byref(c), C.c_void_p(wptr)),
+                "compute")
+
+    def multiply(self, A: CSR, B: CSR) -> CSR:
+        """Host memory space: estimate (if needed) + allocate C + compute."""
+        if self.c_nnz is None:
+            self.work_estimation(A, B)
+        n = max(self.c_nnz, 1)
+        Cm = CSR(A.rows, B.cols, np.zeros(A.rows + 1, np.int32),
+                 np.zeros(n, np.int32), np.zeros(n, np.float32))
+        ws = np.zeros(max(self.ws_bytes, 1), np.uint8)
+        self.compute(A, B, Cm, ws)
+        return CSR(Cm.rows, Cm.cols, Cm.row_ptr, Cm.col_idx[:self.c_nnz],
+                   Cm.values[:self.c_nnz])
+
+    def get_op_counts(self, n: int) -> np.ndarray:
+        out = np.zeros(max(n, 1), np.int64)
+        L.check(self.lib.rvsp_spgemm_get_op_counts(self.h, out.ctypes.data, n),
+                "get_op_counts")
+        return out[:n]
+
+    def class_counts(self):
+        sym = np.zeros(len(L.CLASS_NAMES), np.int32)
+        num = np.zeros(len(L.CLASS_NAMES), np.int32)
+        L.check(self.lib.rvsp_spgemm_get_class_counts(
+            self.h, sym.ctypes.data, num.ctypes.data, len(L.CLASS_NAMES)),
+            "get_class_counts")
+        return dict(zip(L.CLASS_NAMES, sym.tolist())), dict(zip(L.CLASS_NAMES, num.tolist()))
+
+    def phase_times(self, reset: bool = False):
+        ms = np.zeros(len(L.PHASES), np.float64)
+        ln = np.zeros(len(L.PHASES), np.int64)
+        L.check(self.lib.rvsp_spgemm_get_phase_times(
+            self.h, ms.ctypes.data, ln.ctypes.data, len(L.PHASES), int(reset)),
+            "get_phase_times")
+        return {p: (float(ms[i]), int(ln[i])) for i, p in enumerate(L.PHASES)}
+
+    def invalidate_structure(self):
+        self.lib.rvsp_spgemm_invalidate_structure(self.h)
+
+    def synchronize(self):
+        L.check(self.lib.rvsp_spgemm_synchronize(self.h), "synchronize")

@@ -1,0 +1,211 @@
+"""Parity of the CUDA path with the reference scalar backend.
+
+Bar: structure (nnz, row_ptr, col_idx) bit-exact, values bit-exact (each
+output entry accumulates in A's nonzero order with separately rounded
+multiply and add, as the reference does), and per-row op counts exact.
+Checked against the hand-computed fixtures, the committed outputs of the
+reference library, the CPU oracle on seeded inputs that reach every row
+class, and the full-size benchmark workloads.  The FP64 check uses the
+tolerance |c - c64| <= 1e-6 * sum_k |a_ik b_kj| (+1e-30).
+"""
+import numpy as np
+import pytest
+
+from oracle import oracle
+from rvsp import CSR, Descriptor, gen, spgemm_csr
+from rvsp import _lib as L
+
+pytestmark = pytest.mark.gpu
+
+
+def assert_bit_exact(got: CSR, rp, ci, cv, what=""):
+    assert got.nnz == ci.size, what
+    assert np.array_equal(got.row_ptr, rp), f"row_ptr {what}"
+    assert np.array_equal(got.col_idx, ci), f"col_idx {what}"
+    bad = np.nonzero(got.values.view(np.uint32) != cv.view(np.uint32))[0]
+    assert bad.size == 0, f"values {what}: {bad.size} differ, first at {bad[:5]}"
+
+
+def check_against_oracle(A, B, what=""):
+    rp, ci, cv, ops = oracle.spgemm(A, B)
+    got = spgemm_csr(A, B)
+    assert_bit_exact(got, rp, ci, cv, what + " one-shot")
+    with Descriptor() as d:
+        Cm = d.multiply(A, B)
+        assert_bit_exact(Cm, rp, ci, cv, what + " descriptor")
+        assert np.array_equal(d.get_op_counts(A.rows), ops), what
+        sym, num = d.class_counts()
+    return sym, num
+
+
+def test_fixtures(golden_fixtures):
+    for name, A, B, Cx in golden_fixtures:
+        got = spgemm_csr(A, B)
+        assert_bit_exact(got, Cx.row_ptr, Cx.col_idx, Cx.values, name)
+        with Descriptor() as d:
+            assert_bit_exact(d.multiply(A, B), Cx.row_ptr, Cx.col_idx, Cx.values, name)
+
+
+def test_reference_outputs(golden_random):
+    for name, A, B, Cx, ops in golden_random:
+        got = spgemm_csr(A, B)
+        assert_bit_exact(got, Cx.row_ptr, Cx.col_idx, Cx.values, name)
+        with Descriptor() as d:
+            d.work_estimation(A, B)
+            assert np.array_equal(d.get_op_counts(A.rows), ops), name
+
+
+def class_probe(seed: int, b_cols: int = 60000):
+    """A x B whose rows land in every row class: B rows of length 3 (for
+    ESC rows) and 45; A rows select 0..400 of them."""
+    rng = np.random.default_rng(seed)
+    nb = 2000
+    lengths = np.where(np.arange(nb) < 200, 3, 45).astype(np.int64)
+    cols = gen._distinct_sorted_columns(rng, lengths, b_cols)
+    rp = np.zeros(nb + 1, np.int64)
+    np.cumsum(lengths, out=rp[1:])
+    B = CSR(nb, b_cols, rp, cols, rng.uniform(-1, 1, cols.size).astype(np.float32))
+    a_rows = []
+    ks = [0, 1, 2, 3, 5, 8, 12, 20, 30, 45, 70, 100, 150, 250, 400]
+    for r in range(300):
+        k = ks[r % len(ks)]
+        short = r % 2 == 0 and k <= 8
+        pool = np.arange(200) if short else np.arange(200, nb)
+        a_rows.append(np.sort(rng.choice(pool, size=min(k, pool.size), replace=False)))
+    lens = np.array([x.size for x in a_rows], np.int64)
+    arp = np.zeros(len(a_rows) + 1, np.int64)
+    np.cumsum(lens, out=arp[1:])
+    aci = np.concatenate(a_rows) if lens.sum() else np.zeros(0, np.int64)
+    A = CSR(len(a_rows), nb, arp, aci, rng.uniform(-1, 1, aci.size).astype(np.float32))
+    return A, B
+
+
+def test_every_row_class():
+    A, B = class_probe(11)
+    sym, num = check_against_oracle(A, B, "class probe")
+    for cls in L.CLASS_NAMES:
+        assert sym[cls] > 0 or num[cls] > 0, (cls, sym, num)
+
+
+def test_dense_rows_with_global_bitmap():
+    # b_cols beyond the shared-memory bitmap (1.5 Mi columns): dense rows use
+    # the global-memory bitmap in both passes.
+    A, B = class_probe(12, b_cols=2_000_000)
+    sym, num = check_against_oracle(A, B, "wide B")
+    assert sym["dense"] > 0 and num["dense"] > 0
+
+
+@pytest.mark.parametrize("seed", range(8))
+def test_seeded_irregular(seed):
+    A = gen.random_csr(700, 500, 300 + seed, mean_len=3.0 + 3 * (seed % 4),
+                       empty_frac=0.1, heavy_rows=seed % 3, heavy_len=200)
+    B = gen.random_csr(500, 900, 400 + seed, mean_len=2.0 + 4 * (seed % 3),
+                       empty_frac=0.15, heavy_rows=1, heavy_len=300,
+                       value_kind="int" if seed % 2 else "uniform")
+    check_against_oracle(A, B, f"seed {seed}")
+
+
+def test_long_a_rows():
+    # rows with more A nonzeros than the per-thread rowstats path takes
+    A = gen.random_csr(50, 3000, 21, mean_len=5.0, heavy_rows=10, heavy_len=1500)
+    B = gen.random_csr(3000, 400, 22, mean_len=2.0, empty_frac=0.5)
+    check_against_oracle(A, B, "long A rows")
+
+
+def test_edge_cases():
+    one = np.ones(1, np.float32)
+    # empty A
+    A = CSR(3, 4, np.zeros(4), np.zeros(0), np.zeros(0))
+    B = gen.random_csr(4, 5, 1, mean_len=2.0)
+    check_against_oracle(A, B, "empty A")
+    # all-empty B rows
+    A = gen.random_csr(6, 4, 2, mean_len=2.0, empty_frac=0.0)
+    B = CSR(4, 7, np.zeros(5), np.zeros(0), np.zeros(0))
+    check_against_oracle(A, B, "empty B")
+    # 1 x 1
+    A = CSR(1, 1, np.array([0, 1]), np.array([0]), one * 3)
+    B = CSR(1, 1, np.array([0, 1]), np.array([0]), one * -2)
+    check_against_oracle(A, B, "1x1")
+    # signed zeros: 0 * -1 = -0, and +0 + -0 = +0 in the accumulator
+    A = CSR(1, 2, np.array([0, 2]), np.array([0, 1]), np.array([0.0, -0.0], np.float32))
+    B = CSR(2, 2, np.array([0, 2, 4]), np.array([0, 1, 0, 1]),
+            np.array([-1.0, 1.0, 1.0, -1.0], np.float32))
+    check_against_oracle(A, B, "signed zeros")
+    # exact cancellation keeps the structural zero
+    A = CSR(1, 2, np.array([0, 2]), np.array([0, 1]), np.array([1.0, 1.0], np.float32))
+    B = CSR(2, 1, np.array([0, 1, 2]), np.array([0, 0]), np.array([1.0, -1.0], np.float32))
+    got = spgemm_csr(A, B)
+    assert got.nnz == 1 and got.values[0] == 0.0
+    # inf / nan propagate exactly like the scalar backend
+    A = CSR(2, 2, np.array([0, 2, 3]), np.array([0, 1, 1]),
+            np.array([np.inf, 1.0, np.nan], np.float32))
+    B = CSR(2, 2, np.array([0, 1, 2]), np.array([0, 1]), np.array([0.0, 2.0], np.float32))
+    rp, ci, cv, _ = oracle.spgemm(A, B)
+    g = spgemm_csr(A, B)
+    assert np.array_equal(g.col_idx, ci)
+    assert np.array_equal(np.isnan(g.values), np.isnan(cv))
+    assert np.array_equal(g.values[~np.isnan(cv)], cv[~np.isnan(cv)])
+
+
+def test_invalid_csr_rejected():
+    A = gen.random_csr(20, 10, 3, mean_len=3.0, empty_frac=0.0)
+    B = gen.random_csr(10, 10, 4, mean_len=3.0, empty_frac=0.0)
+    for mutate in ("range", "unsorted", "dup", "rowptr"):
+        X = A.copy()
+        if mutate == "range":
+            X.col_idx[5] = 10
+        elif mutate == "unsorted":
+            r = next(i for i in range(X.rows) if X.row_ptr[i + 1] - X.row_ptr[i] >= 2)
+            p = X.row_ptr[r]
+            X.col_idx[p], X.col_idx[p + 1] = X.col_idx[p + 1], X.col_idx[p]
+        elif mutate == "dup":
+            r = next(i for i in range(X.rows) if X.row_ptr[i + 1] - X.row_ptr[i] >= 2)
+            p = X.row_ptr[r]
+            X.col_idx[p + 1] = X.col_idx[p]
+        else:
+            X.row_ptr[3] = X.row_ptr[4] + 1
+        with pytest.raises(L.RvspError) as e:
+            spgemm_csr(X, B)
+        assert e.value.status == L.ERROR_INVALID_CSR, mutate
+
+
+def test_fp64_tolerance():
+    A = gen.random_csr(400, 300, 31, mean_len=20.0)
+    B = gen.random_csr(300, 350, 32, mean_len=20.0)
+    got = spgemm_csr(A, B)
+    v64, mag = oracle.numeric_f64(A, B, got.row_ptr, got.col_idx)
+    assert np.all(np.abs(got.values.astype(np.float64) - v64) <= 1e-6 * mag + 1e-30)
+
+
+def test_uniform_4096_16_per_row_full():
+    # 4096 x 4096, exactly 16 nnz/row, A seed S, B seed S + 1
+    A = gen.uniform_rows(4096, 4096, 16, seed=2024)
+    B = gen.uniform_rows(4096, 4096, 16, seed=2025)
+    st, rp, ci, cv = oracle.ref_spgemm(A, B) if oracle.ref_available() else (0, *oracle.spgemm(A, B)[:3])
+    assert st == 0
+    assert_bit_exact(spgemm_csr(A, B), rp, ci, cv, "uniform 4096")
+
+
+def test_laplacian_2d_1024_full():
+    A = gen.laplacian_2d(1024)
+    assert A.nnz == 5_238_784
+    rp, ci, cv, ops = oracle.spgemm(A, A)
+    assert ci.size == 13_611_012
+    got = spgemm_csr(A, A)
+    assert_bit_exact(got, rp, ci, cv, "laplacian 1024")
+
+
+def test_stencil_3d_27_small():
+    A = gen.stencil_3d_27(24)
+    check_against_oracle(A, A, "27-point 24^3")
+
+
+def test_rmat_panel():
+    A = gen.rmat(14, 16, seed=3)
+    panel = A.row_panel(0, 2048)
+    check_against_oracle(panel, A, "R-MAT 2^14 panel")
+
+
+def test_batched_style_products():
+    for i, (A, B) in enumerate(gen.batched_products(count=6, seed=5, n_hi=4096)):
+        check_against_oracle(A, B, f"batch {i}")
