@@ -210,6 +210,9 @@ def main():
 
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
+    # One dedicated stream carries the L2 flush, the step events and every
+    # kernel of the library (the descriptor is bound to it below).
+    torch.cuda.set_stream(torch.cuda.Stream(dev))
     pg = None
     if world > 1:
         import datetime

@@ -1,0 +1,168 @@
+// Thread-per-row K-way merge for rows with few A nonzeros and modest work.
+//
+// Row i of C is the merge of the B rows its A nonzeros select, each scaled by
+// its A value.  B rows are sorted (canonical CSR), so one thread can produce
+// row i's columns in ascending order by repeatedly taking the smallest head
+// among the K lists: no hash table, no sort, no shared memory.  When several
+// lists share the smallest head column, their terms are added in list order,
+// which is ascending A-nonzero order, into an accumulator that starts at
+// +0.0f, with __fmul_rn / __fadd_rn.  That is exactly the order and rounding
+// of the reference scalar backend (gustavson_core_f32.inc:31-62 with
+// accum_scalar_f32.c:20-71), and the emitted columns are its sorted fill
+// (rvsp_symbolic.c:91-137).
+//
+// The per-list state (position, end, head column, A value) lives in
+// registers: every loop over lists is unrolled over K and guarded by j < k.
+#include <climits>
+
+#include "device_common.cuh"
+#include "kernels.cuh"
+
+namespace rvsp {
+
+namespace {
+
+template <int K>
+struct Lists {
+  int32_t pos[K];
+  int32_t end[K];
+  int32_t cur[K];
+  float a[K];
+};
+
+template <int K, bool kValues>
+__device__ __forceinline__ void open_lists(const Operands &op, int32_t p0,
+                                           int32_t k, Lists<K> &L) {
+#pragma unroll
+  for (int j = 0; j < K; ++j) {
+    L.cur[j] = INT_MAX;
+    L.pos[j] = 0;
+    L.end[j] = 0;
+    L.a[j] = 0.0f;
+    if (j < k) {
+      const int32_t kk = __ldg(op.a_col + p0 + j);
+      if (kValues) L.a[j] = __ldg(op.a_val + p0 + j);
+      const int32_t b0 = __ldg(op.b_rp + kk);
+      const int32_t b1 = __ldg(op.b_rp + kk + 1);
+      L.pos[j] = b0;
+      L.end[j] = b1;
+      if (b0 < b1) L.cur[j] = __ldg(op.b_col + b0);
+    }
+  }
+}
+
+template <int K>
+__device__ __forceinline__ int32_t min_head(const Lists<K> &L) {
+  int32_t m = L.cur[0];
+#pragma unroll
+  for (int j = 1; j < K; ++j) m = min(m, L.cur[j]);
+  return m;
+}
+
+template <int K>
+__global__ void __launch_bounds__(kMergeThreads)
+merge_symbolic_kernel(Operands op, const int32_t *__restrict__ rows,
+                      int32_t nrows, int32_t *__restrict__ counts) {
+  const int32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nrows) return;
+  const int32_t row = rows[t];
+  const int32_t p0 = op.a_rp[row];
+  const int32_t k = op.a_rp[row + 1] - p0;
+  Lists<K> L;
+  open_lists<K, false>(op, p0, k, L);
+  int32_t n = 0;
+  for (;;) {
+    const int32_t mn = min_head<K>(L);
+    if (mn == INT_MAX) break;
+#pragma unroll
+    for (int j = 0; j < K; ++j) {
+      if (L.cur[j] == mn) {
+        const int32_t p = ++L.pos[j];
+        L.cur[j] = p < L.end[j] ? __ldg(op.b_col + p) : INT_MAX;
+      }
+    }
+    ++n;
+  }
+  counts[row] = n;
+}
+
+template <int K>
+__global__ void __launch_bounds__(kMergeThreads)
+merge_numeric_kernel(Operands op, const int32_t *__restrict__ rows, int32_t nrows,
+                     const int32_t *__restrict__ c_rp, int32_t *__restrict__ c_col,
+                     float *__restrict__ c_val, bool fill,
+                     int32_t *__restrict__ status) {
+  const int32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nrows) return;
+  const int32_t row = rows[t];
+  const int32_t p0 = op.a_rp[row];
+  const int32_t k = op.a_rp[row + 1] - p0;
+  Lists<K> L;
+  open_lists<K, true>(op, p0, k, L);
+  int32_t out = c_rp[row];
+  const int32_t out_end = c_rp[row + 1];
+  for (;;) {
+    const int32_t mn = min_head<K>(L);
+    if (mn == INT_MAX) break;
+    float acc = 0.0f;
+#pragma unroll
+    for (int j = 0; j < K; ++j) {
+      if (L.cur[j] == mn) {
+        const int32_t p = L.pos[j];
+        acc = __fadd_rn(acc, __fmul_rn(L.a[j], __ldg(op.b_val + p)));
+        L.pos[j] = p + 1;
+        L.cur[j] = p + 1 < L.end[j] ? __ldg(op.b_col + p + 1) : INT_MAX;
+      }
+    }
+    if (out < out_end) {
+      if (fill) c_col[out] = mn;
+      c_val[out] = acc;
+    }
+    ++out;
+  }
+  if (out != out_end) report(status, kDevCountMismatch);
+}
+
+template <int K>
+void sym(const Operands &op, const int32_t *rows, int32_t nrows, int32_t *counts,
+         cudaStream_t s) {
+  const int grid = (nrows + kMergeThreads - 1) / kMergeThreads;
+  merge_symbolic_kernel<K><<<grid, kMergeThreads, 0, s>>>(op, rows, nrows, counts);
+}
+
+template <int K>
+void num(const Operands &op, const int32_t *rows, int32_t nrows, const int32_t *c_rp,
+         int32_t *c_col, float *c_val, bool fill, int32_t *status, cudaStream_t s) {
+  const int grid = (nrows + kMergeThreads - 1) / kMergeThreads;
+  merge_numeric_kernel<K><<<grid, kMergeThreads, 0, s>>>(op, rows, nrows, c_rp, c_col,
+                                                         c_val, fill, status);
+}
+
+}  // namespace
+
+void launch_merge_symbolic(int cls, const Operands &op, const int32_t *rows,
+                           int32_t nrows, int32_t *counts, cudaStream_t s) {
+  if (nrows <= 0) return;
+  switch (cls) {
+    case kM4: sym<4>(op, rows, nrows, counts, s); break;
+    case kM8: sym<8>(op, rows, nrows, counts, s); break;
+    case kM16: sym<16>(op, rows, nrows, counts, s); break;
+    case kM32: sym<32>(op, rows, nrows, counts, s); break;
+    default: break;
+  }
+}
+
+void launch_merge_numeric(int cls, const Operands &op, const int32_t *rows,
+                          int32_t nrows, const int32_t *c_rp, int32_t *c_col,
+                          float *c_val, bool fill, int32_t *status, cudaStream_t s) {
+  if (nrows <= 0) return;
+  switch (cls) {
+    case kM4: num<4>(op, rows, nrows, c_rp, c_col, c_val, fill, status, s); break;
+    case kM8: num<8>(op, rows, nrows, c_rp, c_col, c_val, fill, status, s); break;
+    case kM16: num<16>(op, rows, nrows, c_rp, c_col, c_val, fill, status, s); break;
+    case kM32: num<32>(op, rows, nrows, c_rp, c_col, c_val, fill, status, s); break;
+    default: break;
+  }
+}
+
+}  // namespace rvsp

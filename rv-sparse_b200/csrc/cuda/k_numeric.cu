@@ -8,10 +8,7 @@
 // A-nonzero order into an accumulator that starts at +0.0f, rounding the
 // product and the sum separately.  Every class here keeps that order exactly:
 //
-//   ESC     all (<= 32) products of the row sit one per lane in flattened
-//           order; a bitonic sort on (column, lane) groups equal columns
-//           with the earlier A nonzero first, and each group's head adds its
-//           run left to right starting from 0.0f.
+//   M<K>    one thread merges the row's sorted B rows (k_merge.cu).
 //   W<T>    warp per row.  "Stepping": one A nonzero at a time, lanes over
 //           its B row (distinct columns), __syncwarp between A nonzeros.
 //           "Tiles" (short B rows): 32 flattened products at a time; lanes
@@ -35,84 +32,6 @@ namespace rvsp {
 namespace {
 
 constexpr int kSteppingMinAvgLen = 16;  // avg B row length that favours stepping
-
-// ---- ESC ---------------------------------------------------------------------
-
-__global__ void __launch_bounds__(kWarpsPerBlock * 32)
-num_esc_kernel(Operands op, const int32_t *__restrict__ rows, int32_t nrows,
-               const int32_t *__restrict__ c_rp, int32_t *__restrict__ c_col,
-               float *__restrict__ c_val, bool fill,
-               int32_t *__restrict__ status) {
-  const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  if (w >= nrows) return;
-  const int lane = lane_id();
-  const int32_t row = rows[w];
-  const int32_t p0 = op.a_rp[row], p1 = op.a_rp[row + 1];
-
-  int32_t col = INT_MAX;  // empty lanes sort last
-  float term = 0.0f;
-  int base = 0;
-  for (int32_t p = p0; p < p1; p += 32) {
-    const AChunk c = load_chunk(op.a_col, op.a_val, op.b_rp, p + lane, p1, true);
-    const int t = lane - base;
-    const bool mine = t >= 0 && t < c.total;
-    const int j = warp_owner_of(c.incl, mine ? t : 0);
-    const int excl = __shfl_sync(kFull, c.incl - c.len, j);
-    const int bbeg = __shfl_sync(kFull, c.bbeg, j);
-    const float a = __shfl_sync(kFull, c.a, j);
-    if (mine) {
-      const int32_t bp = bbeg + (t - excl);
-      col = __ldg(op.b_col + bp);
-      term = __fmul_rn(a, __ldg(op.b_val + bp));
-    }
-    base += c.total;
-  }
-
-  // Bitonic sort of (col, lane) ascending; the value travels with its key.
-  unsigned long long key =
-      (static_cast<unsigned long long>(static_cast<uint32_t>(col)) << 32) |
-      static_cast<uint32_t>(lane);
-  float v = term;
-#pragma unroll
-  for (int k = 2; k <= 32; k <<= 1) {
-#pragma unroll
-    for (int j = k >> 1; j > 0; j >>= 1) {
-      const unsigned long long ok = __shfl_xor_sync(kFull, key, j);
-      const float ov = __shfl_xor_sync(kFull, v, j);
-      const bool keep_min = ((lane & j) == 0) == ((lane & k) == 0);
-      const bool take = keep_min ? (ok < key) : (ok > key);
-      if (take) {
-        key = ok;
-        v = ov;
-      }
-    }
-  }
-  col = static_cast<int32_t>(key >> 32);
-  const bool valid = col != INT_MAX;
-  const int32_t prev = __shfl_up_sync(kFull, col, 1);
-  const bool head = valid && (lane == 0 || prev != col);
-
-  // Each head adds its run in order, starting from +0.0f.
-  float acc = __fadd_rn(0.0f, v);
-  bool cont = true;
-  for (int r = 1; r < 32; ++r) {
-    const int32_t c2 = __shfl_down_sync(kFull, col, r);
-    const float v2 = __shfl_down_sync(kFull, v, r);
-    cont = cont && (lane + r < 32) && (c2 == col);
-    if (cont) acc = __fadd_rn(acc, v2);
-    if (!__any_sync(kFull, cont && head)) break;
-  }
-
-  const unsigned heads = __ballot_sync(kFull, head);
-  const int pos = __popc(heads & lanemask_lt());
-  const int32_t cs = c_rp[row];
-  const int m = c_rp[row + 1] - cs;
-  if (lane == 0 && __popc(heads) != m) report(status, kDevCountMismatch);
-  if (head && pos < m) {
-    if (fill) c_col[cs + pos] = col;
-    c_val[cs + pos] = acc;
-  }
-}
 
 // ---- product walkers for warp-per-row classes --------------------------------
 
@@ -592,13 +511,12 @@ void launch_numeric_class(int cls, const Operands &op, const int64_t *ops,
   if (nrows <= 0) return;
   (void)num_sms;
   switch (cls) {
-    case kEsc: {
-      const int threads = kWarpsPerBlock * 32;
-      const int grid = (nrows + kWarpsPerBlock - 1) / kWarpsPerBlock;
-      num_esc_kernel<<<grid, threads, 0, s>>>(op, rows, nrows, c_rp, c_col, c_val,
-                                              fill, status);
+    case kM4:
+    case kM8:
+    case kM16:
+    case kM32:
+      launch_merge_numeric(cls, op, rows, nrows, c_rp, c_col, c_val, fill, status, s);
       break;
-    }
     case kW64: launch_warp<6>(op, ops, rows, nrows, c_rp, c_col, c_val, fill, status, s); break;
     case kW128: launch_warp<7>(op, ops, rows, nrows, c_rp, c_col, c_val, fill, status, s); break;
     case kW256: launch_warp<8>(op, ops, rows, nrows, c_rp, c_col, c_val, fill, status, s); break;

@@ -97,6 +97,7 @@ partials_scan_kernel(int32_t n, int32_t nt, int64_t *__restrict__ partials,
 __global__ void __launch_bounds__(kThreads)
 tile_apply_kernel(int32_t n, const int32_t *__restrict__ counts,
                   const int64_t *__restrict__ ops,
+                  const int32_t *__restrict__ a_rp,
                   const int64_t *__restrict__ partials,
                   int32_t *__restrict__ row_ptr, uint8_t *__restrict__ cls,
                   int32_t *__restrict__ class_count) {
@@ -116,7 +117,7 @@ tile_apply_kernel(int32_t n, const int32_t *__restrict__ counts,
     int c = kEmpty_;
     if (i < n) {
       m = counts[i];
-      c = classify_row(ops[i], m);
+      c = classify_row(a_rp[i + 1] - a_rp[i], ops[i], m);
       cls[i] = static_cast<uint8_t>(c);
     }
     s_items[skew(idx)] = m;
@@ -160,12 +161,13 @@ size_t scan_partials_bytes(int32_t n) {
 }
 
 void launch_scan_and_class(int32_t n, const int32_t *counts, const int64_t *ops,
-                           int32_t *row_ptr, int64_t *partials, int64_t *total,
-                           uint8_t *cls, int32_t *class_count, cudaStream_t s) {
+                           const int32_t *a_rp, int32_t *row_ptr,
+                           int64_t *partials, int64_t *total, uint8_t *cls,
+                           int32_t *class_count, cudaStream_t s) {
   const int32_t nt = static_cast<int32_t>((static_cast<int64_t>(n) + kTile - 1) / kTile);
   tile_sum_kernel<<<nt, kThreads, 0, s>>>(n, counts, partials);
   partials_scan_kernel<<<1, kThreads, 0, s>>>(n, nt, partials, total, row_ptr);
-  tile_apply_kernel<<<nt, kThreads, 0, s>>>(n, counts, ops, partials, row_ptr,
+  tile_apply_kernel<<<nt, kThreads, 0, s>>>(n, counts, ops, a_rp, partials, row_ptr,
                                             cls, class_count);
 }
 

@@ -3,8 +3,8 @@
 // column in a byte array and counts first touches; here each row class uses
 // the structure that fits its upper bound ub = min(ops_i, b_cols):
 //
-//   ESC     <= 32 products: one product per lane, distinct columns counted
-//           with __match_any_sync (no memory at all)
+//   M<K>    few A nonzeros: one thread merges the sorted B rows and counts
+//           distinct heads (k_merge.cu)
 //   W<T>    warp per row, shared-memory hash set of T >= 2 ub slots
 //   B8192   256-thread block per row, hash set of 8192 slots
 //   DENSE   512-thread block per row, bitmap over all of B's columns (shared
@@ -41,36 +41,6 @@ __device__ __forceinline__ void for_each_product_col(const Operands &op,
       if (v) f(__ldg(op.b_col + bbeg + (t - excl)));
     }
   }
-}
-
-__global__ void __launch_bounds__(kWarpsPerBlock * 32)
-sym_esc_kernel(Operands op, const int32_t *__restrict__ rows, int32_t nrows,
-               int32_t *__restrict__ counts) {
-  const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  if (w >= nrows) return;
-  const int lane = lane_id();
-  const int32_t row = rows[w];
-  const int32_t p0 = op.a_rp[row], p1 = op.a_rp[row + 1];
-  int32_t col = -1 - lane;  // distinct negative sentinel for empty lanes
-  bool valid = false;
-  int base = 0;
-  for (int32_t p = p0; p < p1; p += 32) {
-    const AChunk c = load_chunk(op.a_col, op.a_val, op.b_rp, p + lane, p1, false);
-    const int t = lane - base;
-    const bool mine = t >= 0 && t < c.total;
-    const int j = warp_owner_of(c.incl, mine ? t : 0);
-    const int excl = __shfl_sync(kFull, c.incl - c.len, j);
-    const int bbeg = __shfl_sync(kFull, c.bbeg, j);
-    if (mine) {
-      col = __ldg(op.b_col + bbeg + (t - excl));
-      valid = true;
-    }
-    base += c.total;
-  }
-  const unsigned peers = __match_any_sync(kFull, col);
-  const bool head = valid && (peers & lanemask_lt()) == 0;
-  const int cnt = __popc(__ballot_sync(kFull, head));
-  if (lane == 0) counts[row] = cnt;
 }
 
 template <int LOG2T>
@@ -203,12 +173,10 @@ void launch_symbolic_class(int cls, const Operands &op, const int32_t *rows,
                            cudaStream_t s) {
   if (nrows <= 0) return;
   switch (cls) {
-    case kEsc: {
-      const int threads = kWarpsPerBlock * 32;
-      const int grid = (nrows + kWarpsPerBlock - 1) / kWarpsPerBlock;
-      sym_esc_kernel<<<grid, threads, 0, s>>>(op, rows, nrows, counts);
-      break;
-    }
+    case kM4:
+    case kM8:
+    case kM16:
+    case kM32: launch_merge_symbolic(cls, op, rows, nrows, counts, s); break;
     case kW64: launch_warp_hash<6>(op, rows, nrows, counts, status, s); break;
     case kW128: launch_warp_hash<7>(op, rows, nrows, counts, status, s); break;
     case kW256: launch_warp_hash<8>(op, rows, nrows, counts, status, s); break;

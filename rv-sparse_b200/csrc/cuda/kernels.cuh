@@ -12,14 +12,19 @@ namespace rvsp {
 // by its exact output nnz m_i.  The same table serves both.
 //
 //   EMPTY   no products
-//   ESC     ops_i <= 32: one warp expands every product into registers,
-//           sorts by (column, product order) and reduces each run in order
+//   M<K>    at most K (4, 8, 16, 32) A nonzeros and at most kMergeMaxOps
+//           products: one thread merges the row's K sorted B rows, taking
+//           the smallest head column each step; equal heads are added in
+//           A-nonzero order, and columns come out sorted with no scratch
 //   W<T>    one warp, shared-memory hash table of T slots (bound <= T/2)
 //   B8192   one 256-thread block, hash table of 8192 slots (bound <= 4096)
 //   DENSE   one 512-thread block, dense accumulator over all of B's columns
 enum RowClass : int {
   kEmpty_ = 0,
-  kEsc,
+  kM4,
+  kM8,
+  kM16,
+  kM32,
   kW64,
   kW128,
   kW256,
@@ -31,7 +36,8 @@ enum RowClass : int {
   kNumClasses
 };
 
-constexpr int kEscMaxOps = 32;
+constexpr int kMergeMaxOps = 2048;
+constexpr int kMergeThreads = 128;
 constexpr int kWarpHashMinLog2 = 6;    // W64
 constexpr int kWarpHashMaxLog2 = 11;   // W2048
 constexpr int kBlockHashLog2 = 13;     // B8192
@@ -44,9 +50,11 @@ constexpr int64_t kSmemBitmapMaxCols = 48 * 1024 * 32;
 // rowstats hands rows with more A nonzeros than this to a warp-per-row pass.
 constexpr int kLongRowNnz = 128;
 
-__host__ __device__ inline int classify_row(int64_t ops, int64_t bound) {
+__host__ __device__ inline int classify_row(int32_t nnz_a, int64_t ops,
+                                            int64_t bound) {
   if (ops <= 0) return kEmpty_;
-  if (ops <= kEscMaxOps) return kEsc;
+  if (nnz_a <= 32 && ops <= kMergeMaxOps)
+    return nnz_a <= 4 ? kM4 : nnz_a <= 8 ? kM8 : nnz_a <= 16 ? kM16 : kM32;
   const int64_t need = 2 * bound;
   for (int l = kWarpHashMinLog2; l <= kWarpHashMaxLog2; ++l)
     if (need <= (int64_t(1) << l)) return kW64 + (l - kWarpHashMinLog2);
@@ -90,8 +98,19 @@ void launch_scatter_rows(int32_t n, const uint8_t *cls, const int32_t *class_off
 // Also classes every row for the numeric pass (cls, class_count).
 size_t scan_partials_bytes(int32_t n);
 void launch_scan_and_class(int32_t n, const int32_t *counts, const int64_t *ops,
-                           int32_t *row_ptr, int64_t *partials, int64_t *total,
-                           uint8_t *cls, int32_t *class_count, cudaStream_t s);
+                           const int32_t *a_rp, int32_t *row_ptr,
+                           int64_t *partials, int64_t *total, uint8_t *cls,
+                           int32_t *class_count, cudaStream_t s);
+
+// ---- k_merge.cu ------------------------------------------------------------
+// Thread-per-row K-way merge for the M<K> classes: counts (symbolic) or
+// values and sorted columns (numeric).
+void launch_merge_symbolic(int cls, const Operands &op, const int32_t *rows,
+                           int32_t nrows, int32_t *counts, cudaStream_t s);
+void launch_merge_numeric(int cls, const Operands &op, const int32_t *rows,
+                          int32_t nrows, const int32_t *c_rp, int32_t *c_col,
+                          float *c_val, bool fill, int32_t *status,
+                          cudaStream_t s);
 
 // ---- k_symbolic.cu ---------------------------------------------------------
 // counts[row] = nnz of output row, for the rows of one class.

@@ -299,7 +299,8 @@ rvsp_status_t rvsp_cuda_symbolic(rvsp_cuda_plan_t p, void *stream, int32_t a_row
   }
   {
     PhaseScope ph(p, s, RVSP_PHASE_SCAN);
-    launch_scan_and_class(a_rows, p->counts.p, p->ops.p, c_row_ptr, p->partials.p,
+    launch_scan_and_class(a_rows, p->counts.p, p->ops.p, a_row_ptr, c_row_ptr,
+                          p->partials.p,
                           p->total.p, p->cls.p, misc + kNumCount, s);
     ph.launches = 3;
   }

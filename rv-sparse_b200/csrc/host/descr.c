@@ -208,7 +208,7 @@ static rvsp_status_t upload_structure(rvsp_spgemm_descr_t d,
         st = rvsp_device_check(d->plan, d->stream, A->rows, A->cols,
                                (const int32_t *)d->dA.row_ptr.p,
                                (const int32_t *)d->dA.col_idx.p, d->dA.entries,
-                               RVSP_REJECT_UNSAFE);
+                               RVSP_REJECT_ALL);
         if (st != RVSP_SUCCESS)
             return st;
     }
@@ -222,7 +222,7 @@ static rvsp_status_t upload_structure(rvsp_spgemm_descr_t d,
         st = rvsp_device_check(d->plan, d->stream, B->rows, B->cols,
                                (const int32_t *)d->dB.row_ptr.p,
                                (const int32_t *)d->dB.col_idx.p, d->dB.entries,
-                               RVSP_REJECT_UNSAFE);
+                               RVSP_REJECT_ALL);
         if (st != RVSP_SUCCESS)
             return st;
     }
@@ -270,10 +270,10 @@ rvsp_status_t rvsp_spgemm_work_estimation(rvsp_spgemm_descr_t d,
         b_rp = B->row_ptr;
         b_ci = B->col_idx;
         st = rvsp_device_check(d->plan, d->stream, A->rows, A->cols, a_rp, a_ci,
-                               A->nnz, RVSP_REJECT_UNSAFE);
+                               A->nnz, RVSP_REJECT_ALL);
         if (st == RVSP_SUCCESS && B != A)
             st = rvsp_device_check(d->plan, d->stream, B->rows, B->cols, b_rp, b_ci,
-                                   B->nnz, RVSP_REJECT_UNSAFE);
+                                   B->nnz, RVSP_REJECT_ALL);
         if (st != RVSP_SUCCESS)
             return st;
     }

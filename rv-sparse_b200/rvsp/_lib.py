@@ -39,8 +39,8 @@ MEM_DEVICE = 1
 
 PHASES = ("rowstats", "symbolic", "scan", "numeric", "predict", "fused",
           "compact", "copy", "check")
-CLASS_NAMES = ("empty", "esc", "w64", "w128", "w256", "w512", "w1024", "w2048",
-               "b8192", "dense")
+CLASS_NAMES = ("empty", "m4", "m8", "m16", "m32", "w64", "w128", "w256", "w512",
+               "w1024", "w2048", "b8192", "dense")
 
 CSR_OK, CSR_BAD_ROW_PTR, CSR_COL_OUT_OF_RANGE, CSR_UNSORTED, CSR_DUPLICATE = range(5)
 

@@ -15,6 +15,8 @@ import numpy as np
 from . import _lib as L
 from .csr import CSR
 
+CUDA_STREAM_LEGACY = 0x1  # cudaStreamLegacy
+
 
 def spgemm_csr(A: CSR, B: CSR, backend: int | None = L.BACKEND_CUDA) -> CSR:
     """One-shot C = A * B on host arrays (rvsp_spgemm_csr).  backend=None
@@ -109,6 +111,9 @@ class Descriptor:
                     "set_memory_space")
         if stream is not None:
             ptr = stream.cuda_stream if hasattr(stream, "cuda_stream") else stream
+            # torch reports the legacy default stream as 0, which the C API
+            # reads as "the descriptor's own stream"; name it explicitly.
+            ptr = ptr or CUDA_STREAM_LEGACY
             L.check(self.lib.rvsp_spgemm_set_stream(self.h, C.c_void_p(ptr)),
                     "set_stream")
         if profiling:

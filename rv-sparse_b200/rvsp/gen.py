@@ -32,13 +32,15 @@ def _distinct_sorted_columns(rng, lengths: np.ndarray, n_cols: int) -> np.ndarra
     row_of = np.repeat(np.arange(lengths.size, dtype=np.int64), lengths)
     starts = np.concatenate(([0], np.cumsum(lengths)[:-1]))
     cols = np.empty(total, np.int64)
-    # Dense rows (more than half the columns) take a permutation; the others
-    # use rejection: draw with replacement, redraw rows that drew a repeat.
-    dense = np.nonzero(lengths * 2 > n_cols)[0]
-    for r in dense:
-        cols[starts[r]:starts[r] + lengths[r]] = np.sort(
-            rng.permutation(n_cols)[:lengths[r]])
-    todo = np.nonzero((lengths * 2 <= n_cols) & (lengths > 0))[0]
+    # Rejection (draw with replacement, redraw rows that drew a repeat) is
+    # used only where a row draws no repeat with probability >= ~0.88
+    # (k^2 <= n/4); longer rows take the k smallest of n random keys.
+    crowded = np.nonzero(lengths * lengths * 4 > n_cols)[0]
+    for r in crowded:
+        k = int(lengths[r])
+        keys = rng.random(n_cols)
+        cols[starts[r]:starts[r] + k] = np.sort(np.argpartition(keys, k - 1)[:k])
+    todo = np.nonzero((lengths * lengths * 4 <= n_cols) & (lengths > 0))[0]
     while todo.size:
         sel_len = lengths[todo]
         sel_off = np.concatenate(([0], np.cumsum(sel_len)[:-1]))

@@ -56,22 +56,46 @@ def test_reference_outputs(golden_random):
 
 
 def class_probe(seed: int, b_cols: int = 60000):
-    """A x B whose rows land in every row class: B rows of length 3 (for
-    ESC rows) and 45; A rows select 0..400 of them."""
+    """A x B whose rows land in every row class: 200 short B rows (3 columns
+    out of the first 20), six groups of 200 rows of 8 columns drawn from
+    pools of 20..1024 columns, and 1800 rows of 45 columns over all of B.
+
+    A rows with <= 32 nonzeros give the merge classes; 40 (or 100) rows of
+    one 8-column group give > 32 A nonzeros with at most pool-size outputs
+    (W64 ... W2048); 45..400 long rows give the block-hash and dense
+    classes."""
     rng = np.random.default_rng(seed)
-    nb = 2000
-    lengths = np.where(np.arange(nb) < 200, 3, 45).astype(np.int64)
-    cols = gen._distinct_sorted_columns(rng, lengths, b_cols)
+    pools = [20, 64, 128, 256, 512, 1024]
+    groups = [(200, 3, 20)] + [(200, 8, p) for p in pools] + [(1800, 45, b_cols)]
+    cols, lengths, starts = [], [], []
+    first = 0
+    for n, ln, pool in groups:
+        lens = np.full(n, ln, np.int64)
+        cols.append(gen._distinct_sorted_columns(rng, lens, pool))
+        lengths.append(lens)
+        starts.append(first)
+        first += n
+    lengths = np.concatenate(lengths)
+    cols = np.concatenate(cols)
+    nb = lengths.size
     rp = np.zeros(nb + 1, np.int64)
     np.cumsum(lengths, out=rp[1:])
     B = CSR(nb, b_cols, rp, cols, rng.uniform(-1, 1, cols.size).astype(np.float32))
-    a_rows = []
-    ks = [0, 1, 2, 3, 5, 8, 12, 20, 30, 45, 70, 100, 150, 250, 400]
-    for r in range(300):
-        k = ks[r % len(ks)]
-        short = r % 2 == 0 and k <= 8
-        pool = np.arange(200) if short else np.arange(200, nb)
-        a_rows.append(np.sort(rng.choice(pool, size=min(k, pool.size), replace=False)))
+
+    def pick(group, k):
+        n = groups[group][0]
+        return starts[group] + rng.choice(n, size=k, replace=False)
+
+    a_rows = [np.zeros(0, np.int64)] * 4
+    long_g = len(groups) - 1
+    for k in (1, 2, 3, 4, 5, 8, 12, 16, 20, 30, 32):
+        a_rows += [pick(long_g, k) for _ in range(6)] + [pick(0, min(k, 12))]
+    for g, k in zip(range(1, 7), (40, 40, 40, 40, 40, 100)):
+        a_rows += [pick(g, k) for _ in range(8)]
+    a_rows += [pick(0, 40) for _ in range(8)]
+    for k in (45, 60, 80, 100, 150, 250, 400):
+        a_rows += [pick(long_g, k) for _ in range(6)]
+    a_rows = [np.sort(x) for x in a_rows]
     lens = np.array([x.size for x in a_rows], np.int64)
     arp = np.zeros(len(a_rows) + 1, np.int64)
     np.cumsum(lens, out=arp[1:])
