@@ -101,6 +101,42 @@ rvsp_status_t rvsp_cuda_plan_class_counts(rvsp_cuda_plan_t plan,
                                           int32_t *sym_out, int32_t *num_out,
                                           int32_t n);
 
+/* Size of the library's fixed device scratch for rvsp_cuda_numeric_noalloc,
+ * and the widest B it accepts (one float accumulator per B column). */
+#define RVSP_NOALLOC_SCRATCH_BYTES (16u << 20)
+#define RVSP_NOALLOC_MAX_B_COLS (RVSP_NOALLOC_SCRATCH_BYTES / 4u)
+
+/* Numeric pass that allocates nothing.  No counterpart in the reference: its
+ * CPU scalar backend takes a caller-allocated workspace, and every other
+ * numeric entry point here takes a caller-allocated device workspace.  This
+ * one is for callers that cannot call cudaMalloc when they need C's values:
+ * code running under CUDA graph capture, memory pools that forbid re-entrant
+ * allocation, and latency-bound loops that must not take allocation locks.
+ *
+ * Computes c_values for a structure (c_row_ptr, c_col_idx) that a symbolic
+ * pass already produced for this sparsity pattern; all pointers are device
+ * pointers, the caller passes every input and output.  Values are
+ * bit-identical to rvsp_cuda_numeric's.  Scratch is a fixed 16 MiB device
+ * array inside the library (held by every GPU that loads it until the
+ * process exits).  The first call on each device, with that device current,
+ * looks that array's address up; make it before any stream capture.  Each
+ * call clears the scratch it uses and is asynchronous on `stream`.  All calls
+ * share the one array: calls that overlap on the GPU (different streams or
+ * host threads) race, so serialise them.  b_cols > RVSP_NOALLOC_MAX_B_COLS
+ * (4,194,304) is rejected with RVSP_ERROR_INVALID_ARGUMENT before any device
+ * work; NULL pointers give RVSP_ERROR_NULL_POINTER. */
+rvsp_status_t rvsp_cuda_numeric_noalloc(void *stream, int32_t a_rows,
+                                        int32_t b_rows, int32_t b_cols,
+                                        const int32_t *a_row_ptr,
+                                        const int32_t *a_col_idx,
+                                        const float *a_values,
+                                        const int32_t *b_row_ptr,
+                                        const int32_t *b_col_idx,
+                                        const float *b_values,
+                                        const int32_t *c_row_ptr,
+                                        const int32_t *c_col_idx,
+                                        float *c_values);
+
 #ifdef __cplusplus
 }
 #endif

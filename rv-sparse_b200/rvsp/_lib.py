@@ -114,6 +114,8 @@ SIGNATURES = {
     "rvsp_cuda_plan_set_profiling": (_int, [_vp, _int]),
     "rvsp_cuda_plan_phase_times": (_int, [_vp, _vp, _vp, _i32, _int]),
     "rvsp_cuda_plan_class_counts": (_int, [_vp, _vp, _vp, _i32]),
+    "rvsp_cuda_numeric_noalloc": (_int, [_vp, _i32, _i32, _i32, _vp, _vp, _vp, _vp,
+                                         _vp, _vp, _vp, _vp, _vp]),
 }
 
 _lib = None
