@@ -157,6 +157,35 @@ rvsp_status_t rvsp_spgemm_get_class_counts(rvsp_spgemm_descr_t descr,
                                            int32_t *sym_out, int32_t *num_out,
                                            int32_t n);
 
+/* ---- new: learned binning and single-call products -------------------- */
+
+/* The row-binning model used by RVSP_SPGEMM_ALGO_CUDA_LEARNED (not owned;
+ * keep it alive while the descriptor uses it).  work_estimation with the
+ * learned algorithm and no model returns RVSP_ERROR_INVALID_ARGUMENT. */
+rvsp_status_t rvsp_spgemm_set_model(rvsp_spgemm_descr_t descr, rvsp_mlp_t model);
+
+/* Learned path: each row's slab capacity is
+ * min(bound, ceil(scale * predicted nnz) + 16).  Default 1.15.  Smaller
+ * values save slab memory and send more rows to the plain fallback. */
+rvsp_status_t rvsp_spgemm_set_capacity_scale(rvsp_spgemm_descr_t descr, float scale);
+
+/* Merge-accumulator policy of the descriptor's plan (see
+ * rvsp_cuda_plan_set_merge_policy): 0 automatic, 1 never, 2 whenever
+ * eligible.  Refused after work_estimation. */
+rvsp_status_t rvsp_spgemm_set_merge_policy(rvsp_spgemm_descr_t descr, int32_t policy);
+
+/* Rows the last learned work_estimation redid with the plain path. */
+rvsp_status_t rvsp_spgemm_get_overflow_rows(rvsp_spgemm_descr_t descr, int32_t *n_out);
+
+/* C = A * B in one call through the descriptor (its algorithm, memory space
+ * and stream): work_estimation, allocation of C (host: malloc, owns_data =
+ * 1; device: cudaMalloc, owns_data = 2) and compute.  With the learned
+ * algorithm this is the fused single pass plus a copy into C. */
+rvsp_status_t rvsp_spgemm_multiply(rvsp_spgemm_descr_t descr,
+                                   const rvsp_csr_matrix_t *A,
+                                   const rvsp_csr_matrix_t *B,
+                                   rvsp_csr_matrix_t *C);
+
 /* One-shot C = A * B with A, B and the resulting C in DEVICE memory.  C's
  * arrays are allocated with cudaMalloc and owns_data = 2. */
 rvsp_status_t rvsp_spgemm_csr_device(const rvsp_csr_matrix_t *A,

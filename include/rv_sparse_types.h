@@ -99,6 +99,9 @@ typedef enum {
     RVSP_SPGEMM_ALGO_CUDA_LEARNED = 17
 } rvsp_spgemm_algo_t;
 
+/* The row-binning model of the learned path (new; see rvsp_cuda.h). */
+typedef struct rvsp_mlp *rvsp_mlp_t;
+
 /* Where the arrays handed to the descriptor API live (new). */
 typedef enum {
     RVSP_MEM_HOST = 0,

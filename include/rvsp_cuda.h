@@ -101,6 +101,87 @@ rvsp_status_t rvsp_cuda_plan_class_counts(rvsp_cuda_plan_t plan,
                                           int32_t *sym_out, int32_t *num_out,
                                           int32_t n);
 
+/* ---- the row-binning model (new; no reference counterpart) --------------
+ *
+ * A small MLP, 8 row features -> 32 -> 32 -> 2 (ReLU), trained on the GPU by
+ * hand-written forward/backward/Adam kernels.  Output 0 predicts
+ * log2(1 + nnz of the output row), output 1 is the logit of the accumulator
+ * class (1: the merge accumulator is faster for the row, 0: the warp hash).
+ * The learned SpGEMM path uses it to size each row's hash table and to fuse
+ * the symbolic and numeric passes.  Parameters (1426 floats): W1[32][8],
+ * b1[32], W2[32][32], b2[32], W3[2][32], b3[2], then the per-feature mean[8]
+ * and 1/sd[8] used to standardise the inputs (not trained).
+ *
+ * Features of A row i (log2(1 + x) each): nnz(A row), ops = sum |B row k|,
+ * max |B row k|, ops / nnz, column span of the row's products, min(ops, span),
+ * b_cols, mean |B row| of B.  (rvsp_mlp_t is declared in rv_sparse_types.h.) */
+
+#define RVSP_MLP_NUM_FEATURES 8
+#define RVSP_MLP_NUM_OUTPUTS 2
+#define RVSP_MLP_NUM_PARAMS 1426
+
+/* He-uniform weights from `seed`, zero biases, identity standardisation. */
+rvsp_status_t rvsp_mlp_create(rvsp_mlp_t *model, uint64_t seed);
+void rvsp_mlp_destroy(rvsp_mlp_t model);
+int32_t rvsp_mlp_num_params(void);
+/* Host copies of all RVSP_MLP_NUM_PARAMS parameters (n >= that). */
+rvsp_status_t rvsp_mlp_get_params(rvsp_mlp_t model, float *host_out, int32_t n);
+rvsp_status_t rvsp_mlp_set_params(rvsp_mlp_t model, const float *host_in, int32_t n);
+/* Raw features of every A row into features_out (device, a_rows x 8,
+ * row-major) and, when not NULL, the op counts (device int64). */
+rvsp_status_t rvsp_mlp_features(void *stream, int32_t a_rows, int32_t b_rows,
+                                int32_t b_cols, const int32_t *a_row_ptr,
+                                const int32_t *a_col_idx, const int32_t *b_row_ptr,
+                                const int32_t *b_col_idx, float *features_out,
+                                int64_t *op_counts_out);
+/* Mean loss over n samples (features: device n x 8 raw features; targets:
+ * device n x 2) and its gradient with respect to the 1410 trained
+ * parameters, copied to the host.  Synchronizes `stream`. */
+rvsp_status_t rvsp_mlp_gradient(rvsp_mlp_t model, void *stream, const float *features,
+                                const float *targets, int32_t n,
+                                float *grad_host_out, float *loss_out);
+/* Adam (beta 0.9 / 0.999) over `epochs` passes of contiguous mini-batches of
+ * `batch` samples; loss_history (host, `epochs` floats, may be NULL) receives
+ * each epoch's mean loss. */
+rvsp_status_t rvsp_mlp_train(rvsp_mlp_t model, void *stream, const float *features,
+                             const float *targets, int32_t n, int32_t batch,
+                             int32_t epochs, float lr, float *loss_history);
+/* Per-row outputs (device a_rows x 2) for the product A x B. */
+rvsp_status_t rvsp_mlp_predict(rvsp_mlp_t model, void *stream, int32_t a_rows,
+                               int32_t b_rows, int32_t b_cols,
+                               const int32_t *a_row_ptr, const int32_t *a_col_idx,
+                               const int32_t *b_row_ptr, const int32_t *b_col_idx,
+                               float *pred_out);
+rvsp_status_t rvsp_mlp_save(rvsp_mlp_t model, const char *path);
+rvsp_status_t rvsp_mlp_load(rvsp_mlp_t model, const char *path);
+
+/* Learned analysis: the GPU form of rvsp_symbolic_count
+ * (rvsp_symbolic.c:13-86) for RVSP_SPGEMM_ALGO_CUDA_LEARNED.  The model
+ * predicts each row's output nnz and accumulator class; each row gets a slab
+ * slot of capacity min(ub, ceil(capacity_scale * predicted) + 16); one fused
+ * pass computes every row's sorted columns and values into its slot; rows
+ * that need more than their capacity are detected on the device and redone
+ * by the plain two-pass path.  Results (c_row_ptr, *c_nnz_out, op counts)
+ * are identical to rvsp_cuda_symbolic's; the following rvsp_cuda_numeric
+ * with fill != 0 copies the slab into C, and recomputes the values only if
+ * A's or B's values changed since (checked by a 64-bit fingerprint).
+ * Synchronizes `stream`. */
+rvsp_status_t rvsp_cuda_learned_symbolic(
+    rvsp_cuda_plan_t plan, rvsp_mlp_t model, void *stream, int32_t a_rows,
+    int32_t b_rows, int32_t b_cols, const int32_t *a_row_ptr, const int32_t *a_col_idx,
+    const float *a_values, int32_t a_nnz, const int32_t *b_row_ptr,
+    const int32_t *b_col_idx, const float *b_values, int32_t b_nnz,
+    float capacity_scale, int32_t *c_row_ptr, int64_t *c_nnz_out);
+
+/* Rows the last learned analysis had to redo with the plain path. */
+int32_t rvsp_cuda_plan_overflow_rows(rvsp_cuda_plan_t plan);
+
+/* Which rows may use the thread-per-row merge accumulator (rows of at most
+ * 16 A nonzeros and 2048 products): 0 automatic (when the matrix has at least
+ * 32768 rows), 1 never, 2 whenever a row is eligible.  The autotuner uses 1
+ * and 2 to time both accumulators on the same rows. */
+rvsp_status_t rvsp_cuda_plan_set_merge_policy(rvsp_cuda_plan_t plan, int32_t policy);
+
 /* Size of the library's fixed device scratch for rvsp_cuda_numeric_noalloc,
  * and the widest B it accepts (one float accumulator per B column). */
 #define RVSP_NOALLOC_SCRATCH_BYTES (16u << 20)

@@ -32,6 +32,12 @@ enum DevStatus : int32_t {
 };
 
 __device__ __forceinline__ int lane_id() { return threadIdx.x & 31; }
+
+// The t-th row of a class.  A null list means the class holds every row of
+// the matrix in order (the plan then skips building the list).
+__device__ __forceinline__ int32_t row_of(const int32_t *rows, int32_t t) {
+  return rows ? rows[t] : t;
+}
 __device__ __forceinline__ unsigned lanemask_lt() {
   return (1u << lane_id()) - 1u;
 }
@@ -82,6 +88,15 @@ __device__ __forceinline__ int hash_find(const int32_t *keys, int log2t,
   return -1;
 }
 
+// Fills n (a multiple of 4) 32-bit words at p (16-byte aligned) with v using
+// 128-bit stores; threads [tid, ...) step by nthreads.
+__device__ __forceinline__ void fill_words(void *p, int n, uint32_t v, int tid,
+                                           int nthreads) {
+  uint4 *q = reinterpret_cast<uint4 *>(p);
+  const uint4 x = make_uint4(v, v, v, v);
+  for (int i = tid; i < (n >> 2); i += nthreads) q[i] = x;
+}
+
 __device__ __forceinline__ int warp_incl_scan(int v) {
 #pragma unroll
   for (int o = 1; o < 32; o <<= 1) {
@@ -92,6 +107,12 @@ __device__ __forceinline__ int warp_incl_scan(int v) {
 }
 
 __device__ __forceinline__ int warp_sum(int v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(kFull, v, o);
+  return v;
+}
+
+__device__ __forceinline__ float warp_sum_f(float v) {
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(kFull, v, o);
   return v;

@@ -30,6 +30,13 @@ struct Lists {
   float a[K];
 };
 
+__device__ __forceinline__ void prefetch_l1(const void *p) {
+  asm volatile("prefetch.global.L1 [%0];" ::"l"(p));
+}
+
+// Opens the row's lists.  Every load here is independent of the others, and
+// the lines holding each B row (both ends, columns and values) are
+// prefetched into L1 so the merge loop's dependent loads hit L1.
 template <int K, bool kValues>
 __device__ __forceinline__ void open_lists(const Operands &op, int32_t p0,
                                            int32_t k, Lists<K> &L) {
@@ -46,10 +53,23 @@ __device__ __forceinline__ void open_lists(const Operands &op, int32_t p0,
       const int32_t b1 = __ldg(op.b_rp + kk + 1);
       L.pos[j] = b0;
       L.end[j] = b1;
-      if (b0 < b1) L.cur[j] = __ldg(op.b_col + b0);
+      if (b0 < b1) {
+        prefetch_l1(op.b_col + b1 - 1);
+        if (kValues) {
+          prefetch_l1(op.b_val + b0);
+          prefetch_l1(op.b_val + b1 - 1);
+        }
+        L.cur[j] = __ldg(op.b_col + b0);
+      }
     }
   }
 }
+
+// Blocks per SM the merge kernels ask the compiler to fit (register budget).
+template <int K>
+struct MergeOccupancy {
+  static constexpr int value = K <= 4 ? 16 : K <= 8 ? 10 : 6;
+};
 
 template <int K>
 __device__ __forceinline__ int32_t min_head(const Lists<K> &L) {
@@ -60,12 +80,12 @@ __device__ __forceinline__ int32_t min_head(const Lists<K> &L) {
 }
 
 template <int K>
-__global__ void __launch_bounds__(kMergeThreads)
+__global__ void __launch_bounds__(kMergeThreads, MergeOccupancy<K>::value)
 merge_symbolic_kernel(Operands op, const int32_t *__restrict__ rows,
                       int32_t nrows, int32_t *__restrict__ counts) {
   const int32_t t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= nrows) return;
-  const int32_t row = rows[t];
+  const int32_t row = row_of(rows, t);
   const int32_t p0 = op.a_rp[row];
   const int32_t k = op.a_rp[row + 1] - p0;
   Lists<K> L;
@@ -86,21 +106,25 @@ merge_symbolic_kernel(Operands op, const int32_t *__restrict__ rows,
   counts[row] = n;
 }
 
-template <int K>
-__global__ void __launch_bounds__(kMergeThreads)
+// kFused: the row goes to its slab slot (fo.off[row], capacity fo.cap[row] =
+// its op count, an exact upper bound, so it cannot overflow) and its nnz to
+// fo.counts[row].
+template <int K, bool kFused>
+__global__ void __launch_bounds__(kMergeThreads, MergeOccupancy<K>::value)
 merge_numeric_kernel(Operands op, const int32_t *__restrict__ rows, int32_t nrows,
                      const int32_t *__restrict__ c_rp, int32_t *__restrict__ c_col,
                      float *__restrict__ c_val, bool fill,
-                     int32_t *__restrict__ status) {
+                     int32_t *__restrict__ status, FusedOut fo) {
   const int32_t t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= nrows) return;
-  const int32_t row = rows[t];
+  const int32_t row = row_of(rows, t);
   const int32_t p0 = op.a_rp[row];
   const int32_t k = op.a_rp[row + 1] - p0;
   Lists<K> L;
   open_lists<K, true>(op, p0, k, L);
-  int32_t out = c_rp[row];
-  const int32_t out_end = c_rp[row + 1];
+  const int64_t out0 = kFused ? fo.off[row] : static_cast<int64_t>(c_rp[row]);
+  int64_t out = out0;
+  const int64_t out_end = kFused ? out0 + fo.cap[row] : static_cast<int64_t>(c_rp[row + 1]);
   for (;;) {
     const int32_t mn = min_head<K>(L);
     if (mn == INT_MAX) break;
@@ -115,12 +139,13 @@ merge_numeric_kernel(Operands op, const int32_t *__restrict__ rows, int32_t nrow
       }
     }
     if (out < out_end) {
-      if (fill) c_col[out] = mn;
+      if (fill || kFused) c_col[out] = mn;
       c_val[out] = acc;
     }
     ++out;
   }
-  if (out != out_end) report(status, kDevCountMismatch);
+  if (kFused) fo.counts[row] = static_cast<int32_t>(out - out0);
+  else if (out != out_end) report(status, kDevCountMismatch);
 }
 
 template <int K>
@@ -132,10 +157,15 @@ void sym(const Operands &op, const int32_t *rows, int32_t nrows, int32_t *counts
 
 template <int K>
 void num(const Operands &op, const int32_t *rows, int32_t nrows, const int32_t *c_rp,
-         int32_t *c_col, float *c_val, bool fill, int32_t *status, cudaStream_t s) {
+         int32_t *c_col, float *c_val, bool fill, int32_t *status, const FusedOut *fo,
+         cudaStream_t s) {
   const int grid = (nrows + kMergeThreads - 1) / kMergeThreads;
-  merge_numeric_kernel<K><<<grid, kMergeThreads, 0, s>>>(op, rows, nrows, c_rp, c_col,
-                                                         c_val, fill, status);
+  if (fo)
+    merge_numeric_kernel<K, true><<<grid, kMergeThreads, 0, s>>>(
+        op, rows, nrows, c_rp, c_col, c_val, true, status, *fo);
+  else
+    merge_numeric_kernel<K, false><<<grid, kMergeThreads, 0, s>>>(
+        op, rows, nrows, c_rp, c_col, c_val, fill, status, FusedOut{});
 }
 
 }  // namespace
@@ -147,20 +177,19 @@ void launch_merge_symbolic(int cls, const Operands &op, const int32_t *rows,
     case kM4: sym<4>(op, rows, nrows, counts, s); break;
     case kM8: sym<8>(op, rows, nrows, counts, s); break;
     case kM16: sym<16>(op, rows, nrows, counts, s); break;
-    case kM32: sym<32>(op, rows, nrows, counts, s); break;
     default: break;
   }
 }
 
 void launch_merge_numeric(int cls, const Operands &op, const int32_t *rows,
                           int32_t nrows, const int32_t *c_rp, int32_t *c_col,
-                          float *c_val, bool fill, int32_t *status, cudaStream_t s) {
+                          float *c_val, bool fill, int32_t *status, const FusedOut *fo,
+                          cudaStream_t s) {
   if (nrows <= 0) return;
   switch (cls) {
-    case kM4: num<4>(op, rows, nrows, c_rp, c_col, c_val, fill, status, s); break;
-    case kM8: num<8>(op, rows, nrows, c_rp, c_col, c_val, fill, status, s); break;
-    case kM16: num<16>(op, rows, nrows, c_rp, c_col, c_val, fill, status, s); break;
-    case kM32: num<32>(op, rows, nrows, c_rp, c_col, c_val, fill, status, s); break;
+    case kM4: num<4>(op, rows, nrows, c_rp, c_col, c_val, fill, status, fo, s); break;
+    case kM8: num<8>(op, rows, nrows, c_rp, c_col, c_val, fill, status, fo, s); break;
+    case kM16: num<16>(op, rows, nrows, c_rp, c_col, c_val, fill, status, fo, s); break;
     default: break;
   }
 }

@@ -35,11 +35,18 @@ constexpr int kSteppingMinAvgLen = 16;  // avg B row length that favours steppin
 
 // ---- product walkers for warp-per-row classes --------------------------------
 
+// A walker's `stop` functor is called with the warp converged after each A
+// nonzero (stepping) or each tile (tiles); it returns a warp-uniform bool and
+// true ends the walk.  The plain path never stops (NoStop).
+struct NoStop {
+  __device__ __forceinline__ bool operator()() const { return false; }
+};
+
 // Stepping: f(col, term) for each entry of A nonzero p's B row, lanes over
 // the B row, __syncwarp after each A nonzero.
-template <typename F>
+template <typename F, typename S = NoStop>
 __device__ __forceinline__ void warp_stepping(const Operands &op, int32_t p0,
-                                              int32_t p1, F f) {
+                                              int32_t p1, F f, S stop = S()) {
   const int lane = lane_id();
   for (int32_t p = p0; p < p1; p += 32) {
     const AChunk c = load_chunk(op.a_col, op.a_val, op.b_rp, p + lane, p1, true);
@@ -53,15 +60,16 @@ __device__ __forceinline__ void warp_stepping(const Operands &op, int32_t p0,
         f(col, __fmul_rn(a, __ldg(op.b_val + bbeg + e)));
       }
       __syncwarp();
+      if (stop()) return;
     }
   }
 }
 
 // Tiles: g(valid, col, term) for 32 flattened products at a time (all lanes
 // call g, invalid ones with valid == false).
-template <typename G>
+template <typename G, typename S = NoStop>
 __device__ __forceinline__ void warp_tiles(const Operands &op, int32_t p0,
-                                           int32_t p1, G g) {
+                                           int32_t p1, G g, S stop = S()) {
   const int lane = lane_id();
   for (int32_t p = p0; p < p1; p += 32) {
     const AChunk c = load_chunk(op.a_col, op.a_val, op.b_rp, p + lane, p1, true);
@@ -80,6 +88,7 @@ __device__ __forceinline__ void warp_tiles(const Operands &op, int32_t p0,
         term = __fmul_rn(a, __ldg(op.b_val + bp));
       }
       g(v, col, term);
+      if (stop()) return;
     }
   }
 }
@@ -91,13 +100,34 @@ __device__ __forceinline__ bool use_stepping(const int64_t *ops, int32_t row,
 
 // ---- W<T>: warp per row, fill mode --------------------------------------------
 
+// Output of one row in the fill kernels.  Plain: C at c_rp[row] with the
+// exact nnz c_rp[row + 1] - c_rp[row].  Fused (kFused): the row's slab slot
+// at fo.off[row] with capacity fo.cap[row]; the kernel writes the row's nnz
+// to fo.counts[row], or, when the row needs more than its capacity (or its
+// table fills), marks it -1, appends it to fo.ovf_rows and writes nothing.
+template <bool kFused>
+__device__ __forceinline__ int64_t out_begin(const FusedOut &fo, const int32_t *c_rp,
+                                             int32_t row) {
+  return kFused ? fo.off[row] : static_cast<int64_t>(c_rp[row]);
+}
+template <bool kFused>
+__device__ __forceinline__ int out_limit(const FusedOut &fo, const int32_t *c_rp,
+                                         int32_t row) {
+  return kFused ? fo.cap[row] : c_rp[row + 1] - c_rp[row];
+}
+__device__ __forceinline__ void mark_overflow(const FusedOut &fo, int32_t row) {
+  fo.counts[row] = -1;
+  fo.ovf_rows[atomicAdd(fo.ovf_count, 1)] = row;
+}
+
 // Shared memory per warp: sbuf[T/2] u64 | keys[T] i32 | vals[T] f32 = 12 T bytes.
-template <int LOG2T>
+template <int LOG2T, bool kFused>
 __global__ void __launch_bounds__(kWarpsPerBlock * 32)
 num_warp_fill_kernel(Operands op, const int64_t *__restrict__ ops,
                      const int32_t *__restrict__ rows, int32_t nrows,
                      const int32_t *__restrict__ c_rp, int32_t *__restrict__ c_col,
-                     float *__restrict__ c_val, int32_t *__restrict__ status) {
+                     float *__restrict__ c_val, int32_t *__restrict__ status,
+                     FusedOut fo) {
   constexpr int T = 1 << LOG2T, H = T / 2;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   unsigned char *base = smem_raw + size_t(threadIdx.x >> 5) * (12 * T);
@@ -108,37 +138,58 @@ num_warp_fill_kernel(Operands op, const int64_t *__restrict__ ops,
   const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   if (w >= nrows) return;
   const int lane = lane_id();
-  for (int s = lane; s < T; s += 32) {
-    keys[s] = kEmpty;
-    vals[s] = 0.0f;
-  }
+  fill_words(keys, T, 0xffffffffu, lane, 32);
+  fill_words(vals, T, 0u, lane, 32);  // +0.0f
   __syncwarp();
-  const int32_t row = rows[w];
+  const int32_t row = row_of(rows, w);
   const int32_t p0 = op.a_rp[row], p1 = op.a_rp[row + 1];
+  const int64_t out0 = out_begin<kFused>(fo, c_rp, row);
+  const int m = out_limit<kFused>(fo, c_rp, row);
   bool bad = false;
+  int my_new = 0;     // distinct columns this lane created (stepping)
+  int total_new = 0;  // distinct columns so far (tiles; warp-uniform)
+  bool over = false;  // fused: the row outgrew its capacity (warp-uniform)
   if (use_stepping(ops, row, p1 - p0)) {
-    warp_stepping(op, p0, p1, [&](int32_t col, float term) {
-      bool created;
-      const int s = hash_insert(keys, LOG2T, col, created);
-      if (s >= 0) vals[s] = __fadd_rn(vals[s], term);
-      else bad = true;
-    });
+    warp_stepping(
+        op, p0, p1,
+        [&](int32_t col, float term) {
+          bool created;
+          const int s = hash_insert(keys, LOG2T, col, created);
+          if (s >= 0) vals[s] = __fadd_rn(vals[s], term);
+          else bad = true;
+          my_new += created;
+        },
+        [&]() {
+          if (!kFused) return false;
+          over = warp_sum(my_new) > m || __any_sync(kFull, bad);
+          return over;
+        });
   } else {
-    warp_tiles(op, p0, p1, [&](bool v, int32_t col, float term) {
-      int s = -1;
-      if (v) {
-        bool created;
-        s = hash_insert(keys, LOG2T, col, created);
-        if (s < 0) bad = true;
-      }
-      ordered_apply(vals, v && s >= 0, s, term);
-    });
+    warp_tiles(
+        op, p0, p1,
+        [&](bool v, int32_t col, float term) {
+          int s = -1;
+          bool created = false;
+          if (v) {
+            s = hash_insert(keys, LOG2T, col, created);
+            if (s < 0) bad = true;
+          }
+          total_new += __popc(__ballot_sync(kFull, created));
+          ordered_apply(vals, v && s >= 0, s, term);
+        },
+        [&]() {
+          if (!kFused) return false;
+          over = total_new > m || __any_sync(kFull, bad);
+          return over;
+        });
   }
   __syncwarp();
+  if (kFused && over) {
+    if (lane == 0) mark_overflow(fo, row);
+    return;
+  }
 
   // Compact the occupied slots, sort by column, write the row.
-  const int32_t cs = c_rp[row];
-  const int m = c_rp[row + 1] - cs;
   int n = 0;
   for (int s0 = 0; s0 < T; s0 += 32) {
     const int s = s0 + lane;
@@ -158,13 +209,17 @@ num_warp_fill_kernel(Operands op, const int64_t *__restrict__ ops,
   const int out = kept < m ? kept : m;
   for (int e = lane; e < out; e += 32) {
     const unsigned long long x = sbuf[e];
-    c_col[cs + e] = packed_col(x);
-    c_val[cs + e] = packed_val(x);
+    c_col[out0 + e] = packed_col(x);
+    c_val[out0 + e] = packed_val(x);
   }
   const bool any_bad = __any_sync(kFull, bad);
   if (lane == 0) {
-    if (any_bad) report(status, kDevHashFull);
-    if (n != m) report(status, kDevCountMismatch);
+    if (kFused) {
+      fo.counts[row] = n;
+    } else {
+      if (any_bad) report(status, kDevHashFull);
+      if (n != m) report(status, kDevCountMismatch);
+    }
   }
 }
 
@@ -188,9 +243,9 @@ num_warp_reuse_kernel(Operands op, const int64_t *__restrict__ ops,
   const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   if (w >= nrows) return;
   const int lane = lane_id();
-  for (int s = lane; s < T; s += 32) keys[s] = kEmpty;
+  fill_words(keys, T, 0xffffffffu, lane, 32);
   __syncwarp();
-  const int32_t row = rows[w];
+  const int32_t row = row_of(rows, w);
   const int32_t cs = c_rp[row];
   const int m = c_rp[row + 1] - cs;
   bool bad = false;
@@ -246,10 +301,12 @@ struct AStage {
 };
 
 // f(col, term) for every product of the row, one A nonzero at a time across
-// the whole block, with a barrier between A nonzeros.
-template <typename F>
+// the whole block, with a barrier between A nonzeros.  stop() is evaluated
+// after each barrier and must return the same value on every thread.
+template <typename F, typename S = NoStop>
 __device__ __forceinline__ void block_stepping(const Operands &op, int32_t p0,
-                                               int32_t p1, AStage &st, F f) {
+                                               int32_t p1, AStage &st, F f,
+                                               S stop = S()) {
   for (int32_t p = p0; p < p1; p += kAStage) {
     const int cnt = min(kAStage, p1 - p);
     __syncthreads();
@@ -270,6 +327,7 @@ __device__ __forceinline__ void block_stepping(const Operands &op, int32_t p0,
         f(col, __fmul_rn(a, __ldg(op.b_val + bbeg + e)));
       }
       __syncthreads();
+      if (stop()) return;
     }
   }
 }
@@ -278,31 +336,31 @@ __device__ __forceinline__ void block_stepping(const Operands &op, int32_t p0,
 
 // Shared memory: sbuf[4096] u64 | keys[8192] i32 | vals[8192] f32 (96 KiB) in
 // fill mode; keys | posv | acc[4096] (80 KiB) in reuse mode.
-template <bool kFill>
+template <bool kFill, bool kFused>
 __global__ void __launch_bounds__(kBlockHashThreads)
 num_block_kernel(Operands op, const int32_t *__restrict__ rows,
                  const int32_t *__restrict__ c_rp, int32_t *__restrict__ c_col,
-                 float *__restrict__ c_val, int32_t *__restrict__ status) {
+                 float *__restrict__ c_val, int32_t *__restrict__ status,
+                 FusedOut fo) {
   constexpr int LOG2T = kBlockHashLog2, T = 1 << LOG2T, H = T / 2;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ AStage st;
-  __shared__ int32_t s_n, s_flags;
+  __shared__ int32_t s_n, s_flags, s_new;
   unsigned long long *sbuf = reinterpret_cast<unsigned long long *>(smem_raw);
   int32_t *keys = reinterpret_cast<int32_t *>(smem_raw + (kFill ? 4 * T : 0));
   float *vals = reinterpret_cast<float *>(smem_raw + 8 * T);           // fill
   int32_t *posv = reinterpret_cast<int32_t *>(smem_raw + 4 * T);       // reuse
   float *acc = reinterpret_cast<float *>(smem_raw + 8 * T);            // reuse
 
-  const int32_t row = rows[blockIdx.x];
-  const int32_t cs = c_rp[row];
-  const int m = c_rp[row + 1] - cs;
-  for (int s = threadIdx.x; s < T; s += blockDim.x) {
-    keys[s] = kEmpty;
-    if (kFill) vals[s] = 0.0f;
-  }
+  const int32_t row = row_of(rows, blockIdx.x);
+  const int64_t cs = out_begin<kFused>(fo, c_rp, row);
+  const int m = out_limit<kFused>(fo, c_rp, row);
+  fill_words(keys, T, 0xffffffffu, threadIdx.x, blockDim.x);
+  if (kFill) fill_words(vals, T, 0u, threadIdx.x, blockDim.x);  // +0.0f
   if (threadIdx.x == 0) {
     s_n = 0;
     s_flags = 0;
+    s_new = 0;
   }
   __syncthreads();
   int flags = 0;
@@ -316,22 +374,37 @@ num_block_kernel(Operands op, const int32_t *__restrict__ rows,
     }
   }
   const int32_t p0 = op.a_rp[row], p1 = op.a_rp[row + 1];
-  block_stepping(op, p0, p1, st, [&](int32_t col, float term) {
-    if (kFill) {
-      bool created;
-      const int s = hash_insert(keys, LOG2T, col, created);
-      if (s >= 0) vals[s] = __fadd_rn(vals[s], term);
-      else flags |= 1;
-    } else {
-      const int s = hash_find(keys, LOG2T, col);
-      if (s >= 0) {
-        const int pos = posv[s];
-        acc[pos] = __fadd_rn(acc[pos], term);
-      } else {
-        flags |= 2;
-      }
+  block_stepping(
+      op, p0, p1, st,
+      [&](int32_t col, float term) {
+        if (kFill) {
+          bool created;
+          const int s = hash_insert(keys, LOG2T, col, created);
+          if (s >= 0) vals[s] = __fadd_rn(vals[s], term);
+          else flags |= 1;
+          if (kFused) {
+            if (created) atomicAdd(&s_new, 1);
+            if (s < 0) atomicOr(&s_flags, 1);
+          }
+        } else {
+          const int s = hash_find(keys, LOG2T, col);
+          if (s >= 0) {
+            const int pos = posv[s];
+            acc[pos] = __fadd_rn(acc[pos], term);
+          } else {
+            flags |= 2;
+          }
+        }
+      },
+      [&]() { return kFused && (s_new > m || (s_flags & 1)); });
+  if (kFused) {
+    // The row outgrew its predicted capacity (or its table): leave it to the
+    // plain path.  s_new and s_flags are read after the last barrier.
+    if (s_new > m || (s_flags & 1)) {
+      if (threadIdx.x == 0) mark_overflow(fo, row);
+      return;
     }
-  });
+  }
   if (flags) atomicOr(&s_flags, flags);
   if (kFill) {
     // Compact occupied slots (any order), then sort by column.
@@ -359,7 +432,10 @@ num_block_kernel(Operands op, const int32_t *__restrict__ rows,
       c_col[cs + e] = packed_col(x);
       c_val[cs + e] = packed_val(x);
     }
-    if (threadIdx.x == 0 && n != m) report(status, kDevCountMismatch);
+    if (threadIdx.x == 0) {
+      if (kFused) fo.counts[row] = n;
+      else if (n != m) report(status, kDevCountMismatch);
+    }
   } else {
     __syncthreads();
     for (int e = threadIdx.x; e < m; e += blockDim.x) c_val[cs + e] = acc[e];
@@ -373,13 +449,16 @@ num_block_kernel(Operands op, const int32_t *__restrict__ rows,
 
 // ---- DENSE: block per row, global dense accumulator ------------------------------
 
-template <bool kFill, bool kSmemBits>
+// Fused (kFused, fill only): rows write into their slab slot; the capacity is
+// the row's exact upper bound min(ops, b_cols), so a dense row never
+// overflows, and its nnz goes to fo.counts[row].
+template <bool kFill, bool kSmemBits, bool kFused>
 __global__ void __launch_bounds__(kDenseThreads)
 num_dense_kernel(Operands op, const int32_t *__restrict__ rows, int32_t nrows,
                  const int32_t *__restrict__ c_rp, int32_t *__restrict__ c_col,
                  float *__restrict__ c_val, float *__restrict__ dense_acc,
                  size_t acc_stride, uint32_t *__restrict__ gbits,
-                 size_t bits_stride, int32_t *__restrict__ status) {
+                 size_t bits_stride, int32_t *__restrict__ status, FusedOut fo) {
   extern __shared__ uint32_t smem_u32[];
   __shared__ AStage st;
   __shared__ int32_t s_lo, s_hi, s_total;
@@ -391,9 +470,9 @@ num_dense_kernel(Operands op, const int32_t *__restrict__ rows, int32_t nrows,
     for (int32_t w = threadIdx.x; w < words; w += blockDim.x) bits[w] = 0u;
   }
   for (int32_t r = blockIdx.x; r < nrows; r += gridDim.x) {
-    const int32_t row = rows[r];
-    const int32_t cs = c_rp[row];
-    const int m = c_rp[row + 1] - cs;
+    const int32_t row = row_of(rows, r);
+    const int64_t cs = out_begin<kFused>(fo, c_rp, row);
+    const int m = out_limit<kFused>(fo, c_rp, row);
     if (threadIdx.x == 0) {
       s_lo = INT_MAX;
       s_hi = -1;
@@ -453,7 +532,10 @@ num_dense_kernel(Operands op, const int32_t *__restrict__ rows, int32_t nrows,
         }
         bits[w] = 0u;
       }
-      if (threadIdx.x == 0 && s_total != m) report(status, kDevCountMismatch);
+      if (threadIdx.x == 0) {
+        if (kFused) fo.counts[row] = s_total;
+        else if (s_total != m) report(status, kDevCountMismatch);
+      }
     } else {
       for (int e = threadIdx.x; e < m; e += blockDim.x) {
         const int32_t col = __ldg(c_col + cs + e);
@@ -468,17 +550,25 @@ num_dense_kernel(Operands op, const int32_t *__restrict__ rows, int32_t nrows,
 template <int LOG2T>
 void launch_warp(const Operands &op, const int64_t *ops, const int32_t *rows,
                  int32_t nrows, const int32_t *c_rp, int32_t *c_col,
-                 float *c_val, bool fill, int32_t *status, cudaStream_t s) {
+                 float *c_val, bool fill, int32_t *status, const FusedOut *fo,
+                 cudaStream_t s) {
   constexpr int T = 1 << LOG2T;
   const int threads = kWarpsPerBlock * 32;
   const int grid = (nrows + kWarpsPerBlock - 1) / kWarpsPerBlock;
-  if (fill) {
+  if (fo) {
     const size_t smem = size_t(kWarpsPerBlock) * 12 * T;
-    cudaFuncSetAttribute(num_warp_fill_kernel<LOG2T>,
+    cudaFuncSetAttribute(num_warp_fill_kernel<LOG2T, true>,
                          cudaFuncAttributeMaxDynamicSharedMemorySize,
                          static_cast<int>(smem));
-    num_warp_fill_kernel<LOG2T><<<grid, threads, smem, s>>>(op, ops, rows, nrows,
-                                                            c_rp, c_col, c_val, status);
+    num_warp_fill_kernel<LOG2T, true><<<grid, threads, smem, s>>>(
+        op, ops, rows, nrows, c_rp, c_col, c_val, status, *fo);
+  } else if (fill) {
+    const size_t smem = size_t(kWarpsPerBlock) * 12 * T;
+    cudaFuncSetAttribute(num_warp_fill_kernel<LOG2T, false>,
+                         cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         static_cast<int>(smem));
+    num_warp_fill_kernel<LOG2T, false><<<grid, threads, smem, s>>>(
+        op, ops, rows, nrows, c_rp, c_col, c_val, status, FusedOut{});
   } else {
     const size_t smem = size_t(kWarpsPerBlock) * 10 * T;
     cudaFuncSetAttribute(num_warp_reuse_kernel<LOG2T>,
@@ -502,68 +592,86 @@ size_t dense_slot_bits_bytes(int32_t b_cols) {
   return (b + 255) & ~size_t(255);
 }
 
+namespace {
+
+template <bool kFill, bool kFused>
+void launch_block(const Operands &op, const int32_t *rows, int32_t nrows,
+                  const int32_t *c_rp, int32_t *c_col, float *c_val, int32_t *status,
+                  const FusedOut &fo, cudaStream_t s) {
+  constexpr int T = 1 << kBlockHashLog2;
+  const size_t smem = size_t(kFill ? 12 : 10) * T;
+  cudaFuncSetAttribute(num_block_kernel<kFill, kFused>,
+                       cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       static_cast<int>(smem));
+  num_block_kernel<kFill, kFused><<<nrows, kBlockHashThreads, smem, s>>>(
+      op, rows, c_rp, c_col, c_val, status, fo);
+}
+
+template <bool kFill, bool kSmemBits, bool kFused>
+void launch_dense(const Operands &op, const int32_t *rows, int32_t nrows,
+                  const int32_t *c_rp, int32_t *c_col, float *c_val, float *dense_acc,
+                  uint32_t *dense_bits, int32_t dense_slots, int32_t *status,
+                  const FusedOut &fo, cudaStream_t s) {
+  const size_t acc_stride = dense_slot_acc_bytes(op.b_cols) / sizeof(float);
+  const size_t bits_stride = dense_slot_bits_bytes(op.b_cols) / sizeof(uint32_t);
+  const int grid = nrows < dense_slots ? nrows : dense_slots;
+  size_t smem = 0;
+  if (kFill && kSmemBits) {
+    smem = ((size_t(op.b_cols) + 31) >> 5) * sizeof(uint32_t);
+    cudaFuncSetAttribute(num_dense_kernel<kFill, kSmemBits, kFused>,
+                         cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         static_cast<int>(smem));
+  }
+  num_dense_kernel<kFill, kSmemBits, kFused><<<grid, kDenseThreads, smem, s>>>(
+      op, rows, nrows, c_rp, c_col, c_val, dense_acc, acc_stride,
+      kSmemBits ? nullptr : dense_bits, kSmemBits ? 0 : bits_stride, status, fo);
+}
+
+}  // namespace
+
 void launch_numeric_class(int cls, const Operands &op, const int64_t *ops,
                           const int32_t *rows, int32_t nrows,
                           const int32_t *c_rp, int32_t *c_col, float *c_val,
                           bool fill, float *dense_acc, uint32_t *dense_bits,
                           int32_t dense_slots, int32_t *status, int num_sms,
-                          cudaStream_t s) {
+                          cudaStream_t s, const FusedOut *fo) {
   if (nrows <= 0) return;
   (void)num_sms;
+  const FusedOut none{};
   switch (cls) {
     case kM4:
     case kM8:
     case kM16:
-    case kM32:
-      launch_merge_numeric(cls, op, rows, nrows, c_rp, c_col, c_val, fill, status, s);
+      launch_merge_numeric(cls, op, rows, nrows, c_rp, c_col, c_val, fill, status, fo, s);
       break;
-    case kW64: launch_warp<6>(op, ops, rows, nrows, c_rp, c_col, c_val, fill, status, s); break;
-    case kW128: launch_warp<7>(op, ops, rows, nrows, c_rp, c_col, c_val, fill, status, s); break;
-    case kW256: launch_warp<8>(op, ops, rows, nrows, c_rp, c_col, c_val, fill, status, s); break;
-    case kW512: launch_warp<9>(op, ops, rows, nrows, c_rp, c_col, c_val, fill, status, s); break;
-    case kW1024: launch_warp<10>(op, ops, rows, nrows, c_rp, c_col, c_val, fill, status, s); break;
-    case kW2048: launch_warp<11>(op, ops, rows, nrows, c_rp, c_col, c_val, fill, status, s); break;
-    case kB8192: {
-      constexpr int T = 1 << kBlockHashLog2;
-      if (fill) {
-        const size_t smem = size_t(12) * T;
-        cudaFuncSetAttribute(num_block_kernel<true>,
-                             cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             static_cast<int>(smem));
-        num_block_kernel<true><<<nrows, kBlockHashThreads, smem, s>>>(
-            op, rows, c_rp, c_col, c_val, status);
-      } else {
-        const size_t smem = size_t(10) * T;
-        cudaFuncSetAttribute(num_block_kernel<false>,
-                             cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             static_cast<int>(smem));
-        num_block_kernel<false><<<nrows, kBlockHashThreads, smem, s>>>(
-            op, rows, c_rp, c_col, c_val, status);
-      }
+    case kW64: launch_warp<6>(op, ops, rows, nrows, c_rp, c_col, c_val, fill, status, fo, s); break;
+    case kW128: launch_warp<7>(op, ops, rows, nrows, c_rp, c_col, c_val, fill, status, fo, s); break;
+    case kW256: launch_warp<8>(op, ops, rows, nrows, c_rp, c_col, c_val, fill, status, fo, s); break;
+    case kW512: launch_warp<9>(op, ops, rows, nrows, c_rp, c_col, c_val, fill, status, fo, s); break;
+    case kW1024: launch_warp<10>(op, ops, rows, nrows, c_rp, c_col, c_val, fill, status, fo, s); break;
+    case kW2048: launch_warp<11>(op, ops, rows, nrows, c_rp, c_col, c_val, fill, status, fo, s); break;
+    case kB8192:
+      if (fo) launch_block<true, true>(op, rows, nrows, c_rp, c_col, c_val, status, *fo, s);
+      else if (fill) launch_block<true, false>(op, rows, nrows, c_rp, c_col, c_val, status, none, s);
+      else launch_block<false, false>(op, rows, nrows, c_rp, c_col, c_val, status, none, s);
       break;
-    }
     case kDense: {
-      const size_t acc_stride = dense_slot_acc_bytes(op.b_cols) / sizeof(float);
-      const size_t bits_stride = dense_slot_bits_bytes(op.b_cols) / sizeof(uint32_t);
-      const int grid = nrows < dense_slots ? nrows : dense_slots;
       const bool smem_bits = op.b_cols <= kSmemBitmapMaxCols;
-      if (fill && smem_bits) {
-        const size_t smem = ((size_t(op.b_cols) + 31) >> 5) * sizeof(uint32_t);
-        cudaFuncSetAttribute(num_dense_kernel<true, true>,
-                             cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             static_cast<int>(smem));
-        num_dense_kernel<true, true><<<grid, kDenseThreads, smem, s>>>(
-            op, rows, nrows, c_rp, c_col, c_val, dense_acc, acc_stride, nullptr, 0,
-            status);
-      } else if (fill) {
-        num_dense_kernel<true, false><<<grid, kDenseThreads, 0, s>>>(
-            op, rows, nrows, c_rp, c_col, c_val, dense_acc, acc_stride, dense_bits,
-            bits_stride, status);
-      } else {
-        num_dense_kernel<false, false><<<grid, kDenseThreads, 0, s>>>(
-            op, rows, nrows, c_rp, c_col, c_val, dense_acc, acc_stride, nullptr, 0,
-            status);
-      }
+      if (fo && smem_bits)
+        launch_dense<true, true, true>(op, rows, nrows, c_rp, c_col, c_val, dense_acc,
+                                       dense_bits, dense_slots, status, *fo, s);
+      else if (fo)
+        launch_dense<true, false, true>(op, rows, nrows, c_rp, c_col, c_val, dense_acc,
+                                        dense_bits, dense_slots, status, *fo, s);
+      else if (fill && smem_bits)
+        launch_dense<true, true, false>(op, rows, nrows, c_rp, c_col, c_val, dense_acc,
+                                        dense_bits, dense_slots, status, none, s);
+      else if (fill)
+        launch_dense<true, false, false>(op, rows, nrows, c_rp, c_col, c_val, dense_acc,
+                                         dense_bits, dense_slots, status, none, s);
+      else
+        launch_dense<false, false, false>(op, rows, nrows, c_rp, c_col, c_val, dense_acc,
+                                          dense_bits, dense_slots, status, none, s);
       break;
     }
     default: break;

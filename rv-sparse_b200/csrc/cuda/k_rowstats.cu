@@ -43,7 +43,7 @@ rowstats_kernel(Operands op, int64_t *__restrict__ ops, uint8_t *__restrict__ cl
         const int32_t k = __ldg(op.a_col + p);
         s += __ldg(op.b_rp + k + 1) - __ldg(op.b_rp + k);
       }
-      c = classify_row(p1 - p0, s, s < op.b_cols ? s : op.b_cols);
+      c = classify_row(p1 - p0, s, s < op.b_cols ? s : op.b_cols, op.merge_ok);
       ops[i] = s;
       cls[i] = static_cast<uint8_t>(c);
       if (c == kEmpty_) counts[i] = 0;
@@ -77,7 +77,7 @@ rowstats_long_kernel(Operands op, const int32_t *__restrict__ long_rows,
     }
     s = warp_sum64(s);
     if (lane == 0) {
-      const int c = classify_row(p1 - p0, s, s < op.b_cols ? s : op.b_cols);
+      const int c = classify_row(p1 - p0, s, s < op.b_cols ? s : op.b_cols, op.merge_ok);
       ops[i] = s;
       cls[i] = static_cast<uint8_t>(c);
       if (c == kEmpty_) counts[i] = 0;

@@ -100,7 +100,7 @@ tile_apply_kernel(int32_t n, const int32_t *__restrict__ counts,
                   const int32_t *__restrict__ a_rp,
                   const int64_t *__restrict__ partials,
                   int32_t *__restrict__ row_ptr, uint8_t *__restrict__ cls,
-                  int32_t *__restrict__ class_count) {
+                  int32_t *__restrict__ class_count, bool merge_ok) {
   __shared__ int32_t s_items[kTile + kTile / 32];
   __shared__ long long s_warp[kThreads / 32];
   __shared__ int32_t s_cnt[kNumClasses];
@@ -117,7 +117,7 @@ tile_apply_kernel(int32_t n, const int32_t *__restrict__ counts,
     int c = kEmpty_;
     if (i < n) {
       m = counts[i];
-      c = classify_row(a_rp[i + 1] - a_rp[i], ops[i], m);
+      c = classify_row(a_rp[i + 1] - a_rp[i], ops[i], m, merge_ok);
       cls[i] = static_cast<uint8_t>(c);
     }
     s_items[skew(idx)] = m;
@@ -153,7 +153,59 @@ tile_apply_kernel(int32_t n, const int32_t *__restrict__ counts,
     if (s_cnt[k]) atomicAdd(&class_count[k], s_cnt[k]);
 }
 
+// One block: exclusive scan of partials[0..nt) in place, total to *total.
+__global__ void __launch_bounds__(kThreads)
+partials_scan64_kernel(int32_t nt, int64_t *__restrict__ partials,
+                       int64_t *__restrict__ total) {
+  __shared__ long long s_warp[kThreads / 32];
+  long long carry = 0;
+  for (int32_t b = 0; b < nt; b += kThreads) {
+    const int32_t i = b + threadIdx.x;
+    const long long v = i < nt ? partials[i] : 0;
+    long long chunk_total;
+    const long long ex = block_excl_scan64(v, s_warp, &chunk_total);
+    if (i < nt) partials[i] = carry + ex;
+    carry += chunk_total;
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) *total = carry;
+}
+
+// out[i] = partials[tile] + exclusive prefix of in within the tile (int64).
+__global__ void __launch_bounds__(kThreads)
+tile_apply64_kernel(int32_t n, const int32_t *__restrict__ in,
+                    const int64_t *__restrict__ partials, int64_t *__restrict__ out) {
+  __shared__ int32_t s_items[kTile + kTile / 32];
+  __shared__ long long s_warp[kThreads / 32];
+  const int64_t base = static_cast<int64_t>(blockIdx.x) * kTile;
+#pragma unroll 4
+  for (int r = 0; r < kItems; ++r) {
+    const int idx = r * kThreads + threadIdx.x;
+    s_items[skew(idx)] = base + idx < n ? in[base + idx] : 0;
+  }
+  __syncthreads();
+  long long mine = 0;
+#pragma unroll
+  for (int q = 0; q < kItems; ++q) mine += s_items[skew(threadIdx.x * kItems + q)];
+  long long tile_total;
+  long long run = partials[blockIdx.x] + block_excl_scan64(mine, s_warp, &tile_total);
+#pragma unroll
+  for (int q = 0; q < kItems; ++q) {
+    const int64_t i = base + threadIdx.x * kItems + q;
+    if (i < n) out[i] = run;
+    run += s_items[skew(threadIdx.x * kItems + q)];
+  }
+}
+
 }  // namespace
+
+void launch_scan_i64(int32_t n, const int32_t *in, int64_t *out, int64_t *partials,
+                     int64_t *total, cudaStream_t s) {
+  const int32_t nt = static_cast<int32_t>((static_cast<int64_t>(n) + kTile - 1) / kTile);
+  tile_sum_kernel<<<nt, kThreads, 0, s>>>(n, in, partials);
+  partials_scan64_kernel<<<1, kThreads, 0, s>>>(nt, partials, total);
+  tile_apply64_kernel<<<nt, kThreads, 0, s>>>(n, in, partials, out);
+}
 
 size_t scan_partials_bytes(int32_t n) {
   const size_t nt = (static_cast<size_t>(n) + kTile - 1) / kTile;
@@ -163,12 +215,12 @@ size_t scan_partials_bytes(int32_t n) {
 void launch_scan_and_class(int32_t n, const int32_t *counts, const int64_t *ops,
                            const int32_t *a_rp, int32_t *row_ptr,
                            int64_t *partials, int64_t *total, uint8_t *cls,
-                           int32_t *class_count, cudaStream_t s) {
+                           int32_t *class_count, bool merge_ok, cudaStream_t s) {
   const int32_t nt = static_cast<int32_t>((static_cast<int64_t>(n) + kTile - 1) / kTile);
   tile_sum_kernel<<<nt, kThreads, 0, s>>>(n, counts, partials);
   partials_scan_kernel<<<1, kThreads, 0, s>>>(n, nt, partials, total, row_ptr);
   tile_apply_kernel<<<nt, kThreads, 0, s>>>(n, counts, ops, a_rp, partials, row_ptr,
-                                            cls, class_count);
+                                            cls, class_count, merge_ok);
 }
 
 }  // namespace rvsp

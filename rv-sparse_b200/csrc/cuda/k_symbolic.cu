@@ -49,14 +49,14 @@ sym_warp_hash_kernel(Operands op, const int32_t *__restrict__ rows,
                      int32_t nrows, int32_t *__restrict__ counts,
                      int32_t *__restrict__ status) {
   constexpr int T = 1 << LOG2T;
-  extern __shared__ int32_t smem_i32[];
+  extern __shared__ __align__(16) int32_t smem_i32[];
   int32_t *keys = smem_i32 + (threadIdx.x >> 5) * T;
   const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   if (w >= nrows) return;
   const int lane = lane_id();
-  for (int s = lane; s < T; s += 32) keys[s] = kEmpty;
+  fill_words(keys, T, 0xffffffffu, lane, 32);
   __syncwarp();
-  const int32_t row = rows[w];
+  const int32_t row = row_of(rows, w);
   int cnt = 0;
   bool bad = false;
   for_each_product_col(op, op.a_rp[row], op.a_rp[row + 1], 0, 1,
@@ -75,17 +75,17 @@ sym_block_hash_kernel(Operands op, const int32_t *__restrict__ rows,
                       int32_t *__restrict__ counts,
                       int32_t *__restrict__ status) {
   constexpr int T = 1 << kBlockHashLog2;
-  extern __shared__ int32_t smem_i32[];
+  extern __shared__ __align__(16) int32_t smem_i32[];
   int32_t *keys = smem_i32;
   __shared__ int32_t s_cnt;
   __shared__ int32_t s_bad;
-  for (int s = threadIdx.x; s < T; s += blockDim.x) keys[s] = kEmpty;
+  fill_words(keys, T, 0xffffffffu, threadIdx.x, blockDim.x);
   if (threadIdx.x == 0) {
     s_cnt = 0;
     s_bad = 0;
   }
   __syncthreads();
-  const int32_t row = rows[blockIdx.x];
+  const int32_t row = row_of(rows, blockIdx.x);
   int cnt = 0;
   bool bad = false;
   for_each_product_col(op, op.a_rp[row], op.a_rp[row + 1], threadIdx.x >> 5,
@@ -127,7 +127,7 @@ sym_dense_kernel(Operands op, const int32_t *__restrict__ rows, int32_t nrows,
       s_hi = -1;
     }
     __syncthreads();
-    const int32_t row = rows[r];
+    const int32_t row = row_of(rows, r);
     int cnt = 0, lo = INT_MAX, hi = -1;
     for_each_product_col(op, op.a_rp[row], op.a_rp[row + 1], threadIdx.x >> 5,
                          blockDim.x >> 5, [&](int32_t col) {
@@ -175,8 +175,7 @@ void launch_symbolic_class(int cls, const Operands &op, const int32_t *rows,
   switch (cls) {
     case kM4:
     case kM8:
-    case kM16:
-    case kM32: launch_merge_symbolic(cls, op, rows, nrows, counts, s); break;
+    case kM16: launch_merge_symbolic(cls, op, rows, nrows, counts, s); break;
     case kW64: launch_warp_hash<6>(op, rows, nrows, counts, status, s); break;
     case kW128: launch_warp_hash<7>(op, rows, nrows, counts, status, s); break;
     case kW256: launch_warp_hash<8>(op, rows, nrows, counts, status, s); break;

@@ -5,17 +5,23 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 
+struct rvsp_mlp;
+
 namespace rvsp {
+
+// Device pointer of a model's parameters (model.cu).
+const float *mlp_device_params(const rvsp_mlp *m);
 
 // Row classes.  A row is classed twice: for the symbolic pass by the upper
 // bound ub = min(ops_i, b_cols) on its output nnz, and for the numeric pass
 // by its exact output nnz m_i.  The same table serves both.
 //
 //   EMPTY   no products
-//   M<K>    at most K (4, 8, 16, 32) A nonzeros and at most kMergeMaxOps
-//           products: one thread merges the row's K sorted B rows, taking
-//           the smallest head column each step; equal heads are added in
-//           A-nonzero order, and columns come out sorted with no scratch
+//   M<K>    at most K (4, 8, 16) A nonzeros and at most kMergeMaxOps
+//           products, in a matrix of at least kMergeMinRows rows: one thread
+//           merges the row's K sorted B rows, taking the smallest head
+//           column each step; equal heads are added in A-nonzero order, and
+//           columns come out sorted with no scratch
 //   W<T>    one warp, shared-memory hash table of T slots (bound <= T/2)
 //   B8192   one 256-thread block, hash table of 8192 slots (bound <= 4096)
 //   DENSE   one 512-thread block, dense accumulator over all of B's columns
@@ -24,7 +30,6 @@ enum RowClass : int {
   kM4,
   kM8,
   kM16,
-  kM32,
   kW64,
   kW128,
   kW256,
@@ -37,7 +42,11 @@ enum RowClass : int {
 };
 
 constexpr int kMergeMaxOps = 2048;
+constexpr int kMergeMaxNnz = 16;
 constexpr int kMergeThreads = 128;
+// The merge classes put one row on one thread; below this many rows the GPU
+// would sit mostly idle, so smaller matrices use the warp-per-row classes.
+constexpr int32_t kMergeMinRows = 32768;
 constexpr int kWarpHashMinLog2 = 6;    // W64
 constexpr int kWarpHashMaxLog2 = 11;   // W2048
 constexpr int kBlockHashLog2 = 13;     // B8192
@@ -50,11 +59,12 @@ constexpr int64_t kSmemBitmapMaxCols = 48 * 1024 * 32;
 // rowstats hands rows with more A nonzeros than this to a warp-per-row pass.
 constexpr int kLongRowNnz = 128;
 
+// merge_ok: the matrix has at least kMergeMinRows rows.
 __host__ __device__ inline int classify_row(int32_t nnz_a, int64_t ops,
-                                            int64_t bound) {
+                                            int64_t bound, bool merge_ok) {
   if (ops <= 0) return kEmpty_;
-  if (nnz_a <= 32 && ops <= kMergeMaxOps)
-    return nnz_a <= 4 ? kM4 : nnz_a <= 8 ? kM8 : nnz_a <= 16 ? kM16 : kM32;
+  if (merge_ok && nnz_a <= kMergeMaxNnz && ops <= kMergeMaxOps)
+    return nnz_a <= 4 ? kM4 : nnz_a <= 8 ? kM8 : kM16;
   const int64_t need = 2 * bound;
   for (int l = kWarpHashMinLog2; l <= kWarpHashMaxLog2; ++l)
     if (need <= (int64_t(1) << l)) return kW64 + (l - kWarpHashMinLog2);
@@ -74,6 +84,29 @@ struct Operands {
   const int32_t *b_rp;
   const int32_t *b_col;
   const float *b_val;
+  // Rows may take the merge classes (set by the plan from its merge policy
+  // and the row count; see classify_row).
+  bool merge_ok;
+};
+
+// Merge policies of a plan: automatic (merge classes when the matrix has at
+// least kMergeMinRows rows), never, or whenever a row is eligible.
+enum MergePolicy : int { kMergeAuto = 0, kMergeNever = 1, kMergeAlways = 2 };
+
+inline bool merge_allowed(int policy, int32_t a_rows) {
+  return policy == kMergeAlways || (policy == kMergeAuto && a_rows >= kMergeMinRows);
+}
+
+// Where the fused (learned) pass writes each row: a slot of fo.cap[row]
+// entries at fo.off[row] in the slab (the c_col / c_val pointers of the fill
+// kernels).  The kernel writes the row's nnz to fo.counts[row], or -1 and
+// appends the row to ovf_rows when it needs more than its capacity.
+struct FusedOut {
+  const int64_t *off;
+  const int32_t *cap;
+  int32_t *counts;
+  int32_t *ovf_rows;
+  int32_t *ovf_count;
 };
 
 // ---- k_rowstats.cu ---------------------------------------------------------
@@ -100,7 +133,32 @@ size_t scan_partials_bytes(int32_t n);
 void launch_scan_and_class(int32_t n, const int32_t *counts, const int64_t *ops,
                            const int32_t *a_rp, int32_t *row_ptr,
                            int64_t *partials, int64_t *total, uint8_t *cls,
-                           int32_t *class_count, cudaStream_t s);
+                           int32_t *class_count, bool merge_ok, cudaStream_t s);
+
+// out[i] = sum of in[0..i) as int64 (n entries), *total = sum of all.
+void launch_scan_i64(int32_t n, const int32_t *in, int64_t *out, int64_t *partials,
+                     int64_t *total, cudaStream_t s);
+
+// ---- k_fused.cu ------------------------------------------------------------
+// Copies every non-overflowed row (counts[row] >= 0) from its slab slot to C
+// at row_ptr[row]; values too when with_values.
+void launch_compact(int32_t a_rows, const int32_t *counts, const int64_t *off,
+                    const int32_t *row_ptr, const int32_t *slab_col,
+                    const float *slab_val, int32_t *c_col, float *c_val,
+                    bool with_values, int num_sms, cudaStream_t s);
+// Classes the rows of a list (symbolic: by ub = min(ops, b_cols); numeric: by
+// exact nnz counts[row]); cls_out[j] for list entry j; class_count += rows.
+void launch_list_classify(const int32_t *list, int32_t n, const int64_t *ops,
+                          const int32_t *a_rp, const int32_t *counts, int32_t b_cols,
+                          bool numeric, uint8_t *cls_out, int32_t *class_count,
+                          cudaStream_t s);
+// out[off[c] + r] = list[j] for the entries j of class c (any order).
+void launch_scatter_list(const int32_t *list, int32_t n, const uint8_t *cls,
+                         const int32_t *class_off, int32_t *class_fill, int32_t *out,
+                         cudaStream_t s);
+// Order-independent 64-bit fingerprint of n floats added into *h.
+void launch_values_hash(const float *v, int64_t n, unsigned long long salt,
+                        unsigned long long *h, cudaStream_t s);
 
 // ---- k_merge.cu ------------------------------------------------------------
 // Thread-per-row K-way merge for the M<K> classes: counts (symbolic) or
@@ -110,7 +168,7 @@ void launch_merge_symbolic(int cls, const Operands &op, const int32_t *rows,
 void launch_merge_numeric(int cls, const Operands &op, const int32_t *rows,
                           int32_t nrows, const int32_t *c_rp, int32_t *c_col,
                           float *c_val, bool fill, int32_t *status,
-                          cudaStream_t s);
+                          const FusedOut *fo, cudaStream_t s);
 
 // ---- k_symbolic.cu ---------------------------------------------------------
 // counts[row] = nnz of output row, for the rows of one class.
@@ -127,16 +185,54 @@ void launch_csr_check(int32_t rows, int32_t cols, const int32_t *row_ptr,
                       unsigned long long *result, cudaStream_t s);
 
 // ---- k_numeric.cu ----------------------------------------------------------
-// Values (and, when fill, sorted columns) of the rows of one class.
+// Values (and, when fill, sorted columns) of the rows of one class.  With
+// fo, the fused pass: rows go to their slab slots (c_col / c_val = slab),
+// c_rp is unused and fill is implied.
 void launch_numeric_class(int cls, const Operands &op, const int64_t *ops,
                           const int32_t *rows, int32_t nrows,
                           const int32_t *c_rp, int32_t *c_col, float *c_val,
                           bool fill, float *dense_acc, uint32_t *dense_bits,
                           int32_t dense_slots, int32_t *status, int num_sms,
-                          cudaStream_t s);
+                          cudaStream_t s, const FusedOut *fo = nullptr);
 // Global scratch one dense numeric slot needs (accumulator + bitmap if the
 // bitmap does not fit shared memory), 256-byte aligned.
 size_t dense_slot_acc_bytes(int32_t b_cols);
 size_t dense_slot_bits_bytes(int32_t b_cols);
+
+// ---- k_mlp.cu ----------------------------------------------------------------
+// Parameter layout of the 8 -> 32 -> 32 -> 2 row-binning MLP (floats):
+// W1[32][8] b1[32] W2[32][32] b2[32] W3[2][32] b3[2] (trained), then the
+// per-feature standardisation mean[8] and 1/sd[8] (set, not trained).
+constexpr int kMlpIn = 8, kMlpHidden = 32, kMlpOut = 2;
+constexpr int kW1 = 0;
+constexpr int kB1 = kW1 + kMlpHidden * kMlpIn;
+constexpr int kW2 = kB1 + kMlpHidden;
+constexpr int kB2 = kW2 + kMlpHidden * kMlpHidden;
+constexpr int kW3 = kB2 + kMlpHidden;
+constexpr int kB3 = kW3 + kMlpOut * kMlpHidden;
+constexpr int kMlpTrained = kB3 + kMlpOut;  // 1410
+constexpr int kMu = kMlpTrained;
+constexpr int kInvSd = kMu + kMlpIn;
+constexpr int kMlpParams = kInvSd + kMlpIn;  // 1426
+constexpr int kMlpParamsPad = (kMlpParams + 3) & ~3;
+
+void launch_features(const Operands &op, float b_mean_len, float *feat,
+                     int64_t *ops, int num_sms, cudaStream_t s);
+// pred[row] = (y0, y1); ops (optional) = per-row op counts.
+void launch_predict(const Operands &op, float b_mean_len, const float *params,
+                    float2 *pred, int64_t *ops, int num_sms, cudaStream_t s);
+// Learned binning for the fused pass: ops, class and slab capacity per row
+// (counts[row] = 0 for empty rows) and rows per class.
+void launch_learned_plan(const Operands &op, float b_mean_len, const float *params,
+                         float scale, bool merge_ok, int64_t *ops, uint8_t *cls,
+                         int32_t *cap, int32_t *counts, int32_t *class_count,
+                         int num_sms, cudaStream_t s);
+// grad (kMlpTrained floats, accumulated) and *loss_sum (accumulated) of the
+// mean loss over n_total samples, for samples [0, n).
+void launch_mlp_grad(const float *params, const float *feat, const float *target,
+                     int32_t n, int32_t n_total, float *grad, float *loss_sum,
+                     cudaStream_t s);
+void launch_mlp_adam(float *params, const float *grad, float *m, float *v, float lr,
+                     float b1, float b2, float eps, int step, cudaStream_t s);
 
 }  // namespace rvsp

@@ -77,6 +77,7 @@ struct rvsp_cuda_plan {
   int num_sms = 148;
 
   int analysed = 0;
+  int merge_policy = kMergeAuto;
   int32_t a_rows = 0, b_rows = 0, b_cols = 0;
   int64_t c_nnz = 0;
 
@@ -99,6 +100,27 @@ struct rvsp_cuda_plan {
   int32_t num_off[kNumClasses] = {};
   int32_t dense_slots = 0;
   size_t numeric_ws = 0;
+  int num_whole = -1;  // numeric class holding every row (no row list), or -1
+
+  // Learned (fused) analysis: per-row capacity and slab slot, the slab with
+  // every non-overflowed row's sorted columns and values, the overflow rows
+  // grouped by numeric class, and the fingerprint of the values used.
+  int learned = 0;
+  DevArray<int32_t> cap;
+  DevArray<int64_t> slab_off;
+  DevArray<int32_t> slab_col;
+  DevArray<float> slab_val;
+  DevArray<int32_t> ovf_rows, ovf_sorted;
+  DevArray<uint8_t> ovf_cls;
+  DevArray<char> fused_ws;
+  DevArray<unsigned long long> vhash;
+  unsigned long long *h_vhash = nullptr;  // pinned, 2 words
+  unsigned long long est_hash = 0;
+  int32_t n_ovf = 0;
+  int32_t a_nnz = 0, b_nnz = 0;
+  int32_t ovf_num_count[kNumClasses] = {};
+  int32_t ovf_num_off[kNumClasses] = {};
+  int64_t slab_total = 0;
 
   bool profiling = false;
   struct Pending {
@@ -164,6 +186,81 @@ rvsp_status_t device_status_to_rvsp(int32_t st) {
   return st == kDevOk ? RVSP_SUCCESS : RVSP_ERROR_DEVICE;
 }
 
+// The class that holds every non-empty row, when there is exactly one and
+// its kernel may also see the empty rows (merge kernels handle them; the
+// others are used only when there are none).  Its rows then need no list.
+int whole_matrix_class(const int32_t *count, int32_t a_rows) {
+  int found = -1;
+  for (int c = kEmpty_ + 1; c < kNumClasses; ++c) {
+    if (count[c] <= 0) continue;
+    if (found >= 0) return -1;
+    found = c;
+  }
+  if (found < 0 || count[found] + count[kEmpty_] != a_rows) return -1;
+  const bool merge = found == kM4 || found == kM8 || found == kM16;
+  return (count[kEmpty_] == 0 || merge) ? found : -1;
+}
+
+// After the final scan (class counts of the numeric pass in h_misc): host
+// offsets, the row lists (unless one class holds every row) and the dense
+// workspace the numeric pass will need.
+void finish_numeric_bins(rvsp_cuda_plan *p, int32_t a_rows, int32_t b_cols,
+                         cudaStream_t s) {
+  int32_t *misc = p->misc.p;
+  int32_t off = 0;
+  for (int c = 0; c < kNumClasses; ++c) {
+    p->num_count[c] = p->h_misc[kNumCount + c];
+    p->num_off[c] = off;
+    if (c != kEmpty_) off += p->num_count[c];
+  }
+  p->num_whole = whole_matrix_class(p->num_count, a_rows);
+  if (p->num_whole < 0) {
+    PhaseScope ph(p, s, RVSP_PHASE_SCAN);
+    launch_class_offsets(misc + kNumCount, misc + kNumOff, s);
+    launch_scatter_rows(a_rows, p->cls.p, misc + kNumOff, misc + kNumFill,
+                        p->rows_num.p, s);
+    ph.launches = 2;
+  }
+  if (p->num_count[kDense] > 0) {
+    p->dense_slots = p->num_count[kDense] < p->num_sms ? p->num_count[kDense] : p->num_sms;
+    p->numeric_ws = size_t(p->dense_slots) *
+                    (dense_slot_acc_bytes(b_cols) + dense_slot_bits_bytes(b_cols));
+  } else {
+    p->dense_slots = 0;
+    p->numeric_ws = 0;
+  }
+}
+
+// Reserves (and zeroes when grown) the global bitmaps dense symbolic rows use
+// when B is too wide for a shared-memory bitmap; returns the slot count.
+cudaError_t ensure_sym_bits(rvsp_cuda_plan *p, int32_t dense_rows, int32_t b_cols,
+                            cudaStream_t s, int32_t *slots_out) {
+  *slots_out = 0;
+  const size_t bits_bytes = dense_slot_bits_bytes(b_cols);
+  if (dense_rows <= 0 || bits_bytes == 0) return cudaSuccess;
+  const int32_t slots = dense_rows < p->num_sms ? dense_rows : p->num_sms;
+  const size_t words = bits_bytes / sizeof(uint32_t) * size_t(slots);
+  if (words > p->sym_bits.cap) {
+    cudaError_t e = p->sym_bits.reserve(words);
+    if (e != cudaSuccess) return e;
+    cudaMemsetAsync(p->sym_bits.p, 0, words * sizeof(uint32_t), s);
+  }
+  p->sym_bits_slots = slots;
+  *slots_out = slots;
+  return cudaSuccess;
+}
+
+unsigned long long values_fingerprint_launch(rvsp_cuda_plan *p, const float *a_val,
+                                             int64_t a_n, const float *b_val, int64_t b_n,
+                                             cudaStream_t s) {
+  cudaMemsetAsync(p->vhash.p, 0, sizeof(unsigned long long), s);
+  launch_values_hash(a_val, a_n, 0x41ull, p->vhash.p, s);
+  launch_values_hash(b_val, b_n, 0x42ull << 40, p->vhash.p, s);
+  cudaMemcpyAsync(p->h_vhash, p->vhash.p, sizeof(unsigned long long),
+                  cudaMemcpyDeviceToHost, s);
+  return 0;
+}
+
 }  // namespace
 
 extern "C" {
@@ -192,6 +289,8 @@ rvsp_status_t rvsp_cuda_plan_create(rvsp_cuda_plan_t *plan) {
   if (e == cudaSuccess) e = cudaMallocHost(reinterpret_cast<void **>(&p->h_misc), kMiscWords * sizeof(int32_t));
   if (e == cudaSuccess) e = cudaMallocHost(reinterpret_cast<void **>(&p->h_total), sizeof(int64_t));
   if (e == cudaSuccess) e = cudaMallocHost(reinterpret_cast<void **>(&p->h_check), sizeof(unsigned long long));
+  if (e == cudaSuccess) e = cudaMallocHost(reinterpret_cast<void **>(&p->h_vhash), 2 * sizeof(unsigned long long));
+  if (e == cudaSuccess) e = p->vhash.reserve(2);
   if (e == cudaSuccess) e = cudaMemset(p->misc.p, 0, kMiscWords * sizeof(int32_t));
   if (e != cudaSuccess) {
     rvsp_cuda_plan_destroy(p);
@@ -216,9 +315,19 @@ void rvsp_cuda_plan_destroy(rvsp_cuda_plan_t p) {
   p->total.release();
   p->sym_bits.release();
   p->check.release();
+  p->cap.release();
+  p->slab_off.release();
+  p->slab_col.release();
+  p->slab_val.release();
+  p->ovf_rows.release();
+  p->ovf_sorted.release();
+  p->ovf_cls.release();
+  p->fused_ws.release();
+  p->vhash.release();
   if (p->h_misc) cudaFreeHost(p->h_misc);
   if (p->h_total) cudaFreeHost(p->h_total);
   if (p->h_check) cudaFreeHost(p->h_check);
+  if (p->h_vhash) cudaFreeHost(p->h_vhash);
   delete p;
 }
 
@@ -247,7 +356,8 @@ rvsp_status_t rvsp_cuda_symbolic(rvsp_cuda_plan_t p, void *stream, int32_t a_row
   if (e != cudaSuccess) return map_cuda(e);
 
   const Operands op{a_rows, b_cols, a_row_ptr, a_col_idx, nullptr,
-                    b_row_ptr, b_col_idx, nullptr};
+                    b_row_ptr, b_col_idx, nullptr,
+                    merge_allowed(p->merge_policy, a_rows)};
   int32_t *misc = p->misc.p;
   cudaMemsetAsync(misc, 0, kMiscWords * sizeof(int32_t), s);
   {
@@ -285,23 +395,30 @@ rvsp_status_t rvsp_cuda_symbolic(rvsp_cuda_plan_t p, void *stream, int32_t a_row
   }
   {
     PhaseScope ph(p, s, RVSP_PHASE_SYMBOLIC);
-    launch_class_offsets(misc + kSymCount, misc + kSymOff, s);
-    launch_scatter_rows(a_rows, p->cls.p, misc + kSymOff, misc + kSymFill,
-                        p->rows_sym.p, s);
-    ph.launches = 2;
-    for (int c = kEmpty_ + 1; c < kNumClasses; ++c) {
-      if (p->sym_count[c] <= 0) continue;
-      launch_symbolic_class(c, op, p->rows_sym.p + sym_off[c],
-                            p->sym_count[c], p->counts.p, p->sym_bits.p, slots,
-                            misc + kStatus, p->num_sms, s);
-      ph.launches += 1;
+    const int whole = whole_matrix_class(p->sym_count, a_rows);
+    if (whole >= 0) {
+      launch_symbolic_class(whole, op, nullptr, a_rows, p->counts.p, p->sym_bits.p,
+                            slots, misc + kStatus, p->num_sms, s);
+      ph.launches = 1;
+    } else {
+      launch_class_offsets(misc + kSymCount, misc + kSymOff, s);
+      launch_scatter_rows(a_rows, p->cls.p, misc + kSymOff, misc + kSymFill,
+                          p->rows_sym.p, s);
+      ph.launches = 2;
+      for (int c = kEmpty_ + 1; c < kNumClasses; ++c) {
+        if (p->sym_count[c] <= 0) continue;
+        launch_symbolic_class(c, op, p->rows_sym.p + sym_off[c],
+                              p->sym_count[c], p->counts.p, p->sym_bits.p, slots,
+                              misc + kStatus, p->num_sms, s);
+        ph.launches += 1;
+      }
     }
   }
   {
     PhaseScope ph(p, s, RVSP_PHASE_SCAN);
     launch_scan_and_class(a_rows, p->counts.p, p->ops.p, a_row_ptr, c_row_ptr,
                           p->partials.p,
-                          p->total.p, p->cls.p, misc + kNumCount, s);
+                          p->total.p, p->cls.p, misc + kNumCount, op.merge_ok, s);
     ph.launches = 3;
   }
   cudaMemcpyAsync(p->h_misc + kNumCount, misc + kNumCount,
@@ -316,31 +433,11 @@ rvsp_status_t rvsp_cuda_symbolic(rvsp_cuda_plan_t p, void *stream, int32_t a_row
   const int64_t total = *p->h_total;
   if (total > INT32_MAX) return RVSP_ERROR_ALLOCATION_FAILED;
 
-  off = 0;
-  for (int c = 0; c < kNumClasses; ++c) {
-    p->num_count[c] = p->h_misc[kNumCount + c];
-    p->num_off[c] = off;
-    if (c != kEmpty_) off += p->num_count[c];
-  }
-  {
-    PhaseScope ph(p, s, RVSP_PHASE_SCAN);
-    launch_class_offsets(misc + kNumCount, misc + kNumOff, s);
-    launch_scatter_rows(a_rows, p->cls.p, misc + kNumOff, misc + kNumFill,
-                        p->rows_num.p, s);
-    ph.launches = 2;
-  }
-
-  if (p->num_count[kDense] > 0) {
-    p->dense_slots = p->num_count[kDense] < p->num_sms ? p->num_count[kDense] : p->num_sms;
-    p->numeric_ws = size_t(p->dense_slots) *
-                    (dense_slot_acc_bytes(b_cols) + dense_slot_bits_bytes(b_cols));
-  } else {
-    p->dense_slots = 0;
-    p->numeric_ws = 0;
-  }
+  finish_numeric_bins(p, a_rows, b_cols, s);
   e = cudaGetLastError();
   if (e != cudaSuccess) return map_cuda(e);
 
+  p->learned = 0;
   p->a_rows = a_rows;
   p->b_rows = b_rows;
   p->b_cols = b_cols;
@@ -348,6 +445,214 @@ rvsp_status_t rvsp_cuda_symbolic(rvsp_cuda_plan_t p, void *stream, int32_t a_row
   p->analysed = 1;
   *c_nnz_out = total;
   return RVSP_SUCCESS;
+}
+
+rvsp_status_t rvsp_cuda_learned_symbolic(
+    rvsp_cuda_plan_t p, rvsp_mlp_t model, void *stream, int32_t a_rows, int32_t b_rows,
+    int32_t b_cols, const int32_t *a_row_ptr, const int32_t *a_col_idx,
+    const float *a_values, int32_t a_nnz, const int32_t *b_row_ptr,
+    const int32_t *b_col_idx, const float *b_values, int32_t b_nnz,
+    float capacity_scale, int32_t *c_row_ptr, int64_t *c_nnz_out) {
+  if (!p || !model || !a_row_ptr || !a_col_idx || !a_values || !b_row_ptr ||
+      !b_col_idx || !b_values || !c_row_ptr || !c_nnz_out)
+    return RVSP_ERROR_NULL_POINTER;
+  if (a_rows <= 0 || b_rows <= 0 || b_cols <= 0 || a_nnz < 0 || b_nnz < 0 ||
+      !(capacity_scale > 0.0f))
+    return RVSP_ERROR_INVALID_ARGUMENT;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  p->analysed = 0;
+  p->learned = 0;
+  const size_t n = static_cast<size_t>(a_rows);
+  cudaError_t e = p->ops.reserve(n);
+  if (e == cudaSuccess) e = p->cls.reserve(n);
+  if (e == cudaSuccess) e = p->counts.reserve(n);
+  if (e == cudaSuccess) e = p->rows_sym.reserve(n);
+  if (e == cudaSuccess) e = p->rows_num.reserve(n);
+  if (e == cudaSuccess) e = p->cap.reserve(n);
+  if (e == cudaSuccess) e = p->slab_off.reserve(n);
+  if (e == cudaSuccess) e = p->ovf_rows.reserve(n);
+  if (e == cudaSuccess) e = p->partials.reserve(scan_partials_bytes(a_rows) / sizeof(int64_t));
+  if (e != cudaSuccess) return map_cuda(e);
+
+  const Operands op{a_rows, b_cols, a_row_ptr, a_col_idx, a_values,
+                    b_row_ptr, b_col_idx, b_values,
+                    merge_allowed(p->merge_policy, a_rows)};
+  int32_t *misc = p->misc.p;
+  cudaMemsetAsync(misc, 0, kMiscWords * sizeof(int32_t), s);
+  // 1. Predict every row's class and capacity; slab offsets = scan of capacities.
+  {
+    PhaseScope ph(p, s, RVSP_PHASE_PREDICT);
+    const float b_mean = static_cast<float>(b_nnz) / static_cast<float>(b_rows);
+    launch_learned_plan(op, b_mean, mlp_device_params(model), capacity_scale,
+                        op.merge_ok, p->ops.p, p->cls.p, p->cap.p,
+                        p->counts.p, misc + kSymCount, p->num_sms, s);
+    launch_scan_i64(a_rows, p->cap.p, p->slab_off.p, p->partials.p, p->total.p, s);
+    ph.launches = 4;
+  }
+  cudaMemcpyAsync(p->h_misc, misc, kNumClasses * sizeof(int32_t), cudaMemcpyDeviceToHost, s);
+  cudaMemcpyAsync(p->h_total, p->total.p, sizeof(int64_t), cudaMemcpyDeviceToHost, s);
+  e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) return map_cuda(e);
+  int32_t pred_off[kNumClasses];
+  int32_t off = 0;
+  for (int c = 0; c < kNumClasses; ++c) {
+    p->sym_count[c] = p->h_misc[kSymCount + c];
+    pred_off[c] = off;
+    if (c != kEmpty_) off += p->sym_count[c];
+  }
+  p->slab_total = *p->h_total;
+  e = p->slab_col.reserve(size_t(p->slab_total));
+  if (e == cudaSuccess) e = p->slab_val.reserve(size_t(p->slab_total));
+  if (e != cudaSuccess) return map_cuda(e);
+  // Dense rows of the fused pass use a plan-owned dense workspace.
+  int32_t fslots = 0;
+  float *facc = nullptr;
+  uint32_t *fbits = nullptr;
+  if (p->sym_count[kDense] > 0) {
+    fslots = p->sym_count[kDense] < p->num_sms ? p->sym_count[kDense] : p->num_sms;
+    const size_t acc_b = dense_slot_acc_bytes(b_cols), bits_b = dense_slot_bits_bytes(b_cols);
+    const size_t need = size_t(fslots) * (acc_b + bits_b);
+    e = p->fused_ws.reserve(need);
+    if (e != cudaSuccess) return map_cuda(e);
+    cudaMemsetAsync(p->fused_ws.p, 0, need, s);
+    facc = reinterpret_cast<float *>(p->fused_ws.p);
+    fbits = reinterpret_cast<uint32_t *>(p->fused_ws.p + size_t(fslots) * acc_b);
+  }
+
+  // 2. The fused pass: every row into its slab slot, or onto the overflow list.
+  const FusedOut fo{p->slab_off.p, p->cap.p, p->counts.p, p->ovf_rows.p,
+                    misc + kLongCount};
+  {
+    PhaseScope ph(p, s, RVSP_PHASE_FUSED);
+    const int whole = whole_matrix_class(p->sym_count, a_rows);
+    if (whole < 0) {
+      launch_class_offsets(misc + kSymCount, misc + kSymOff, s);
+      launch_scatter_rows(a_rows, p->cls.p, misc + kSymOff, misc + kSymFill,
+                          p->rows_sym.p, s);
+      ph.launches = 2;
+    }
+    for (int c = kEmpty_ + 1; c < kNumClasses; ++c) {
+      if (p->sym_count[c] <= 0) continue;
+      const bool all = c == whole;
+      launch_numeric_class(c, op, p->ops.p, all ? nullptr : p->rows_sym.p + pred_off[c],
+                           all ? a_rows : p->sym_count[c], nullptr, p->slab_col.p,
+                           p->slab_val.p, true, facc, fbits, fslots, misc + kStatus,
+                           p->num_sms, s, &fo);
+      ph.launches += 1;
+    }
+  }
+  // 3. Optimistic scan (valid when nothing overflowed) and the fingerprint of
+  //    the values the fused pass used.
+  {
+    PhaseScope ph(p, s, RVSP_PHASE_SCAN);
+    launch_scan_and_class(a_rows, p->counts.p, p->ops.p, a_row_ptr, c_row_ptr,
+                          p->partials.p, p->total.p, p->cls.p, misc + kNumCount,
+                            op.merge_ok, s);
+    ph.launches = 3;
+  }
+  values_fingerprint_launch(p, a_values, a_nnz, b_values, b_nnz, s);
+  cudaMemcpyAsync(p->h_misc + kNumCount, misc + kNumCount,
+                  (kMiscWords - kNumCount) * sizeof(int32_t), cudaMemcpyDeviceToHost, s);
+  cudaMemcpyAsync(p->h_total, p->total.p, sizeof(int64_t), cudaMemcpyDeviceToHost, s);
+  e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) return map_cuda(e);
+  if (p->h_misc[kStatus] != kDevOk) {
+    cudaMemsetAsync(misc + kStatus, 0, sizeof(int32_t), s);
+    return RVSP_ERROR_DEVICE;
+  }
+  p->est_hash = p->h_vhash[0];
+  p->n_ovf = p->h_misc[kLongCount];
+
+  // 4. Overflowed rows: the plain symbolic pass, then the scan again.
+  if (p->n_ovf > 0) {
+    e = p->ovf_cls.reserve(size_t(p->n_ovf));
+    if (e == cudaSuccess) e = p->ovf_sorted.reserve(size_t(p->n_ovf));
+    if (e != cudaSuccess) return map_cuda(e);
+    cudaMemsetAsync(misc + kSymCount, 0, 3 * kNumClasses * sizeof(int32_t), s);
+    launch_list_classify(p->ovf_rows.p, p->n_ovf, p->ops.p, a_row_ptr, p->counts.p, b_cols,
+                         false, p->ovf_cls.p, misc + kSymCount, s);
+    cudaMemcpyAsync(p->h_misc, misc, kNumClasses * sizeof(int32_t), cudaMemcpyDeviceToHost, s);
+    e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return map_cuda(e);
+    int32_t ocount[kNumClasses], ooff[kNumClasses];
+    off = 0;
+    for (int c = 0; c < kNumClasses; ++c) {
+      ocount[c] = p->h_misc[kSymCount + c];
+      ooff[c] = off;
+      if (c != kEmpty_) off += ocount[c];
+    }
+    int32_t slots = 0;
+    e = ensure_sym_bits(p, ocount[kDense], b_cols, s, &slots);
+    if (e != cudaSuccess) return map_cuda(e);
+    {
+      PhaseScope ph(p, s, RVSP_PHASE_SYMBOLIC);
+      launch_class_offsets(misc + kSymCount, misc + kSymOff, s);
+      launch_scatter_list(p->ovf_rows.p, p->n_ovf, p->ovf_cls.p, misc + kSymOff,
+                          misc + kSymFill, p->rows_sym.p, s);
+      ph.launches = 3;
+      for (int c = kEmpty_ + 1; c < kNumClasses; ++c) {
+        if (ocount[c] <= 0) continue;
+        launch_symbolic_class(c, op, p->rows_sym.p + ooff[c], ocount[c], p->counts.p,
+                              p->sym_bits.p, slots, misc + kStatus, p->num_sms, s);
+        ph.launches += 1;
+      }
+    }
+    {
+      PhaseScope ph(p, s, RVSP_PHASE_SCAN);
+      cudaMemsetAsync(misc + kNumCount, 0, kNumClasses * sizeof(int32_t), s);
+      launch_scan_and_class(a_rows, p->counts.p, p->ops.p, a_row_ptr, c_row_ptr,
+                            p->partials.p, p->total.p, p->cls.p, misc + kNumCount,
+                            op.merge_ok, s);
+      // The overflow rows by numeric class, for the first compute.
+      cudaMemsetAsync(misc + kSymCount, 0, 3 * kNumClasses * sizeof(int32_t), s);
+      launch_list_classify(p->ovf_rows.p, p->n_ovf, p->ops.p, a_row_ptr, p->counts.p,
+                           b_cols, true, p->ovf_cls.p, misc + kSymCount, s);
+      launch_class_offsets(misc + kSymCount, misc + kSymOff, s);
+      launch_scatter_list(p->ovf_rows.p, p->n_ovf, p->ovf_cls.p, misc + kSymOff,
+                          misc + kSymFill, p->ovf_sorted.p, s);
+      ph.launches = 6;
+    }
+    cudaMemcpyAsync(p->h_misc, misc, kMiscWords * sizeof(int32_t), cudaMemcpyDeviceToHost, s);
+    cudaMemcpyAsync(p->h_total, p->total.p, sizeof(int64_t), cudaMemcpyDeviceToHost, s);
+    e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return map_cuda(e);
+    if (p->h_misc[kStatus] != kDevOk) {
+      cudaMemsetAsync(misc + kStatus, 0, sizeof(int32_t), s);
+      return RVSP_ERROR_DEVICE;
+    }
+    off = 0;
+    for (int c = 0; c < kNumClasses; ++c) {
+      p->ovf_num_count[c] = p->h_misc[kSymCount + c];
+      p->ovf_num_off[c] = off;
+      if (c != kEmpty_) off += p->ovf_num_count[c];
+    }
+  }
+  const int64_t total = *p->h_total;
+  if (total > INT32_MAX) return RVSP_ERROR_ALLOCATION_FAILED;
+  finish_numeric_bins(p, a_rows, b_cols, s);
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return map_cuda(e);
+  p->learned = 1;
+  p->a_nnz = a_nnz;
+  p->b_nnz = b_nnz;
+  p->a_rows = a_rows;
+  p->b_rows = b_rows;
+  p->b_cols = b_cols;
+  p->c_nnz = total;
+  p->analysed = 1;
+  *c_nnz_out = total;
+  return RVSP_SUCCESS;
+}
+
+rvsp_status_t rvsp_cuda_plan_set_merge_policy(rvsp_cuda_plan_t p, int32_t policy) {
+  if (!p) return RVSP_ERROR_NULL_POINTER;
+  if (policy < kMergeAuto || policy > kMergeAlways) return RVSP_ERROR_INVALID_ARGUMENT;
+  p->merge_policy = policy;
+  return RVSP_SUCCESS;
+}
+
+int32_t rvsp_cuda_plan_overflow_rows(rvsp_cuda_plan_t p) {
+  return (p && p->analysed && p->learned) ? p->n_ovf : 0;
 }
 
 size_t rvsp_cuda_numeric_workspace_bytes(rvsp_cuda_plan_t p) {
@@ -369,7 +674,8 @@ rvsp_status_t rvsp_cuda_numeric(rvsp_cuda_plan_t p, void *stream,
     return workspace ? RVSP_ERROR_INVALID_ARGUMENT : RVSP_ERROR_NULL_POINTER;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   const Operands op{p->a_rows, p->b_cols, a_row_ptr, a_col_idx, a_values,
-                    b_row_ptr, b_col_idx, b_values};
+                    b_row_ptr, b_col_idx, b_values,
+                    merge_allowed(p->merge_policy, p->a_rows)};
   float *dense_acc = static_cast<float *>(workspace);
   uint32_t *dense_bits = nullptr;
   if (p->numeric_ws > 0) {
@@ -381,14 +687,41 @@ rvsp_status_t rvsp_cuda_numeric(rvsp_cuda_plan_t p, void *stream,
         static_cast<char *>(workspace) +
         size_t(p->dense_slots) * dense_slot_acc_bytes(p->b_cols));
   }
+  if (p->learned && fill) {
+    // The fused pass already holds every non-overflowed row, sorted, with
+    // its values: copy them; the overflowed rows take the plain fill.
+    {
+      PhaseScope ph(p, s, RVSP_PHASE_COMPACT);
+      launch_compact(p->a_rows, p->counts.p, p->slab_off.p, c_row_ptr, p->slab_col.p,
+                     p->slab_val.p, c_col_idx, c_values, true, p->num_sms, s);
+      ph.launches = 1;
+      for (int c = kEmpty_ + 1; c < kNumClasses && p->n_ovf > 0; ++c) {
+        if (p->ovf_num_count[c] <= 0) continue;
+        launch_numeric_class(c, op, p->ops.p, p->ovf_sorted.p + p->ovf_num_off[c],
+                             p->ovf_num_count[c], c_row_ptr, c_col_idx, c_values, true,
+                             dense_acc, dense_bits, p->dense_slots, p->misc.p + kStatus,
+                             p->num_sms, s);
+        ph.launches += 1;
+      }
+    }
+    // Those values are the ones A and B held at estimation; if they changed
+    // since, recompute every value with the structure now in C.
+    values_fingerprint_launch(p, a_values, p->a_nnz, b_values, p->b_nnz, s);
+    cudaError_t e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return map_cuda(e);
+    if (p->h_vhash[0] == p->est_hash) return map_cuda(cudaGetLastError());
+    fill = 0;
+  }
   {
     PhaseScope ph(p, s, RVSP_PHASE_NUMERIC);
     for (int c = kEmpty_ + 1; c < kNumClasses; ++c) {
       if (p->num_count[c] <= 0) continue;
-      launch_numeric_class(c, op, p->ops.p, p->rows_num.p + p->num_off[c],
-                           p->num_count[c], c_row_ptr, c_col_idx, c_values,
-                           fill != 0, dense_acc, dense_bits, p->dense_slots,
-                           p->misc.p + kStatus, p->num_sms, s);
+      const bool whole = c == p->num_whole;
+      launch_numeric_class(c, op, p->ops.p,
+                           whole ? nullptr : p->rows_num.p + p->num_off[c],
+                           whole ? p->a_rows : p->num_count[c], c_row_ptr,
+                           c_col_idx, c_values, fill != 0, dense_acc, dense_bits,
+                           p->dense_slots, p->misc.p + kStatus, p->num_sms, s);
       ph.launches += 1;
     }
   }

@@ -33,6 +33,9 @@ struct rvsp_spgemm_descr {
     int profiling;
 
     rvsp_cuda_plan_t plan;
+    rvsp_mlp_t model;      /* learned algorithm only; not owned */
+    float capacity_scale;  /* learned algorithm only */
+    int32_t merge_policy;
 
     int32_t c_nnz;
     rvsp_dbuf_t c_row_ptr; /* analysed row pointers, device, a_rows + 1 */
@@ -50,7 +53,8 @@ struct rvsp_spgemm_descr {
 
 static int algo_supported(rvsp_spgemm_algo_t algo)
 {
-    return algo == RVSP_SPGEMM_ALGO_DEFAULT || algo == RVSP_SPGEMM_ALGO_CUDA_PLAIN;
+    return algo == RVSP_SPGEMM_ALGO_DEFAULT || algo == RVSP_SPGEMM_ALGO_CUDA_PLAIN ||
+           algo == RVSP_SPGEMM_ALGO_CUDA_LEARNED;
 }
 
 rvsp_status_t rvsp_spgemm_descr_create(rvsp_spgemm_descr_t *descr)
@@ -64,7 +68,48 @@ rvsp_status_t rvsp_spgemm_descr_create(rvsp_spgemm_descr_t *descr)
         return RVSP_ERROR_ALLOCATION_FAILED;
     d->algo = RVSP_SPGEMM_ALGO_DEFAULT;
     d->mem = RVSP_MEM_HOST;
+    d->capacity_scale = 1.15f;
     *descr = d;
+    return RVSP_SUCCESS;
+}
+
+rvsp_status_t rvsp_spgemm_set_model(rvsp_spgemm_descr_t d, rvsp_mlp_t model)
+{
+    if (d == NULL)
+        return RVSP_ERROR_NULL_POINTER;
+    if (d->estimated)
+        return RVSP_ERROR_INVALID_ARGUMENT;
+    d->model = model;
+    return RVSP_SUCCESS;
+}
+
+rvsp_status_t rvsp_spgemm_set_capacity_scale(rvsp_spgemm_descr_t d, float scale)
+{
+    if (d == NULL)
+        return RVSP_ERROR_NULL_POINTER;
+    if (!(scale > 0.0f) || scale > 1e6f)
+        return RVSP_ERROR_INVALID_ARGUMENT;
+    d->capacity_scale = scale;
+    return RVSP_SUCCESS;
+}
+
+rvsp_status_t rvsp_spgemm_set_merge_policy(rvsp_spgemm_descr_t d, int32_t policy)
+{
+    if (d == NULL)
+        return RVSP_ERROR_NULL_POINTER;
+    if (d->estimated || policy < 0 || policy > 2)
+        return RVSP_ERROR_INVALID_ARGUMENT;
+    d->merge_policy = policy;
+    return RVSP_SUCCESS;
+}
+
+rvsp_status_t rvsp_spgemm_get_overflow_rows(rvsp_spgemm_descr_t d, int32_t *n_out)
+{
+    if (d == NULL || n_out == NULL)
+        return RVSP_ERROR_NULL_POINTER;
+    if (!d->estimated)
+        return RVSP_ERROR_INVALID_ARGUMENT;
+    *n_out = rvsp_cuda_plan_overflow_rows(d->plan);
     return RVSP_SUCCESS;
 }
 
@@ -184,7 +229,7 @@ static rvsp_status_t ensure_device(rvsp_spgemm_descr_t d)
     }
     if (!d->user_stream)
         d->stream = d->own_stream;
-    return RVSP_SUCCESS;
+    return rvsp_cuda_plan_set_merge_policy(d->plan, d->merge_policy);
 }
 
 static int same_structure(const rvsp_csr_matrix_t *X, const rvsp_csr_matrix_t *Y)
@@ -229,6 +274,26 @@ static rvsp_status_t upload_structure(rvsp_spgemm_descr_t d,
     return RVSP_SUCCESS;
 }
 
+/* Host memory space: brings A's values (and B's, into their own array unless
+ * B is A with the same values) to the device; *b_vals_out is B's device
+ * values. */
+static rvsp_status_t upload_values(rvsp_spgemm_descr_t d, const rvsp_csr_matrix_t *A,
+                                   const rvsp_csr_matrix_t *B, const float **b_vals_out)
+{
+    cudaStream_t s = d->stream;
+    rvsp_status_t st = rvsp_dev_csr_upload_values(&d->dA, A, s);
+    const int b_values_alias = d->b_aliases_a && A->values == B->values;
+    if (st == RVSP_SUCCESS && !d->b_aliases_a)
+        st = rvsp_dev_csr_upload_values(&d->dB, B, s);
+    if (st == RVSP_SUCCESS && d->b_aliases_a && !b_values_alias) {
+        /* Same pattern, different values: B gets its own value array. */
+        d->dB.entries = d->dA.entries;
+        st = rvsp_dev_csr_upload_values(&d->dB, B, s);
+    }
+    *b_vals_out = (const float *)(b_values_alias ? d->dA.values.p : d->dB.values.p);
+    return st;
+}
+
 rvsp_status_t rvsp_spgemm_work_estimation(rvsp_spgemm_descr_t d,
                                           const rvsp_csr_matrix_t *A,
                                           const rvsp_csr_matrix_t *B,
@@ -271,7 +336,7 @@ rvsp_status_t rvsp_spgemm_work_estimation(rvsp_spgemm_descr_t d,
         b_ci = B->col_idx;
         st = rvsp_device_check(d->plan, d->stream, A->rows, A->cols, a_rp, a_ci,
                                A->nnz, RVSP_REJECT_ALL);
-        if (st == RVSP_SUCCESS && B != A)
+        if (st == RVSP_SUCCESS && !same_structure(A, B))
             st = rvsp_device_check(d->plan, d->stream, B->rows, B->cols, b_rp, b_ci,
                                    B->nnz, RVSP_REJECT_ALL);
         if (st != RVSP_SUCCESS)
@@ -282,8 +347,29 @@ rvsp_status_t rvsp_spgemm_work_estimation(rvsp_spgemm_descr_t d,
     if (st != RVSP_SUCCESS)
         return st;
     int64_t total = 0;
-    st = rvsp_cuda_symbolic(d->plan, d->stream, A->rows, B->rows, B->cols, a_rp, a_ci,
-                            b_rp, b_ci, (int32_t *)d->c_row_ptr.p, &total);
+    if (d->algo == RVSP_SPGEMM_ALGO_CUDA_LEARNED) {
+        if (d->model == NULL)
+            return RVSP_ERROR_INVALID_ARGUMENT;
+        /* The fused pass computes values too, so it needs them now.  The
+         * value counts are those of the arrays on the device. */
+        const float *a_v = (const float *)A->values, *b_v = (const float *)B->values;
+        int32_t a_n = A->nnz, b_n = B->nnz;
+        if (d->mem == RVSP_MEM_HOST) {
+            st = upload_values(d, A, B, &b_v);
+            if (st != RVSP_SUCCESS)
+                return st;
+            a_v = (const float *)d->dA.values.p;
+            a_n = d->dA.entries;
+            b_n = d->b_aliases_a ? d->dA.entries : d->dB.entries;
+        }
+        st = rvsp_cuda_learned_symbolic(d->plan, d->model, d->stream, A->rows, B->rows,
+                                        B->cols, a_rp, a_ci, a_v, a_n, b_rp, b_ci, b_v,
+                                        b_n, d->capacity_scale,
+                                        (int32_t *)d->c_row_ptr.p, &total);
+    } else {
+        st = rvsp_cuda_symbolic(d->plan, d->stream, A->rows, B->rows, B->cols, a_rp,
+                                a_ci, b_rp, b_ci, (int32_t *)d->c_row_ptr.p, &total);
+    }
     if (st != RVSP_SUCCESS)
         return st;
 
@@ -354,20 +440,11 @@ rvsp_status_t rvsp_spgemm_compute(rvsp_spgemm_descr_t d, const rvsp_csr_matrix_t
         st = upload_structure(d, A, B, 0);
         if (st != RVSP_SUCCESS)
             return st;
-        st = rvsp_dev_csr_upload_values(&d->dA, A, s);
-        const int b_values_alias = d->b_aliases_a && A->values == B->values;
-        if (st == RVSP_SUCCESS && !d->b_aliases_a)
-            st = rvsp_dev_csr_upload_values(&d->dB, B, s);
-        if (st == RVSP_SUCCESS && d->b_aliases_a && !b_values_alias) {
-            /* Same pattern, different values: B gets its own value array. */
-            d->dB.entries = d->dA.entries;
-            st = rvsp_dev_csr_upload_values(&d->dB, B, s);
-        }
+        const float *b_vals = NULL;
+        st = upload_values(d, A, B, &b_vals);
         if (st != RVSP_SUCCESS)
             return st;
         const rvsp_dev_csr_t *bsrc = d->b_aliases_a ? &d->dA : &d->dB;
-        const float *b_vals = (const float *)(b_values_alias ? d->dA.values.p
-                                                             : d->dB.values.p);
         st = rvsp_dbuf_reserve(&d->dC_col, nnz_c * sizeof(int32_t));
         if (st == RVSP_SUCCESS)
             st = rvsp_dbuf_reserve(&d->dC_val, nnz_c * sizeof(float));
@@ -428,4 +505,62 @@ rvsp_status_t rvsp_spgemm_get_class_counts(rvsp_spgemm_descr_t d, int32_t *sym_o
     if (!d->estimated)
         return RVSP_ERROR_INVALID_ARGUMENT;
     return rvsp_cuda_plan_class_counts(d->plan, sym_out, num_out, n);
+}
+
+rvsp_status_t rvsp_spgemm_multiply(rvsp_spgemm_descr_t d, const rvsp_csr_matrix_t *A,
+                                   const rvsp_csr_matrix_t *B, rvsp_csr_matrix_t *C)
+{
+    if (d == NULL || A == NULL || B == NULL || C == NULL)
+        return RVSP_ERROR_NULL_POINTER;
+    size_t ws_bytes = 0;
+    int32_t nnz = 0;
+    rvsp_status_t st = rvsp_spgemm_work_estimation(d, A, B, &ws_bytes, &nnz);
+    if (st != RVSP_SUCCESS)
+        return st;
+    const size_t alloc = (size_t)(nnz > 0 ? nnz : 1);
+    const size_t rp_bytes = ((size_t)A->rows + 1) * sizeof(int32_t);
+    rvsp_csr_matrix_t out;
+    memset(&out, 0, sizeof(out));
+    out.rows = A->rows;
+    out.cols = B->cols;
+    out.nnz = nnz;
+    out.dtype = RVSP_DTYPE_FP32;
+    out.format = RVSP_FORMAT_CSR;
+    if (d->mem == RVSP_MEM_HOST) {
+        out.owns_data = 1;
+        out.row_ptr = (int32_t *)malloc(rp_bytes);
+        out.col_idx = (int32_t *)malloc(alloc * sizeof(int32_t));
+        out.values = malloc(alloc * sizeof(float));
+        void *ws = malloc(ws_bytes > 0 ? ws_bytes : 1);
+        if (!out.row_ptr || !out.col_idx || !out.values || !ws)
+            st = RVSP_ERROR_ALLOCATION_FAILED;
+        else
+            st = rvsp_spgemm_compute(d, A, B, &out, ws);
+        free(ws);
+    } else {
+        out.owns_data = 2;
+        cudaError_t e = cudaMalloc((void **)&out.row_ptr, rp_bytes);
+        if (e == cudaSuccess)
+            e = cudaMalloc((void **)&out.col_idx, alloc * sizeof(int32_t));
+        if (e == cudaSuccess)
+            e = cudaMalloc(&out.values, alloc * sizeof(float));
+        st = rvsp_map_cuda(e);
+        if (st == RVSP_SUCCESS)
+            st = rvsp_dbuf_reserve(&d->d_ws, ws_bytes);
+        if (st == RVSP_SUCCESS)
+            st = rvsp_spgemm_compute(d, A, B, &out, d->d_ws.p);
+        if (st == RVSP_SUCCESS)
+            st = rvsp_spgemm_synchronize(d);
+    }
+    if (st != RVSP_SUCCESS) {
+        rvsp_csr_destroy(&out);
+        C->row_ptr = NULL;
+        C->col_idx = NULL;
+        C->values = NULL;
+        C->nnz = 0;
+        C->owns_data = 0;
+        return st;
+    }
+    *C = out;
+    return RVSP_SUCCESS;
 }

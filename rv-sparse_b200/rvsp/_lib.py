@@ -39,7 +39,7 @@ MEM_DEVICE = 1
 
 PHASES = ("rowstats", "symbolic", "scan", "numeric", "predict", "fused",
           "compact", "copy", "check")
-CLASS_NAMES = ("empty", "m4", "m8", "m16", "m32", "w64", "w128", "w256", "w512",
+CLASS_NAMES = ("empty", "m4", "m8", "m16", "w64", "w128", "w256", "w512",
                "w1024", "w2048", "b8192", "dense")
 
 CSR_OK, CSR_BAD_ROW_PTR, CSR_COL_OUT_OF_RANGE, CSR_UNSORTED, CSR_DUPLICATE = range(5)
@@ -116,6 +116,27 @@ SIGNATURES = {
     "rvsp_cuda_plan_class_counts": (_int, [_vp, _vp, _vp, _i32]),
     "rvsp_cuda_numeric_noalloc": (_int, [_vp, _i32, _i32, _i32, _vp, _vp, _vp, _vp,
                                          _vp, _vp, _vp, _vp, _vp]),
+    "rvsp_mlp_create": (_int, [_P(_vp), C.c_uint64]),
+    "rvsp_mlp_destroy": (None, [_vp]),
+    "rvsp_mlp_num_params": (_i32, []),
+    "rvsp_mlp_get_params": (_int, [_vp, _vp, _i32]),
+    "rvsp_mlp_set_params": (_int, [_vp, _vp, _i32]),
+    "rvsp_mlp_features": (_int, [_vp, _i32, _i32, _i32, _vp, _vp, _vp, _vp, _vp, _vp]),
+    "rvsp_mlp_gradient": (_int, [_vp, _vp, _vp, _vp, _i32, _vp, _P(C.c_float)]),
+    "rvsp_mlp_train": (_int, [_vp, _vp, _vp, _vp, _i32, _i32, _i32, C.c_float, _vp]),
+    "rvsp_mlp_predict": (_int, [_vp, _vp, _i32, _i32, _i32, _vp, _vp, _vp, _vp, _vp]),
+    "rvsp_mlp_save": (_int, [_vp, C.c_char_p]),
+    "rvsp_mlp_load": (_int, [_vp, C.c_char_p]),
+    "rvsp_cuda_learned_symbolic": (_int, [_vp, _vp, _vp, _i32, _i32, _i32, _vp, _vp, _vp,
+                                          _i32, _vp, _vp, _vp, _i32, C.c_float, _vp,
+                                          _P(_i64)]),
+    "rvsp_cuda_plan_overflow_rows": (_i32, [_vp]),
+    "rvsp_cuda_plan_set_merge_policy": (_int, [_vp, _i32]),
+    "rvsp_spgemm_set_merge_policy": (_int, [_vp, _i32]),
+    "rvsp_spgemm_set_model": (_int, [_vp, _vp]),
+    "rvsp_spgemm_set_capacity_scale": (_int, [_vp, C.c_float]),
+    "rvsp_spgemm_get_overflow_rows": (_int, [_vp, _P(_i32)]),
+    "rvsp_spgemm_multiply": (_int, [_vp, _P(CsrMatrix), _P(CsrMatrix), _P(CsrMatrix)]),
 }
 
 _lib = None

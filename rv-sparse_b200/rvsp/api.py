@@ -204,3 +204,74 @@ class Descriptor:
 
     def synchronize(self):
         L.check(self.lib.rvsp_spgemm_synchronize(self.h), "synchronize")
+
+    def set_model(self, model):
+        """Row-binning model (rvsp.learn.RowModel) for ALGO_CUDA_LEARNED."""
+        self._keep.append(model)
+        L.check(self.lib.rvsp_spgemm_set_model(self.h, model.h), "set_model")
+
+    def set_capacity_scale(self, scale: float):
+        L.check(self.lib.rvsp_spgemm_set_capacity_scale(self.h, C.c_float(scale)),
+                "set_capacity_scale")
+
+    def set_merge_policy(self, policy: int):
+        L.check(self.lib.rvsp_spgemm_set_merge_policy(self.h, policy), "set_merge_policy")
+
+    def overflow_rows(self) -> int:
+        n = C.c_int32()
+        L.check(self.lib.rvsp_spgemm_get_overflow_rows(self.h, C.byref(n)), "overflow_rows")
+        return n.value
+
+    def multiply_once(self, A, B):
+        """rvsp_spgemm_multiply: C = A * B in one call.  Host memory space
+        returns a host CSR; device memory space returns a DeviceResult."""
+        a, b = A.struct(), B.struct()
+        c = L.CsrMatrix()
+        L.check(self.lib.rvsp_spgemm_multiply(self.h, C.byref(a), C.byref(b), C.byref(c)),
+                "multiply")
+        if self.memory == L.MEM_DEVICE:
+            return DeviceResult(c)
+        try:
+            n = c.nnz
+            rp = np.ctypeslib.as_array(C.cast(c.row_ptr, C.POINTER(C.c_int32)),
+                                       shape=(c.rows + 1,)).copy()
+            ci = np.ctypeslib.as_array(C.cast(c.col_idx, C.POINTER(C.c_int32)),
+                                       shape=(max(n, 1),))[:n].copy()
+            cv = np.ctypeslib.as_array(C.cast(c.values, C.POINTER(C.c_float)),
+                                       shape=(max(n, 1),))[:n].copy()
+            return CSR(c.rows, c.cols, rp, ci, cv)
+        finally:
+            self.lib.rvsp_csr_destroy(C.byref(c))
+
+
+class DeviceResult:
+    """A C produced in device memory by the library (owns_data = 2)."""
+
+    def __init__(self, c: L.CsrMatrix):
+        self.c = c
+        self.rows, self.cols, self.nnz = c.rows, c.cols, c.nnz
+
+    def to_host(self) -> CSR:
+        import cuda.bindings.runtime as rt
+        rp = np.zeros(self.rows + 1, np.int32)
+        ci = np.zeros(max(self.nnz, 1), np.int32)
+        cv = np.zeros(max(self.nnz, 1), np.float32)
+        for dst, src, nb in ((rp, self.c.row_ptr, rp.nbytes),
+                             (ci, self.c.col_idx, 4 * self.nnz),
+                             (cv, self.c.values, 4 * self.nnz)):
+            if nb:
+                err, = rt.cudaMemcpy(dst.ctypes.data, src, nb,
+                                     rt.cudaMemcpyKind.cudaMemcpyDeviceToHost)
+                if int(err) != 0:
+                    raise RuntimeError(f"cudaMemcpy failed ({int(err)})")
+        return CSR(self.rows, self.cols, rp, ci[:self.nnz], cv[:self.nnz])
+
+    def free(self):
+        if self.c.row_ptr:
+            L.load().rvsp_csr_destroy(C.byref(self.c))
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass

@@ -126,7 +126,10 @@ def rmat(scale: int, edge_factor: int, probs=(0.57, 0.19, 0.19, 0.05),
         cbit = ((u >= a) & (u < a + b)) | (u >= a + b + c)
         row = (row << 1) | rbit
         col = (col << 1) | cbit
-    key = np.unique(row * n + col)
+    key = row * n + col
+    key.sort()
+    if key.size:
+        key = key[np.concatenate(([True], key[1:] != key[:-1]))]
     r = key // n
     cl = (key % n).astype(np.int32)
     counts = np.bincount(r, minlength=n)

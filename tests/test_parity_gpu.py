@@ -95,6 +95,13 @@ def class_probe(seed: int, b_cols: int = 60000):
     a_rows += [pick(0, 40) for _ in range(8)]
     for k in (45, 60, 80, 100, 150, 250, 400):
         a_rows += [pick(long_g, k) for _ in range(6)]
+    # The merge classes need a matrix of at least 32768 rows: pad with rows of
+    # 1..16 A nonzeros (long and short B rows alternately).
+    r = 0
+    while len(a_rows) < 33000:
+        k = 1 + r % 16
+        a_rows.append(pick(long_g if r % 3 else 0, min(k, 12) if r % 3 == 0 else k))
+        r += 1
     a_rows = [np.sort(x) for x in a_rows]
     lens = np.array([x.size for x in a_rows], np.int64)
     arp = np.zeros(len(a_rows) + 1, np.int64)
@@ -127,6 +134,21 @@ def test_seeded_irregular(seed):
                        empty_frac=0.15, heavy_rows=1, heavy_len=300,
                        value_kind="int" if seed % 2 else "uniform")
     check_against_oracle(A, B, f"seed {seed}")
+
+
+def test_single_merge_class_with_empty_rows():
+    # every non-empty row has 3 A nonzeros (one merge class) and a fifth of
+    # the rows are empty: the class is run over the whole matrix, no row list
+    rng = np.random.default_rng(8)
+    n = 40000
+    lengths = np.where(rng.random(n) < 0.2, 0, 3).astype(np.int64)
+    cols = gen._distinct_sorted_columns(rng, lengths, 5000)
+    rp = np.zeros(n + 1, np.int64)
+    np.cumsum(lengths, out=rp[1:])
+    A = CSR(n, 5000, rp, cols, rng.uniform(-1, 1, cols.size).astype(np.float32))
+    B = gen.random_csr(5000, 7000, 9, mean_len=4.0, empty_frac=0.1)
+    sym, num = check_against_oracle(A, B, "one merge class")
+    assert sym["m4"] > 0 and sym["empty"] > 0
 
 
 def test_long_a_rows():
