@@ -49,6 +49,8 @@ WORKLOADS = {
     "uniform4096": "4096x4096, exactly 16 nnz/row uniform columns, values U[-1,1], C=A*B, full product",
     "stencil3d": "3D 27-point stencil 128^3 (n=2,097,152, nnz=55,742,968), C=A*A, full product",
     "stencil3d_reuse": "3D 27-point stencil 128^3, C=A*A, numeric-only repeats (values perturbed U[-0.01,0.01])",
+    "rmat16": "R-MAT n=2^16, 16 edges/row, (0.57,0.19,0.19,0.05), values U(0,1], C=A*A, full product",
+    "rmat18": "R-MAT n=2^18, 16 edges/row, (0.57,0.19,0.19,0.05), values U(0,1], C=A*A, full product",
 }
 
 
@@ -61,6 +63,9 @@ def build_inputs(name: str, seed: int = 2024):
         return gen.uniform_rows(4096, 4096, 16, seed), gen.uniform_rows(4096, 4096, 16, seed + 1)
     if name in ("stencil3d", "stencil3d_reuse"):
         A = gen.stencil_3d_27(128)
+        return A, A
+    if name.startswith("rmat"):
+        A = gen.rmat(int(name[4:]), 16, seed=1)
         return A, A
     raise ValueError(name)
 
@@ -194,6 +199,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--workload", default="laplace2d", choices=sorted(WORKLOADS))
     ap.add_argument("--impl", default="ours", choices=("ours", "reference"))
+    ap.add_argument("--path", default="plain", choices=("plain", "learned"),
+                    help="plain GPU Gustavson, or the learned (MLP-binned, fused) path")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=10)
     args = ap.parse_args()
@@ -230,7 +237,20 @@ def main():
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
     reuse = args.workload.endswith("_reuse")
 
-    d = Descriptor(memory=L.MEM_DEVICE, stream=stream, profiling=True)
+    model = None
+    algo = L.ALGO_CUDA_PLAIN
+    if args.path == "learned":
+        from rvsp.learn import DEFAULT_WEIGHTS, RowModel
+        model = RowModel(path=DEFAULT_WEIGHTS)
+        algo = L.ALGO_CUDA_LEARNED
+
+    def make_descr(memory, **kw):
+        dd = Descriptor(algo=algo, memory=memory, **kw)
+        if model is not None:
+            dd.set_model(model)
+        return dd
+
+    d = make_descr(L.MEM_DEVICE, stream=stream, profiling=True)
     ws_bytes, c_nnz = d.work_estimation(dA, dB)
     dC = DeviceCSR.empty(A.rows, B.cols, c_nnz, dev)
     ws = torch.zeros(max(ws_bytes, 1), dtype=torch.uint8, device=dev)
@@ -306,7 +326,7 @@ def main():
         hC = CSR(A.rows, B.cols, pinned(np.zeros(A.rows + 1, np.int32)),
                  pinned(np.zeros(n, np.int32)), pinned(np.zeros(n, np.float32)))
         hws = np.zeros(256, np.uint8)
-        he = Descriptor(memory=L.MEM_HOST)
+        he = make_descr(L.MEM_HOST)
         he.work_estimation(hA, hB)
         he.compute(hA, hB, hC, hws)
         if reuse:
@@ -349,16 +369,18 @@ def main():
     d.close()
     if rank == 0:
         sym, num = {}, {}
-        with Descriptor(memory=L.MEM_DEVICE, stream=stream) as dd:
+        with make_descr(L.MEM_DEVICE, stream=stream) as dd:
             dd.work_estimation(dA, dB)
             sym, num = dd.class_counts()
+            overflow = dd.overflow_rows()
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32", "data": "synthetic",
             "config": {"workload": args.workload, "description": WORKLOADS[args.workload],
-                       "path": "plain", "rows": A.rows, "nnz_a": A.nnz, "nnz_b": B.nnz,
+                       "path": args.path, "rows": A.rows, "nnz_a": A.nnz, "nnz_b": B.nnz,
+                       "overflow_rows": overflow,
                        "nnz_c": c_nnz, "products": int(ops.sum()),
                        "flops_per_step": flops, "algorithmic_bytes_per_step": alg_bytes,
                        "l2": "flushed between steps (256 MiB write outside the step events)",

@@ -181,20 +181,34 @@ __device__ __forceinline__ AChunk load_chunk(const int32_t *__restrict__ a_col,
   return c;
 }
 
-// Ordered accumulation of one 32-product tile into acc[slot].  Lanes are in
-// flattened product order, so among lanes that hit the same slot the lower
-// lane holds the earlier A nonzero; rounds apply rank 0 first, then rank 1 ...
-// Each round touches distinct slots.  Invalid lanes pass valid = false.
+// Ordered accumulation of one 32-product tile into acc[slot] (shared or
+// global memory).  Lanes are in flattened product order, so among lanes that
+// hit the same slot the lower lane holds the earlier A nonzero.  The lowest
+// lane of each group loads the slot once, adds its own term and then its
+// peers' terms in ascending lane order (fetched by shuffle), and stores once:
+// the same sequence of roundings as applying the lanes one by one, with one
+// memory round trip per group however many terms a hot column collects.
+// Invalid lanes pass valid = false.
 __device__ __forceinline__ void ordered_apply(float *acc, bool valid, int slot,
                                               float term) {
-  const int key = valid ? slot : (-1 - lane_id());
+  const int lane = lane_id();
+  const int key = valid ? slot : (-1 - lane);
   const unsigned peers = __match_any_sync(kFull, key);
-  const int rank = __popc(peers & lanemask_lt());
-  for (int r = 0;; ++r) {
-    if (valid && rank == r) acc[slot] = __fadd_rn(acc[slot], term);
-    __syncwarp();
-    if (!__any_sync(kFull, valid && rank > r)) break;
+  const bool leader = valid && (peers & lanemask_lt()) == 0u;
+  const unsigned longest = __reduce_max_sync(kFull, valid ? __popc(peers) : 0u);
+  float a = 0.0f;
+  if (leader) a = __fadd_rn(acc[slot], term);
+  unsigned rest = peers & ~(1u << lane);  // the group's later lanes, ascending
+  for (unsigned r = 1; r < longest; ++r) {
+    const int src = rest ? __ffs(rest) - 1 : lane;
+    const float t = __shfl_sync(kFull, term, src);
+    if (leader && rest) {
+      a = __fadd_rn(a, t);
+      rest &= rest - 1u;
+    }
   }
+  if (leader) acc[slot] = a;
+  __syncwarp();
 }
 
 // Bitonic sort of n (power of two) 64-bit keys in shared memory by one warp.

@@ -582,12 +582,13 @@ void launch_warp(const Operands &op, const int64_t *ops, const int32_t *rows,
 }  // namespace
 
 size_t dense_slot_acc_bytes(int32_t b_cols) {
+  if (heavy_fits(b_cols)) return 0;  // the heavy kernels need no global scratch
   const size_t b = size_t(b_cols > 0 ? b_cols : 1) * sizeof(float);
   return (b + 255) & ~size_t(255);
 }
 
 size_t dense_slot_bits_bytes(int32_t b_cols) {
-  if (b_cols <= kSmemBitmapMaxCols) return 0;
+  if (heavy_fits(b_cols) || b_cols <= kSmemBitmapMaxCols) return 0;
   const size_t b = ((size_t(b_cols) + 31) >> 5) * sizeof(uint32_t);
   return (b + 255) & ~size_t(255);
 }
@@ -636,7 +637,10 @@ void launch_numeric_class(int cls, const Operands &op, const int64_t *ops,
                           int32_t dense_slots, int32_t *status, int num_sms,
                           cudaStream_t s, const FusedOut *fo) {
   if (nrows <= 0) return;
-  (void)num_sms;
+  if ((cls == kB8192 || cls == kDense) && heavy_fits(op.b_cols)) {
+    launch_heavy_numeric(op, rows, nrows, c_rp, c_col, c_val, fill, status, fo, num_sms, s);
+    return;
+  }
   const FusedOut none{};
   switch (cls) {
     case kM4:

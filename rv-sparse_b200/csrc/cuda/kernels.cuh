@@ -177,6 +177,20 @@ void launch_symbolic_class(int cls, const Operands &op, const int32_t *rows,
                            int32_t gbitmap_slots, int32_t *status, int num_sms,
                            cudaStream_t s);
 
+// ---- k_heavy.cu ------------------------------------------------------------
+// B8192 and DENSE rows when B has at most kHeavyMaxCols columns: block per
+// row, shared-memory column bitmap, accumulation at output positions.
+constexpr int32_t kHeavyMaxCols = 1 << 20;
+bool heavy_fits(int32_t b_cols);
+void launch_heavy_symbolic(const Operands &op, const int32_t *rows, int32_t nrows,
+                           int32_t *counts, int num_sms, cudaStream_t s);
+// fill: write C's sorted columns too (fo: the fused pass's slab slots, with
+// overflow when a row needs more than its capacity); else reuse C's columns.
+void launch_heavy_numeric(const Operands &op, const int32_t *rows, int32_t nrows,
+                          const int32_t *c_rp, int32_t *c_col, float *c_val, bool fill,
+                          int32_t *status, const FusedOut *fo, int num_sms,
+                          cudaStream_t s);
+
 // ---- k_check.cu ------------------------------------------------------------
 // *result (initialised to ~0ull) receives min over bad rows of
 // ((row + 1) << 8 | code); row -1 means row_ptr[0] != 0.

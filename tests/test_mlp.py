@@ -92,7 +92,7 @@ def test_gpu_training_reduces_loss_and_predicts_like_oracle(tmp_path):
     A = gen.rmat(13, 8, seed=11)
     dA = DeviceCSR.from_host(A)
     feat, _ = features(dA, dA)
-    rp, _, _, _ = oracle.symbolic(A, A)
+    rp, _, _ = oracle.symbolic(A, A)
     m_rows = np.diff(rp)
     t = np.stack([np.log2(1.0 + m_rows), (np.diff(A.row_ptr) <= 4).astype(float)], 1)
     tgt = torch.from_numpy(t.astype(np.float32)).cuda()
@@ -102,8 +102,14 @@ def test_gpu_training_reduces_loss_and_predicts_like_oracle(tmp_path):
     hist = model.train(feat, tgt, batch=512, epochs=30, lr=3e-3)
     assert hist[-1] < 0.25 * hist[0]
     pred = model.predict(dA, dA).cpu().numpy()
-    *_, y = M.forward(model.params().astype(np.float64), M.features(A, A))
-    assert np.allclose(pred, y, rtol=1e-3, atol=1e-3)
+    p64 = model.params().astype(np.float64)
+    # FP32 inference against the FP64 forward pass of the same features ...
+    *_, y_same = M.forward(p64, f.astype(np.float64))
+    assert np.allclose(pred, y_same, rtol=1e-4, atol=1e-3)
+    # ... and against the oracle's own FP64 features (outputs reach |y| ~ 20,
+    # so FP32 feature rounding moves them by a few 1e-4)
+    *_, y = M.forward(p64, M.features(A, A))
+    assert np.allclose(pred, y, rtol=1e-3, atol=5e-3)
     path = tmp_path / "m.bin"
     model.save(path)
     other = RowModel(seed=99, path=path)

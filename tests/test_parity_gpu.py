@@ -26,7 +26,9 @@ def assert_bit_exact(got: CSR, rp, ci, cv, what=""):
     assert bad.size == 0, f"values {what}: {bad.size} differ, first at {bad[:5]}"
 
 
-def check_against_oracle(A, B, what=""):
+def check_against_oracle(A, B, what="", reuse=False):
+    """One-shot and descriptor products against the oracle; with reuse, also
+    a numeric-only repeat after A's values change."""
     rp, ci, cv, ops = oracle.spgemm(A, B)
     got = spgemm_csr(A, B)
     assert_bit_exact(got, rp, ci, cv, what + " one-shot")
@@ -35,6 +37,11 @@ def check_against_oracle(A, B, what=""):
         assert_bit_exact(Cm, rp, ci, cv, what + " descriptor")
         assert np.array_equal(d.get_op_counts(A.rows), ops), what
         sym, num = d.class_counts()
+        if reuse:
+            A2 = A.with_values((A.values * -0.75).astype(np.float32))
+            _, _, cv2, _ = oracle.spgemm(A2, B)
+            d.compute(A2, B, Cm, np.zeros(max(d.ws_bytes, 1), np.uint8))
+            assert_bit_exact(Cm, rp, ci, cv2, what + " numeric-only reuse")
     return sym, num
 
 
@@ -113,7 +120,7 @@ def class_probe(seed: int, b_cols: int = 60000):
 
 def test_every_row_class():
     A, B = class_probe(11)
-    sym, num = check_against_oracle(A, B, "class probe")
+    sym, num = check_against_oracle(A, B, "class probe", reuse=True)
     for cls in L.CLASS_NAMES:
         assert sym[cls] > 0 or num[cls] > 0, (cls, sym, num)
 
@@ -122,8 +129,38 @@ def test_dense_rows_with_global_bitmap():
     # b_cols beyond the shared-memory bitmap (1.5 Mi columns): dense rows use
     # the global-memory bitmap in both passes.
     A, B = class_probe(12, b_cols=2_000_000)
-    sym, num = check_against_oracle(A, B, "wide B")
+    sym, num = check_against_oracle(A, B, "wide B", reuse=True)
     assert sym["dense"] > 0 and num["dense"] > 0
+
+
+def test_dense_rows_wide_smem_bitmap():
+    # 2^20 < b_cols <= 1.5 Mi: the block-hash and dense kernels with the
+    # bitmap in shared memory and the accumulator in global memory.
+    A, B = class_probe(13, b_cols=1_200_000)
+    sym, num = check_against_oracle(A, B, "1.2M columns", reuse=True)
+    assert sym["dense"] > 0 and num["dense"] > 0
+
+
+def test_heavy_rows_at_bitmap_limit():
+    # b_cols = 2^20, the widest B the heavy-row kernels take: the largest
+    # bitmap, and rows whose nnz exceeds the shared-memory accumulator
+    # (accumulation in C's value array).
+    A, B = class_probe(14, b_cols=1 << 20)
+    sym, num = check_against_oracle(A, B, "2^20 columns", reuse=True)
+    assert sym["dense"] > 0 and num["dense"] > 0
+    nnz = np.diff(spgemm_csr(A, B).row_ptr)
+    assert nnz.max() > 12000
+
+
+def test_rmat_hub_rows():
+    # The first rows of an R-MAT matrix are its hubs: thousands of A
+    # nonzeros, popular output columns shared by many B rows, and rows of
+    # more output nnz than the shared-memory accumulator holds.
+    A = gen.rmat(16, 16, seed=1)
+    panel = A.row_panel(0, 192)
+    check_against_oracle(panel, A, "R-MAT 2^16 hub rows", reuse=True)
+    nnz = np.diff(spgemm_csr(panel, A).row_ptr)
+    assert nnz.max() > 20000
 
 
 @pytest.mark.parametrize("seed", range(8))
