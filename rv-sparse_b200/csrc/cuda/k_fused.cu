@@ -11,21 +11,30 @@ namespace {
 
 constexpr int kThreads = 256;
 
-// One warp per row; coalesced copies.
+// Rows of at least this many entries are copied by whole blocks.
+constexpr int32_t kCompactLarge = 4096;
+
+// kLarge = false: one warp per row below kCompactLarge entries; true: one
+// block per row of kCompactLarge or more (a power-law matrix has rows of
+// tens of thousands of entries, which would leave one warp copying long
+// after the rest).  Coalesced copies either way.
+template <bool kLarge>
 __global__ void __launch_bounds__(kThreads)
 compact_kernel(int32_t a_rows, const int32_t *__restrict__ counts,
                const int64_t *__restrict__ off, const int32_t *__restrict__ row_ptr,
                const int32_t *__restrict__ slab_col, const float *__restrict__ slab_val,
                int32_t *__restrict__ c_col, float *__restrict__ c_val, bool with_values) {
-  const int warps = (gridDim.x * blockDim.x) >> 5;
-  const int lane = lane_id();
-  for (int32_t row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; row < a_rows;
-       row += warps) {
+  const int lanes = kLarge ? kThreads : 32;
+  const int me = kLarge ? threadIdx.x : lane_id();
+  const int32_t first = kLarge ? blockIdx.x : (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int32_t stride = kLarge ? gridDim.x : (gridDim.x * blockDim.x) >> 5;
+  for (int32_t row = first; row < a_rows; row += stride) {
     const int32_t m = counts[row];
     if (m <= 0) continue;  // empty, or redone by the plain path
+    if ((m >= kCompactLarge) != kLarge) continue;
     const int64_t src = off[row];
     const int32_t dst = row_ptr[row];
-    for (int32_t e = lane; e < m; e += 32) {
+    for (int32_t e = me; e < m; e += lanes) {
       c_col[dst + e] = slab_col[src + e];
       if (with_values) c_val[dst + e] = slab_val[src + e];
     }
@@ -86,8 +95,10 @@ void launch_compact(int32_t a_rows, const int32_t *counts, const int64_t *off,
                     const int32_t *row_ptr, const int32_t *slab_col,
                     const float *slab_val, int32_t *c_col, float *c_val,
                     bool with_values, int num_sms, cudaStream_t s) {
-  compact_kernel<<<num_sms * 8, kThreads, 0, s>>>(a_rows, counts, off, row_ptr, slab_col,
-                                                 slab_val, c_col, c_val, with_values);
+  compact_kernel<false><<<num_sms * 8, kThreads, 0, s>>>(
+      a_rows, counts, off, row_ptr, slab_col, slab_val, c_col, c_val, with_values);
+  compact_kernel<true><<<num_sms * 8, kThreads, 0, s>>>(
+      a_rows, counts, off, row_ptr, slab_col, slab_val, c_col, c_val, with_values);
 }
 
 void launch_list_classify(const int32_t *list, int32_t n, const int64_t *ops,

@@ -96,12 +96,27 @@ __device__ __forceinline__ int heavy_scan(int v, HeavyShared &sh, int *total) {
   return sh.wsum[w] + incl - v;
 }
 
+// First index i in [0, n) with c[i] >= key (n if none); c sorted.
+__device__ __forceinline__ int32_t lower_bound_col(const int32_t *__restrict__ c,
+                                                   int32_t n, int32_t key) {
+  int32_t lo = 0, hi = n;
+  while (lo < hi) {
+    const int32_t mid = (lo + hi) >> 1;
+    if (__ldg(c + mid) < key) lo = mid + 1;
+    else hi = mid;
+  }
+  return lo;
+}
+
 // Stages A nonzeros [pc, min(pc + kHStage, p1)) and returns their product
-// count; the stage is visible to the whole block on return.  Every thread
-// must call it, and no thread may still read the previous stage.
+// count; the stage is visible to the whole block on return.  With a window
+// (c_lo <= c_hi), each B row is cut to its entries in columns [c_lo, c_hi],
+// which are contiguous since B's rows are sorted.  Every thread must call it,
+// and no thread may still read the previous stage.
 template <bool kValues>
 __device__ __forceinline__ long long heavy_stage(const Operands &op, int32_t pc,
-                                                 int32_t p1, StageShared &st) {
+                                                 int32_t p1, StageShared &st,
+                                                 int32_t c_lo = 0, int32_t c_hi = -1) {
   const int tid = threadIdx.x, lane = lane_id(), w = tid >> 5;
   const int na = min(kHStage, p1 - pc);
   int len = 0;
@@ -112,6 +127,12 @@ __device__ __forceinline__ long long heavy_stage(const Operands &op, int32_t pc,
     if (kValues) av = __ldg(op.a_val + pc + tid);
     bb = __ldg(op.b_rp + k);
     len = __ldg(op.b_rp + k + 1) - bb;
+    if (c_lo <= c_hi && len > 0) {
+      const int32_t s = lower_bound_col(op.b_col + bb, len, c_lo);
+      const int32_t e = s + lower_bound_col(op.b_col + bb + s, len - s, c_hi + 1);
+      bb += s;
+      len = e - s;
+    }
   }
   long long x = len;
 #pragma unroll
@@ -159,16 +180,30 @@ __device__ __forceinline__ int32_t heavy_locate(const StageShared &st, long long
 __device__ __forceinline__ void heavy_mark(const Operands &op, int32_t p0, int32_t p1,
                                            uint32_t *bits, StageShared &st, int &lo,
                                            int &hi) {
+  auto mark = [&](int32_t col) {
+    uint32_t *wp = bits + (col >> 5);
+    const uint32_t bit = 1u << (col & 31);
+    if (!(*reinterpret_cast<volatile uint32_t *>(wp) & bit)) atomicOr(wp, bit);
+    lo = min(lo, col);
+    hi = max(hi, col);
+  };
   for (int32_t pc = p0; pc < p1; pc += kHStage) {
     const long long total = heavy_stage<false>(op, pc, p1, st);
-    for (long long q = threadIdx.x; q < total; q += kHT) {
-      int j;
-      const int32_t col = __ldg(op.b_col + heavy_locate(st, q, j));
-      uint32_t *wp = bits + (col >> 5);
-      const uint32_t bit = 1u << (col & 31);
-      if (!(*reinterpret_cast<volatile uint32_t *>(wp) & bit)) atomicOr(wp, bit);
-      lo = min(lo, col);
-      hi = max(hi, col);
+    const int na = min(kHStage, p1 - pc);
+    if (total >= static_cast<long long>(kStepMinAvgLen) * na) {
+      // long B rows: each one strided over the block (no order needed, so
+      // no barrier between them)
+      for (int j = 0; j < na; ++j) {
+        const long long ex = j ? st.incl[j - 1] : 0;
+        const int32_t len = static_cast<int32_t>(st.incl[j] - ex);
+        const int32_t bb = st.bbeg[j];
+        for (int32_t e = threadIdx.x; e < len; e += kHT) mark(__ldg(op.b_col + bb + e));
+      }
+    } else {
+      for (long long q = threadIdx.x; q < total; q += kHT) {
+        int j;
+        mark(__ldg(op.b_col + heavy_locate(st, q, j)));
+      }
     }
     __syncthreads();  // the next stage overwrites this one
   }
@@ -188,6 +223,21 @@ __device__ __forceinline__ void heavy_range(int lo, int hi, int32_t *s_lo, int32
 __device__ __forceinline__ void heavy_overflow(const FusedOut &fo, int32_t row) {
   fo.counts[row] = -1;
   fo.ovf_rows[atomicAdd(fo.ovf_count, 1)] = row;
+}
+
+// Bit position of the n-th (from 0) set bit of w; n < popc(w).
+__device__ __forceinline__ int nth_set_bit(uint32_t w, int n) {
+  int pos = 0;
+#pragma unroll
+  for (int s = 16; s >= 1; s >>= 1) {
+    const int c = __popc(w & ((1u << s) - 1u));
+    if (n >= c) {
+      n -= c;
+      w >>= s;
+      pos += s;
+    }
+  }
+  return pos;
 }
 
 __device__ __forceinline__ int popc4(const uint4 q) {
@@ -423,6 +473,7 @@ heavy_numeric_kernel(Operands op, const int32_t *__restrict__ rows, int32_t nrow
       gpre[g] = pos;
       pos += popc4(bits4[g]);
     }
+    __syncthreads();  // gpre complete
     // m is block-uniform: so are these branches.
     bool skip = false;
     if (kFused && m > lim) {
@@ -437,25 +488,45 @@ heavy_numeric_kernel(Operands op, const int32_t *__restrict__ rows, int32_t nrow
     }
     if (!skip) {
       if (kFill) {
-        int32_t at = ga < gb ? gpre[ga] : 0;
-        for (int32_t w = ga * 4; w < gb * 4; ++w) {
-          uint32_t word = hbits[w];
-          while (word) {
-            c_col[cs + at++] = (w << 5) + (__ffs(word) - 1);
-            word &= word - 1u;
+        // Columns in order: warp-strided chunks of 32 words (8 groups, so a
+        // chunk starts at gpre of its first group), each written with
+        // coalesced stores.
+        const int lane = lane_id();
+        const int32_t wend = (g0 + ng) * 4;
+        for (int32_t c0 = g0 * 4 + (tid >> 5) * 32; c0 < wend; c0 += kHW * 32) {
+          const int32_t w = c0 + lane;
+          const uint32_t word = w < wend ? hbits[w] : 0u;
+          const int cnt = __popc(word);
+          const int incl = warp_incl_scan(cnt);
+          const int n = __shfl_sync(kFull, incl, 31);
+          const int32_t base = gpre[c0 >> 2];
+          for (int t0 = 0; t0 < n; t0 += 32) {
+            const int t = t0 + lane;
+            const bool v = t < n;
+            const int j = warp_owner_of(incl, v ? t : 0);
+            const uint32_t wj = __shfl_sync(kFull, word, j);
+            const int before = __shfl_sync(kFull, incl - cnt, j);
+            if (v) c_col[cs + base + t] = ((c0 + j) << 5) + nth_set_bit(wj, t - before);
           }
         }
       }
       if (kFused && tid == 0) fo.counts[row] = m;
       // Output positions in windows of acc_cap, each accumulated in shared
-      // memory; a row wider than one window reads its products once per
-      // window.
+      // memory.  A row wider than one window stages each B row cut to the
+      // window's columns (read back from C's columns).
+      const bool windows = m > acc_cap;
+      if (windows) __syncthreads();  // the columns written above
       for (int32_t wlo = 0; wlo < m; wlo += acc_cap) {
         const int32_t wn = min(acc_cap, m - wlo);
+        int32_t c_lo = 0, c_hi = -1;
+        if (windows) {
+          c_lo = c_col[cs + wlo];
+          c_hi = c_col[cs + wlo + wn - 1];
+        }
         for (int32_t e = tid; e < wn; e += kHT) sacc[e] = 0.0f;
         for (int32_t pc = p0; pc < p1; pc += kHStage) {
           // (heavy_stage's barriers also publish gpre and the zeroed window)
-          const long long total = heavy_stage<true>(op, pc, p1, sh.st);
+          const long long total = heavy_stage<true>(op, pc, p1, sh.st, c_lo, c_hi);
           const int na = min(kHStage, p1 - pc);
           if (total >= static_cast<long long>(kStepMinAvgLen) * na)
             heavy_steps(op, sh.st, na, hbits, gpre, sacc, wlo, wn, missing);

@@ -694,7 +694,7 @@ rvsp_status_t rvsp_cuda_numeric(rvsp_cuda_plan_t p, void *stream,
       PhaseScope ph(p, s, RVSP_PHASE_COMPACT);
       launch_compact(p->a_rows, p->counts.p, p->slab_off.p, c_row_ptr, p->slab_col.p,
                      p->slab_val.p, c_col_idx, c_values, true, p->num_sms, s);
-      ph.launches = 1;
+      ph.launches = 2;
       for (int c = kEmpty_ + 1; c < kNumClasses && p->n_ovf > 0; ++c) {
         if (p->ovf_num_count[c] <= 0) continue;
         launch_numeric_class(c, op, p->ops.p, p->ovf_sorted.p + p->ovf_num_off[c],
