@@ -51,7 +51,18 @@ WORKLOADS = {
     "stencil3d_reuse": "3D 27-point stencil 128^3, C=A*A, numeric-only repeats (values perturbed U[-0.01,0.01])",
     "rmat16": "R-MAT n=2^16, 16 edges/row, (0.57,0.19,0.19,0.05), values U(0,1], C=A*A, full product",
     "rmat18": "R-MAT n=2^18, 16 edges/row, (0.57,0.19,0.19,0.05), values U(0,1], C=A*A, full product",
+    "batch512": ("512 independent products C_i=A_i*B_i, n log-uniform in [256, 65536], "
+                 "Poisson(mu) row lengths with mu U[8,32], uniform columns, values U[-1,1]; "
+                 "one batch analysis + fill, then numeric-only repeats with every value "
+                 "redrawn (CUDA graph replay)"),
 }
+
+BATCH_COUNT, BATCH_SEED = 512, 7
+
+
+def batch_inputs():
+    from rvsp import gen
+    return gen.batched_products(count=BATCH_COUNT, seed=BATCH_SEED)
 
 
 def build_inputs(name: str, seed: int = 2024):
@@ -153,21 +164,37 @@ def run_reference(args, world, rank):
     sys.path.insert(0, str(ROOT))
     from oracle import oracle
     from rvsp import intermediate_products
-    A, B = build_inputs(args.workload)
-    flops = 2.0 * float(intermediate_products(A, B).sum())
     threads = os.cpu_count() or 1
     kind = "reference" if oracle.ref_available() else "port"
-    per_step = []
-    for i in range(args.warmup + args.steps):
-        runs, el = oracle.time_reference_oneshot(A, B, seconds=0.0, threads=threads,
-                                                 max_runs=threads)
-        if i >= args.warmup:
-            per_step.append((runs, el))
-    runs = sum(r for r, _ in per_step)
-    el = sum(e for _, e in per_step)
-    value = flops * runs / el / 1e9
-    sample = (f"{runs} full one-shot products of {args.workload} "
-              f"({args.steps} steps x {threads} threads)")
+    if args.workload == "batch512":
+        # each step: the next `threads` products of the batch, one per thread
+        prods = batch_inputs()
+        pflops = [2.0 * float(intermediate_products(A, B).sum()) for A, B in prods]
+        fl, el = 0.0, 0.0
+        for i in range(args.warmup + args.steps):
+            lo = (i * threads) % len(prods)
+            sample = [prods[(lo + j) % len(prods)] for j in range(threads)]
+            done, t = oracle.time_reference_batch(sample, seconds=1e9, threads=threads)
+            if i >= args.warmup:
+                fl += sum(pflops[(lo + j) % len(prods)] for j in done)
+                el += t
+        value = fl / el / 1e9
+        sample = (f"{args.steps * threads} of the {len(prods)} products, one per thread "
+                  f"({args.steps} steps x {threads} threads)")
+    else:
+        A, B = build_inputs(args.workload)
+        flops = 2.0 * float(intermediate_products(A, B).sum())
+        per_step = []
+        for i in range(args.warmup + args.steps):
+            runs, el = oracle.time_reference_oneshot(A, B, seconds=0.0, threads=threads,
+                                                     max_runs=threads)
+            if i >= args.warmup:
+                per_step.append((runs, el))
+        runs = sum(r for r, _ in per_step)
+        el = sum(e for _, e in per_step)
+        value = flops * runs / el / 1e9
+        sample = (f"{runs} full one-shot products of {args.workload} "
+                  f"({args.steps} steps x {threads} threads)")
     line = {"metric": METRIC, "value": value, "unit": UNIT, "impl": "reference",
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": 1e3 * el / max(args.steps, 1), "higher_is_better": True,
@@ -178,6 +205,189 @@ def run_reference(args, world, rank):
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_batch(args, world, rank, local):
+    """batch512: the batch API in device memory space.  A step is one
+    numeric-only compute of all 512 products (the captured graph: value
+    refresh + numeric pass of every group) after every value of every A_i and
+    B_i was redrawn; the redraw (device copies from pre-drawn pools) and the
+    L2 flush happen before each step's start event."""
+    import ctypes as C
+    import torch
+    import rvsp
+    from rvsp import Batch, CSR, DeviceCSR, intermediate_products
+    from rvsp import _lib as L
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    torch.cuda.set_stream(torch.cuda.Stream(dev))
+    stream = torch.cuda.current_stream(dev)
+    pg = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=dev)
+        pg = dist
+
+    prods = batch_inputs()
+    ops = [int(intermediate_products(A, B).sum()) for A, B in prods]
+    flops = 2.0 * float(sum(ops))
+    dprods = [(DeviceCSR.from_host(A, dev), DeviceCSR.from_host(B, dev)) for A, B in prods]
+    gen_t = torch.Generator(device=dev)
+    gen_t.manual_seed(11)
+    pools = [[(torch.rand(dA.nnz, generator=gen_t, device=dev) * 2 - 1,
+               torch.rand(dB.nnz, generator=gen_t, device=dev) * 2 - 1)
+              for dA, dB in dprods] for _ in range(2)]
+
+    def redraw(i):
+        for (dA, dB), (va, vb) in zip(dprods, pools[i % 2]):
+            dA.values.copy_(va)
+            dB.values.copy_(vb)
+
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    b = Batch(memory=L.MEM_DEVICE, stream=stream, autotune=True)
+    for dA, dB in dprods:
+        b.add(dA, dB)
+    torch.cuda.synchronize(dev)
+    e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+    e0.record(stream)
+    total_nnz = b.work_estimation()
+    e1.record(stream)
+    b.compute()  # first compute: columns and values
+    e2.record(stream)
+    b.synchronize()
+    analysis_ms, fill_ms = e0.elapsed_time(e1), e1.elapsed_time(e2)
+    nnz = [b.nnz(i) for i in range(len(prods))]
+    alg_bytes = sum(rvsp.algorithmic_bytes(A, B, n) for (A, B), n in zip(prods, nnz))
+
+    sampler = ClockSampler(local)
+    sampler.start()
+    for i in range(args.warmup):
+        redraw(i)
+        flush.zero_()
+        b.compute()
+    b.synchronize()
+    if pg:
+        pg.barrier()
+    torch.cuda.synchronize(dev)
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+          for _ in range(args.steps)]
+    for i in range(args.steps):
+        redraw(i)
+        flush.zero_()
+        ev[i][0].record(stream)
+        b.compute()
+        ev[i][1].record(stream)
+    torch.cuda.synchronize(dev)
+    b.synchronize()
+    clocks = sampler.stop()
+    total_ms = float(sum(a.elapsed_time(c) for a, c in ev))
+    if pg:
+        t = torch.tensor([total_ms], device=dev)
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        total_ms = float(t.item())
+    ms_per_step = total_ms / args.steps
+    value = world * flops * args.steps / (total_ms * 1e-3) / 1e9
+    stats = b.stats()
+    peak, peak_kind = measured_peaks()
+    achieved = alg_bytes / (ms_per_step * 1e-3) / 1e9
+
+    # End to end: host memory space, pinned operands; each step uploads every
+    # value (inside compute) and copies every C_i back (row_ptr, col_idx,
+    # values) into one pinned buffer sized for the largest product.
+    e2e = None
+    if rank == 0 or world > 1:
+        def pinned(x):
+            return torch.from_numpy(np.ascontiguousarray(x)).pin_memory().numpy()
+        hprods = [(CSR(A.rows, A.cols, pinned(A.row_ptr), pinned(A.col_idx), pinned(A.values)),
+                   CSR(B.rows, B.cols, pinned(B.row_ptr), pinned(B.col_idx), pinned(B.values)))
+                  for A, B in prods]
+        hb = Batch(memory=L.MEM_HOST, merge_policy=stats["merge_policy"])
+        for A, B in hprods:
+            hb.add(A, B)
+        hb.work_estimation()
+        mx_rows = max(A.rows for A, _ in prods)
+        mx_nnz = max(max(nnz), 1)
+        out_rp = pinned(np.zeros(mx_rows + 1, np.int32))
+        out_ci = pinned(np.zeros(mx_nnz, np.int32))
+        out_v = pinned(np.zeros(mx_nnz, np.float32))
+
+        def e2e_step():
+            hb.compute()
+            for i, (A, B) in enumerate(hprods):
+                c = L.CsrMatrix()
+                c.rows, c.cols, c.nnz = A.rows, B.cols, mx_nnz
+                c.row_ptr, c.col_idx = out_rp.ctypes.data, out_ci.ctypes.data
+                c.values, c.dtype = out_v.ctypes.data, L.DTYPE_FP32
+                hb.copy_result_into(i, c)
+        e2e_step()
+        e2e_step()
+        torch.cuda.synchronize(dev)
+        t0 = time.perf_counter()
+        for _ in range(args.e2e_steps):
+            e2e_step()
+        torch.cuda.synchronize(dev)
+        el = time.perf_counter() - t0
+        h2d = sum(A.values.nbytes + B.values.nbytes for A, B in prods)
+        d2h = sum(4 * (A.rows + 1) + 8 * n for (A, _), n in zip(prods, nnz))
+        e2e = {"value": world * flops * args.e2e_steps / el / 1e9, "unit": UNIT,
+               "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+               "steps": args.e2e_steps,
+               "api": "rvsp_spgemm_batch_compute + rvsp_spgemm_batch_copy_result per "
+                      "product, host memory space (numeric-only repeats)"}
+        hb.close()
+        del hprods
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        sys.path.insert(0, str(ROOT))
+        from oracle import oracle
+        threads = os.cpu_count() or 1
+        done, el = oracle.time_reference_batch(prods, seconds=12.0, threads=threads)
+        cpu = {"value": sum(2.0 * ops[i] for i in done) / el / 1e9, "unit": UNIT,
+               "cores": threads, "kind": "reference" if oracle.ref_available() else "port",
+               "sample": f"first {len(done)} of {len(prods)} products (one-shot each, "
+                         f"one per thread) on {threads} threads in {el:.1f} s"}
+
+    b.close()
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32", "data": "synthetic",
+            "config": {"workload": args.workload, "description": WORKLOADS[args.workload],
+                       "path": "batch", "products": len(prods), "seed": BATCH_SEED,
+                       "rows_total": sum(A.rows for A, _ in prods),
+                       "nnz_a_total": sum(A.nnz for A, _ in prods),
+                       "nnz_b_total": sum(B.nnz for _, B in prods),
+                       "nnz_c_total": int(total_nnz), "intermediate_products": int(sum(ops)),
+                       "flops_per_step": flops, "algorithmic_bytes_per_step": alg_bytes,
+                       "groups": stats["groups"],
+                       "merge_policy_autotuned": stats["merge_policy"],
+                       "graph_nodes": stats["graph_nodes"],
+                       "analysis_ms": analysis_ms, "first_fill_ms": fill_ms,
+                       "first_product_gflops": flops / ((analysis_ms + fill_ms) * 1e-3) / 1e9,
+                       "l2": "flushed between steps (256 MiB write outside the step events)",
+                       "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
+            "hbm_frac": achieved / peak,
+            "roofline": {"bound": "hbm", "kernel": "numeric-only batch graph",
+                         "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak,
+                         "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)"
+                         if peak_kind == "measured" else "fallback 6.65 TB/s",
+                         "traffic": committed_traffic(args.workload, "numeric"),
+                         "algorithmic_bytes_per_launch": alg_bytes},
+            "clocks": clocks, "e2e": e2e, "gpu_launches": stats["graph_nodes"],
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    if pg:
+        pg.barrier()
+        pg.destroy_process_group()
     return 0
 
 
@@ -209,6 +419,8 @@ def main():
 
     if args.impl == "reference":
         return run_reference(args, world, rank)
+    if args.workload == "batch512":
+        return run_batch(args, world, rank, local)
 
     import torch
     import rvsp

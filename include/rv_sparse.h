@@ -193,6 +193,76 @@ rvsp_status_t rvsp_spgemm_csr_device(const rvsp_csr_matrix_t *A,
                                      rvsp_csr_matrix_t *C,
                                      const rvsp_spgemm_options_t *options);
 
+/* ---- Batches (new; the reference computes one product per call) ---------
+ *
+ * Many independent products C_i = A_i * B_i of any sizes, computed together:
+ *
+ *   rvsp_spgemm_batch_create(&b);
+ *   rvsp_spgemm_batch_add(b, &A_i, &B_i, &i);       for each product
+ *   rvsp_spgemm_batch_work_estimation(b, &nnz);     structure of every C_i
+ *   rvsp_spgemm_batch_compute(b);                   columns and values
+ *   ... change the values of the A_i / B_i in place ...
+ *   rvsp_spgemm_batch_compute(b);                   values only (graph replay)
+ *   rvsp_spgemm_batch_get_result(b, i, &C_i);       device view of C_i
+ *   rvsp_spgemm_batch_destroy(b);
+ *
+ * The batch keeps the A_i / B_i structs given to add (not copies of their
+ * arrays): their arrays must stay valid, with unchanged structure, until
+ * destroy; their values may change between computes.  Host memory space
+ * (the default) takes host arrays; RVSP_MEM_DEVICE takes device arrays.
+ *
+ * work_estimation checks every operand (RVSP_ERROR_INVALID_CSR as
+ * rvsp_spgemm_work_estimation does), packs the products into groups of at
+ * most INT32_MAX intermediate products (multiply-adds) each, which keeps
+ * every group's nnz(C) in int32, and runs one symbolic pass per group; every
+ * row class is one launch over the rows of every product of the group.  The
+ * first compute fills columns and values; every later compute is a
+ * numeric-only repeat, captured into a CUDA graph on its first run and
+ * replayed after.  Results are bit-identical to computing each product on
+ * its own.  With autotune on, work_estimation times the merge-accumulator
+ * policies (automatic, never, always) on the batch's own rows and keeps the
+ * fastest. */
+typedef struct rvsp_spgemm_batch *rvsp_spgemm_batch_t;
+
+rvsp_status_t rvsp_spgemm_batch_create(rvsp_spgemm_batch_t *batch);
+void rvsp_spgemm_batch_destroy(rvsp_spgemm_batch_t batch);
+/* Before the first add. */
+rvsp_status_t rvsp_spgemm_batch_set_memory_space(rvsp_spgemm_batch_t batch,
+                                                 rvsp_memory_space_t space);
+/* cudaStream_t for all device work of the batch (NULL: its own stream). */
+rvsp_status_t rvsp_spgemm_batch_set_stream(rvsp_spgemm_batch_t batch, void *stream);
+rvsp_status_t rvsp_spgemm_batch_set_autotune(rvsp_spgemm_batch_t batch, int enable);
+rvsp_status_t rvsp_spgemm_batch_set_merge_policy(rvsp_spgemm_batch_t batch, int32_t policy);
+/* Largest op count of one group (default INT32_MAX; smaller values split a
+ * batch into more groups). */
+rvsp_status_t rvsp_spgemm_batch_set_group_ops(rvsp_spgemm_batch_t batch, int64_t max_ops);
+/* Refused after work_estimation (RVSP_ERROR_INVALID_ARGUMENT); A->cols must
+ * equal B->rows, both FP32. */
+rvsp_status_t rvsp_spgemm_batch_add(rvsp_spgemm_batch_t batch, const rvsp_csr_matrix_t *A,
+                                    const rvsp_csr_matrix_t *B, int32_t *index_out);
+rvsp_status_t rvsp_spgemm_batch_work_estimation(rvsp_spgemm_batch_t batch,
+                                                int64_t *total_nnz_out);
+rvsp_status_t rvsp_spgemm_batch_compute(rvsp_spgemm_batch_t batch);
+/* Waits for the batch's work and reports device-side errors. */
+rvsp_status_t rvsp_spgemm_batch_synchronize(rvsp_spgemm_batch_t batch);
+rvsp_status_t rvsp_spgemm_batch_get_nnz(rvsp_spgemm_batch_t batch, int32_t index,
+                                        int32_t *nnz_out);
+/* C_i as a CSR of DEVICE arrays owned by the batch (owns_data = 0), valid
+ * until the next work_estimation or destroy; values are current after the
+ * last compute. */
+rvsp_status_t rvsp_spgemm_batch_get_result(rvsp_spgemm_batch_t batch, int32_t index,
+                                           rvsp_csr_matrix_t *C_out);
+/* Copies C_i into the caller's HOST arrays of C (row_ptr of rows + 1
+ * entries, col_idx and values of at least nnz); synchronizes. */
+rvsp_status_t rvsp_spgemm_batch_copy_result(rvsp_spgemm_batch_t batch, int32_t index,
+                                            rvsp_csr_matrix_t *C);
+/* Groups, total products (op count), the merge policy in use and the nodes
+ * of the numeric-only graph (0 before its first capture); NULL outputs are
+ * skipped. */
+rvsp_status_t rvsp_spgemm_batch_get_stats(rvsp_spgemm_batch_t batch, int32_t *groups_out,
+                                          int64_t *ops_out, int32_t *merge_policy_out,
+                                          int32_t *graph_nodes_out);
+
 #ifdef __cplusplus
 }
 #endif

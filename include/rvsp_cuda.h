@@ -218,6 +218,63 @@ rvsp_status_t rvsp_cuda_numeric_noalloc(void *stream, int32_t a_rows,
                                         const int32_t *c_col_idx,
                                         float *c_values);
 
+/* ---- Batches ------------------------------------------------------------
+ * No reference counterpart: the reference computes one product per call.
+ * A batch of independent products C_i = A_i * B_i is packed, a group of
+ * products at a time, into one operand pair: A_g stacks the rows of the A_i
+ * with each column index offset by the first row of B_i inside B_g, and B_g
+ * stacks the rows of the B_i with their own column indices.  Row r of
+ * A_g * B_g is then the matching row of its C_i, with the same terms in the
+ * same order, and one symbolic and one numeric pass (one launch per row
+ * class over the rows of every product) compute the whole group. */
+
+/* One product, device pointers.  a_nnz / b_nnz are the entry counts
+ * (row_ptr[rows]); rvsp_cuda_batch_entries fills them in. */
+typedef struct {
+    int32_t a_rows, b_rows, b_cols;
+    int32_t a_nnz, b_nnz;
+    const int32_t *a_row_ptr, *a_col_idx;
+    const float *a_values;
+    const int32_t *b_row_ptr, *b_col_idx;
+    const float *b_values;
+} rvsp_cuda_batch_item_t;
+
+/* Where product i of a group starts inside A_g and B_g. */
+typedef struct {
+    int32_t a_row, a_nnz, b_row, b_nnz;
+} rvsp_cuda_batch_offset_t;
+
+/* items[i].a_nnz = a_row_ptr[a_rows] and items[i].b_nnz = b_row_ptr[b_rows]
+ * for the `count` products of the device array `items`. */
+rvsp_status_t rvsp_cuda_batch_entries(void *stream, rvsp_cuda_batch_item_t *items,
+                                      int32_t count);
+
+/* ops[i] += the products of item i (sum over A_i's nonzeros of the length of
+ * the B_i row they select); *err |= 1 when an A_i column is not a B_i row
+ * (that nonzero is skipped). */
+rvsp_status_t rvsp_cuda_batch_op_counts(void *stream, const rvsp_cuda_batch_item_t *items,
+                                        int32_t count, int64_t *ops, int32_t *err);
+
+/* Packs the `count` products of `items` at offsets `off` into A_g and B_g:
+ * structure and values when with_structure, values only otherwise.  *err
+ * |= 2 / 4 for an A / B column out of range, 8 for a row_ptr[0] != 0. */
+rvsp_status_t rvsp_cuda_batch_pack(void *stream, const rvsp_cuda_batch_item_t *items,
+                                   const rvsp_cuda_batch_offset_t *off, int32_t count,
+                                   int with_structure, int32_t *a_row_ptr,
+                                   int32_t *a_col_idx, float *a_values,
+                                   int32_t *b_row_ptr, int32_t *b_col_idx,
+                                   float *b_values, int32_t *err);
+
+/* Per-product views of C_g (row_ptr from 0):
+ * c_rp_out[crp_off[i] + r] = c_row_ptr[off[i].a_row + r] -
+ * c_row_ptr[off[i].a_row] for r = 0 .. a_rows, base_out[i] =
+ * c_row_ptr[off[i].a_row] and nnz_out[i] = the product's nnz. */
+rvsp_status_t rvsp_cuda_batch_views(void *stream, const rvsp_cuda_batch_item_t *items,
+                                    const rvsp_cuda_batch_offset_t *off,
+                                    const int64_t *crp_off, int32_t count,
+                                    const int32_t *c_row_ptr, int32_t *c_rp_out,
+                                    int32_t *base_out, int32_t *nnz_out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -268,3 +268,39 @@ def time_reference_oneshot(A, B, seconds: float = 10.0, threads: int = 1,
     for th in ths:
         th.join()
     return sum(done), time.perf_counter() - t0
+
+
+def time_reference_batch(products, seconds: float = 10.0, threads: int = 1):
+    """Times the reference one-shot product over a list of (A, B) pairs taken
+    in order by `threads` Python threads (one product per call, as a CPU
+    batch would run), stopping once `seconds` have passed.  Returns (indices
+    of the products done, elapsed_s)."""
+    import threading
+    use_ref = ref_available()
+    lock = threading.Lock()
+    nxt = [0]
+    done = []
+    stop_at = time.perf_counter() + seconds
+
+    def worker():
+        while True:
+            with lock:
+                if nxt[0] >= len(products) or time.perf_counter() >= stop_at:
+                    return
+                i = nxt[0]
+                nxt[0] += 1
+            A, B = products[i]
+            if use_ref:
+                ref_spgemm(A, B)
+            else:
+                spgemm(A, B)
+            with lock:
+                done.append(i)
+
+    t0 = time.perf_counter()
+    ths = [threading.Thread(target=worker) for _ in range(threads)]
+    for th in ths:
+        th.start()
+    for th in ths:
+        th.join()
+    return sorted(done), time.perf_counter() - t0

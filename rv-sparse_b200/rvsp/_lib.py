@@ -137,6 +137,28 @@ SIGNATURES = {
     "rvsp_spgemm_set_capacity_scale": (_int, [_vp, C.c_float]),
     "rvsp_spgemm_get_overflow_rows": (_int, [_vp, _P(_i32)]),
     "rvsp_spgemm_multiply": (_int, [_vp, _P(CsrMatrix), _P(CsrMatrix), _P(CsrMatrix)]),
+    # batches (rv_sparse.h)
+    "rvsp_spgemm_batch_create": (_int, [_P(_vp)]),
+    "rvsp_spgemm_batch_destroy": (None, [_vp]),
+    "rvsp_spgemm_batch_set_memory_space": (_int, [_vp, _int]),
+    "rvsp_spgemm_batch_set_stream": (_int, [_vp, _vp]),
+    "rvsp_spgemm_batch_set_autotune": (_int, [_vp, _int]),
+    "rvsp_spgemm_batch_set_merge_policy": (_int, [_vp, _i32]),
+    "rvsp_spgemm_batch_set_group_ops": (_int, [_vp, _i64]),
+    "rvsp_spgemm_batch_add": (_int, [_vp, _P(CsrMatrix), _P(CsrMatrix), _P(_i32)]),
+    "rvsp_spgemm_batch_work_estimation": (_int, [_vp, _P(_i64)]),
+    "rvsp_spgemm_batch_compute": (_int, [_vp]),
+    "rvsp_spgemm_batch_synchronize": (_int, [_vp]),
+    "rvsp_spgemm_batch_get_nnz": (_int, [_vp, _i32, _P(_i32)]),
+    "rvsp_spgemm_batch_get_result": (_int, [_vp, _i32, _P(CsrMatrix)]),
+    "rvsp_spgemm_batch_copy_result": (_int, [_vp, _i32, _P(CsrMatrix)]),
+    "rvsp_spgemm_batch_get_stats": (_int, [_vp, _P(_i32), _P(_i64), _P(_i32), _P(_i32)]),
+    # batches (rvsp_cuda.h)
+    "rvsp_cuda_batch_entries": (_int, [_vp, _vp, _i32]),
+    "rvsp_cuda_batch_op_counts": (_int, [_vp, _vp, _i32, _vp, _vp]),
+    "rvsp_cuda_batch_pack": (_int, [_vp, _vp, _vp, _i32, _int, _vp, _vp, _vp, _vp, _vp,
+                                    _vp, _vp]),
+    "rvsp_cuda_batch_views": (_int, [_vp, _vp, _vp, _vp, _i32, _vp, _vp, _vp, _vp]),
 }
 
 _lib = None

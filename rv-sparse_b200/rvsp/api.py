@@ -275,3 +275,109 @@ class DeviceResult:
             self.free()
         except Exception:
             pass
+
+
+class Batch:
+    """rvsp_spgemm_batch_t: many independent products computed together.
+
+    Operands are host CSRs (memory=MEM_HOST) or DeviceCSRs (MEM_DEVICE).  The
+    batch keeps references to them: change their values in place between
+    computes (numeric-only repeats), never their structure."""
+
+    def __init__(self, memory: int = L.MEM_HOST, stream=None, autotune: bool = False,
+                 merge_policy: int | None = None, group_ops: int | None = None):
+        self.lib = L.load()
+        self.h = C.c_void_p()
+        L.check(self.lib.rvsp_spgemm_batch_create(C.byref(self.h)), "batch_create")
+        if memory != L.MEM_HOST:
+            L.check(self.lib.rvsp_spgemm_batch_set_memory_space(self.h, memory),
+                    "batch_set_memory_space")
+        if stream is not None:
+            ptr = stream.cuda_stream if hasattr(stream, "cuda_stream") else stream
+            L.check(self.lib.rvsp_spgemm_batch_set_stream(
+                self.h, C.c_void_p(ptr or CUDA_STREAM_LEGACY)), "batch_set_stream")
+        if autotune:
+            L.check(self.lib.rvsp_spgemm_batch_set_autotune(self.h, 1), "batch_set_autotune")
+        if merge_policy is not None:
+            L.check(self.lib.rvsp_spgemm_batch_set_merge_policy(self.h, merge_policy),
+                    "batch_set_merge_policy")
+        if group_ops is not None:
+            L.check(self.lib.rvsp_spgemm_batch_set_group_ops(self.h, group_ops),
+                    "batch_set_group_ops")
+        self.memory = memory
+        self.operands = []
+        self.total_nnz = None
+
+    def add(self, A, B) -> int:
+        a, b = A.struct(), B.struct()
+        idx = C.c_int32()
+        L.check(self.lib.rvsp_spgemm_batch_add(self.h, C.byref(a), C.byref(b),
+                                               C.byref(idx)), "batch_add")
+        self.operands.append((A, B))
+        return idx.value
+
+    def work_estimation(self) -> int:
+        n = C.c_int64()
+        L.check(self.lib.rvsp_spgemm_batch_work_estimation(self.h, C.byref(n)),
+                "batch_work_estimation")
+        self.total_nnz = n.value
+        return n.value
+
+    def compute(self) -> None:
+        L.check(self.lib.rvsp_spgemm_batch_compute(self.h), "batch_compute")
+
+    def synchronize(self) -> None:
+        L.check(self.lib.rvsp_spgemm_batch_synchronize(self.h), "batch_synchronize")
+
+    def nnz(self, i: int) -> int:
+        n = C.c_int32()
+        L.check(self.lib.rvsp_spgemm_batch_get_nnz(self.h, i, C.byref(n)), "batch_get_nnz")
+        return n.value
+
+    def result(self, i: int) -> CSR:
+        """C_i copied to host arrays (rvsp_spgemm_batch_copy_result)."""
+        A, B = self.operands[i]
+        n = self.nnz(i)
+        out = CSR(A.rows, B.cols, np.zeros(A.rows + 1, np.int32),
+                  np.zeros(max(n, 1), np.int32), np.zeros(max(n, 1), np.float32))
+        c = out.struct(nnz=max(n, 1))
+        L.check(self.lib.rvsp_spgemm_batch_copy_result(self.h, i, C.byref(c)),
+                "batch_copy_result")
+        return CSR(out.rows, out.cols, out.row_ptr, out.col_idx[:n], out.values[:n])
+
+    def copy_result_into(self, i: int, c: L.CsrMatrix) -> None:
+        """rvsp_spgemm_batch_copy_result into a caller-built struct."""
+        L.check(self.lib.rvsp_spgemm_batch_copy_result(self.h, i, C.byref(c)),
+                "batch_copy_result")
+
+    def view(self, i: int) -> L.CsrMatrix:
+        """C_i as device arrays owned by the batch (rvsp_spgemm_batch_get_result)."""
+        c = L.CsrMatrix()
+        L.check(self.lib.rvsp_spgemm_batch_get_result(self.h, i, C.byref(c)),
+                "batch_get_result")
+        return c
+
+    def stats(self):
+        g, ops, pol, nodes = C.c_int32(), C.c_int64(), C.c_int32(), C.c_int32()
+        L.check(self.lib.rvsp_spgemm_batch_get_stats(self.h, C.byref(g), C.byref(ops),
+                                                     C.byref(pol), C.byref(nodes)),
+                "batch_get_stats")
+        return {"groups": g.value, "ops": ops.value, "merge_policy": pol.value,
+                "graph_nodes": nodes.value}
+
+    def close(self):
+        if self.h:
+            self.lib.rvsp_spgemm_batch_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
