@@ -218,6 +218,25 @@ rvsp_status_t rvsp_cuda_numeric_noalloc(void *stream, int32_t a_rows,
                                         const int32_t *c_col_idx,
                                         float *c_values);
 
+/* Reuse map (no reference counterpart; the reference's numeric-only reuse,
+ * spgemm_descr.c:330-351, reruns its dense accumulator).  Builds, for the
+ * analysed structure already written into c_row_ptr / c_col_idx, the
+ * position in C's row of every product of the warp-per-row rows (uint16 per
+ * product, at most 24 GiB and a quarter of free device memory); later
+ * rvsp_cuda_numeric calls with fill == 0 and this c_col_idx use it instead
+ * of hashing C's columns.  rvsp_cuda_numeric builds it by itself on its first
+ * numeric-only call outside stream capture; call this first when the repeats
+ * will be captured.  *map_entries_out = products mapped (0 when the map does
+ * not apply).  Synchronizes `stream`. */
+rvsp_status_t rvsp_cuda_plan_prepare_reuse(rvsp_cuda_plan_t plan, void *stream,
+                                           const int32_t *a_row_ptr,
+                                           const int32_t *a_col_idx,
+                                           const int32_t *b_row_ptr,
+                                           const int32_t *b_col_idx,
+                                           const int32_t *c_row_ptr,
+                                           const int32_t *c_col_idx,
+                                           int64_t *map_entries_out);
+
 /* ---- Batches ------------------------------------------------------------
  * No reference counterpart: the reference computes one product per call.
  * A batch of independent products C_i = A_i * B_i is packed, a group of

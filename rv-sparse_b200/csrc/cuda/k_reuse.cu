@@ -1,0 +1,227 @@
+// Reuse map: numeric-only repeats of the warp-per-row (W<T>) classes.
+//
+// A numeric-only compute (structure already in C) must find, for every
+// product, the position of its column in C's row; the plain reuse kernel
+// does that with a hash of C's row, rebuilt on every call.  The reuse map
+// does it once per structure: map[moff[row] + t] is the position in C's row
+// of the row's t-th product in flattened order (ascending A nonzero, then B
+// position), as uint16 (a W<T> row has at most T/2 <= 1024 outputs).  The
+// repeats then skip B's column indices and every hash probe:
+//
+//   acc[map[k]] += a * b_val      in a shared-memory accumulator of m floats
+//
+// Order is the plain path's: stepping (one A nonzero at a time, lanes over
+// its B row, whose positions are distinct) for long B rows, flattened tiles
+// with ordered_apply for short ones; each output receives its terms in
+// ascending A-nonzero order from +0.0f, rounded separately
+// (gustavson_core_f32.inc:31-62, accum_scalar_f32.c:20-71).
+#include <climits>
+
+#include "device_common.cuh"
+#include "kernels.cuh"
+
+namespace rvsp {
+
+namespace {
+
+constexpr int kMapSteppingMinAvgLen = 16;  // same rule as the plain walkers
+
+__global__ void __launch_bounds__(256)
+map_ops_kernel(const int32_t *__restrict__ rows, int32_t nrows,
+               const int64_t *__restrict__ ops, int32_t *__restrict__ mops,
+               int32_t *__restrict__ too_long) {
+  const int32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nrows) return;
+  const int32_t row = row_of(rows, i);
+  const int64_t o = ops[row];
+  if (o > INT32_MAX / 2) {
+    atomicOr(too_long, 1);
+    return;
+  }
+  mops[row] = static_cast<int32_t>(o);
+}
+
+// Shared memory per warp: keys[T] i32 | posv[T] i32 = 8 T bytes.
+template <int LOG2T>
+__global__ void __launch_bounds__(kWarpsPerBlock * 32)
+map_build_kernel(Operands op, const int32_t *__restrict__ rows, int32_t nrows,
+                 const int32_t *__restrict__ c_rp, const int32_t *__restrict__ c_col,
+                 const int64_t *__restrict__ moff, uint16_t *__restrict__ map,
+                 int32_t *__restrict__ status) {
+  constexpr int T = 1 << LOG2T;
+  extern __shared__ __align__(16) int32_t smem_i32[];
+  int32_t *keys = smem_i32 + size_t(threadIdx.x >> 5) * 2 * T;
+  int32_t *posv = keys + T;
+  const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (w >= nrows) return;
+  const int lane = lane_id();
+  fill_words(keys, T, 0xffffffffu, lane, 32);
+  __syncwarp();
+  const int32_t row = row_of(rows, w);
+  const int32_t cs = c_rp[row];
+  const int m = c_rp[row + 1] - cs;
+  bool bad = false;
+  for (int e = lane; e < m; e += 32) {
+    bool created;
+    const int s = hash_insert(keys, LOG2T, __ldg(c_col + cs + e), created);
+    if (s >= 0) posv[s] = e;
+    else bad = true;
+  }
+  __syncwarp();
+  const int64_t base = moff[row];
+  const int32_t p0 = op.a_rp[row], p1 = op.a_rp[row + 1];
+  int64_t run = 0;
+  for (int32_t p = p0; p < p1; p += 32) {
+    const AChunk c = load_chunk(op.a_col, op.a_val, op.b_rp, p + lane, p1, false);
+    for (int t0 = 0; t0 < c.total; t0 += 32) {
+      const int t = t0 + lane;
+      const bool v = t < c.total;
+      const int j = warp_owner_of(c.incl, v ? t : 0);
+      const int excl = __shfl_sync(kFull, c.incl - c.len, j);
+      const int bbeg = __shfl_sync(kFull, c.bbeg, j);
+      if (v) {
+        const int s = hash_find(keys, LOG2T, __ldg(op.b_col + bbeg + (t - excl)));
+        if (s < 0) bad = true;
+        map[base + run + t] = s >= 0 ? static_cast<uint16_t>(posv[s]) : uint16_t(0xffff);
+      }
+    }
+    run += c.total;
+  }
+  if (__any_sync(kFull, bad) && lane == 0) report(status, kDevKeyMissing);
+}
+
+// Shared memory per warp: acc[T/2] f32 = 2 T bytes.
+template <int LOG2T>
+__global__ void __launch_bounds__(kWarpsPerBlock * 32)
+map_numeric_kernel(Operands op, const int64_t *__restrict__ ops,
+                   const int32_t *__restrict__ rows, int32_t nrows,
+                   const int32_t *__restrict__ c_rp, float *__restrict__ c_val,
+                   const int64_t *__restrict__ moff, const uint16_t *__restrict__ map,
+                   int32_t *__restrict__ status) {
+  constexpr int H = 1 << (LOG2T - 1);
+  extern __shared__ __align__(16) float smem_f32[];
+  float *acc = smem_f32 + size_t(threadIdx.x >> 5) * H;
+  const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (w >= nrows) return;
+  const int lane = lane_id();
+  const int32_t row = row_of(rows, w);
+  const int32_t cs = c_rp[row];
+  const int m = c_rp[row + 1] - cs;
+  for (int e = lane; e < m; e += 32) acc[e] = 0.0f;
+  __syncwarp();
+  const int64_t base = moff[row];
+  const int32_t p0 = op.a_rp[row], p1 = op.a_rp[row + 1];
+  const bool stepping =
+      ops[row] >= static_cast<int64_t>(kMapSteppingMinAvgLen) * (p1 - p0);
+  bool bad = false;
+  int64_t run = 0;
+  for (int32_t p = p0; p < p1; p += 32) {
+    const AChunk c = load_chunk(op.a_col, op.a_val, op.b_rp, p + lane, p1, true);
+    if (stepping) {
+      const int cnt = min(32, p1 - p);
+      for (int jj = 0; jj < cnt; ++jj) {
+        const int len = __shfl_sync(kFull, c.len, jj);
+        const int bbeg = __shfl_sync(kFull, c.bbeg, jj);
+        const float a = __shfl_sync(kFull, c.a, jj);
+        const int64_t k0 = base + run + __shfl_sync(kFull, c.incl - c.len, jj);
+        for (int e = lane; e < len; e += 32) {
+          const int pos = __ldg(map + k0 + e);
+          const float term = __fmul_rn(a, __ldg(op.b_val + bbeg + e));
+          if (pos < m) acc[pos] = __fadd_rn(acc[pos], term);
+          else bad = true;
+        }
+        __syncwarp();
+      }
+    } else {
+      for (int t0 = 0; t0 < c.total; t0 += 32) {
+        const int t = t0 + lane;
+        bool v = t < c.total;
+        const int j = warp_owner_of(c.incl, v ? t : 0);
+        const int excl = __shfl_sync(kFull, c.incl - c.len, j);
+        const int bbeg = __shfl_sync(kFull, c.bbeg, j);
+        const float a = __shfl_sync(kFull, c.a, j);
+        int pos = 0;
+        float term = 0.0f;
+        if (v) {
+          pos = __ldg(map + base + run + t);
+          if (pos >= m) {
+            bad = true;
+            v = false;
+          } else {
+            term = __fmul_rn(a, __ldg(op.b_val + bbeg + (t - excl)));
+          }
+        }
+        ordered_apply(acc, v, pos, term);
+      }
+    }
+    run += c.total;
+  }
+  __syncwarp();
+  for (int e = lane; e < m; e += 32) c_val[cs + e] = acc[e];
+  if (__any_sync(kFull, bad) && lane == 0) report(status, kDevKeyMissing);
+}
+
+template <int LOG2T>
+void launch_build(const Operands &op, const int32_t *rows, int32_t nrows,
+                  const int32_t *c_rp, const int32_t *c_col, const int64_t *moff,
+                  uint16_t *map, int32_t *status, cudaStream_t s) {
+  const size_t smem = size_t(kWarpsPerBlock) * 8 * (size_t(1) << LOG2T);
+  cudaFuncSetAttribute(map_build_kernel<LOG2T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       static_cast<int>(smem));
+  const int grid = (nrows + kWarpsPerBlock - 1) / kWarpsPerBlock;
+  map_build_kernel<LOG2T><<<grid, kWarpsPerBlock * 32, smem, s>>>(op, rows, nrows, c_rp,
+                                                                  c_col, moff, map, status);
+}
+
+template <int LOG2T>
+void launch_numeric(const Operands &op, const int64_t *ops, const int32_t *rows,
+                    int32_t nrows, const int32_t *c_rp, float *c_val, const int64_t *moff,
+                    const uint16_t *map, int32_t *status, cudaStream_t s) {
+  const size_t smem = size_t(kWarpsPerBlock) * 2 * (size_t(1) << LOG2T);
+  const int grid = (nrows + kWarpsPerBlock - 1) / kWarpsPerBlock;
+  map_numeric_kernel<LOG2T><<<grid, kWarpsPerBlock * 32, smem, s>>>(
+      op, ops, rows, nrows, c_rp, c_val, moff, map, status);
+}
+
+}  // namespace
+
+bool map_class(int cls) { return cls >= kW64 && cls <= kW2048; }
+
+void launch_map_ops(const int32_t *rows, int32_t nrows, const int64_t *ops, int32_t *mops,
+                    int32_t *too_long, cudaStream_t s) {
+  if (nrows <= 0) return;
+  map_ops_kernel<<<(nrows + 255) / 256, 256, 0, s>>>(rows, nrows, ops, mops, too_long);
+}
+
+void launch_map_build(int cls, const Operands &op, const int32_t *rows, int32_t nrows,
+                      const int32_t *c_rp, const int32_t *c_col, const int64_t *moff,
+                      uint16_t *map, int32_t *status, cudaStream_t s) {
+  if (nrows <= 0) return;
+  switch (cls) {
+    case kW64: launch_build<6>(op, rows, nrows, c_rp, c_col, moff, map, status, s); break;
+    case kW128: launch_build<7>(op, rows, nrows, c_rp, c_col, moff, map, status, s); break;
+    case kW256: launch_build<8>(op, rows, nrows, c_rp, c_col, moff, map, status, s); break;
+    case kW512: launch_build<9>(op, rows, nrows, c_rp, c_col, moff, map, status, s); break;
+    case kW1024: launch_build<10>(op, rows, nrows, c_rp, c_col, moff, map, status, s); break;
+    case kW2048: launch_build<11>(op, rows, nrows, c_rp, c_col, moff, map, status, s); break;
+    default: break;
+  }
+}
+
+void launch_map_numeric(int cls, const Operands &op, const int64_t *ops, const int32_t *rows,
+                        int32_t nrows, const int32_t *c_rp, float *c_val,
+                        const int64_t *moff, const uint16_t *map, int32_t *status,
+                        cudaStream_t s) {
+  if (nrows <= 0) return;
+  switch (cls) {
+    case kW64: launch_numeric<6>(op, ops, rows, nrows, c_rp, c_val, moff, map, status, s); break;
+    case kW128: launch_numeric<7>(op, ops, rows, nrows, c_rp, c_val, moff, map, status, s); break;
+    case kW256: launch_numeric<8>(op, ops, rows, nrows, c_rp, c_val, moff, map, status, s); break;
+    case kW512: launch_numeric<9>(op, ops, rows, nrows, c_rp, c_val, moff, map, status, s); break;
+    case kW1024: launch_numeric<10>(op, ops, rows, nrows, c_rp, c_val, moff, map, status, s); break;
+    case kW2048: launch_numeric<11>(op, ops, rows, nrows, c_rp, c_val, moff, map, status, s); break;
+    default: break;
+  }
+}
+
+}  // namespace rvsp

@@ -191,6 +191,23 @@ void launch_heavy_numeric(const Operands &op, const int32_t *rows, int32_t nrows
                           int32_t *status, const FusedOut *fo, int num_sms,
                           cudaStream_t s);
 
+// ---- k_reuse.cu ------------------------------------------------------------
+// Reuse map of the W<T> classes: per product, its position in C's row.
+bool map_class(int cls);
+// mops[row] = ops[row] for the listed rows (the caller zeroes mops);
+// *too_long |= 1 when a row has more than INT32_MAX / 2 products.
+void launch_map_ops(const int32_t *rows, int32_t nrows, const int64_t *ops, int32_t *mops,
+                    int32_t *too_long, cudaStream_t s);
+// map[moff[row] + t] = position in C's row of the row's t-th product.
+void launch_map_build(int cls, const Operands &op, const int32_t *rows, int32_t nrows,
+                      const int32_t *c_rp, const int32_t *c_col, const int64_t *moff,
+                      uint16_t *map, int32_t *status, cudaStream_t s);
+// Values of the listed rows of class cls from the map (structure in C).
+void launch_map_numeric(int cls, const Operands &op, const int64_t *ops, const int32_t *rows,
+                        int32_t nrows, const int32_t *c_rp, float *c_val,
+                        const int64_t *moff, const uint16_t *map, int32_t *status,
+                        cudaStream_t s);
+
 // ---- k_check.cu ------------------------------------------------------------
 // *result (initialised to ~0ull) receives min over bad rows of
 // ((row + 1) << 8 | code); row -1 means row_ptr[0] != 0.

@@ -122,6 +122,16 @@ struct rvsp_cuda_plan {
   int32_t ovf_num_off[kNumClasses] = {};
   int64_t slab_total = 0;
 
+  // Reuse map of the W<T> rows (k_reuse.cu), built for one C column array
+  // (rmap_col) of the current analysis; rmap_state 0 = not tried, 1 = built,
+  // -1 = not used (no W rows, over the memory budget, or a row too long).
+  DevArray<uint16_t> rmap;
+  DevArray<int64_t> rmap_off;
+  DevArray<int32_t> rmap_ops;
+  const int32_t *rmap_col = nullptr;
+  int rmap_state = 0;
+  int64_t rmap_entries = 0;
+
   bool profiling = false;
   struct Pending {
     cudaEvent_t a, b;
@@ -304,6 +314,9 @@ void rvsp_cuda_plan_destroy(rvsp_cuda_plan_t p) {
   if (!p) return;
   resolve_pending(p);
   for (cudaEvent_t e : p->pool) cudaEventDestroy(e);
+  p->rmap.release();
+  p->rmap_off.release();
+  p->rmap_ops.release();
   p->ops.release();
   p->cls.release();
   p->counts.release();
@@ -344,6 +357,8 @@ rvsp_status_t rvsp_cuda_symbolic(rvsp_cuda_plan_t p, void *stream, int32_t a_row
   if (a_rows <= 0 || b_rows <= 0 || b_cols <= 0) return RVSP_ERROR_INVALID_ARGUMENT;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   p->analysed = 0;
+  p->rmap_state = 0;
+  p->rmap_col = nullptr;
   const size_t n = static_cast<size_t>(a_rows);
 
   cudaError_t e = p->ops.reserve(n);
@@ -462,6 +477,8 @@ rvsp_status_t rvsp_cuda_learned_symbolic(
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   p->analysed = 0;
   p->learned = 0;
+  p->rmap_state = 0;
+  p->rmap_col = nullptr;
   const size_t n = static_cast<size_t>(a_rows);
   cudaError_t e = p->ops.reserve(n);
   if (e == cudaSuccess) e = p->cls.reserve(n);
@@ -659,6 +676,86 @@ size_t rvsp_cuda_numeric_workspace_bytes(rvsp_cuda_plan_t p) {
   return (p && p->analysed) ? p->numeric_ws : 0;
 }
 
+namespace {
+
+// The reuse map may take at most this much device memory (and a quarter of
+// what is free).
+constexpr size_t kReuseMapMaxBytes = size_t(24) << 30;
+
+// Builds the reuse map of the W<T> rows for the structure in c_col (written
+// by an earlier fill).  Leaves rmap_state -1 when the map does not apply:
+// no W rows, a row of more than INT32_MAX / 2 products, or over the memory
+// budget.  Synchronizes s.
+cudaError_t build_reuse_map(rvsp_cuda_plan *p, cudaStream_t s, const Operands &op,
+                            const int32_t *c_rp, const int32_t *c_col) {
+  p->rmap_state = -1;
+  p->rmap_col = nullptr;
+  bool any = false;
+  for (int c = kEmpty_ + 1; c < kNumClasses; ++c)
+    any = any || (map_class(c) && p->num_count[c] > 0);
+  if (!any) return cudaSuccess;
+  const size_t n = static_cast<size_t>(p->a_rows);
+  cudaError_t e = p->rmap_ops.reserve(n + 1);
+  if (e == cudaSuccess) e = p->rmap_off.reserve(n);
+  if (e != cudaSuccess) return e;
+  cudaMemsetAsync(p->rmap_ops.p, 0, (n + 1) * sizeof(int32_t), s);
+  for (int c = kEmpty_ + 1; c < kNumClasses; ++c) {
+    if (!map_class(c) || p->num_count[c] <= 0) continue;
+    const bool whole = c == p->num_whole;
+    launch_map_ops(whole ? nullptr : p->rows_num.p + p->num_off[c],
+                   whole ? p->a_rows : p->num_count[c], p->ops.p, p->rmap_ops.p,
+                   p->rmap_ops.p + n, s);
+  }
+  launch_scan_i64(p->a_rows, p->rmap_ops.p, p->rmap_off.p, p->partials.p, p->total.p, s);
+  int32_t too_long = 0;
+  int64_t entries = 0;
+  e = cudaMemcpyAsync(&entries, p->total.p, sizeof(int64_t), cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(&too_long, p->rmap_ops.p + n, sizeof(int32_t), cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) return e;
+  size_t free_b = 0, total_b = 0;
+  if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) return cudaGetLastError();
+  const size_t bytes = static_cast<size_t>(entries) * sizeof(uint16_t);
+  if (too_long || entries <= 0 || bytes > kReuseMapMaxBytes || bytes > free_b / 4)
+    return cudaSuccess;
+  if (p->rmap.reserve(static_cast<size_t>(entries)) != cudaSuccess) {
+    cudaGetLastError();  // out of memory: keep the hash path
+    return cudaSuccess;
+  }
+  for (int c = kEmpty_ + 1; c < kNumClasses; ++c) {
+    if (!map_class(c) || p->num_count[c] <= 0) continue;
+    const bool whole = c == p->num_whole;
+    launch_map_build(c, op, whole ? nullptr : p->rows_num.p + p->num_off[c],
+                     whole ? p->a_rows : p->num_count[c], c_rp, c_col, p->rmap_off.p,
+                     p->rmap.p, p->misc.p + kStatus, s);
+  }
+  p->rmap_state = 1;
+  p->rmap_col = c_col;
+  p->rmap_entries = entries;
+  return cudaGetLastError();
+}
+
+}  // namespace
+
+rvsp_status_t rvsp_cuda_plan_prepare_reuse(rvsp_cuda_plan_t p, void *stream,
+                                           const int32_t *a_row_ptr, const int32_t *a_col_idx,
+                                           const int32_t *b_row_ptr, const int32_t *b_col_idx,
+                                           const int32_t *c_row_ptr, const int32_t *c_col_idx,
+                                           int64_t *map_entries_out) {
+  if (!p || !a_row_ptr || !a_col_idx || !b_row_ptr || !b_col_idx || !c_row_ptr ||
+      !c_col_idx)
+    return RVSP_ERROR_NULL_POINTER;
+  if (!p->analysed) return RVSP_ERROR_INVALID_ARGUMENT;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  const Operands op{p->a_rows, p->b_cols, a_row_ptr, a_col_idx, nullptr,
+                    b_row_ptr, b_col_idx, nullptr,
+                    merge_allowed(p->merge_policy, p->a_rows)};
+  const cudaError_t e = build_reuse_map(p, s, op, c_row_ptr, c_col_idx);
+  if (map_entries_out) *map_entries_out = p->rmap_state == 1 ? p->rmap_entries : 0;
+  return map_cuda(e);
+}
+
 rvsp_status_t rvsp_cuda_numeric(rvsp_cuda_plan_t p, void *stream,
                                 const int32_t *a_row_ptr, const int32_t *a_col_idx,
                                 const float *a_values, const int32_t *b_row_ptr,
@@ -712,16 +809,30 @@ rvsp_status_t rvsp_cuda_numeric(rvsp_cuda_plan_t p, void *stream,
     if (p->h_vhash[0] == p->est_hash) return map_cuda(cudaGetLastError());
     fill = 0;
   }
+  if (fill == 0 && (p->rmap_state == 0 || (p->rmap_state == 1 && p->rmap_col != c_col_idx))) {
+    // First numeric-only call on this structure: build the reuse map, unless
+    // the stream is being captured (building synchronizes).
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(s, &cap) == cudaSuccess && cap == cudaStreamCaptureStatusNone) {
+      const cudaError_t e = build_reuse_map(p, s, op, c_row_ptr, c_col_idx);
+      if (e != cudaSuccess) return map_cuda(e);
+    }
+  }
+  const bool use_map = fill == 0 && p->rmap_state == 1 && p->rmap_col == c_col_idx;
   {
     PhaseScope ph(p, s, RVSP_PHASE_NUMERIC);
     for (int c = kEmpty_ + 1; c < kNumClasses; ++c) {
       if (p->num_count[c] <= 0) continue;
       const bool whole = c == p->num_whole;
-      launch_numeric_class(c, op, p->ops.p,
-                           whole ? nullptr : p->rows_num.p + p->num_off[c],
-                           whole ? p->a_rows : p->num_count[c], c_row_ptr,
-                           c_col_idx, c_values, fill != 0, dense_acc, dense_bits,
-                           p->dense_slots, p->misc.p + kStatus, p->num_sms, s);
+      const int32_t *rows = whole ? nullptr : p->rows_num.p + p->num_off[c];
+      const int32_t nrows = whole ? p->a_rows : p->num_count[c];
+      if (use_map && map_class(c))
+        launch_map_numeric(c, op, p->ops.p, rows, nrows, c_row_ptr, c_values,
+                           p->rmap_off.p, p->rmap.p, p->misc.p + kStatus, s);
+      else
+        launch_numeric_class(c, op, p->ops.p, rows, nrows, c_row_ptr, c_col_idx, c_values,
+                             fill != 0, dense_acc, dense_bits, p->dense_slots,
+                             p->misc.p + kStatus, p->num_sms, s);
       ph.launches += 1;
     }
   }

@@ -729,6 +729,16 @@ rvsp_status_t rvsp_spgemm_batch_compute(rvsp_spgemm_batch_t b)
         return st;
     if (!b->filled) {
         st = run_groups(b, 1);
+        /* The repeats are captured, so build each group's reuse map now. */
+        for (int32_t k = 0; k < b->ngroups && st == RVSP_SUCCESS; k++) {
+            const batch_group_t *g = &b->groups[k];
+            st = rvsp_cuda_plan_prepare_reuse(g->plan, b->stream, (const int32_t *)g->a_rp.p,
+                                              (const int32_t *)g->a_ci.p,
+                                              (const int32_t *)g->b_rp.p,
+                                              (const int32_t *)g->b_ci.p,
+                                              (const int32_t *)g->c_rp.p,
+                                              (const int32_t *)g->c_ci.p, NULL);
+        }
         if (st == RVSP_SUCCESS)
             b->filled = 1;
         return st;

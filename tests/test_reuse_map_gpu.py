@@ -1,0 +1,119 @@
+"""The reuse map (rvsp_cuda_plan_prepare_reuse) through the C-ABI.
+
+Numeric-only repeats of the warp-per-row classes read each product's
+position in C's row from the map instead of hashing C's columns.  Bar: the
+map covers exactly the products of those rows, and values computed through
+it are bit-exact against the oracle, for new values, for a second C buffer
+holding the same structure (the map is rebuilt for it), and when built
+implicitly by the first numeric-only call.
+"""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from oracle import oracle
+from rvsp import DeviceCSR, gen
+from rvsp import _lib as L
+
+pytestmark = pytest.mark.gpu
+
+
+def _stream():
+    import torch
+    return C.c_void_p(torch.cuda.current_stream().cuda_stream or 1)
+
+
+def _symbolic(lib, plan, dA, dB):
+    import torch
+    rp = torch.zeros(dA.rows + 1, dtype=torch.int32, device="cuda")
+    total = C.c_int64()
+    L.check(lib.rvsp_cuda_symbolic(plan, _stream(), dA.rows, dB.rows, dB.cols,
+                                   dA.row_ptr.data_ptr(), dA.col_idx.data_ptr(),
+                                   dB.row_ptr.data_ptr(), dB.col_idx.data_ptr(),
+                                   rp.data_ptr(), C.byref(total)), "symbolic")
+    return rp, total.value
+
+
+def _numeric(lib, plan, dA, dB, rp, ci, cv, fill):
+    ws_b = max(lib.rvsp_cuda_numeric_workspace_bytes(plan), 256)
+    import torch
+    ws = torch.zeros(ws_b, dtype=torch.uint8, device="cuda")
+    L.check(lib.rvsp_cuda_numeric(plan, _stream(), dA.row_ptr.data_ptr(), dA.col_idx.data_ptr(),
+                                  dA.values.data_ptr(), dB.row_ptr.data_ptr(),
+                                  dB.col_idx.data_ptr(), dB.values.data_ptr(), rp.data_ptr(),
+                                  ci.data_ptr(), cv.data_ptr(), fill, ws.data_ptr(), ws_b),
+            "numeric")
+    torch.cuda.synchronize()
+    L.check(lib.rvsp_cuda_plan_status(plan, _stream()), "status")
+
+
+def _mapped_ops(A, B, m_rows):
+    """Products of the rows the warp classes take (output nnz 33..1024 and more
+    than 16 A nonzeros or more than 2048 products, matching classify_row for a
+    matrix below the merge-class row count)."""
+    ops = oracle.spgemm(A, B)[3]
+    return int(ops[(m_rows > 0) & (2 * m_rows <= 2048)].sum())
+
+
+def test_reuse_map_explicit_and_rebuilt():
+    import torch
+    lib = L.load()
+    A = gen.uniform_rows(3000, 4000, 12, 5)
+    B = gen.random_csr(4000, 5000, 6, mean_len=20.0)
+    dA, dB = DeviceCSR.from_host(A), DeviceCSR.from_host(B)
+    plan = C.c_void_p()
+    L.check(lib.rvsp_cuda_plan_create(C.byref(plan)), "plan_create")
+    try:
+        rp, n = _symbolic(lib, plan, dA, dB)
+        ci = torch.zeros(n, dtype=torch.int32, device="cuda")
+        cv = torch.zeros(n, dtype=torch.float32, device="cuda")
+        _numeric(lib, plan, dA, dB, rp, ci, cv, 1)
+        entries = C.c_int64()
+        L.check(lib.rvsp_cuda_plan_prepare_reuse(plan, _stream(), dA.row_ptr.data_ptr(),
+                                                 dA.col_idx.data_ptr(), dB.row_ptr.data_ptr(),
+                                                 dB.col_idx.data_ptr(), rp.data_ptr(),
+                                                 ci.data_ptr(), C.byref(entries)),
+                "prepare_reuse")
+        m_rows = np.diff(rp.cpu().numpy())
+        assert entries.value == _mapped_ops(A, B, m_rows) > 0
+        for k, scale in enumerate((-0.5, 1.75)):
+            A2 = A.with_values((A.values * np.float32(scale)).astype(np.float32))
+            dA.values.copy_(torch.from_numpy(A2.values))
+            torch.cuda.synchronize()
+            cv.zero_()
+            _numeric(lib, plan, dA, dB, rp, ci, cv, 0)
+            want = oracle.spgemm(A2, B)[2]
+            assert np.array_equal(cv.cpu().numpy().view(np.uint32), want.view(np.uint32)), k
+        # a second C buffer with the same structure: the map is rebuilt for it
+        ci2, cv2 = ci.clone(), torch.zeros_like(cv)
+        torch.cuda.synchronize()
+        _numeric(lib, plan, dA, dB, rp, ci2, cv2, 0)
+        assert np.array_equal(cv2.cpu().numpy().view(np.uint32), want.view(np.uint32))
+    finally:
+        lib.rvsp_cuda_plan_destroy(plan)
+
+
+def test_reuse_map_implicit_on_stencil():
+    import torch
+    lib = L.load()
+    A = gen.stencil_3d_27(20)
+    dA = DeviceCSR.from_host(A)
+    plan = C.c_void_p()
+    L.check(lib.rvsp_cuda_plan_create(C.byref(plan)), "plan_create")
+    try:
+        rp, n = _symbolic(lib, plan, dA, dA)
+        ci = torch.zeros(n, dtype=torch.int32, device="cuda")
+        cv = torch.zeros(n, dtype=torch.float32, device="cuda")
+        _numeric(lib, plan, dA, dA, rp, ci, cv, 1)
+        rng = np.random.default_rng(3)
+        for _ in range(2):  # the first numeric-only call builds the map
+            vals = (A.values + rng.uniform(-0.01, 0.01, A.nnz)).astype(np.float32)
+            dA.values.copy_(torch.from_numpy(vals))
+            torch.cuda.synchronize()
+            _numeric(lib, plan, dA, dA, rp, ci, cv, 0)
+            A2 = A.with_values(vals)
+            want = oracle.spgemm(A2, A2)[2]
+            assert np.array_equal(cv.cpu().numpy().view(np.uint32), want.view(np.uint32))
+    finally:
+        lib.rvsp_cuda_plan_destroy(plan)
