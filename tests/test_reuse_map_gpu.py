@@ -94,6 +94,35 @@ def test_reuse_map_explicit_and_rebuilt():
         lib.rvsp_cuda_plan_destroy(plan)
 
 
+@pytest.mark.parametrize("a_len,b_len,b_cols", [(150, 20, 900), (40, 30, 700), (12, 3, 80)])
+def test_reuse_map_stepping_and_tiles(a_len, b_len, b_cols):
+    # long B rows step one A nonzero at a time; short ones (3 entries) take
+    # flattened tiles with ordered accumulation; 150 x 20 products into 900
+    # columns repeat every column many times
+    import torch
+    lib = L.load()
+    A = gen.uniform_rows(1500, 2000, a_len, 7)
+    B = gen.uniform_rows(2000, b_cols, b_len, 8)
+    dA, dB = DeviceCSR.from_host(A), DeviceCSR.from_host(B)
+    plan = C.c_void_p()
+    L.check(lib.rvsp_cuda_plan_create(C.byref(plan)), "plan_create")
+    try:
+        rp, n = _symbolic(lib, plan, dA, dB)
+        ci = torch.zeros(n, dtype=torch.int32, device="cuda")
+        cv = torch.zeros(n, dtype=torch.float32, device="cuda")
+        _numeric(lib, plan, dA, dB, rp, ci, cv, 1)
+        for scale in (0.25, -3.0):
+            A2 = A.with_values((A.values * np.float32(scale)).astype(np.float32))
+            dA.values.copy_(torch.from_numpy(A2.values))
+            torch.cuda.synchronize()
+            cv.zero_()
+            _numeric(lib, plan, dA, dB, rp, ci, cv, 0)
+            want = oracle.spgemm(A2, B)[2]
+            assert np.array_equal(cv.cpu().numpy().view(np.uint32), want.view(np.uint32))
+    finally:
+        lib.rvsp_cuda_plan_destroy(plan)
+
+
 def test_reuse_map_implicit_on_stencil():
     import torch
     lib = L.load()
