@@ -57,6 +57,12 @@ WORKLOADS = {
                  "redrawn (CUDA graph replay)"),
 }
 
+WORKLOADS["rmat20_panels"] = (
+    "R-MAT n=2^20, 16 edges/row, (0.57,0.19,0.19,0.05), values U(0,1], C=A*A as row panels "
+    "of A of at most 2^28 products each (nnz(C) ~9e9 exceeds int32), every panel a full "
+    "product per step")
+PANEL_MAX_OPS = 1 << 28
+
 BATCH_COUNT, BATCH_SEED = 512, 7
 
 
@@ -181,6 +187,25 @@ def run_reference(args, world, rank):
         value = fl / el / 1e9
         sample = (f"{args.steps * threads} of the {len(prods)} products, one per thread "
                   f"({args.steps} steps x {threads} threads)")
+    elif args.workload == "rmat20_panels":
+        # C does not fit the reference (nnz(C) ~9e9 > INT32_MAX): each step
+        # times `threads` panels of 256 rows spread over the matrix, one per
+        # thread
+        from rvsp import gen
+        A = gen.rmat(20, 16, seed=1)
+        ops = intermediate_products(A, A)
+        starts = np.linspace(0, A.rows - 256, 64).astype(int)
+        fl, el = 0.0, 0.0
+        for i in range(args.warmup + args.steps):
+            rs = [int(starts[(i * threads + j) % len(starts)]) for j in range(threads)]
+            sample = [(A.row_panel(r, r + 256), A) for r in rs]
+            done, t = oracle.time_reference_batch(sample, seconds=1e9, threads=threads)
+            if i >= args.warmup:
+                fl += sum(2.0 * float(ops[rs[j]:rs[j] + 256].sum()) for j in done)
+                el += t
+        value = fl / el / 1e9
+        sample = (f"{args.steps * threads} panels of 256 rows spread over the matrix, one "
+                  f"per thread ({args.steps} steps x {threads} threads)")
     else:
         A, B = build_inputs(args.workload)
         flops = 2.0 * float(intermediate_products(A, B).sum())
@@ -199,7 +224,8 @@ def run_reference(args, world, rank):
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": 1e3 * el / max(args.steps, 1), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-            "data": "synthetic", "config": {"workload": WORKLOADS[args.workload]},
+            "data": "synthetic",
+            "config": {"workload": args.workload, "description": WORKLOADS[args.workload]},
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": kind,
                              "sample": sample},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
@@ -391,6 +417,203 @@ def run_batch(args, world, rank, local):
     return 0
 
 
+def run_panels(args, world, rank, local):
+    """rmat20_panels: C = A x A for R-MAT 2^20 as row panels of A (each a
+    full product per step: work_estimation + compute, device memory space).
+    With N ranks the panels are shared out by op count (no data crosses GPUs;
+    each rank holds all of B), so the total work is fixed: strong scaling."""
+    import torch
+    import rvsp
+    from rvsp import CSR, Descriptor, DeviceCSR, gen, intermediate_products
+    from rvsp import _lib as L
+    from rvsp.panels import assign_panels, panel_bounds_fast
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    torch.cuda.set_stream(torch.cuda.Stream(dev))
+    stream = torch.cuda.current_stream(dev)
+    pg = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=dev)
+        pg = dist
+
+    A = gen.rmat(20, 16, seed=1)
+    ops = intermediate_products(A, A)
+    bounds = panel_bounds_fast(ops, PANEL_MAX_OPS)
+    mine = assign_panels(bounds, ops, world)[rank]
+    panels = [A.row_panel(*bounds[i]) for i in mine]
+    my_ops = int(sum(int(ops[bounds[i][0]:bounds[i][1]].sum()) for i in mine))
+    flops_all = 2.0 * float(ops.sum())
+    dB = DeviceCSR.from_host(A, dev)
+    dP = [DeviceCSR.from_host(P, dev) for P in panels]
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+
+    model = None
+    algo = L.ALGO_CUDA_PLAIN
+    if args.path == "learned":
+        from rvsp.learn import DEFAULT_WEIGHTS, RowModel
+        model = RowModel(path=DEFAULT_WEIGHTS)
+        algo = L.ALGO_CUDA_LEARNED
+    descs = []
+    for _ in dP:
+        d = Descriptor(algo=algo, memory=L.MEM_DEVICE, stream=stream, profiling=True)
+        if model is not None:
+            d.set_model(model)
+        descs.append(d)
+    nnz = []
+    ws_max = 1
+    for d, P in zip(descs, dP):
+        ws_b, n = d.work_estimation(P, dB)
+        nnz.append(n)
+        ws_max = max(ws_max, ws_b)
+    mx = max(nnz) if nnz else 1
+    dC = DeviceCSR.empty(max((P.rows for P in panels), default=1), A.cols, mx, dev)
+    ws = torch.zeros(ws_max, dtype=torch.uint8, device=dev)
+
+    def step():
+        for d, P, n in zip(descs, dP, nnz):
+            C_ = DeviceCSR(P.rows, A.cols, dC.row_ptr[:P.rows + 1], dC.col_idx[:max(n, 1)],
+                           dC.values[:max(n, 1)])
+            d.work_estimation(P, dB)
+            d.compute(P, dB, C_, ws)
+
+    sampler = ClockSampler(local)
+    sampler.start()
+    for _ in range(args.warmup):
+        flush.zero_()
+        step()
+    torch.cuda.synchronize(dev)
+    for d in descs:
+        d.synchronize()
+        d.phase_times(reset=True)
+    if pg:
+        pg.barrier()
+    torch.cuda.synchronize(dev)
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+          for _ in range(args.steps)]
+    for i in range(args.steps):
+        flush.zero_()
+        ev[i][0].record(stream)
+        step()
+        ev[i][1].record(stream)
+    torch.cuda.synchronize(dev)
+    for d in descs:
+        d.synchronize()
+    clocks = sampler.stop()
+    total_ms = float(sum(a.elapsed_time(c) for a, c in ev))
+    if pg:
+        t = torch.tensor([total_ms], device=dev)
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        total_ms = float(t.item())
+    ms_per_step = total_ms / args.steps
+    value = flops_all * args.steps / (total_ms * 1e-3) / 1e9
+    phases = {}
+    for d in descs:
+        for k, (ms, nl) in d.phase_times(reset=True).items():
+            a = phases.setdefault(k, [0.0, 0])
+            a[0] += ms
+            a[1] += nl
+    per_step = {k: (v[0] / args.steps, v[1] / args.steps) for k, v in phases.items() if v[1]}
+    alg_bytes = sum(rvsp.algorithmic_bytes(P, A, n) for P, n in zip(panels, nnz))
+    peak, peak_kind = measured_peaks()
+    dom = max(per_step, key=lambda k: per_step[k][0]) if per_step else "numeric"
+    dom_ms = per_step.get(dom, (ms_per_step, 0))[0]
+    launches = int(sum(v[1] for v in per_step.values()))
+    overflow = sum(d.overflow_rows() for d in descs)
+
+    # End to end: one host-memory-space descriptor, panel by panel, pinned
+    # operands and one pinned C buffer of the largest panel.
+    e2e = None
+    if (rank == 0 or world > 1) and args.e2e_steps > 0:
+        def pinned(x):
+            return torch.from_numpy(np.ascontiguousarray(x)).pin_memory().numpy()
+        hB = CSR(A.rows, A.cols, pinned(A.row_ptr), pinned(A.col_idx), pinned(A.values))
+        hP = [CSR(P.rows, P.cols, pinned(P.row_ptr), pinned(P.col_idx), pinned(P.values))
+              for P in panels]
+        hC = CSR(max(P.rows for P in panels), A.cols, pinned(np.zeros(max(P.rows for P in panels) + 1, np.int32)),
+                 pinned(np.zeros(mx, np.int32)), pinned(np.zeros(mx, np.float32)))
+        he = Descriptor(algo=algo, memory=L.MEM_HOST)
+        if model is not None:
+            he.set_model(model)
+
+        def e2e_step():
+            for P, n in zip(hP, nnz):
+                he.work_estimation(P, hB)
+                C_ = CSR(P.rows, A.cols, hC.row_ptr[:P.rows + 1], hC.col_idx[:max(n, 1)],
+                         hC.values[:max(n, 1)])
+                he.compute(P, hB, C_, np.zeros(256, np.uint8))
+        e2e_step()
+        torch.cuda.synchronize(dev)
+        t0 = time.perf_counter()
+        for _ in range(args.e2e_steps):
+            e2e_step()
+        torch.cuda.synchronize(dev)
+        el = time.perf_counter() - t0
+        h2d = sum(P.nbytes() + A.nbytes() for P in panels)
+        d2h = sum(4 * (P.rows + 1) + 8 * n for P, n in zip(panels, nnz))
+        e2e_val = 2.0 * my_ops * args.e2e_steps / el / 1e9
+        if pg:
+            t = torch.tensor([el], device=dev)
+            pg.all_reduce(t, op=pg.ReduceOp.MAX)
+            e2e_val = flops_all * args.e2e_steps / float(t.item()) / 1e9
+        e2e = {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+               "d2h_bytes_per_step": int(d2h), "steps": args.e2e_steps,
+               "api": "rvsp_spgemm_work_estimation + rvsp_spgemm_compute per panel, "
+                      "host memory space (B uploaded with every panel)"}
+        he.close()
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        # the reference on a bounded sample: small panels spread over the rows
+        sys.path.insert(0, str(ROOT))
+        from oracle import oracle
+        threads = os.cpu_count() or 1
+        rows = np.linspace(0, A.rows - 256, 64).astype(int)
+        sample = [(A.row_panel(int(r), int(r) + 256), A) for r in rows]
+        sops = [int(ops[int(r):int(r) + 256].sum()) for r in rows]
+        done, el = oracle.time_reference_batch(sample, seconds=20.0, threads=threads)
+        cpu = {"value": sum(2.0 * sops[i] for i in done) / el / 1e9, "unit": UNIT,
+               "cores": threads, "kind": "reference" if oracle.ref_available() else "port",
+               "sample": f"{len(done)} panels of 256 rows spread over the matrix, one-shot "
+                         f"each, on {threads} threads in {el:.1f} s"}
+
+    for d in descs:
+        d.close()
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
+            "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
+            "dtype": "f32", "data": "synthetic",
+            "config": {"workload": args.workload, "description": WORKLOADS[args.workload],
+                       "path": args.path, "rows": A.rows, "nnz_a": A.nnz,
+                       "panels": len(bounds), "panels_this_rank": len(mine),
+                       "panel_max_ops": PANEL_MAX_OPS, "overflow_rows": overflow,
+                       "nnz_c_this_rank": int(sum(nnz)), "products": int(ops.sum()),
+                       "flops_per_step": flops_all, "algorithmic_bytes_per_step": alg_bytes,
+                       "l2": "flushed between steps (256 MiB write outside the step events)",
+                       "parallelism": f"panels over {world} GPUs" if world > 1 else "single GPU"},
+            "hbm_frac": alg_bytes / (ms_per_step * 1e-3) / 1e9 / peak,
+            "phase_ms_per_step": {k: v[0] for k, v in per_step.items()},
+            "roofline": {"bound": "hbm", "kernel": f"{dom} phase",
+                         "achieved": alg_bytes / (dom_ms * 1e-3) / 1e9, "peak": peak,
+                         "unit": "GB/s", "frac": alg_bytes / (dom_ms * 1e-3) / 1e9 / peak,
+                         "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)"
+                         if peak_kind == "measured" else "fallback 6.65 TB/s",
+                         "traffic": committed_traffic(args.workload, dom),
+                         "algorithmic_bytes_per_launch": alg_bytes},
+            "clocks": clocks, "e2e": e2e, "gpu_launches": launches, "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    if pg:
+        pg.barrier()
+        pg.destroy_process_group()
+    return 0
+
+
 def cpu_baseline(A, B, flops, seconds=12.0):
     sys.path.insert(0, str(ROOT))
     from oracle import oracle
@@ -421,6 +644,8 @@ def main():
         return run_reference(args, world, rank)
     if args.workload == "batch512":
         return run_batch(args, world, rank, local)
+    if args.workload == "rmat20_panels":
+        return run_panels(args, world, rank, local)
 
     import torch
     import rvsp

@@ -8,6 +8,8 @@
 // One addition keeps the check itself in bounds: a row pointer outside
 // [0, nnz] is reported as a malformed row pointer before any column of that
 // row is read (the reference would read past the array there).
+#include <climits>
+
 #include "device_common.cuh"
 #include "kernels.cuh"
 
@@ -24,6 +26,20 @@ __device__ __forceinline__ unsigned long long pack(int32_t row, int code) {
          static_cast<unsigned>(code);
 }
 
+// Rows longer than this are checked by a warp each (long_row_check_kernel);
+// one thread walking a power-law hub row of tens of thousands of entries
+// would hold up the whole check.
+constexpr int32_t kCheckLongRow = 256;
+
+// Violation code of column c at a position whose predecessor in the row is
+// last (-1 at the row's start), 0 if none.
+__device__ __forceinline__ int col_code(int32_t c, int32_t last, int32_t cols) {
+  if (c < 0 || c >= cols) return kColRange;
+  if (c == last) return kDuplicate;
+  if (c < last) return kUnsorted;
+  return 0;
+}
+
 __global__ void __launch_bounds__(kThreads)
 csr_check_kernel(int32_t rows, int32_t cols, const int32_t *__restrict__ row_ptr,
                  const int32_t *__restrict__ col_idx, int32_t nnz,
@@ -35,17 +51,45 @@ csr_check_kernel(int32_t rows, int32_t cols, const int32_t *__restrict__ row_ptr
   int code = 0;
   if (hi < lo || lo < 0 || hi > nnz) {
     code = kBadRowPtr;
-  } else {
+  } else if (hi - lo <= kCheckLongRow) {
     int32_t last = -1;
-    for (int32_t p = lo; p < hi; ++p) {
+    for (int32_t p = lo; p < hi && !code; ++p) {
       const int32_t c = col_idx[p];
-      if (c < 0 || c >= cols) { code = kColRange; break; }
-      if (c == last) { code = kDuplicate; break; }
-      if (c < last) { code = kUnsorted; break; }
+      code = col_code(c, last, cols);
       last = c;
     }
   }
   if (code) atomicMin(result, pack(r, code));
+}
+
+// One warp per long row (rows strided over the grid's warps): 32 columns at a
+// time, each compared with its predecessor; the lowest violating position
+// of the first chunk that has one is the row's first violation.
+__global__ void __launch_bounds__(kThreads)
+long_row_check_kernel(int32_t rows, int32_t cols, const int32_t *__restrict__ row_ptr,
+                      const int32_t *__restrict__ col_idx, int32_t nnz,
+                      unsigned long long *__restrict__ result) {
+  const int lane = lane_id();
+  const int32_t warps = (gridDim.x * blockDim.x) >> 5;
+  for (int32_t r = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; r < rows; r += warps) {
+    const int32_t lo = row_ptr[r], hi = row_ptr[r + 1];
+    if (hi < lo || lo < 0 || hi > nnz || hi - lo <= kCheckLongRow) continue;  // uniform
+    int32_t prev_last = -1;
+    for (int32_t p0 = lo; p0 < hi; p0 += 32) {
+      const int32_t p = p0 + lane;
+      const int32_t c = p < hi ? col_idx[p] : INT32_MAX;
+      int32_t last = __shfl_up_sync(kFull, c, 1);
+      if (lane == 0) last = prev_last;
+      const int code = p < hi ? col_code(c, last, cols) : 0;
+      const unsigned bad = __ballot_sync(kFull, code != 0);
+      if (bad) {
+        const int first = __ffs(bad) - 1;
+        if (lane == first) atomicMin(result, pack(r, code));
+        break;  // uniform
+      }
+      prev_last = __shfl_sync(kFull, c, 31);
+    }
+  }
 }
 
 }  // namespace
@@ -56,6 +100,13 @@ void launch_csr_check(int32_t rows, int32_t cols, const int32_t *row_ptr,
   const int grid = rows > 0 ? (rows + kThreads - 1) / kThreads : 1;
   csr_check_kernel<<<grid, kThreads, 0, s>>>(rows, cols, row_ptr, col_idx, nnz,
                                              result);
+  if (rows > 0 && nnz > kCheckLongRow) {
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    long_row_check_kernel<<<sms * 8, kThreads, 0, s>>>(rows, cols, row_ptr, col_idx, nnz,
+                                                       result);
+  }
 }
 
 }  // namespace rvsp

@@ -252,6 +252,48 @@ def test_invalid_csr_rejected():
         assert e.value.status == L.ERROR_INVALID_CSR, mutate
 
 
+def test_device_check_long_rows_matches_oracle():
+    # Rows over 256 entries are checked by a warp each: the (code, first bad
+    # row) pair must still be the reference's, for violations at chunk
+    # boundaries, deep in long rows, and in short rows before or after them.
+    import ctypes as C
+    import torch
+    lib = L.load()
+    rng = np.random.default_rng(17)
+    base = gen.random_csr(300, 5000, 18, mean_len=8.0, heavy_rows=12, heavy_len=2000)
+    long_rows = np.nonzero(np.diff(base.row_ptr) > 256)[0]
+    plan = C.c_void_p()
+    L.check(lib.rvsp_cuda_plan_create(C.byref(plan)), "plan_create")
+    try:
+        cases = [None]
+        for r in long_rows[:4]:
+            for pos in (0, 31, 32, 33, 500, int(base.row_ptr[r + 1] - base.row_ptr[r]) - 1):
+                for kind in ("range", "dup", "unsorted"):
+                    cases.append((int(r), pos, kind))
+        cases.append((int(rng.integers(0, long_rows[0] + 1)), 0, "range"))
+        for case in cases:
+            X = base.copy()
+            if case is not None:
+                r, pos, kind = case
+                p = int(X.row_ptr[r]) + pos
+                if kind == "range":
+                    X.col_idx[p] = X.cols
+                elif kind == "dup" and pos > 0:
+                    X.col_idx[p] = X.col_idx[p - 1]
+                elif kind == "unsorted" and pos > 0:
+                    X.col_idx[p] = X.col_idx[p - 1] - 1
+            rp = torch.from_numpy(X.row_ptr).cuda()
+            ci = torch.from_numpy(X.col_idx).cuda()
+            code, bad = C.c_int32(), C.c_int32()
+            L.check(lib.rvsp_cuda_csr_check(plan, C.c_void_p(0), X.rows, X.cols,
+                                            rp.data_ptr(), ci.data_ptr(), X.nnz,
+                                            C.byref(code), C.byref(bad)), "csr_check")
+            assert (code.value, bad.value) == oracle.csr_check(X.rows, X.cols, X.row_ptr,
+                                                               X.col_idx), case
+    finally:
+        lib.rvsp_cuda_plan_destroy(plan)
+
+
 def test_fp64_tolerance():
     A = gen.random_csr(400, 300, 31, mean_len=20.0)
     B = gen.random_csr(300, 350, 32, mean_len=20.0)
@@ -287,6 +329,24 @@ def test_rmat_panel():
     A = gen.rmat(14, 16, seed=3)
     panel = A.row_panel(0, 2048)
     check_against_oracle(panel, A, "R-MAT 2^14 panel")
+
+
+def test_rmat20_sampled_panels():
+    # The power-law configuration runs as row panels (its whole C exceeds
+    # int32).  Sampled panels: the hubs (rows of up to ~10^7 products and
+    # ~10^5-10^6 outputs, over B's 2^20 columns: the widest heavy-row
+    # bitmap and many accumulator windows), a middle block, the last rows;
+    # plain and learned paths, and a numeric-only repeat on the hubs.
+    from rvsp.learn import DEFAULT_WEIGHTS, RowModel
+    A = gen.rmat(20, 16, seed=1)
+    model = RowModel(path=DEFAULT_WEIGHTS)
+    for r0, r1 in ((0, 32), (500000, 500512), (A.rows - 512, A.rows)):
+        P = A.row_panel(r0, r1)
+        check_against_oracle(P, A, f"R-MAT 2^20 rows {r0}:{r1}", reuse=(r0 == 0))
+        rp, ci, cv, _ = oracle.spgemm(P, A)
+        with Descriptor(algo=L.ALGO_CUDA_LEARNED) as d:
+            d.set_model(model)
+            assert_bit_exact(d.multiply(P, A), rp, ci, cv, f"learned rows {r0}:{r1}")
 
 
 def test_batched_style_products():
