@@ -151,8 +151,9 @@ rvsp_status_t rvsp_spgemm_synchronize(rvsp_spgemm_descr_t descr);
 /* Rows per row class of the last analysis: symbolic classes (sized by the
  * op-count bound) in sym_out and numeric classes (sized by the exact row
  * nnz) in num_out, n entries each; either pointer may be NULL.  Classes in
- * order: empty, ESC (<= 32 products), warp hash 64 / 128 / 256 / 512 / 1024 /
- * 2048 slots, block hash 8192 slots, dense. */
+ * order (12): empty; thread-per-row merge of at most 4 / 8 / 16 A nonzeros;
+ * warp hash 64 / 128 / 256 / 512 / 1024 / 2048 slots; block 8192 (output
+ * bound <= 4096); dense. */
 rvsp_status_t rvsp_spgemm_get_class_counts(rvsp_spgemm_descr_t descr,
                                            int32_t *sym_out, int32_t *num_out,
                                            int32_t n);

@@ -54,7 +54,6 @@ rvsp_status_t rvsp_device_check(rvsp_cuda_plan_t plan, cudaStream_t s,
                                 unsigned mask);
 
 #define RVSP_REJECT_ALL 0x1Eu      /* BAD_ROW_PTR, RANGE, UNSORTED, DUPLICATE */
-#define RVSP_REJECT_UNSAFE 0x16u   /* BAD_ROW_PTR, RANGE, DUPLICATE */
 
 /* Reference check_operand (spgemm_descr.c:137-160). */
 rvsp_status_t rvsp_check_operand(const rvsp_csr_matrix_t *M);
