@@ -43,7 +43,8 @@ __device__ __forceinline__ int col_code(int32_t c, int32_t last, int32_t cols) {
 __global__ void __launch_bounds__(kThreads)
 csr_check_kernel(int32_t rows, int32_t cols, const int32_t *__restrict__ row_ptr,
                  const int32_t *__restrict__ col_idx, int32_t nnz,
-                 unsigned long long *__restrict__ result) {
+                 unsigned long long *__restrict__ result, int32_t *__restrict__ long_rows,
+                 int32_t long_cap) {
   const int32_t r = blockIdx.x * blockDim.x + threadIdx.x;
   if (r == 0 && row_ptr[0] != 0) atomicMin(result, pack(-1, kBadRowPtr));
   if (r >= rows) return;
@@ -51,7 +52,11 @@ csr_check_kernel(int32_t rows, int32_t cols, const int32_t *__restrict__ row_ptr
   int code = 0;
   if (hi < lo || lo < 0 || hi > nnz) {
     code = kBadRowPtr;
-  } else if (hi - lo <= kCheckLongRow) {
+  } else if (hi - lo > kCheckLongRow) {
+    // rows of more than kCheckLongRow entries (at most nnz / 257 of them)
+    const int32_t at = atomicAdd(long_rows, 1);
+    if (at < long_cap) long_rows[1 + at] = r;
+  } else {
     int32_t last = -1;
     for (int32_t p = lo; p < hi && !code; ++p) {
       const int32_t c = col_idx[p];
@@ -62,18 +67,20 @@ csr_check_kernel(int32_t rows, int32_t cols, const int32_t *__restrict__ row_ptr
   if (code) atomicMin(result, pack(r, code));
 }
 
-// One warp per long row (rows strided over the grid's warps): 32 columns at a
-// time, each compared with its predecessor; the lowest violating position
-// of the first chunk that has one is the row's first violation.
+// One warp per listed long row: 32 columns at a time, each compared with its
+// predecessor; the lowest violating position of the first chunk that has one
+// is the row's first violation.
 __global__ void __launch_bounds__(kThreads)
-long_row_check_kernel(int32_t rows, int32_t cols, const int32_t *__restrict__ row_ptr,
-                      const int32_t *__restrict__ col_idx, int32_t nnz,
-                      unsigned long long *__restrict__ result) {
+long_row_check_kernel(int32_t cols, const int32_t *__restrict__ row_ptr,
+                      const int32_t *__restrict__ col_idx,
+                      unsigned long long *__restrict__ result,
+                      const int32_t *__restrict__ long_rows, int32_t long_cap) {
   const int lane = lane_id();
   const int32_t warps = (gridDim.x * blockDim.x) >> 5;
-  for (int32_t r = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; r < rows; r += warps) {
+  const int32_t n = min(long_rows[0], long_cap);
+  for (int32_t i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < n; i += warps) {
+    const int32_t r = long_rows[1 + i];
     const int32_t lo = row_ptr[r], hi = row_ptr[r + 1];
-    if (hi < lo || lo < 0 || hi > nnz || hi - lo <= kCheckLongRow) continue;  // uniform
     int32_t prev_last = -1;
     for (int32_t p0 = lo; p0 < hi; p0 += 32) {
       const int32_t p = p0 + lane;
@@ -94,18 +101,25 @@ long_row_check_kernel(int32_t rows, int32_t cols, const int32_t *__restrict__ ro
 
 }  // namespace
 
+int32_t check_long_rows_cap(int32_t rows, int32_t nnz) {
+  const int32_t by_nnz = nnz / (kCheckLongRow + 1) + 1;
+  return rows < by_nnz ? rows : by_nnz;
+}
+
 void launch_csr_check(int32_t rows, int32_t cols, const int32_t *row_ptr,
                       const int32_t *col_idx, int32_t nnz,
-                      unsigned long long *result, cudaStream_t s) {
+                      unsigned long long *result, int32_t *long_rows,
+                      cudaStream_t s) {
+  const int32_t cap = check_long_rows_cap(rows, nnz);
   const int grid = rows > 0 ? (rows + kThreads - 1) / kThreads : 1;
-  csr_check_kernel<<<grid, kThreads, 0, s>>>(rows, cols, row_ptr, col_idx, nnz,
-                                             result);
+  csr_check_kernel<<<grid, kThreads, 0, s>>>(rows, cols, row_ptr, col_idx, nnz, result,
+                                             long_rows, cap);
   if (rows > 0 && nnz > kCheckLongRow) {
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    long_row_check_kernel<<<sms * 8, kThreads, 0, s>>>(rows, cols, row_ptr, col_idx, nnz,
-                                                       result);
+    long_row_check_kernel<<<sms * 2, kThreads, 0, s>>>(cols, row_ptr, col_idx, result,
+                                                       long_rows, cap);
   }
 }
 

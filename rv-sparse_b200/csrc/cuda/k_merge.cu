@@ -11,8 +11,11 @@
 // accum_scalar_f32.c:20-71), and the emitted columns are its sorted fill
 // (rvsp_symbolic.c:91-137).
 //
-// The per-list state (position, end, head column, A value) lives in
-// registers: every loop over lists is unrolled over K and guarded by j < k.
+// The per-list state lives in registers: every loop over lists is unrolled
+// over K and guarded by j < k.  Each list also holds its NEXT entry (column,
+// and value in the numeric pass), loaded when the list advances and used
+// only at its following advance, so the merge loop never waits on a load it
+// has just issued.
 #include <climits>
 
 #include "device_common.cuh"
@@ -24,9 +27,12 @@ namespace {
 
 template <int K>
 struct Lists {
-  int32_t pos[K];
+  int32_t pos[K];  // position of the head in B
   int32_t end[K];
-  int32_t cur[K];
+  int32_t cur[K];  // head column (INT_MAX when the list is done)
+  int32_t nxt[K];  // column after the head (INT_MAX past the end)
+  float curv[K];   // head value, next value (numeric pass)
+  float nxtv[K];
   float a[K];
 };
 
@@ -36,16 +42,19 @@ __device__ __forceinline__ void prefetch_l1(const void *p) {
 
 // Opens the row's lists.  Every load here is independent of the others, and
 // the lines holding each B row (both ends, columns and values) are
-// prefetched into L1 so the merge loop's dependent loads hit L1.
+// prefetched into L1 so the lookahead loads hit L1.
 template <int K, bool kValues>
 __device__ __forceinline__ void open_lists(const Operands &op, int32_t p0,
                                            int32_t k, Lists<K> &L) {
 #pragma unroll
   for (int j = 0; j < K; ++j) {
     L.cur[j] = INT_MAX;
+    L.nxt[j] = INT_MAX;
     L.pos[j] = 0;
     L.end[j] = 0;
     L.a[j] = 0.0f;
+    L.curv[j] = 0.0f;
+    L.nxtv[j] = 0.0f;
     if (j < k) {
       const int32_t kk = __ldg(op.a_col + p0 + j);
       if (kValues) L.a[j] = __ldg(op.a_val + p0 + j);
@@ -55,20 +64,39 @@ __device__ __forceinline__ void open_lists(const Operands &op, int32_t p0,
       L.end[j] = b1;
       if (b0 < b1) {
         prefetch_l1(op.b_col + b1 - 1);
-        if (kValues) {
-          prefetch_l1(op.b_val + b0);
-          prefetch_l1(op.b_val + b1 - 1);
-        }
+        if (kValues) prefetch_l1(op.b_val + b1 - 1);
         L.cur[j] = __ldg(op.b_col + b0);
+        if (kValues) L.curv[j] = __ldg(op.b_val + b0);
+        if (b0 + 1 < b1) {
+          L.nxt[j] = __ldg(op.b_col + b0 + 1);
+          if (kValues) L.nxtv[j] = __ldg(op.b_val + b0 + 1);
+        }
       }
     }
   }
 }
 
-// Blocks per SM the merge kernels ask the compiler to fit (register budget).
-template <int K>
+// Moves list j past its head: the lookahead entry becomes the head and the
+// entry after it is loaded.
+template <int K, bool kValues>
+__device__ __forceinline__ void advance(const Operands &op, Lists<K> &L, int j) {
+  const int32_t p = ++L.pos[j];
+  L.cur[j] = L.nxt[j];
+  if (kValues) L.curv[j] = L.nxtv[j];
+  if (p + 1 < L.end[j]) {
+    L.nxt[j] = __ldg(op.b_col + p + 1);
+    if (kValues) L.nxtv[j] = __ldg(op.b_val + p + 1);
+  } else {
+    L.nxt[j] = INT_MAX;
+  }
+}
+
+// Blocks per SM the merge kernels ask the compiler to fit: the register
+// budget of K lists (the numeric pass also keeps two values per list).
+template <int K, bool kValues>
 struct MergeOccupancy {
-  static constexpr int value = K <= 4 ? 16 : K <= 8 ? 10 : 6;
+  static constexpr int value = kValues ? (K <= 4 ? 12 : K <= 8 ? 8 : 4)
+                                       : (K <= 4 ? 16 : K <= 8 ? 10 : 6);
 };
 
 template <int K>
@@ -80,7 +108,7 @@ __device__ __forceinline__ int32_t min_head(const Lists<K> &L) {
 }
 
 template <int K>
-__global__ void __launch_bounds__(kMergeThreads, MergeOccupancy<K>::value)
+__global__ void __launch_bounds__(kMergeThreads, MergeOccupancy<K, false>::value)
 merge_symbolic_kernel(Operands op, const int32_t *__restrict__ rows,
                       int32_t nrows, int32_t *__restrict__ counts) {
   const int32_t t = blockIdx.x * blockDim.x + threadIdx.x;
@@ -95,12 +123,8 @@ merge_symbolic_kernel(Operands op, const int32_t *__restrict__ rows,
     const int32_t mn = min_head<K>(L);
     if (mn == INT_MAX) break;
 #pragma unroll
-    for (int j = 0; j < K; ++j) {
-      if (L.cur[j] == mn) {
-        const int32_t p = ++L.pos[j];
-        L.cur[j] = p < L.end[j] ? __ldg(op.b_col + p) : INT_MAX;
-      }
-    }
+    for (int j = 0; j < K; ++j)
+      if (L.cur[j] == mn) advance<K, false>(op, L, j);
     ++n;
   }
   counts[row] = n;
@@ -110,7 +134,7 @@ merge_symbolic_kernel(Operands op, const int32_t *__restrict__ rows,
 // its op count, an exact upper bound, so it cannot overflow) and its nnz to
 // fo.counts[row].
 template <int K, bool kFused>
-__global__ void __launch_bounds__(kMergeThreads, MergeOccupancy<K>::value)
+__global__ void __launch_bounds__(kMergeThreads, MergeOccupancy<K, true>::value)
 merge_numeric_kernel(Operands op, const int32_t *__restrict__ rows, int32_t nrows,
                      const int32_t *__restrict__ c_rp, int32_t *__restrict__ c_col,
                      float *__restrict__ c_val, bool fill,
@@ -132,10 +156,8 @@ merge_numeric_kernel(Operands op, const int32_t *__restrict__ rows, int32_t nrow
 #pragma unroll
     for (int j = 0; j < K; ++j) {
       if (L.cur[j] == mn) {
-        const int32_t p = L.pos[j];
-        acc = __fadd_rn(acc, __fmul_rn(L.a[j], __ldg(op.b_val + p)));
-        L.pos[j] = p + 1;
-        L.cur[j] = p + 1 < L.end[j] ? __ldg(op.b_col + p + 1) : INT_MAX;
+        acc = __fadd_rn(acc, __fmul_rn(L.a[j], L.curv[j]));
+        advance<K, true>(op, L, j);
       }
     }
     if (out < out_end) {

@@ -210,10 +210,14 @@ void launch_map_numeric(int cls, const Operands &op, const int64_t *ops, const i
 
 // ---- k_check.cu ------------------------------------------------------------
 // *result (initialised to ~0ull) receives min over bad rows of
-// ((row + 1) << 8 | code); row -1 means row_ptr[0] != 0.
+// ((row + 1) << 8 | code); row -1 means row_ptr[0] != 0.  long_rows: scratch
+// of 1 + check_long_rows_cap(rows, nnz) ints, long_rows[0] zeroed by the
+// caller (the count of rows over 256 entries, listed after it).
+int32_t check_long_rows_cap(int32_t rows, int32_t nnz);
 void launch_csr_check(int32_t rows, int32_t cols, const int32_t *row_ptr,
                       const int32_t *col_idx, int32_t nnz,
-                      unsigned long long *result, cudaStream_t s);
+                      unsigned long long *result, int32_t *long_rows,
+                      cudaStream_t s);
 
 // ---- k_numeric.cu ----------------------------------------------------------
 // Values (and, when fill, sorted columns) of the rows of one class.  With

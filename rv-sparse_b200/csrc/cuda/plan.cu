@@ -89,6 +89,7 @@ struct rvsp_cuda_plan {
   DevArray<int64_t> partials, total;
   DevArray<uint32_t> sym_bits;
   DevArray<unsigned long long> check;
+  DevArray<int32_t> check_long;  // count + list of the long rows the check met
   int32_t sym_bits_slots = 0;
 
   int32_t *h_misc = nullptr;  // pinned, kMiscWords
@@ -328,6 +329,7 @@ void rvsp_cuda_plan_destroy(rvsp_cuda_plan_t p) {
   p->total.release();
   p->sym_bits.release();
   p->check.release();
+  p->check_long.release();
   p->cap.release();
   p->slab_off.release();
   p->slab_col.release();
@@ -876,11 +878,14 @@ rvsp_status_t rvsp_cuda_csr_check(rvsp_cuda_plan_t p, void *stream, int32_t rows
   if (!row_ptr || rows < 0 || cols < 0 || nnz < 0) return RVSP_SUCCESS;
   if (nnz > 0 && !col_idx) return RVSP_SUCCESS;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
+  cudaError_t re = p->check_long.reserve(1 + size_t(check_long_rows_cap(rows, nnz)));
+  if (re != cudaSuccess) return map_cuda(re);
   cudaMemsetAsync(p->check.p, 0xff, sizeof(unsigned long long), s);
+  cudaMemsetAsync(p->check_long.p, 0, sizeof(int32_t), s);
   {
     PhaseScope ph(p, s, RVSP_PHASE_CHECK);
-    launch_csr_check(rows, cols, row_ptr, col_idx, nnz, p->check.p, s);
-    ph.launches = 1;
+    launch_csr_check(rows, cols, row_ptr, col_idx, nnz, p->check.p, p->check_long.p, s);
+    ph.launches = 2;
   }
   cudaMemcpyAsync(p->h_check, p->check.p, sizeof(unsigned long long),
                   cudaMemcpyDeviceToHost, s);
