@@ -675,10 +675,12 @@ def main():
     reuse = args.workload.endswith("_reuse")
 
     model = None
+    model_file = None
     algo = L.ALGO_CUDA_PLAIN
     if args.path == "learned":
-        from rvsp.learn import DEFAULT_WEIGHTS, RowModel
-        model = RowModel(path=DEFAULT_WEIGHTS)
+        from rvsp.learn import RowModel, weights_for
+        model_file = weights_for(args.workload)
+        model = RowModel(path=model_file)
         algo = L.ALGO_CUDA_LEARNED
 
     def make_descr(memory, **kw):
@@ -816,7 +818,9 @@ def main():
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32", "data": "synthetic",
             "config": {"workload": args.workload, "description": WORKLOADS[args.workload],
-                       "path": args.path, "rows": A.rows, "nnz_a": A.nnz, "nnz_b": B.nnz,
+                       "path": args.path,
+                       "model": model_file.name if model_file is not None else None,
+                       "rows": A.rows, "nnz_a": A.nnz, "nnz_b": B.nnz,
                        "overflow_rows": overflow,
                        "nnz_c": c_nnz, "products": int(ops.sum()),
                        "flops_per_step": flops, "algorithmic_bytes_per_step": alg_bytes,

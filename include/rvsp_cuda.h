@@ -237,6 +237,13 @@ rvsp_status_t rvsp_cuda_plan_prepare_reuse(rvsp_cuda_plan_t plan, void *stream,
                                            const int32_t *c_col_idx,
                                            int64_t *map_entries_out);
 
+/* Rows of the reuse map that read another row's identical map (a structured
+ * matrix repeats a few position patterns over most rows; such rows share one
+ * copy, found by fingerprint and confirmed entry by entry).  0 when no map
+ * is built.  Synchronizes `stream`. */
+rvsp_status_t rvsp_cuda_plan_reuse_shared_rows(rvsp_cuda_plan_t plan, void *stream,
+                                               int32_t *shared_rows_out);
+
 /* ---- Batches ------------------------------------------------------------
  * No reference counterpart: the reference computes one product per call.
  * A batch of independent products C_i = A_i * B_i is packed, a group of

@@ -14,30 +14,88 @@ constexpr int kThreads = 256;
 // Rows of at least this many entries are copied by whole blocks.
 constexpr int32_t kCompactLarge = 4096;
 
-// kLarge = false: one warp per row below kCompactLarge entries; true: one
-// block per row of kCompactLarge or more (a power-law matrix has rows of
-// tens of thousands of entries, which would leave one warp copying long
-// after the rest).  Coalesced copies either way.
-template <bool kLarge>
+// Rows of kCompactLarge entries or more, listed by compact_small_kernel in
+// big[1..big[0]]: one block per row (a power-law matrix has rows of tens of
+// thousands of entries).  Coalesced copies.
 __global__ void __launch_bounds__(kThreads)
-compact_kernel(int32_t a_rows, const int32_t *__restrict__ counts,
-               const int64_t *__restrict__ off, const int32_t *__restrict__ row_ptr,
-               const int32_t *__restrict__ slab_col, const float *__restrict__ slab_val,
-               int32_t *__restrict__ c_col, float *__restrict__ c_val, bool with_values) {
-  const int lanes = kLarge ? kThreads : 32;
-  const int me = kLarge ? threadIdx.x : lane_id();
-  const int32_t first = kLarge ? blockIdx.x : (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int32_t stride = kLarge ? gridDim.x : (gridDim.x * blockDim.x) >> 5;
-  for (int32_t row = first; row < a_rows; row += stride) {
+compact_large_kernel(const int32_t *__restrict__ big, const int32_t *__restrict__ counts,
+                     const int64_t *__restrict__ off, const int32_t *__restrict__ row_ptr,
+                     const int32_t *__restrict__ slab_col,
+                     const float *__restrict__ slab_val, int32_t *__restrict__ c_col,
+                     float *__restrict__ c_val, bool with_values) {
+  const int32_t n = big[0];
+  for (int32_t i = blockIdx.x; i < n; i += gridDim.x) {
+    const int32_t row = big[1 + i];
     const int32_t m = counts[row];
-    if (m <= 0) continue;  // empty, or redone by the plain path
-    if ((m >= kCompactLarge) != kLarge) continue;
     const int64_t src = off[row];
     const int32_t dst = row_ptr[row];
-    for (int32_t e = me; e < m; e += lanes) {
+    for (int32_t e = threadIdx.x; e < m; e += kThreads) {
       c_col[dst + e] = slab_col[src + e];
       if (with_values) c_val[dst + e] = slab_val[src + e];
     }
+  }
+}
+
+// Shorter rows: a block takes `rows_per_chunk` (a power of two, at most
+// kThreads) consecutive rows and copies all of their entries as one flat
+// range, each thread finding the row of its entry by binary search over the
+// block's prefix of row lengths, so short rows keep every thread busy and
+// reads and writes stay contiguous.  Rows of kCompactLarge entries or more
+// are appended to big[1..] for compact_large_kernel.
+__global__ void __launch_bounds__(kThreads)
+compact_small_kernel(int32_t a_rows, int rows_per_chunk, const int32_t *__restrict__ counts,
+                     const int64_t *__restrict__ off, const int32_t *__restrict__ row_ptr,
+                     const int32_t *__restrict__ slab_col,
+                     const float *__restrict__ slab_val, int32_t *__restrict__ c_col,
+                     float *__restrict__ c_val, bool with_values,
+                     int32_t *__restrict__ big) {
+  __shared__ int32_t s_incl[kThreads];
+  __shared__ int64_t s_src[kThreads];
+  __shared__ int32_t s_dst[kThreads];
+  __shared__ int32_t s_wsum[kThreads / 32];
+  const int tid = threadIdx.x, lane = lane_id(), w = tid >> 5;
+  const int64_t chunks = (int64_t(a_rows) + rows_per_chunk - 1) / rows_per_chunk;
+  for (int64_t ch = blockIdx.x; ch < chunks; ch += gridDim.x) {
+    const int64_t row = ch * rows_per_chunk + tid;
+    int32_t m = (tid < rows_per_chunk && row < a_rows) ? counts[row] : 0;
+    const bool large = m >= kCompactLarge;
+    const unsigned large_mask = __ballot_sync(kFull, large);
+    if (large_mask) {
+      int32_t base = 0;
+      if (lane == 0) base = atomicAdd(big, __popc(large_mask));
+      base = __shfl_sync(kFull, base, 0);
+      if (large) big[1 + base + __popc(large_mask & ((1u << lane) - 1))] = int32_t(row);
+    }
+    if (m < 0 || large) m = 0;  // redone by the plain path / copied by blocks
+    int64_t src = 0;
+    int32_t dst = 0;
+    if (m > 0) {
+      src = off[row];
+      dst = row_ptr[row];
+    }
+    const int incl = warp_incl_scan(m);
+    if (lane == 31) s_wsum[w] = incl;
+    __syncthreads();
+    int wbase = 0, total = 0;
+#pragma unroll
+    for (int i = 0; i < kThreads / 32; ++i) {
+      if (i < w) wbase += s_wsum[i];
+      total += s_wsum[i];
+    }
+    s_incl[tid] = wbase + incl;
+    s_src[tid] = src;
+    s_dst[tid] = dst;
+    __syncthreads();
+    for (int32_t e = tid; e < total; e += kThreads) {
+      // the first row j with s_incl[j] > e (e < total, so j < rows_per_chunk)
+      int j = 0;
+      for (int sz = rows_per_chunk >> 1; sz >= 1; sz >>= 1)
+        if (s_incl[j + sz - 1] <= e) j += sz;
+      const int32_t k = e - (j ? s_incl[j - 1] : 0);
+      c_col[s_dst[j] + k] = slab_col[s_src[j] + k];
+      if (with_values) c_val[s_dst[j] + k] = slab_val[s_src[j] + k];
+    }
+    __syncthreads();  // the next chunk overwrites the tables
   }
 }
 
@@ -94,11 +152,19 @@ values_hash_kernel(const float *__restrict__ v, int64_t n, unsigned long long sa
 void launch_compact(int32_t a_rows, const int32_t *counts, const int64_t *off,
                     const int32_t *row_ptr, const int32_t *slab_col,
                     const float *slab_val, int32_t *c_col, float *c_val,
-                    bool with_values, int num_sms, cudaStream_t s) {
-  compact_kernel<false><<<num_sms * 8, kThreads, 0, s>>>(
-      a_rows, counts, off, row_ptr, slab_col, slab_val, c_col, c_val, with_values);
-  compact_kernel<true><<<num_sms * 8, kThreads, 0, s>>>(
-      a_rows, counts, off, row_ptr, slab_col, slab_val, c_col, c_val, with_values);
+                    bool with_values, int32_t *big, int num_sms, cudaStream_t s) {
+  if (a_rows <= 0) return;
+  const int blocks = num_sms * 8;
+  // enough chunks to give every block some: 32 .. kThreads rows each
+  int rows_per_chunk = kThreads;
+  while (rows_per_chunk > 32 && int64_t(a_rows) < int64_t(rows_per_chunk) * blocks)
+    rows_per_chunk >>= 1;
+  cudaMemsetAsync(big, 0, sizeof(int32_t), s);
+  compact_small_kernel<<<blocks, kThreads, 0, s>>>(a_rows, rows_per_chunk, counts, off,
+                                                   row_ptr, slab_col, slab_val, c_col,
+                                                   c_val, with_values, big);
+  compact_large_kernel<<<blocks, kThreads, 0, s>>>(big, counts, off, row_ptr, slab_col,
+                                                   slab_val, c_col, c_val, with_values);
 }
 
 void launch_list_classify(const int32_t *list, int32_t n, const int64_t *ops,

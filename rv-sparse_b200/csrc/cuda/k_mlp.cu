@@ -81,17 +81,38 @@ __device__ __forceinline__ RowFeat warp_row_features(const Operands &op, int32_t
 // y = MLP(x) with the hidden units spread over the 32 lanes (unit j on lane
 // j); every lane returns both outputs.  P holds the parameters in the layout
 // of MlpLayout (shared memory).
+// Copies the parameters into shared memory with W1 and W2 transposed
+// (W1T[i][j] at kW1 + i * 32 + j, W2T[k][j] at kW2 + k * 32 + j), so that in
+// warp_mlp lane j's reads of row j fall in 32 different banks.
+__device__ __forceinline__ void load_params_transposed(float *P,
+                                                       const float *__restrict__ params) {
+  for (int i = threadIdx.x; i < kMlpParams; i += blockDim.x) {
+    float v = params[i];
+    int at = i;
+    if (i >= kW1 && i < kB1) {
+      const int j = (i - kW1) / kMlpIn, c = (i - kW1) % kMlpIn;
+      at = kW1 + c * kMlpHidden + j;
+    } else if (i >= kW2 && i < kB2) {
+      const int j = (i - kW2) / kMlpHidden, c = (i - kW2) % kMlpHidden;
+      at = kW2 + c * kMlpHidden + j;
+    }
+    P[at] = v;
+  }
+}
+
+// Forward pass of one row on one warp (lane j = hidden unit j), with P laid
+// out by load_params_transposed.
 __device__ __forceinline__ void warp_mlp(const float *P, const float *x, float &y0,
                                          float &y1) {
   const int j = lane_id();
   float a = P[kB1 + j];
 #pragma unroll
-  for (int i = 0; i < kMlpIn; ++i) a = fmaf(P[kW1 + j * kMlpIn + i], x[i], a);
+  for (int i = 0; i < kMlpIn; ++i) a = fmaf(P[kW1 + i * kMlpHidden + j], x[i], a);
   const float h1 = fmaxf(a, 0.0f);
   float b = P[kB2 + j];
 #pragma unroll
   for (int k = 0; k < kMlpHidden; ++k)
-    b = fmaf(P[kW2 + j * kMlpHidden + k], __shfl_sync(kFull, h1, k), b);
+    b = fmaf(P[kW2 + k * kMlpHidden + j], __shfl_sync(kFull, h1, k), b);
   const float h2 = fmaxf(b, 0.0f);
   float o0 = P[kW3 + j] * h2;
   float o1 = P[kW3 + kMlpHidden + j] * h2;
@@ -125,7 +146,7 @@ __global__ void __launch_bounds__(kThreads)
 predict_kernel(Operands op, float b_mean_len, const float *__restrict__ params,
                float2 *__restrict__ pred, int64_t *__restrict__ ops_out) {
   __shared__ float P[kMlpParamsPad];
-  for (int i = threadIdx.x; i < kMlpParams; i += blockDim.x) P[i] = params[i];
+  load_params_transposed(P, params);
   __syncthreads();
   const int warps = (gridDim.x * blockDim.x) >> 5;
   for (int32_t row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; row < op.a_rows;
@@ -154,6 +175,7 @@ predict_kernel(Operands op, float b_mean_len, const float *__restrict__ params,
 // A row whose nnz exceeds its capacity is caught by the fused kernel and
 // redone by the plain two-pass path.
 constexpr int kCapPad = 16;
+constexpr int kThreadRowNnz = 32;  // rows up to this many A nonzeros: a thread each
 
 __global__ void __launch_bounds__(kThreads)
 learned_plan_kernel(Operands op, float b_mean_len, const float *__restrict__ params,
@@ -162,48 +184,101 @@ learned_plan_kernel(Operands op, float b_mean_len, const float *__restrict__ par
                     int32_t *__restrict__ counts, int32_t *__restrict__ class_count) {
   __shared__ float P[kMlpParamsPad];
   __shared__ int32_t s_cnt[kNumClasses];
-  for (int i = threadIdx.x; i < kMlpParams; i += blockDim.x) P[i] = params[i];
+  load_params_transposed(P, params);
   for (int c = threadIdx.x; c < kNumClasses; c += blockDim.x) s_cnt[c] = 0;
   __syncthreads();
-  const int warps = (gridDim.x * blockDim.x) >> 5;
-  const int first = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  // Every warp of the block runs the same number of iterations so the final
-  // __syncthreads is reached by all of them.
-  const int iters = (op.a_rows + warps - 1) / warps;
-  for (int it = 0; it < iters; ++it) {
-    const int32_t row = first + it * warps;
-    if (row >= op.a_rows) continue;
-    const RowFeat r = warp_row_features(op, row, b_mean_len);
-    float x[kMlpIn];
-#pragma unroll
-    for (int i = 0; i < kMlpIn; ++i) x[i] = (r.f[i] - P[kMu + i]) * P[kInvSd + i];
-    float y0, y1;
-    warp_mlp(P, x, y0, y1);
-    if (lane_id() == 0) {
-      const int32_t nnz = op.a_rp[row + 1] - op.a_rp[row];
-      const long long ops = r.ops;
-      const long long ub = ops < op.b_cols ? ops : op.b_cols;
-      int c;
-      long long cap;
-      if (ops == 0) {
-        c = kEmpty_;
-        cap = 0;
-        counts[row] = 0;
-      } else if (merge_ok && nnz <= kMergeMaxNnz && ops <= kMergeMaxOps && y1 > 0.0f) {
-        c = nnz <= 4 ? kM4 : nnz <= 8 ? kM8 : kM16;
-        cap = ops;
-      } else {
-        const float mhat = exp2f(fminf(y0, 40.0f)) - 1.0f;
-        const float want = ceilf(scale * fmaxf(mhat, 0.0f)) + kCapPad;
-        cap = want >= static_cast<float>(ub) ? ub : static_cast<long long>(want);
-        if (cap < 1) cap = 1;
-        c = classify_row(nnz, ops, cap, false);
-        if (c == kDense) cap = ub;
+  auto decide = [&](int32_t row, int32_t nnz, long long ops, float y0, float y1) {
+    const long long ub = ops < op.b_cols ? ops : op.b_cols;
+    int c;
+    long long cap;
+    if (ops == 0) {
+      c = kEmpty_;
+      cap = 0;
+      counts[row] = 0;
+    } else if (merge_ok && nnz <= kMergeMaxNnz && ops <= kMergeMaxOps && y1 > 0.0f) {
+      c = nnz <= 4 ? kM4 : nnz <= 8 ? kM8 : kM16;
+      cap = ops;
+    } else {
+      const float mhat = exp2f(fminf(y0, 40.0f)) - 1.0f;
+      const float want = ceilf(scale * fmaxf(mhat, 0.0f)) + kCapPad;
+      cap = want >= static_cast<float>(ub) ? ub : static_cast<long long>(want);
+      if (cap < 1) cap = 1;
+      c = classify_row(nnz, ops, cap, false);
+      if (c == kDense) cap = ub;
+    }
+    ops_out[row] = ops;
+    cls_out[row] = static_cast<uint8_t>(c);
+    cap_out[row] = static_cast<int32_t>(cap);
+    atomicAdd(&s_cnt[c], 1);
+  };
+  // Rows of at most kThreadRowNnz A nonzeros: one thread each, features and
+  // MLP in registers (every thread reads the same weight at the same time, a
+  // shared-memory broadcast).  Their loads all start at once instead of one
+  // row after another on a warp.
+  const int32_t tstride = gridDim.x * blockDim.x;
+  for (int32_t row = blockIdx.x * blockDim.x + threadIdx.x; row < op.a_rows; row += tstride) {
+    const int32_t p0 = op.a_rp[row], p1 = op.a_rp[row + 1];
+    if (p1 - p0 > kThreadRowNnz) continue;
+    long long ops = 0;
+    int maxlen = 0, lo = INT_MAX, hi = -1;
+    for (int32_t p = p0; p < p1; ++p) {
+      const int32_t k = __ldg(op.a_col + p);
+      const int32_t b0 = __ldg(op.b_rp + k), b1 = __ldg(op.b_rp + k + 1);
+      const int len = b1 - b0;
+      ops += len;
+      maxlen = max(maxlen, len);
+      if (len > 0) {
+        lo = min(lo, __ldg(op.b_col + b0));
+        hi = max(hi, __ldg(op.b_col + b1 - 1));
       }
-      ops_out[row] = ops;
-      cls_out[row] = static_cast<uint8_t>(c);
-      cap_out[row] = static_cast<int32_t>(cap);
-      atomicAdd(&s_cnt[c], 1);
+    }
+    const float nnz = static_cast<float>(p1 - p0), fops = static_cast<float>(ops);
+    const float span = hi >= lo ? static_cast<float>(hi - lo + 1) : 0.0f;
+    float f[kMlpIn] = {lg(nnz), lg(fops), lg(static_cast<float>(maxlen)),
+                       lg(nnz > 0 ? fops / nnz : 0.0f), lg(span), lg(fminf(fops, span)),
+                       lg(static_cast<float>(op.b_cols)), lg(b_mean_len)};
+#pragma unroll
+    for (int i = 0; i < kMlpIn; ++i) f[i] = (f[i] - P[kMu + i]) * P[kInvSd + i];
+    float h1[kMlpHidden];
+#pragma unroll
+    for (int j = 0; j < kMlpHidden; ++j) {
+      float a = P[kB1 + j];
+#pragma unroll
+      for (int i = 0; i < kMlpIn; ++i) a = fmaf(P[kW1 + i * kMlpHidden + j], f[i], a);
+      h1[j] = fmaxf(a, 0.0f);
+    }
+    float y0 = P[kB3], y1 = P[kB3 + 1];
+#pragma unroll 4
+    for (int j = 0; j < kMlpHidden; ++j) {
+      float b = P[kB2 + j];
+#pragma unroll
+      for (int k = 0; k < kMlpHidden; ++k) b = fmaf(P[kW2 + k * kMlpHidden + j], h1[k], b);
+      const float h2 = fmaxf(b, 0.0f);
+      y0 = fmaf(P[kW3 + j], h2, y0);
+      y1 = fmaf(P[kW3 + kMlpHidden + j], h2, y1);
+    }
+    decide(row, p1 - p0, ops, y0, y1);
+  }
+  // Longer rows: one warp each (features over the lanes, hidden unit j on
+  // lane j), found 32 rows at a time.
+  const int32_t wstride = tstride >> 5;
+  const int lane = lane_id();
+  for (int32_t base = ((blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 32; base < op.a_rows;
+       base += wstride * 32) {
+    const int32_t mine = base + lane;
+    const bool longrow =
+        mine < op.a_rows && op.a_rp[mine + 1] - op.a_rp[mine] > kThreadRowNnz;
+    unsigned todo = __ballot_sync(kFull, longrow);
+    while (todo) {
+      const int32_t row = base + __ffs(todo) - 1;
+      todo &= todo - 1u;
+      const RowFeat r = warp_row_features(op, row, b_mean_len);
+      float x[kMlpIn];
+#pragma unroll
+      for (int i = 0; i < kMlpIn; ++i) x[i] = (r.f[i] - P[kMu + i]) * P[kInvSd + i];
+      float y0, y1;
+      warp_mlp(P, x, y0, y1);
+      if (lane == 0) decide(row, op.a_rp[row + 1] - op.a_rp[row], r.ops, y0, y1);
     }
   }
   __syncthreads();

@@ -141,11 +141,12 @@ void launch_scan_i64(int32_t n, const int32_t *in, int64_t *out, int64_t *partia
 
 // ---- k_fused.cu ------------------------------------------------------------
 // Copies every non-overflowed row (counts[row] >= 0) from its slab slot to C
-// at row_ptr[row]; values too when with_values.
+// at row_ptr[row]; values too when with_values.  big: scratch of a_rows + 1
+// words (count and list of the rows copied by whole blocks).
 void launch_compact(int32_t a_rows, const int32_t *counts, const int64_t *off,
                     const int32_t *row_ptr, const int32_t *slab_col,
                     const float *slab_val, int32_t *c_col, float *c_val,
-                    bool with_values, int num_sms, cudaStream_t s);
+                    bool with_values, int32_t *big, int num_sms, cudaStream_t s);
 // Classes the rows of a list (symbolic: by ub = min(ops, b_cols); numeric: by
 // exact nnz counts[row]); cls_out[j] for list entry j; class_count += rows.
 void launch_list_classify(const int32_t *list, int32_t n, const int64_t *ops,
@@ -198,10 +199,27 @@ bool map_class(int cls);
 // *too_long |= 1 when a row has more than INT32_MAX / 2 products.
 void launch_map_ops(const int32_t *rows, int32_t nrows, const int64_t *ops, int32_t *mops,
                     int32_t *too_long, cudaStream_t s);
-// map[moff[row] + t] = position in C's row of the row's t-th product.
+// map[moff[row] + t] = position in C's row of the row's t-th product;
+// key[row] (when key is not null) = fingerprint of the row's map, 0 when the
+// row met a missing column.
 void launch_map_build(int cls, const Operands &op, const int32_t *rows, int32_t nrows,
                       const int32_t *c_rp, const int32_t *c_col, const int64_t *moff,
-                      uint16_t *map, int32_t *status, cudaStream_t s);
+                      uint16_t *map, unsigned long long *key, int32_t *status,
+                      cudaStream_t s);
+// Sharing of identical maps: insert every listed row's key into the table
+// (tkey zeroed, trow filled with 0x7f bytes, mask + 1 a power of two at least
+// twice the rows inserted over all calls); then resolve, which points
+// moff[row] at the map of the smallest row with an identical map and adds
+// the rows so redirected to *shared_rows.
+void launch_map_dedup_insert(const int32_t *rows, int32_t nrows,
+                             const unsigned long long *key, unsigned long long *tkey,
+                             int32_t *trow, unsigned long long mask, cudaStream_t s);
+void launch_map_dedup_resolve(const int32_t *rows, int32_t nrows,
+                              const unsigned long long *key,
+                              const unsigned long long *tkey, const int32_t *trow,
+                              unsigned long long mask, const int32_t *c_rp,
+                              const int32_t *mops, int64_t *moff, const uint16_t *map,
+                              int32_t *shared_rows, cudaStream_t s);
 // Values of the listed rows of class cls from the map (structure in C).
 void launch_map_numeric(int cls, const Operands &op, const int64_t *ops, const int32_t *rows,
                         int32_t nrows, const int32_t *c_rp, float *c_val,

@@ -112,6 +112,7 @@ struct rvsp_cuda_plan {
   DevArray<int32_t> slab_col;
   DevArray<float> slab_val;
   DevArray<int32_t> ovf_rows, ovf_sorted;
+  DevArray<int32_t> big_rows;  // count + list of the rows compacted by whole blocks
   DevArray<uint8_t> ovf_cls;
   DevArray<char> fused_ws;
   DevArray<unsigned long long> vhash;
@@ -129,6 +130,10 @@ struct rvsp_cuda_plan {
   DevArray<uint16_t> rmap;
   DevArray<int64_t> rmap_off;
   DevArray<int32_t> rmap_ops;
+  // Sharing of identical maps: per-row fingerprints, the table they meet in,
+  // and a counter of the rows that read another row's map.
+  DevArray<unsigned long long> rmap_key, rmap_tkey;
+  DevArray<int32_t> rmap_trow, rmap_shared;
   const int32_t *rmap_col = nullptr;
   int rmap_state = 0;
   int64_t rmap_entries = 0;
@@ -318,6 +323,10 @@ void rvsp_cuda_plan_destroy(rvsp_cuda_plan_t p) {
   p->rmap.release();
   p->rmap_off.release();
   p->rmap_ops.release();
+  p->rmap_key.release();
+  p->rmap_tkey.release();
+  p->rmap_trow.release();
+  p->rmap_shared.release();
   p->ops.release();
   p->cls.release();
   p->counts.release();
@@ -490,6 +499,7 @@ rvsp_status_t rvsp_cuda_learned_symbolic(
   if (e == cudaSuccess) e = p->cap.reserve(n);
   if (e == cudaSuccess) e = p->slab_off.reserve(n);
   if (e == cudaSuccess) e = p->ovf_rows.reserve(n);
+  if (e == cudaSuccess) e = p->big_rows.reserve(n + 1);
   if (e == cudaSuccess) e = p->partials.reserve(scan_partials_bytes(a_rows) / sizeof(int64_t));
   if (e != cudaSuccess) return map_cuda(e);
 
@@ -725,12 +735,48 @@ cudaError_t build_reuse_map(rvsp_cuda_plan *p, cudaStream_t s, const Operands &o
     cudaGetLastError();  // out of memory: keep the hash path
     return cudaSuccess;
   }
+  // Fingerprints for sharing identical maps (skipped when the table does not
+  // fit: every row then keeps its own map).
+  int64_t map_rows = 0;
+  for (int c = kEmpty_ + 1; c < kNumClasses; ++c)
+    if (map_class(c) && p->num_count[c] > 0) map_rows += p->num_count[c];
+  size_t tcap = 64;
+  while (tcap < size_t(2 * map_rows)) tcap <<= 1;
+  bool dedup = p->rmap_key.reserve(n) == cudaSuccess &&
+               p->rmap_tkey.reserve(tcap) == cudaSuccess &&
+               p->rmap_trow.reserve(tcap) == cudaSuccess &&
+               p->rmap_shared.reserve(1) == cudaSuccess;
+  if (!dedup) {
+    cudaGetLastError();
+    if (p->rmap_shared.p) cudaMemsetAsync(p->rmap_shared.p, 0, sizeof(int32_t), s);
+  }
   for (int c = kEmpty_ + 1; c < kNumClasses; ++c) {
     if (!map_class(c) || p->num_count[c] <= 0) continue;
     const bool whole = c == p->num_whole;
     launch_map_build(c, op, whole ? nullptr : p->rows_num.p + p->num_off[c],
                      whole ? p->a_rows : p->num_count[c], c_rp, c_col, p->rmap_off.p,
-                     p->rmap.p, p->misc.p + kStatus, s);
+                     p->rmap.p, dedup ? p->rmap_key.p : nullptr, p->misc.p + kStatus, s);
+  }
+  if (dedup) {
+    const unsigned long long mask = tcap - 1;
+    cudaMemsetAsync(p->rmap_tkey.p, 0, tcap * sizeof(unsigned long long), s);
+    cudaMemsetAsync(p->rmap_trow.p, 0x7f, tcap * sizeof(int32_t), s);
+    cudaMemsetAsync(p->rmap_shared.p, 0, sizeof(int32_t), s);
+    for (int pass = 0; pass < 2; ++pass) {
+      for (int c = kEmpty_ + 1; c < kNumClasses; ++c) {
+        if (!map_class(c) || p->num_count[c] <= 0) continue;
+        const bool whole = c == p->num_whole;
+        const int32_t *rows = whole ? nullptr : p->rows_num.p + p->num_off[c];
+        const int32_t nrows = whole ? p->a_rows : p->num_count[c];
+        if (pass == 0)
+          launch_map_dedup_insert(rows, nrows, p->rmap_key.p, p->rmap_tkey.p,
+                                  p->rmap_trow.p, mask, s);
+        else
+          launch_map_dedup_resolve(rows, nrows, p->rmap_key.p, p->rmap_tkey.p,
+                                   p->rmap_trow.p, mask, c_rp, p->rmap_ops.p,
+                                   p->rmap_off.p, p->rmap.p, p->rmap_shared.p, s);
+      }
+    }
   }
   p->rmap_state = 1;
   p->rmap_col = c_col;
@@ -755,6 +801,18 @@ rvsp_status_t rvsp_cuda_plan_prepare_reuse(rvsp_cuda_plan_t p, void *stream,
                     merge_allowed(p->merge_policy, p->a_rows)};
   const cudaError_t e = build_reuse_map(p, s, op, c_row_ptr, c_col_idx);
   if (map_entries_out) *map_entries_out = p->rmap_state == 1 ? p->rmap_entries : 0;
+  return map_cuda(e);
+}
+
+rvsp_status_t rvsp_cuda_plan_reuse_shared_rows(rvsp_cuda_plan_t p, void *stream,
+                                               int32_t *shared_rows_out) {
+  if (!p || !shared_rows_out) return RVSP_ERROR_NULL_POINTER;
+  *shared_rows_out = 0;
+  if (p->rmap_state != 1 || !p->rmap_shared.p) return RVSP_SUCCESS;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  cudaError_t e = cudaMemcpyAsync(shared_rows_out, p->rmap_shared.p, sizeof(int32_t),
+                                  cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
   return map_cuda(e);
 }
 
@@ -792,7 +850,8 @@ rvsp_status_t rvsp_cuda_numeric(rvsp_cuda_plan_t p, void *stream,
     {
       PhaseScope ph(p, s, RVSP_PHASE_COMPACT);
       launch_compact(p->a_rows, p->counts.p, p->slab_off.p, c_row_ptr, p->slab_col.p,
-                     p->slab_val.p, c_col_idx, c_values, true, p->num_sms, s);
+                     p->slab_val.p, c_col_idx, c_values, true, p->big_rows.p,
+                     p->num_sms, s);
       ph.launches = 2;
       for (int c = kEmpty_ + 1; c < kNumClasses && p->n_ovf > 0; ++c) {
         if (p->ovf_num_count[c] <= 0) continue;

@@ -155,6 +155,7 @@ SIGNATURES = {
     "rvsp_spgemm_batch_get_stats": (_int, [_vp, _P(_i32), _P(_i64), _P(_i32), _P(_i32)]),
     "rvsp_cuda_plan_prepare_reuse": (_int, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp,
                                             _P(_i64)]),
+    "rvsp_cuda_plan_reuse_shared_rows": (_int, [_vp, _vp, _P(_i32)]),
     # batches (rvsp_cuda.h)
     "rvsp_cuda_batch_entries": (_int, [_vp, _vp, _i32]),
     "rvsp_cuda_batch_op_counts": (_int, [_vp, _vp, _i32, _vp, _vp]),

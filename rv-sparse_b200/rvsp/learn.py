@@ -18,6 +18,17 @@ N_PARAMS = 1426
 N_TRAINED = 1410
 MU, INV_SD = 1410, 1418
 DEFAULT_WEIGHTS = Path(__file__).resolve().parent.parent / "weights" / "rowmlp_rmat.bin"
+# Trained on R-MAT plus stencil, Laplacian, uniform and Poisson-row products
+# (python -m rvsp.train --families ... --name mixed).
+MIXED_WEIGHTS = DEFAULT_WEIGHTS.parent / "rowmlp_mixed.bin"
+
+
+def weights_for(workload: str) -> Path:
+    """The R-MAT model for power-law inputs, the general one otherwise (when
+    it exists)."""
+    if workload.startswith("rmat") or not MIXED_WEIGHTS.exists():
+        return DEFAULT_WEIGHTS
+    return MIXED_WEIGHTS
 
 
 def _stream():

@@ -144,5 +144,52 @@ def test_reuse_map_implicit_on_stencil():
             A2 = A.with_values(vals)
             want = oracle.spgemm(A2, A2)[2]
             assert np.array_equal(cv.cpu().numpy().view(np.uint32), want.view(np.uint32))
+        # interior rows (at distance >= 2 from every face) repeat one
+        # position pattern: all but one of them read a shared map
+        shared = C.c_int32()
+        L.check(lib.rvsp_cuda_plan_reuse_shared_rows(plan, _stream(), C.byref(shared)),
+                "reuse_shared_rows")
+        assert shared.value >= (20 - 4) ** 3 - 1
+    finally:
+        lib.rvsp_cuda_plan_destroy(plan)
+
+
+def test_reuse_map_shared_patterns_with_distinct_rows():
+    # a few row patterns repeated many times, mixed with random rows: the
+    # repeats share maps, every value stays bit-exact
+    import torch
+    from rvsp.csr import CSR
+    lib = L.load()
+    rng = np.random.default_rng(11)
+    B = gen.uniform_rows(3000, 2500, 24, 12)
+    pats = [np.sort(rng.choice(3000, 20, replace=False)) for _ in range(3)]
+    rows = []
+    for i in range(4000):
+        rows.append(pats[i % 3] if i % 2 == 0 else np.sort(rng.choice(3000, 20, replace=False)))
+    rp = np.zeros(len(rows) + 1, np.int32)
+    rp[1:] = np.cumsum([len(r) for r in rows])
+    ci = np.concatenate(rows).astype(np.int32)
+    A = CSR(len(rows), 3000, rp, ci, rng.uniform(-1, 1, ci.size).astype(np.float32))
+    dA, dB = DeviceCSR.from_host(A), DeviceCSR.from_host(B)
+    plan = C.c_void_p()
+    L.check(lib.rvsp_cuda_plan_create(C.byref(plan)), "plan_create")
+    try:
+        crp, n = _symbolic(lib, plan, dA, dB)
+        cci = torch.zeros(n, dtype=torch.int32, device="cuda")
+        cv = torch.zeros(n, dtype=torch.float32, device="cuda")
+        _numeric(lib, plan, dA, dB, crp, cci, cv, 1)
+        for scale in (0.5, -2.0):
+            A2 = A.with_values((A.values * np.float32(scale)).astype(np.float32))
+            dA.values.copy_(torch.from_numpy(A2.values))
+            torch.cuda.synchronize()
+            cv.zero_()
+            _numeric(lib, plan, dA, dB, crp, cci, cv, 0)
+            want = oracle.spgemm(A2, B)[2]
+            assert np.array_equal(cv.cpu().numpy().view(np.uint32), want.view(np.uint32))
+        shared = C.c_int32()
+        L.check(lib.rvsp_cuda_plan_reuse_shared_rows(plan, _stream(), C.byref(shared)),
+                "reuse_shared_rows")
+        # 2000 rows repeat 3 patterns; the random rows share nothing
+        assert shared.value == 2000 - 3
     finally:
         lib.rvsp_cuda_plan_destroy(plan)
