@@ -71,7 +71,7 @@ def batch_inputs():
     return gen.batched_products(count=BATCH_COUNT, seed=BATCH_SEED)
 
 
-def build_inputs(name: str, seed: int = 2024):
+def build_inputs(name: str, seed: int = 2024, grid: int = 128):
     from rvsp import gen
     if name == "laplace2d":
         A = gen.laplacian_2d(1024)
@@ -79,7 +79,7 @@ def build_inputs(name: str, seed: int = 2024):
     if name == "uniform4096":
         return gen.uniform_rows(4096, 4096, 16, seed), gen.uniform_rows(4096, 4096, 16, seed + 1)
     if name in ("stencil3d", "stencil3d_reuse"):
-        A = gen.stencil_3d_27(128)
+        A = gen.stencil_3d_27(grid)
         return A, A
     if name.startswith("rmat"):
         A = gen.rmat(int(name[4:]), 16, seed=1)
@@ -207,7 +207,7 @@ def run_reference(args, world, rank):
         sample = (f"{args.steps * threads} panels of 256 rows spread over the matrix, one "
                   f"per thread ({args.steps} steps x {threads} threads)")
     else:
-        A, B = build_inputs(args.workload)
+        A, B = build_inputs(args.workload, grid=args.grid)
         flops = 2.0 * float(intermediate_products(A, B).sum())
         per_step = []
         for i in range(args.warmup + args.steps):
@@ -225,7 +225,8 @@ def run_reference(args, world, rank):
             "ms_per_step": 1e3 * el / max(args.steps, 1), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic",
-            "config": {"workload": args.workload, "description": WORKLOADS[args.workload]},
+            "config": {"workload": args.workload, "description": WORKLOADS[args.workload],
+                       "grid": args.grid if "stencil" in args.workload else None},
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": kind,
                              "sample": sample},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
@@ -635,6 +636,9 @@ def main():
     ap.add_argument("--path", default="plain", choices=("plain", "learned"),
                     help="plain GPU Gustavson, or the learned (MLP-binned, fused) path")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--grid", type=int, default=128,
+                    help="stencil workloads: grid edge (128 is the benchmark; smaller "
+                         "grids are for profiler captures)")
     ap.add_argument("--e2e-steps", type=int, default=10)
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
@@ -665,7 +669,7 @@ def main():
                                 device_id=dev)
         pg = dist
 
-    A, B = build_inputs(args.workload)
+    A, B = build_inputs(args.workload, grid=args.grid)
     ops = intermediate_products(A, B)
     flops = 2.0 * float(ops.sum())
     dA = DeviceCSR.from_host(A, dev)
@@ -820,6 +824,7 @@ def main():
             "config": {"workload": args.workload, "description": WORKLOADS[args.workload],
                        "path": args.path,
                        "model": model_file.name if model_file is not None else None,
+                       "grid": args.grid if "stencil" in args.workload else None,
                        "rows": A.rows, "nnz_a": A.nnz, "nnz_b": B.nnz,
                        "overflow_rows": overflow,
                        "nnz_c": c_nnz, "products": int(ops.sum()),

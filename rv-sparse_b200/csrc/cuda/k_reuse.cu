@@ -25,7 +25,6 @@ namespace rvsp {
 namespace {
 
 constexpr int kMapSteppingMinAvgLen = 16;  // same rule as the plain walkers
-constexpr int kMapBatch = 8;               // stepping: A nonzeros loaded per round
 
 __global__ void __launch_bounds__(256)
 map_ops_kernel(const int32_t *__restrict__ rows, int32_t nrows,
@@ -150,12 +149,14 @@ map_dedup_resolve_kernel(const int32_t *__restrict__ rows, int32_t nrows,
                          const int32_t *__restrict__ trow, unsigned long long mask,
                          const int32_t *__restrict__ c_rp, const int32_t *__restrict__ mops,
                          int64_t *__restrict__ moff, const uint16_t *__restrict__ map,
-                         int32_t *__restrict__ shared_rows) {
+                         int32_t *__restrict__ shared_rows, int32_t *__restrict__ canon,
+                         int32_t *__restrict__ share_count) {
   const int64_t w = (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
   if (w >= nrows) return;
   const int lane = lane_id();
   const int32_t row = row_of(rows, static_cast<int32_t>(w));
   const unsigned long long k = key[row];
+  if (lane == 0) canon[row] = k == 0 ? -1 : row;
   if (k == 0) return;
   int32_t c = row;
   if (lane == 0) {
@@ -182,7 +183,9 @@ map_dedup_resolve_kernel(const int32_t *__restrict__ rows, int32_t nrows,
   }
   if (lane == 0) {
     moff[row] = moff[c];
+    canon[row] = c;
     atomicAdd(shared_rows, 1);
+    atomicAdd(share_count + c, 1);
   }
 }
 
@@ -213,38 +216,8 @@ map_numeric_kernel(Operands op, const int64_t *__restrict__ ops,
   int64_t run = 0;
   for (int32_t p = p0; p < p1; p += 32) {
     const AChunk c = load_chunk(op.a_col, op.a_val, op.b_rp, p + lane, p1, true);
-    const int cnt = min(32, p1 - p);
-    if (stepping && __all_sync(kFull, c.len <= 32)) {
-      // Every B row of the chunk fits one lane per entry: issue the loads of
-      // kMapBatch steps together, then apply the steps in order (one DRAM
-      // latency per batch instead of per step).
-      for (int j0 = 0; j0 < cnt; j0 += kMapBatch) {
-        int pos[kMapBatch];
-        float term[kMapBatch];
-#pragma unroll
-        for (int g = 0; g < kMapBatch; ++g) {
-          const int jj = j0 + g;
-          const int len = __shfl_sync(kFull, c.len, jj & 31);
-          const int bbeg = __shfl_sync(kFull, c.bbeg, jj & 31);
-          const float a = __shfl_sync(kFull, c.a, jj & 31);
-          const int excl = __shfl_sync(kFull, c.incl - c.len, jj & 31);
-          pos[g] = -1;
-          term[g] = 0.0f;
-          if (jj < cnt && lane < len) {
-            pos[g] = __ldg(map + base + run + excl + lane);
-            term[g] = __fmul_rn(a, __ldg(op.b_val + bbeg + lane));
-          }
-        }
-#pragma unroll
-        for (int g = 0; g < kMapBatch; ++g) {
-          if (pos[g] >= 0) {
-            if (pos[g] < m) acc[pos[g]] = __fadd_rn(acc[pos[g]], term[g]);
-            else bad = true;
-          }
-          __syncwarp();
-        }
-      }
-    } else if (stepping) {
+    if (stepping) {
+      const int cnt = min(32, p1 - p);
       for (int jj = 0; jj < cnt; ++jj) {
         const int len = __shfl_sync(kFull, c.len, jj);
         const int bbeg = __shfl_sync(kFull, c.bbeg, jj);
@@ -349,11 +322,13 @@ void launch_map_dedup_resolve(const int32_t *rows, int32_t nrows,
                               const unsigned long long *tkey, const int32_t *trow,
                               unsigned long long mask, const int32_t *c_rp,
                               const int32_t *mops, int64_t *moff, const uint16_t *map,
-                              int32_t *shared_rows, cudaStream_t s) {
+                              int32_t *shared_rows, int32_t *canon, int32_t *share_count,
+                              cudaStream_t s) {
   if (nrows <= 0) return;
   const int64_t grid = (int64_t(nrows) * 32 + 255) / 256;
   map_dedup_resolve_kernel<<<static_cast<unsigned>(grid), 256, 0, s>>>(
-      rows, nrows, key, tkey, trow, mask, c_rp, mops, moff, map, shared_rows);
+      rows, nrows, key, tkey, trow, mask, c_rp, mops, moff, map, shared_rows, canon,
+      share_count);
 }
 
 void launch_map_numeric(int cls, const Operands &op, const int64_t *ops, const int32_t *rows,

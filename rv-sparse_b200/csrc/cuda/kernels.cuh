@@ -209,8 +209,10 @@ void launch_map_build(int cls, const Operands &op, const int32_t *rows, int32_t 
 // Sharing of identical maps: insert every listed row's key into the table
 // (tkey zeroed, trow filled with 0x7f bytes, mask + 1 a power of two at least
 // twice the rows inserted over all calls); then resolve, which points
-// moff[row] at the map of the smallest row with an identical map and adds
-// the rows so redirected to *shared_rows.
+// moff[row] at the map of the smallest row c with an identical map, sets
+// canon[row] = c (row itself when no other row shares its map, -1 for a row
+// without a fingerprint), adds 1 to share_count[c] (zeroed by the caller)
+// and the rows so redirected to *shared_rows.
 void launch_map_dedup_insert(const int32_t *rows, int32_t nrows,
                              const unsigned long long *key, unsigned long long *tkey,
                              int32_t *trow, unsigned long long mask, cudaStream_t s);
@@ -219,12 +221,45 @@ void launch_map_dedup_resolve(const int32_t *rows, int32_t nrows,
                               const unsigned long long *tkey, const int32_t *trow,
                               unsigned long long mask, const int32_t *c_rp,
                               const int32_t *mops, int64_t *moff, const uint16_t *map,
-                              int32_t *shared_rows, cudaStream_t s);
+                              int32_t *shared_rows, int32_t *canon, int32_t *share_count,
+                              cudaStream_t s);
 // Values of the listed rows of class cls from the map (structure in C).
 void launch_map_numeric(int cls, const Operands &op, const int64_t *ops, const int32_t *rows,
                         int32_t nrows, const int32_t *c_rp, float *c_val,
                         const int64_t *moff, const uint16_t *map, int32_t *status,
                         cudaStream_t s);
+
+// ---- k_pattern.cu ----------------------------------------------------------
+// Term tables of the rows that share a reuse map (see k_pattern.cu).
+// Select: canonical rows shared by at least min_share rows (itself included)
+// whose row fits a table get pat_of[row] = id (pat_of filled with -1 by the
+// caller), pat_canon[id], pat_cap[id] records; *npat counts them;
+// maxima[0] / maxima[1] (zeroed by the caller) receive the largest products
+// (rounded up to 32) and C row of the tables.
+void launch_pat_select(const int32_t *rows, int32_t nrows, const int32_t *canon,
+                       const int32_t *share_count, int32_t min_share, const int32_t *a_rp,
+                       const int32_t *c_rp, const int32_t *mops, int32_t *pat_of,
+                       int32_t *pat_canon, int32_t *pat_cap, int32_t *npat, int32_t *maxima,
+                       cudaStream_t s);
+// Build: the npat tables at rec + pat_off[id]; psteps[id] = steps, or -1.
+void launch_pat_build(int32_t npat, const int32_t *pat_canon, const int32_t *a_rp,
+                      const int32_t *a_col, const int32_t *b_rp, const int32_t *c_rp,
+                      const int64_t *moff, const uint16_t *map, const int64_t *pat_off,
+                      const int32_t *pat_cap, uint32_t *rec, int32_t *psteps,
+                      cudaStream_t s);
+// Split a class's rows into table rows (pat_rows / pat_ids, appended at
+// *pat_n) and the rest (res_rows, appended at *res_n).
+void launch_pat_split(const int32_t *rows, int32_t nrows, const int32_t *canon,
+                      const int32_t *pat_of, const int32_t *psteps, const int32_t *a_rp,
+                      const int32_t *a_col, const int32_t *b_rp, int32_t *pat_rows,
+                      int32_t *pat_ids, int32_t *pat_n, int32_t *res_rows, int32_t *res_n,
+                      cudaStream_t s);
+// Values of the n table rows (structure in C); max_ops / max_out: the
+// maxima the select step found.
+void launch_pat_numeric(const Operands &op, const int64_t *ops, const int32_t *pat_rows,
+                        const int32_t *pat_ids, int32_t n, const int32_t *c_rp, float *c_val,
+                        const int64_t *pat_off, const int32_t *psteps, const uint32_t *rec,
+                        int32_t max_ops, int32_t max_out, cudaStream_t s);
 
 // ---- k_check.cu ------------------------------------------------------------
 // *result (initialised to ~0ull) receives min over bad rows of

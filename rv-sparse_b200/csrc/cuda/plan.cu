@@ -69,6 +69,9 @@ constexpr int kNumFill = 5 * kNumClasses;
 constexpr int kStatus = 6 * kNumClasses;
 constexpr int kLongCount = 6 * kNumClasses + 1;
 constexpr int kMiscWords = 6 * kNumClasses + 2;
+// A map shared by at least this many rows gets a term table.
+constexpr int32_t kPatMinShare = 16;
+constexpr int kPatCountWords = 4 + kNumClasses;
 
 }  // namespace
 
@@ -133,7 +136,21 @@ struct rvsp_cuda_plan {
   // Sharing of identical maps: per-row fingerprints, the table they meet in,
   // and a counter of the rows that read another row's map.
   DevArray<unsigned long long> rmap_key, rmap_tkey;
-  DevArray<int32_t> rmap_trow, rmap_shared;
+  DevArray<int32_t> rmap_trow, rmap_shared, rmap_canon, rmap_share_count;
+  // Term tables of the shared maps (k_pattern.cu): per table its records,
+  // offset and steps; the rows that use one (pat_rows, pat_ids) and, per W
+  // class, the rows that keep the map (res_rows at res_off[c], res_count[c]).
+  int pat_ready = 0;
+  int32_t n_pat = 0, n_pat_rows = 0;
+  int32_t res_off[kNumClasses] = {};
+  int32_t res_count[kNumClasses] = {};
+  DevArray<int32_t> pat_of, pat_canon, pat_cap, pat_steps, pat_rows, pat_ids, res_rows;
+  // [0] tables, [1] table rows, [2 + c] map rows of class c, then the
+  // tables' largest products and C row
+  DevArray<int32_t> pat_counts;
+  int32_t pat_max_ops = 0, pat_max_out = 0;
+  DevArray<int64_t> pat_off;
+  DevArray<uint32_t> pat_rec;
   const int32_t *rmap_col = nullptr;
   int rmap_state = 0;
   int64_t rmap_entries = 0;
@@ -327,6 +344,18 @@ void rvsp_cuda_plan_destroy(rvsp_cuda_plan_t p) {
   p->rmap_tkey.release();
   p->rmap_trow.release();
   p->rmap_shared.release();
+  p->rmap_canon.release();
+  p->rmap_share_count.release();
+  p->pat_of.release();
+  p->pat_canon.release();
+  p->pat_cap.release();
+  p->pat_steps.release();
+  p->pat_rows.release();
+  p->pat_ids.release();
+  p->res_rows.release();
+  p->pat_counts.release();
+  p->pat_off.release();
+  p->pat_rec.release();
   p->ops.release();
   p->cls.release();
   p->counts.release();
@@ -698,6 +727,83 @@ constexpr size_t kReuseMapMaxBytes = size_t(24) << 30;
 // by an earlier fill).  Leaves rmap_state -1 when the map does not apply:
 // no W rows, a row of more than INT32_MAX / 2 products, or over the memory
 // budget.  Synchronizes s.
+// Term tables for the maps that many rows share (k_pattern.cu), and the
+// split of the W rows into table rows and map rows.  Leaves pat_ready 0 (all
+// W rows on the map) when no map is shared widely enough or the tables would
+// take more than an eighth of the map's bytes.  Synchronizes `s`.
+cudaError_t build_term_tables(rvsp_cuda_plan *p, cudaStream_t s, const Operands &op,
+                              const int32_t *c_rp, int64_t map_entries) {
+  const size_t n = static_cast<size_t>(p->a_rows);
+  cudaError_t e = p->pat_of.reserve(n);
+  if (e == cudaSuccess) e = p->pat_canon.reserve(n);
+  if (e == cudaSuccess) e = p->pat_cap.reserve(n);
+  if (e == cudaSuccess) e = p->pat_counts.reserve(kPatCountWords);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return cudaSuccess;
+  }
+  cudaMemsetAsync(p->pat_of.p, 0xff, n * sizeof(int32_t), s);
+  cudaMemsetAsync(p->pat_counts.p, 0, kPatCountWords * sizeof(int32_t), s);
+  for (int c = kEmpty_ + 1; c < kNumClasses; ++c) {
+    if (!map_class(c) || p->num_count[c] <= 0) continue;
+    const bool whole = c == p->num_whole;
+    launch_pat_select(whole ? nullptr : p->rows_num.p + p->num_off[c],
+                      whole ? p->a_rows : p->num_count[c], p->rmap_canon.p,
+                      p->rmap_share_count.p, kPatMinShare, op.a_rp, c_rp, p->rmap_ops.p,
+                      p->pat_of.p, p->pat_canon.p, p->pat_cap.p, p->pat_counts.p,
+                      p->pat_counts.p + 2 + kNumClasses, s);
+  }
+  int32_t npat = 0;
+  e = cudaMemcpyAsync(&npat, p->pat_counts.p, sizeof(int32_t), cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) return e;
+  if (npat <= 0) return cudaSuccess;
+  e = p->pat_off.reserve(size_t(npat));
+  if (e == cudaSuccess) e = p->pat_steps.reserve(size_t(npat));
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return cudaSuccess;
+  }
+  launch_scan_i64(npat, p->pat_cap.p, p->pat_off.p, p->partials.p, p->total.p, s);
+  int64_t records = 0;
+  e = cudaMemcpyAsync(&records, p->total.p, sizeof(int64_t), cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) return e;
+  const int64_t budget = map_entries * int64_t(sizeof(uint16_t)) / 8;
+  if (records <= 0 || records * int64_t(sizeof(uint32_t)) > budget) return cudaSuccess;
+  if (p->pat_rec.reserve(size_t(records)) != cudaSuccess ||
+      p->pat_rows.reserve(n) != cudaSuccess || p->pat_ids.reserve(n) != cudaSuccess ||
+      p->res_rows.reserve(n) != cudaSuccess) {
+    cudaGetLastError();
+    return cudaSuccess;
+  }
+  launch_pat_build(npat, p->pat_canon.p, op.a_rp, op.a_col, op.b_rp, c_rp, p->rmap_off.p,
+                   p->rmap.p, p->pat_off.p, p->pat_cap.p, p->pat_rec.p, p->pat_steps.p, s);
+  int32_t off = 0;
+  for (int c = kEmpty_ + 1; c < kNumClasses; ++c) {
+    p->res_off[c] = off;
+    if (!map_class(c) || p->num_count[c] <= 0) continue;
+    const bool whole = c == p->num_whole;
+    launch_pat_split(whole ? nullptr : p->rows_num.p + p->num_off[c],
+                     whole ? p->a_rows : p->num_count[c], p->rmap_canon.p, p->pat_of.p,
+                     p->pat_steps.p, op.a_rp, op.a_col, op.b_rp, p->pat_rows.p,
+                     p->pat_ids.p, p->pat_counts.p + 1, p->res_rows.p + off,
+                     p->pat_counts.p + 2 + c, s);
+    off += whole ? p->a_rows : p->num_count[c];
+  }
+  int32_t h[kPatCountWords] = {};
+  e = cudaMemcpyAsync(h, p->pat_counts.p, sizeof(h), cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) return e;
+  p->n_pat = npat;
+  p->n_pat_rows = h[1];
+  for (int c = 0; c < kNumClasses; ++c) p->res_count[c] = h[2 + c];
+  p->pat_max_ops = h[2 + kNumClasses];
+  p->pat_max_out = h[3 + kNumClasses];
+  p->pat_ready = 1;
+  return cudaSuccess;
+}
+
 cudaError_t build_reuse_map(rvsp_cuda_plan *p, cudaStream_t s, const Operands &op,
                             const int32_t *c_rp, const int32_t *c_col) {
   p->rmap_state = -1;
@@ -745,7 +851,9 @@ cudaError_t build_reuse_map(rvsp_cuda_plan *p, cudaStream_t s, const Operands &o
   bool dedup = p->rmap_key.reserve(n) == cudaSuccess &&
                p->rmap_tkey.reserve(tcap) == cudaSuccess &&
                p->rmap_trow.reserve(tcap) == cudaSuccess &&
-               p->rmap_shared.reserve(1) == cudaSuccess;
+               p->rmap_shared.reserve(1) == cudaSuccess &&
+               p->rmap_canon.reserve(n) == cudaSuccess &&
+               p->rmap_share_count.reserve(n) == cudaSuccess;
   if (!dedup) {
     cudaGetLastError();
     if (p->rmap_shared.p) cudaMemsetAsync(p->rmap_shared.p, 0, sizeof(int32_t), s);
@@ -762,6 +870,7 @@ cudaError_t build_reuse_map(rvsp_cuda_plan *p, cudaStream_t s, const Operands &o
     cudaMemsetAsync(p->rmap_tkey.p, 0, tcap * sizeof(unsigned long long), s);
     cudaMemsetAsync(p->rmap_trow.p, 0x7f, tcap * sizeof(int32_t), s);
     cudaMemsetAsync(p->rmap_shared.p, 0, sizeof(int32_t), s);
+    cudaMemsetAsync(p->rmap_share_count.p, 0, n * sizeof(int32_t), s);
     for (int pass = 0; pass < 2; ++pass) {
       for (int c = kEmpty_ + 1; c < kNumClasses; ++c) {
         if (!map_class(c) || p->num_count[c] <= 0) continue;
@@ -774,9 +883,15 @@ cudaError_t build_reuse_map(rvsp_cuda_plan *p, cudaStream_t s, const Operands &o
         else
           launch_map_dedup_resolve(rows, nrows, p->rmap_key.p, p->rmap_tkey.p,
                                    p->rmap_trow.p, mask, c_rp, p->rmap_ops.p,
-                                   p->rmap_off.p, p->rmap.p, p->rmap_shared.p, s);
+                                   p->rmap_off.p, p->rmap.p, p->rmap_shared.p,
+                                   p->rmap_canon.p, p->rmap_share_count.p, s);
       }
     }
+  }
+  p->pat_ready = 0;
+  if (dedup) {
+    e = build_term_tables(p, s, op, c_rp, entries);
+    if (e != cudaSuccess) return e;
   }
   p->rmap_state = 1;
   p->rmap_col = c_col;
@@ -882,12 +997,23 @@ rvsp_status_t rvsp_cuda_numeric(rvsp_cuda_plan_t p, void *stream,
   const bool use_map = fill == 0 && p->rmap_state == 1 && p->rmap_col == c_col_idx;
   {
     PhaseScope ph(p, s, RVSP_PHASE_NUMERIC);
+    if (use_map && p->pat_ready && p->n_pat_rows > 0) {
+      launch_pat_numeric(op, p->ops.p, p->pat_rows.p, p->pat_ids.p, p->n_pat_rows,
+                         c_row_ptr, c_values, p->pat_off.p, p->pat_steps.p, p->pat_rec.p,
+                         p->pat_max_ops, p->pat_max_out, s);
+      ph.launches += 1;
+    }
     for (int c = kEmpty_ + 1; c < kNumClasses; ++c) {
       if (p->num_count[c] <= 0) continue;
       const bool whole = c == p->num_whole;
       const int32_t *rows = whole ? nullptr : p->rows_num.p + p->num_off[c];
       const int32_t nrows = whole ? p->a_rows : p->num_count[c];
-      if (use_map && map_class(c))
+      if (use_map && map_class(c) && p->pat_ready) {
+        if (p->res_count[c] > 0)
+          launch_map_numeric(c, op, p->ops.p, p->res_rows.p + p->res_off[c],
+                             p->res_count[c], c_row_ptr, c_values, p->rmap_off.p,
+                             p->rmap.p, p->misc.p + kStatus, s);
+      } else if (use_map && map_class(c))
         launch_map_numeric(c, op, p->ops.p, rows, nrows, c_row_ptr, c_values,
                            p->rmap_off.p, p->rmap.p, p->misc.p + kStatus, s);
       else

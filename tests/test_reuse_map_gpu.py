@@ -193,3 +193,46 @@ def test_reuse_map_shared_patterns_with_distinct_rows():
         assert shared.value == 2000 - 3
     finally:
         lib.rvsp_cuda_plan_destroy(plan)
+
+
+def test_term_tables_need_equal_b_row_lengths():
+    # rows of type 1 take B rows of 40 + 40 columns, rows of type 2 B rows of
+    # 20 + 60 covering the same 80 columns: the same positions in the same
+    # order (one shared map), but the table of the first type names B entries
+    # that the second type's rows do not have; those rows must keep the map
+    import torch
+    from rvsp.csr import CSR
+    lib = L.load()
+    rng = np.random.default_rng(21)
+    brows = [np.arange(0, 40), np.arange(40, 80), np.arange(0, 20), np.arange(20, 80)]
+    brp = np.zeros(5, np.int32)
+    brp[1:] = np.cumsum([len(r) for r in brows])
+    bci = np.concatenate(brows).astype(np.int32)
+    B = CSR(4, 80, brp, bci, rng.uniform(-1, 1, bci.size).astype(np.float32))
+    arows = [[0, 1] if i % 2 == 0 else [2, 3] for i in range(64)]
+    arp = np.zeros(65, np.int32)
+    arp[1:] = np.cumsum([len(r) for r in arows])
+    aci = np.concatenate(arows).astype(np.int32)
+    A = CSR(64, 4, arp, aci, rng.uniform(-1, 1, aci.size).astype(np.float32))
+    dA, dB = DeviceCSR.from_host(A), DeviceCSR.from_host(B)
+    plan = C.c_void_p()
+    L.check(lib.rvsp_cuda_plan_create(C.byref(plan)), "plan_create")
+    try:
+        crp, n = _symbolic(lib, plan, dA, dB)
+        cci = torch.zeros(n, dtype=torch.int32, device="cuda")
+        cv = torch.zeros(n, dtype=torch.float32, device="cuda")
+        _numeric(lib, plan, dA, dB, crp, cci, cv, 1)
+        for scale in (1.5, -0.25):
+            A2 = A.with_values((A.values * np.float32(scale)).astype(np.float32))
+            dA.values.copy_(torch.from_numpy(A2.values))
+            torch.cuda.synchronize()
+            cv.zero_()
+            _numeric(lib, plan, dA, dB, crp, cci, cv, 0)
+            want = oracle.spgemm(A2, B)[2]
+            assert np.array_equal(cv.cpu().numpy().view(np.uint32), want.view(np.uint32))
+        shared = C.c_int32()
+        L.check(lib.rvsp_cuda_plan_reuse_shared_rows(plan, _stream(), C.byref(shared)),
+                "reuse_shared_rows")
+        assert shared.value == 63  # every row reads row 0's map
+    finally:
+        lib.rvsp_cuda_plan_destroy(plan)
