@@ -116,6 +116,32 @@ rvsp_csr_status_t rvsp_csr_check(int32_t rows, int32_t cols,
 /* rvsp_spgemm.h:53 */
 const char *rvsp_csr_status_string(rvsp_csr_status_t status);
 
+/* Matrix Market reader (no library counterpart: the reference's reader is
+ * the tool function assemble_csr_matrix, tools/src/mtx_to_csr_formatter.c:
+ * 148-325, returning vec_t arrays).  Reads a coordinate file into canonical
+ * FP32 CSR the way that function does -- banner on the first line
+ * ("pattern": values 1.0f; "symmetric": off-diagonal entries mirrored after
+ * all stored ones), '%' lines skipped, "M N L", then up to L 1-based entries
+ * read as fscanf reads them -- with the rows sorted by column and repeated
+ * entries summed in file order on the GPU (rvsp_cuda_coo_to_csr); values are
+ * the reference's bit for bit.  The text is parsed on all host cores.
+ * space RVSP_MEM_HOST: host arrays (owns_data = 1); RVSP_MEM_DEVICE: device
+ * arrays (owns_data = 2); free either with rvsp_csr_destroy.  cols = N.
+ * Errors: unreadable file or size line -> RVSP_ERROR_INVALID_ARGUMENT; an
+ * index outside 1..M x 1..N -> RVSP_ERROR_INVALID_CSR (the reference does
+ * not check); no device -> RVSP_ERROR_UNSUPPORTED_BACKEND. */
+rvsp_status_t rvsp_csr_read_mtx(const char *path, rvsp_memory_space_t space,
+                                rvsp_csr_matrix_t *out);
+/* The same on text already in memory (len bytes, need not end in NUL). */
+rvsp_status_t rvsp_csr_parse_mtx(const char *text, size_t len, rvsp_memory_space_t space,
+                                 rvsp_csr_matrix_t *out);
+
+/* Copies the arrays of src into the arrays dst already holds (rows + 1 row
+ * pointers, nnz columns and values; dst->rows and dst->nnz must equal
+ * src's).  Either side may be host or device memory.  No reference
+ * counterpart (its matrices live in host memory only). */
+rvsp_status_t rvsp_csr_copy_arrays(const rvsp_csr_matrix_t *src, rvsp_csr_matrix_t *dst);
+
 /* rvsp_spgemm.h:34.  Host workspace bytes of a descriptor compute() in host
  * memory space for a given b_cols. */
 rvsp_status_t rvsp_spgemm_buffer_size(int32_t b_cols, size_t *bytes_out);

@@ -244,6 +244,27 @@ rvsp_status_t rvsp_cuda_plan_prepare_reuse(rvsp_cuda_plan_t plan, void *stream,
 rvsp_status_t rvsp_cuda_plan_reuse_shared_rows(rvsp_cuda_plan_t plan, void *stream,
                                                int32_t *shared_rows_out);
 
+/* ---- Matrix Market ingest ------------------------------------------------
+ * COO entries to canonical CSR on the device: the canonicalisation of the
+ * reference's Matrix Market reader (tools/src/mtx_to_csr_formatter.c:67-146,
+ * :214-311).  row / col / val: n device entries, 0-based, in file order.
+ * symmetric != 0 appends the mirror (col, row, val) of every off-diagonal
+ * entry after all stored entries, as the reference does.  Each row is sorted
+ * by column; entries repeating a (row, column) are summed in that order from
+ * the first (acc = v0, then acc = fl(acc + v)), so the result is the
+ * reference's bit for bit.  c_row_ptr: device array of rows + 1, written.
+ * *c_col_out / *c_val_out: device arrays of *c_nnz_out entries (at least
+ * one), allocated here with cudaMalloc and owned by the caller (cudaFree).
+ * An index outside [0, rows) x [0, cols) (or a mirror outside it) gives
+ * RVSP_ERROR_INVALID_CSR (the reference does not check); more than
+ * INT32_MAX output entries give RVSP_ERROR_ALLOCATION_FAILED.  Synchronizes
+ * `stream`. */
+rvsp_status_t rvsp_cuda_coo_to_csr(void *stream, int32_t rows, int32_t cols, int64_t n,
+                                   int symmetric, const int32_t *row, const int32_t *col,
+                                   const float *val, int32_t *c_row_ptr,
+                                   int32_t **c_col_out, float **c_val_out,
+                                   int32_t *c_nnz_out);
+
 /* ---- Batches ------------------------------------------------------------
  * No reference counterpart: the reference computes one product per call.
  * A batch of independent products C_i = A_i * B_i is packed, a group of

@@ -65,8 +65,87 @@ def orc() -> C.CDLL:
         lib.orc_numeric_f32_rows.argtypes = [i32, i32, vp, vp, vp, vp, vp, vp, vp, vp,
                                              vp, vp]
         lib.orc_numeric_f32_rows.restype = None
+        lib.orc_mtx_to_csr.argtypes = [C.c_char_p, C.c_size_t, C.POINTER(i32), C.POINTER(i32),
+                                       C.POINTER(C.c_int64), C.POINTER(vp), C.POINTER(vp),
+                                       C.POINTER(vp)]
+        lib.orc_mtx_to_csr.restype = C.c_int
+        lib.orc_free.argtypes = [vp]
+        lib.orc_free.restype = None
         _orc = lib
     return _orc
+
+
+MTX_ERRORS = {-1: "malformed size line", -2: "index out of range", -3: "out of memory"}
+
+
+def mtx_to_csr(text: bytes):
+    """(rows, cols, row_ptr, col_idx, values) of Matrix Market text, by the
+    restatement of the reference reader (mtx_oracle.c)."""
+    lib = orc()
+    rows, cols, nnz = C.c_int32(), C.c_int32(), C.c_int64()
+    rp, ci, cv = C.c_void_p(), C.c_void_p(), C.c_void_p()
+    rc = lib.orc_mtx_to_csr(text, len(text), C.byref(rows), C.byref(cols), C.byref(nnz),
+                            C.byref(rp), C.byref(ci), C.byref(cv))
+    if rc != 0:
+        raise ValueError(MTX_ERRORS.get(rc, str(rc)))
+    try:
+        n, m = rows.value, nnz.value
+        row_ptr = np.ctypeslib.as_array(C.cast(rp, C.POINTER(C.c_int32)), (n + 1,)).copy()
+        col_idx = (np.ctypeslib.as_array(C.cast(ci, C.POINTER(C.c_int32)), (m,)).copy()
+                   if m else np.zeros(0, np.int32))
+        values = (np.ctypeslib.as_array(C.cast(cv, C.POINTER(C.c_float)), (m,)).copy()
+                  if m else np.zeros(0, np.float32))
+    finally:
+        for p in (rp, ci, cv):
+            lib.orc_free(p)
+    return n, cols.value, row_ptr, col_idx, values
+
+
+MTX_REF_PATH = HERE / "_ref" / "librvsp_mtx_ref.so"
+_mtx_ref = None
+
+
+class _Vec(C.Structure):
+    _fields_ = [("data", C.c_void_p), ("size", C.c_size_t), ("capacity", C.c_size_t),
+                ("elem_size", C.c_size_t)]
+
+
+class _RefMtxCsr(C.Structure):
+    _fields_ = [("row_ptr", C.POINTER(_Vec)), ("col_ind", C.POINTER(_Vec)),
+                ("val", C.POINTER(_Vec))]
+
+
+def ref_mtx_available() -> bool:
+    return MTX_REF_PATH.exists()
+
+
+def ref_mtx_to_csr(path):
+    """(row_ptr, col_idx, values) from the reference's own reader
+    (tools/src/mtx_to_csr_formatter.c assemble_csr_matrix, built into
+    oracle/_ref/librvsp_mtx_ref.so), or None when it fails."""
+    global _mtx_ref
+    if _mtx_ref is None:
+        lib = C.CDLL(str(MTX_REF_PATH), mode=C.RTLD_LOCAL)
+        lib.assemble_csr_matrix.argtypes = [C.c_char_p]
+        lib.assemble_csr_matrix.restype = _RefMtxCsr
+        lib.vector_free.argtypes = [C.POINTER(_Vec)]
+        lib.vector_free.restype = None
+        _mtx_ref = lib
+    r = _mtx_ref.assemble_csr_matrix(str(path).encode())
+    if not r.row_ptr or not r.col_ind or not r.val:
+        return None
+
+    def take(v, ctype, dtype):
+        n = v.contents.size
+        if n == 0:
+            return np.zeros(0, dtype)
+        return np.ctypeslib.as_array(C.cast(v.contents.data, C.POINTER(ctype)), (n,)).copy()
+    try:
+        return (take(r.row_ptr, C.c_int32, np.int32), take(r.col_ind, C.c_int32, np.int32),
+                take(r.val, C.c_float, np.float32))
+    finally:
+        for v in (r.row_ptr, r.col_ind, r.val):
+            _mtx_ref.vector_free(v)
 
 
 def _arrs(M):

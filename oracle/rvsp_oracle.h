@@ -72,6 +72,14 @@ void orc_numeric_f32_rows(int32_t row_begin, int32_t row_end,
                           const int32_t *c_row_ptr, const int32_t *c_col_idx,
                           float *c_values, float *acc);
 
+/* Matrix Market coordinate text to canonical CSR (mtx_oracle.c).  Returns 0,
+ * -1 for a malformed size line, -2 for an index out of range, -3 when out of
+ * memory.  The three arrays are malloc'd: release them with orc_free. */
+int orc_mtx_to_csr(const char *text, size_t len, int32_t *rows_out, int32_t *cols_out,
+                   int64_t *nnz_out, int32_t **row_ptr_out, int32_t **col_idx_out,
+                   float **values_out);
+void orc_free(void *p);
+
 #ifdef __cplusplus
 }
 #endif

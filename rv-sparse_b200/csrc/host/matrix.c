@@ -104,6 +104,26 @@ void rvsp_csr_destroy(rvsp_csr_matrix_t *A)
     A->owns_data = 0;
 }
 
+rvsp_status_t rvsp_csr_copy_arrays(const rvsp_csr_matrix_t *src, rvsp_csr_matrix_t *dst)
+{
+    if (!src || !dst)
+        return RVSP_ERROR_NULL_POINTER;
+    if (src->rows != dst->rows || src->nnz != dst->nnz || src->rows < 0 || src->nnz < 0)
+        return RVSP_ERROR_INVALID_ARGUMENT;
+    if (!src->row_ptr || !dst->row_ptr ||
+        (src->nnz > 0 && (!src->col_idx || !src->values || !dst->col_idx || !dst->values)))
+        return RVSP_ERROR_NULL_POINTER;
+    cudaError_t e = cudaMemcpy(dst->row_ptr, src->row_ptr,
+                               ((size_t)src->rows + 1) * sizeof(int32_t), cudaMemcpyDefault);
+    if (e == cudaSuccess && src->nnz > 0)
+        e = cudaMemcpy(dst->col_idx, src->col_idx, (size_t)src->nnz * sizeof(int32_t),
+                       cudaMemcpyDefault);
+    if (e == cudaSuccess && src->nnz > 0)
+        e = cudaMemcpy(dst->values, src->values, (size_t)src->nnz * sizeof(float),
+                       cudaMemcpyDefault);
+    return rvsp_map_cuda(e);
+}
+
 rvsp_csr_status_t rvsp_csr_check(int32_t rows, int32_t cols,
                                  const int32_t *row_ptr,
                                  const int32_t *col_idx, int32_t *bad_row_out)

@@ -89,6 +89,11 @@ SIGNATURES = {
     "rvsp_spgemm_get_op_counts": (_int, [_vp, _vp, _i32]),
     "rvsp_spgemm_invalidate_structure": (None, [_vp]),
     "rvsp_csr_check": (_int, [_i32, _i32, _vp, _vp, _P(_i32)]),
+    "rvsp_csr_read_mtx": (_int, [C.c_char_p, _int, _P(CsrMatrix)]),
+    "rvsp_csr_parse_mtx": (_int, [C.c_char_p, C.c_size_t, _int, _P(CsrMatrix)]),
+    "rvsp_csr_copy_arrays": (_int, [_P(CsrMatrix), _P(CsrMatrix)]),
+    "rvsp_cuda_coo_to_csr": (_int, [_vp, _i32, _i32, _i64, _int, _vp, _vp, _vp, _vp,
+                                    _P(_vp), _P(_vp), _P(_i32)]),
     "rvsp_csr_status_string": (C.c_char_p, [_int]),
     "rvsp_spgemm_buffer_size": (_int, [_i32, _P(_sz)]),
     "rvsp_spgemm_set_memory_space": (_int, [_vp, _int]),

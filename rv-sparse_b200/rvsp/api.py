@@ -47,6 +47,40 @@ def spgemm_csr(A: CSR, B: CSR, backend: int | None = L.BACKEND_CUDA) -> CSR:
         lib.rvsp_csr_destroy(C.byref(c))
 
 
+def read_mtx(source, device: bool = False):
+    """A Matrix Market file (path) or its text (bytes) as canonical CSR
+    (rvsp_csr_read_mtx / rvsp_csr_parse_mtx): a host CSR, or with
+    device=True a DeviceCSR whose tensors hold the library's device result."""
+    lib = L.load()
+    m = L.CsrMatrix()
+    space = L.MEM_DEVICE if device else L.MEM_HOST
+    if isinstance(source, (bytes, bytearray)):
+        st = lib.rvsp_csr_parse_mtx(bytes(source), len(source), space, C.byref(m))
+    else:
+        st = lib.rvsp_csr_read_mtx(str(source).encode(), space, C.byref(m))
+    L.check(st, "rvsp_csr_read_mtx")
+    try:
+        if device:
+            out = DeviceCSR.empty(m.rows, m.cols, m.nnz)
+            L.check(lib.rvsp_csr_copy_arrays(C.byref(m), C.byref(out.struct(m.nnz))),
+                    "rvsp_csr_copy_arrays")
+            if m.nnz == 0:
+                out.col_idx, out.values = out.col_idx[:0], out.values[:0]
+            return out
+        rp = np.ctypeslib.as_array(C.cast(m.row_ptr, C.POINTER(C.c_int32)),
+                                   shape=(m.rows + 1,)).copy()
+        if m.nnz > 0:
+            ci = np.ctypeslib.as_array(C.cast(m.col_idx, C.POINTER(C.c_int32)),
+                                       shape=(m.nnz,)).copy()
+            cv = np.ctypeslib.as_array(C.cast(m.values, C.POINTER(C.c_float)),
+                                       shape=(m.nnz,)).copy()
+        else:
+            ci, cv = np.zeros(0, np.int32), np.zeros(0, np.float32)
+        return CSR(m.rows, m.cols, rp, ci, cv)
+    finally:
+        lib.rvsp_csr_destroy(C.byref(m))
+
+
 class DeviceCSR:
     """CSR arrays in device memory (torch CUDA tensors, used only as storage)."""
 
