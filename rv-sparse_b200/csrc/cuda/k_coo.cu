@@ -266,10 +266,13 @@ rvsp_status_t status_of(cudaError_t e) {
   return e == cudaErrorMemoryAllocation ? RVSP_ERROR_ALLOCATION_FAILED : RVSP_ERROR_DEVICE;
 }
 
+// Device scratch of one call, freed when the call returns.
 struct Scratch {
-  void *p[8] = {};
+  static constexpr int kSlots = 16;
+  void *p[kSlots] = {};
   int n = 0;
   cudaError_t alloc(void **out, size_t bytes) {
+    if (n >= kSlots) return cudaErrorMemoryAllocation;  // more buffers than slots
     cudaError_t e = cudaMalloc(out, bytes ? bytes : 1);
     if (e == cudaSuccess) p[n++] = *out;
     return e;
