@@ -20,6 +20,7 @@
 #include <cuda_runtime.h>
 
 #include <climits>
+#include <mutex>
 
 #include "device_common.cuh"
 #include "kernels.cuh"
@@ -266,19 +267,57 @@ rvsp_status_t status_of(cudaError_t e) {
   return e == cudaErrorMemoryAllocation ? RVSP_ERROR_ALLOCATION_FAILED : RVSP_ERROR_DEVICE;
 }
 
-// Device scratch of one call, freed when the call returns.
+// A stream-ordered memory pool per device, owned by this file: the
+// canonicalisation's scratch (a few buffers per call, tens of MB for large
+// files) comes from it, and up to kPoolKeepBytes stay reserved between calls,
+// so repeated reads pay no cudaMalloc / cudaFree (which synchronise and map
+// or unmap pages).  Created on first use on each device.
+constexpr int kMaxDevices = 64;
+constexpr unsigned long long kPoolKeepBytes = 1ull << 30;
+cudaMemPool_t g_pool[kMaxDevices] = {};
+std::once_flag g_pool_once[kMaxDevices];
+
+cudaMemPool_t scratch_pool() {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return nullptr;
+  std::call_once(g_pool_once[dev], [dev] {
+    cudaMemPoolProps props = {};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = dev;
+    cudaMemPool_t pool = nullptr;
+    if (cudaMemPoolCreate(&pool, &props) == cudaSuccess) {
+      unsigned long long keep = kPoolKeepBytes;
+      cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+      g_pool[dev] = pool;
+    } else {
+      cudaGetLastError();
+    }
+  });
+  return g_pool[dev];
+}
+
+// Device scratch of one call, from the pool (cudaMalloc when the pool could
+// not be made), released in stream order when the call returns.
 struct Scratch {
   static constexpr int kSlots = 16;
   void *p[kSlots] = {};
   int n = 0;
+  cudaStream_t s = nullptr;
+  cudaMemPool_t pool = nullptr;
+  explicit Scratch(cudaStream_t st) : s(st), pool(scratch_pool()) {}
   cudaError_t alloc(void **out, size_t bytes) {
     if (n >= kSlots) return cudaErrorMemoryAllocation;  // more buffers than slots
-    cudaError_t e = cudaMalloc(out, bytes ? bytes : 1);
+    const size_t b = bytes ? bytes : 1;
+    cudaError_t e = pool ? cudaMallocFromPoolAsync(out, b, pool, s) : cudaMalloc(out, b);
     if (e == cudaSuccess) p[n++] = *out;
     return e;
   }
   ~Scratch() {
-    for (int i = 0; i < n; ++i) cudaFree(p[i]);
+    for (int i = 0; i < n; ++i) {
+      if (pool) cudaFreeAsync(p[i], s);
+      else cudaFree(p[i]);
+    }
   }
 };
 
@@ -301,7 +340,7 @@ extern "C" rvsp_status_t rvsp_cuda_coo_to_csr(void *stream, int32_t rows, int32_
   *c_val_out = nullptr;
   *c_nnz_out = 0;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
-  Scratch sc;
+  Scratch sc(s);
   int32_t *counts = nullptr, *cursor = nullptr, *flags = nullptr, *mid = nullptr, *big = nullptr;
   int64_t *seg = nullptr, *partials = nullptr, *total = nullptr;
   const size_t nr = size_t(rows) + 1;
