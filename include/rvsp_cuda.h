@@ -244,6 +244,34 @@ rvsp_status_t rvsp_cuda_plan_prepare_reuse(rvsp_cuda_plan_t plan, void *stream,
 rvsp_status_t rvsp_cuda_plan_reuse_shared_rows(rvsp_cuda_plan_t plan, void *stream,
                                                int32_t *shared_rows_out);
 
+/* ---- FP64 and INT8 -> INT32 products ----------------------------------------
+ * The values pass of the reference's legacy scalar kernels
+ * (src/kernels/spgemm/legacy/csr_scalar_f64.c:196-262, csr_scalar_i8.c:
+ * 137-185) for a structure already in c_row_ptr / c_col_idx (from
+ * rvsp_cuda_symbolic and a fill by rvsp_cuda_numeric, whose columns do not
+ * depend on the values).  in_dtype RVSP_DTYPE_FP64: double values, each entry
+ * acc = fl(acc + fl(a * b)) over A's nonzeros in order from 0.0;
+ * RVSP_DTYPE_INT8: int8 values, int32 sums of int32 products (wrapping).
+ * c_values (double or int32, row_ptr[a_rows] entries) must be zeroed by the
+ * caller.  Stream-ordered; other dtypes: RVSP_ERROR_UNSUPPORTED_DTYPE. */
+rvsp_status_t rvsp_cuda_typed_numeric(void *stream, int32_t in_dtype, int32_t a_rows,
+                                      const int32_t *a_row_ptr, const int32_t *a_col_idx,
+                                      const void *a_values, const int32_t *b_row_ptr,
+                                      const int32_t *b_col_idx, const void *b_values,
+                                      const int32_t *c_row_ptr, const int32_t *c_col_idx,
+                                      void *c_values);
+
+/* Removes the entries equal to zero (the legacy kernels store only acc != 0;
+ * -0.0 goes too), keeping row and column order: out_* receive the kept
+ * entries (out arrays sized for nnz entries), *out_nnz their count.
+ * out_dtype RVSP_DTYPE_FP64 (double values) or RVSP_DTYPE_INT32.  Allocates
+ * its scratch; synchronizes `stream`. */
+rvsp_status_t rvsp_cuda_drop_zeros(void *stream, int32_t out_dtype, int32_t rows,
+                                   const int32_t *c_row_ptr, int64_t nnz,
+                                   const int32_t *c_col_idx, const void *c_values,
+                                   int32_t *out_row_ptr, int32_t *out_col_idx,
+                                   void *out_values, int32_t *out_nnz);
+
 /* ---- Matrix Market ingest ------------------------------------------------
  * COO entries to canonical CSR on the device: the canonicalisation of the
  * reference's Matrix Market reader (tools/src/mtx_to_csr_formatter.c:67-146,

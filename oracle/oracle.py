@@ -71,6 +71,11 @@ def orc() -> C.CDLL:
         lib.orc_mtx_to_csr.restype = C.c_int
         lib.orc_free.argtypes = [vp]
         lib.orc_free.restype = None
+        for name in ("orc_spgemm_f64", "orc_spgemm_i8"):
+            f = getattr(lib, name)
+            f.argtypes = [i32, i32, vp, vp, vp, vp, vp, vp, C.POINTER(vp), C.POINTER(vp),
+                          C.POINTER(vp), C.POINTER(C.c_int64)]
+            f.restype = C.c_int
         _orc = lib
     return _orc
 
@@ -383,3 +388,70 @@ def time_reference_batch(products, seconds: float = 10.0, threads: int = 1):
     for th in ths:
         th.join()
     return sorted(done), time.perf_counter() - t0
+
+
+# ---- FP64 and INT8 -> INT32 products (legacy scalar kernels) ----------------
+
+_TYPED = {"f64": (np.float64, np.float64, 4, 4), "i8": (np.int8, np.int32, 0, 1)}
+
+
+def _take(ptr, ctype, n, dtype):
+    if n == 0:
+        return np.zeros(0, dtype)
+    return np.ctypeslib.as_array(C.cast(ptr, C.POINTER(ctype)), shape=(n,)).copy().view(dtype)
+
+
+def spgemm_typed(A, B, kind: str):
+    """(row_ptr, col_idx, values) of A x B by the restatement of the legacy
+    scalar kernel; kind "f64" (float64 values) or "i8" (int8 in, int32 out).
+    A and B are (rows, cols, row_ptr, col_idx, values) tuples."""
+    vin, vout, _, _ = _TYPED[kind]
+    ar, ac, arp, aci, av = A
+    br, bc, brp, bci, bv = B
+    arp, aci, brp, bci = (np.ascontiguousarray(x, np.int32) for x in (arp, aci, brp, bci))
+    av, bv = np.ascontiguousarray(av, vin), np.ascontiguousarray(bv, vin)
+    rp, ci, cv, nnz = C.c_void_p(), C.c_void_p(), C.c_void_p(), C.c_int64()
+    f = orc().orc_spgemm_f64 if kind == "f64" else orc().orc_spgemm_i8
+    rc = f(ar, bc, arp.ctypes.data, aci.ctypes.data, av.ctypes.data, brp.ctypes.data,
+           bci.ctypes.data, bv.ctypes.data, C.byref(rp), C.byref(ci), C.byref(cv),
+           C.byref(nnz))
+    if rc != 0:
+        raise MemoryError("oracle out of memory")
+    try:
+        n = nnz.value
+        out_ct = C.c_double if kind == "f64" else C.c_int32
+        return (_take(rp, C.c_int32, ar + 1, np.int32), _take(ci, C.c_int32, n, np.int32),
+                _take(cv, out_ct, n, vout))
+    finally:
+        for p in (rp, ci, cv):
+            orc().orc_free(p)
+
+
+def ref_spgemm_typed(A, B, kind: str):
+    """rvsp_spgemm_csr of the reference library with RVSP_BACKEND_SCALAR and
+    {FP64, FP64} or {INT8, INT32}: (status, row_ptr, col_idx, values)."""
+    vin, vout, in_code, out_code = _TYPED[kind]
+    keep = []
+
+    def st(M):
+        rows, cols, rp, ci, v = M
+        rp, ci = np.ascontiguousarray(rp, np.int32), np.ascontiguousarray(ci, np.int32)
+        v = np.ascontiguousarray(v, vin)
+        keep.extend([rp, ci, v])
+        s = _RefCsr()
+        s.rows, s.cols, s.nnz = rows, cols, int(rp[-1])
+        s.row_ptr, s.col_idx, s.values = rp.ctypes.data, ci.ctypes.data, v.ctypes.data
+        s.dtype, s.format, s.owns_data = in_code, 0, 0
+        return s
+    a, b = st(A), st(B)
+    c = _RefCsr()
+    status = ref().rvsp_spgemm_csr(C.byref(a), C.byref(b), C.byref(c),
+                                   C.byref(_RefOpts(0, in_code, out_code)))
+    if status != 0:
+        return status, None, None, None
+    n = c.nnz
+    out_ct = C.c_double if kind == "f64" else C.c_int32
+    res = (status, _take(c.row_ptr, C.c_int32, c.rows + 1, np.int32),
+           _take(c.col_idx, C.c_int32, n, np.int32), _take(c.values, out_ct, n, vout))
+    ref().rvsp_csr_destroy(C.byref(c))
+    return res

@@ -80,6 +80,17 @@ int orc_mtx_to_csr(const char *text, size_t len, int32_t *rows_out, int32_t *col
                    float **values_out);
 void orc_free(void *p);
 
+/* FP64 and INT8 -> INT32 products of the legacy scalar kernels
+ * (typed_oracle.c).  0, or -3 when out of memory; outputs for orc_free. */
+int orc_spgemm_f64(int32_t a_rows, int32_t b_cols, const int32_t *a_rp, const int32_t *a_ci,
+                   const double *a_v, const int32_t *b_rp, const int32_t *b_ci,
+                   const double *b_v, int32_t **rp_out, int32_t **ci_out, double **v_out,
+                   int64_t *nnz_out);
+int orc_spgemm_i8(int32_t a_rows, int32_t b_cols, const int32_t *a_rp, const int32_t *a_ci,
+                  const int8_t *a_v, const int32_t *b_rp, const int32_t *b_ci,
+                  const int8_t *b_v, int32_t **rp_out, int32_t **ci_out, int32_t **v_out,
+                  int64_t *nnz_out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -58,6 +58,11 @@ rvsp_status_t rvsp_device_check(rvsp_cuda_plan_t plan, cudaStream_t s,
 /* Reference check_operand (spgemm_descr.c:137-160). */
 rvsp_status_t rvsp_check_operand(const rvsp_csr_matrix_t *M);
 
+/* FP64 -> FP64 and INT8 -> INT32 one-shot products on the GPU (typed.c);
+ * in_dtype RVSP_DTYPE_FP64 or RVSP_DTYPE_INT8. */
+rvsp_status_t rvsp_typed_oneshot(const rvsp_csr_matrix_t *A, const rvsp_csr_matrix_t *B,
+                                 rvsp_csr_matrix_t *C, rvsp_dtype_t in_dtype);
+
 /* Host-side prefix of rvsp_csr_check that needs no column reads: negative
  * dims, NULL row_ptr, row_ptr[0] != 0, and (when col_idx is NULL) a
  * non-empty row.  Returns RVSP_CSR_OK when the device check must decide. */

@@ -8,7 +8,9 @@
  * INVALID_ARGUMENT, non-canonical CSR gives INVALID_CSR, C's arrays are
  * malloc'd by the library with owns_data = 1, and on failure C is nulled.
  * CPU backends are not provided: RVSP_BACKEND_SCALAR, _SCALAR_UNROLL4 and
- * _RVV_INTRINSICS report UNSUPPORTED_BACKEND.
+ * _RVV_INTRINSICS report UNSUPPORTED_BACKEND.  RVSP_BACKEND_CUDA with
+ * {FP64, FP64} or {INT8, INT32} runs the legacy kernels' products on the GPU
+ * (typed.c, the reference's spgemm.c:179-193).
  *
  * Each host thread keeps one cached device context (plan, stream, device
  * buffers) for one-shot calls, created on first use and released when the
@@ -256,6 +258,15 @@ rvsp_status_t rvsp_spgemm_csr(const rvsp_csr_matrix_t *A, const rvsp_csr_matrix_
 {
     if (!A || !B || !C)
         return RVSP_ERROR_NULL_POINTER;
+    /* FP64 and INT8 -> INT32: the legacy kernels' products (typed.c) */
+    if (options && options->backend == RVSP_BACKEND_CUDA &&
+        ((options->input_dtype == RVSP_DTYPE_FP64 && options->output_dtype == RVSP_DTYPE_FP64) ||
+         (options->input_dtype == RVSP_DTYPE_INT8 && options->output_dtype == RVSP_DTYPE_INT32))) {
+        rvsp_status_t ts = rvsp_typed_oneshot(A, B, C, options->input_dtype);
+        if (ts != RVSP_SUCCESS)
+            null_c(C);
+        return ts;
+    }
     int is_cuda = 0;
     rvsp_status_t st = resolve_options(options, &is_cuda);
     if (st != RVSP_SUCCESS)

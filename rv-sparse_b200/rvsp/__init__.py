@@ -7,8 +7,8 @@ tests and benchmarks: ctypes bindings (`_lib`), a host CSR container
 """
 from . import _lib as lib
 from ._lib import RvspError, check, load
-from .api import Batch, Descriptor, DeviceCSR, read_mtx, spgemm_csr
+from .api import Batch, Descriptor, DeviceCSR, read_mtx, spgemm_csr, spgemm_typed
 from .csr import CSR, algorithmic_bytes, intermediate_products
 
 __all__ = ["lib", "RvspError", "check", "load", "Batch", "Descriptor", "DeviceCSR",
-           "read_mtx", "spgemm_csr", "CSR", "algorithmic_bytes", "intermediate_products"]
+           "read_mtx", "spgemm_csr", "spgemm_typed", "CSR", "algorithmic_bytes", "intermediate_products"]

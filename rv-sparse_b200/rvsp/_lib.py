@@ -94,6 +94,10 @@ SIGNATURES = {
     "rvsp_csr_copy_arrays": (_int, [_P(CsrMatrix), _P(CsrMatrix)]),
     "rvsp_cuda_coo_to_csr": (_int, [_vp, _i32, _i32, _i64, _int, _vp, _vp, _vp, _vp,
                                     _P(_vp), _P(_vp), _P(_i32)]),
+    "rvsp_cuda_typed_numeric": (_int, [_vp, _i32, _i32, _vp, _vp, _vp, _vp, _vp, _vp, _vp,
+                                       _vp, _vp]),
+    "rvsp_cuda_drop_zeros": (_int, [_vp, _i32, _i32, _vp, _i64, _vp, _vp, _vp, _vp, _vp,
+                                    _P(_i32)]),
     "rvsp_csr_status_string": (C.c_char_p, [_int]),
     "rvsp_spgemm_buffer_size": (_int, [_i32, _P(_sz)]),
     "rvsp_spgemm_set_memory_space": (_int, [_vp, _int]),

@@ -47,6 +47,50 @@ def spgemm_csr(A: CSR, B: CSR, backend: int | None = L.BACKEND_CUDA) -> CSR:
         lib.rvsp_csr_destroy(C.byref(c))
 
 
+_TYPED_CODES = {"f64": (L.DTYPE_FP64, L.DTYPE_FP64, np.float64, np.float64, C.c_double),
+                "i8": (L.DTYPE_INT8, L.DTYPE_INT32, np.int8, np.int32, C.c_int32)}
+
+
+def spgemm_typed(A, B, kind: str, backend: int = L.BACKEND_CUDA):
+    """One-shot FP64 (kind "f64") or INT8 -> INT32 (kind "i8") product
+    through rvsp_spgemm_csr with options {backend, dtypes}.  A and B are
+    (rows, cols, row_ptr, col_idx, values) tuples of host arrays; returns
+    (row_ptr, col_idx, values) or raises RvspError."""
+    lib = L.load()
+    din, dout, vin, vout, ct = _TYPED_CODES[kind]
+    keep = []
+
+    def struct(M):
+        rows, cols, rp, ci, v = M
+        rp, ci = np.ascontiguousarray(rp, np.int32), np.ascontiguousarray(ci, np.int32)
+        v = np.ascontiguousarray(v, vin)
+        keep.extend([rp, ci, v])
+        m = L.CsrMatrix()
+        m.rows, m.cols, m.nnz = rows, cols, int(rp[-1]) if rp.size else 0
+        m.row_ptr, m.col_idx, m.values = rp.ctypes.data, ci.ctypes.data, v.ctypes.data
+        m.dtype, m.format, m.owns_data = din, L.FORMAT_CSR, 0
+        return m
+    a, b = struct(A), struct(B)
+    c = L.CsrMatrix()
+    opts = L.SpgemmOptions(backend, din, dout)
+    L.check(lib.rvsp_spgemm_csr(C.byref(a), C.byref(b), C.byref(c), C.byref(opts)),
+            "rvsp_spgemm_csr")
+    try:
+        n = c.nnz
+        rp = np.ctypeslib.as_array(C.cast(c.row_ptr, C.POINTER(C.c_int32)),
+                                   shape=(c.rows + 1,)).copy()
+        if n > 0:
+            ci = np.ctypeslib.as_array(C.cast(c.col_idx, C.POINTER(C.c_int32)),
+                                       shape=(n,)).copy()
+            cv = np.ctypeslib.as_array(C.cast(c.values, C.POINTER(ct)), shape=(n,)).copy()
+        else:
+            ci, cv = np.zeros(0, np.int32), np.zeros(0, vout)
+        assert c.dtype == dout
+        return rp, ci, cv.astype(vout, copy=False)
+    finally:
+        lib.rvsp_csr_destroy(C.byref(c))
+
+
 def read_mtx(source, device: bool = False):
     """A Matrix Market file (path) or its text (bytes) as canonical CSR
     (rvsp_csr_read_mtx / rvsp_csr_parse_mtx): a host CSR, or with
