@@ -177,7 +177,17 @@ def test_oneshot_argument_errors(golden_fixtures):
         o = L.SpgemmOptions(backend, L.DTYPE_FP32, L.DTYPE_FP32)
         assert lib.rvsp_spgemm_csr(C.byref(a), C.byref(b), C.byref(c),
                                    C.byref(o)) == L.ERROR_UNSUPPORTED_BACKEND
+    # FP64 options reach the FP64 product, whose wrapper refuses FP32 operands
+    # with INVALID_ARGUMENT (csr_spgemm_wrappers.c:362-365); INT8 options
+    # refuse them with UNSUPPORTED_DTYPE (:43-46); other dtype pairs have no
+    # kernel
     o = L.SpgemmOptions(L.BACKEND_CUDA, L.DTYPE_FP64, L.DTYPE_FP64)
+    assert lib.rvsp_spgemm_csr(C.byref(a), C.byref(b), C.byref(c),
+                               C.byref(o)) == L.ERROR_INVALID_ARGUMENT
+    o = L.SpgemmOptions(L.BACKEND_CUDA, L.DTYPE_INT8, L.DTYPE_INT32)
+    assert lib.rvsp_spgemm_csr(C.byref(a), C.byref(b), C.byref(c),
+                               C.byref(o)) == L.ERROR_UNSUPPORTED_DTYPE
+    o = L.SpgemmOptions(L.BACKEND_CUDA, L.DTYPE_FP32, L.DTYPE_FP64)
     assert lib.rvsp_spgemm_csr(C.byref(a), C.byref(b), C.byref(c),
                                C.byref(o)) == L.ERROR_UNSUPPORTED_BACKEND
     f64 = L.CsrMatrix.from_buffer_copy(a)
