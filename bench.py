@@ -317,6 +317,76 @@ def run_mtx(args, world, rank, local):
     return 0
 
 
+def typed_inputs(args):
+    """The workload's matrices with float64 values (the FP32 values widened)
+    or int8 values (seeded, in [-8, 8])."""
+    A, B = build_inputs(args.workload, grid=args.grid)
+    rng = np.random.default_rng(42)
+
+    def vals(M):
+        if args.dtype == "f64":
+            return M.values.astype(np.float64)
+        return rng.integers(-8, 9, M.nnz).astype(np.int8)
+    ta = (A.rows, A.cols, A.row_ptr, A.col_idx, vals(A))
+    tb = ta if B is A else (B.rows, B.cols, B.row_ptr, B.col_idx, vals(B))
+    return A, B, ta, tb
+
+
+def run_typed(args, world, rank, local):
+    """--dtype f64 / i8: a step is one rvsp_spgemm_csr of the workload's
+    matrices with {RVSP_BACKEND_CUDA, FP64, FP64} or {.., INT8, INT32}: host
+    arrays in, host arrays out (the only form the reference offers for these
+    dtypes), timed on the host clock.  The reference's legacy scalar kernel
+    on the same inputs, one thread, is the CPU baseline."""
+    import torch
+    from rvsp import intermediate_products, spgemm_typed
+    if rank != 0:
+        return 0
+    torch.cuda.set_device(local)
+    sys.path.insert(0, str(ROOT))
+    from oracle import oracle
+    A, B, ta, tb = typed_inputs(args)
+    flops = 2.0 * float(intermediate_products(A, B).sum())
+    sampler = ClockSampler(local)
+    sampler.start()
+    for _ in range(args.warmup):
+        rp, ci, cv = spgemm_typed(ta, tb, args.dtype)
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        rp, ci, cv = spgemm_typed(ta, tb, args.dtype)
+        times.append(time.perf_counter() - t0)
+    clocks = sampler.stop()
+    el = float(sum(times))
+    value = flops * args.steps / el / 1e9
+    cpu = None
+    if not args.no_cpu_baseline and oracle.ref_available():
+        t0 = time.perf_counter()
+        st = oracle.ref_spgemm_typed(ta, tb, args.dtype)[0]
+        t = time.perf_counter() - t0
+        if st == 0:
+            cpu = {"value": flops / t / 1e9, "unit": UNIT, "cores": 1, "kind": "reference",
+                   "sample": "one product by the reference's legacy scalar kernel"}
+    in_b = sum(x[2].nbytes + x[3].nbytes + x[4].nbytes for x in ((ta, tb) if tb is not ta else (ta,)))
+    out_b = rp.nbytes + ci.nbytes + cv.nbytes
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * el / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64" if args.dtype == "f64" else "i8->i32", "data": "synthetic",
+            "config": {"workload": args.workload, "description": WORKLOADS[args.workload],
+                       "path": f"one-shot {args.dtype} (host arrays)",
+                       "products": int(flops / 2), "nnz_c": int(rp[-1]),
+                       "timing": "host clock around rvsp_spgemm_csr (host in, host out)"},
+            "clocks": clocks,
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": int(in_b),
+                    "d2h_bytes_per_step": int(out_b),
+                    "api": "rvsp_spgemm_csr {RVSP_BACKEND_CUDA, " +
+                           ("FP64, FP64}" if args.dtype == "f64" else "INT8, INT32}")},
+            "gpu_launches": None, "cpu_baseline": cpu}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def run_reference(args, world, rank):
     """The reference scalar CPU backend (oracle/_ref/librvsp_ref.so, built from
     the reference sources; the C restatement if that is absent) on all host
@@ -796,6 +866,9 @@ def main():
                     help="stencil workloads: grid edge (128 is the benchmark; smaller "
                          "grids are for profiler captures)")
     ap.add_argument("--e2e-steps", type=int, default=10)
+    ap.add_argument("--dtype", default="f32", choices=("f32", "f64", "i8"),
+                    help="f64 / i8: the FP64 or INT8->INT32 one-shot product of the "
+                         "workload's matrices (host arrays in and out)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     world, rank, local = dist_setup()
@@ -819,6 +892,8 @@ def main():
         return run_reference(args, world, rank)
     if args.workload == "mtx_ingest":
         return run_mtx(args, world, rank, local)
+    if args.dtype != "f32":
+        return run_typed(args, world, rank, local)
     if args.workload == "batch512":
         return run_batch(args, world, rank, local)
     if args.workload == "rmat20_panels":

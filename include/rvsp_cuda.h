@@ -264,11 +264,15 @@ rvsp_status_t rvsp_cuda_typed_numeric(void *stream, int32_t in_dtype, int32_t a_
 /* Removes the entries equal to zero (the legacy kernels store only acc != 0;
  * -0.0 goes too), keeping row and column order: out_* receive the kept
  * entries (out arrays sized for nnz entries), *out_nnz their count.
- * out_dtype RVSP_DTYPE_FP64 (double values) or RVSP_DTYPE_INT32.  Allocates
- * its scratch; synchronizes `stream`. */
+ * out_dtype RVSP_DTYPE_FP64 (double values) or RVSP_DTYPE_INT32.  scratch:
+ * device memory of rvsp_cuda_drop_zeros_scratch_bytes(nnz) bytes, 256-byte
+ * aligned.  Synchronizes `stream` once (for the count), then leaves the
+ * compaction queued on it. */
+size_t rvsp_cuda_drop_zeros_scratch_bytes(int64_t nnz);
 rvsp_status_t rvsp_cuda_drop_zeros(void *stream, int32_t out_dtype, int32_t rows,
                                    const int32_t *c_row_ptr, int64_t nnz,
                                    const int32_t *c_col_idx, const void *c_values,
+                                   void *scratch, size_t scratch_bytes,
                                    int32_t *out_row_ptr, int32_t *out_col_idx,
                                    void *out_values, int32_t *out_nnz);
 

@@ -133,42 +133,44 @@ rvsp_status_t typed_status(cudaError_t e) {
   return e == cudaErrorMemoryAllocation ? RVSP_ERROR_ALLOCATION_FAILED : RVSP_ERROR_DEVICE;
 }
 
+size_t align256(size_t b) { return (b + 255) & ~size_t(255); }
+
+// Scratch layout: keep int32[n] | off int64[n] | scan partials | total int64.
+size_t drop_scratch_bytes(int64_t n) {
+  const size_t nb = size_t(n > 0 ? n : 1);
+  return align256(nb * sizeof(int32_t)) + align256(nb * sizeof(int64_t)) +
+         align256(scan_partials_bytes(static_cast<int32_t>(n > 0 ? n : 1))) +
+         align256(sizeof(int64_t));
+}
+
 template <typename T>
 rvsp_status_t drop_zeros(cudaStream_t s, int32_t rows, const int32_t *c_rp, int64_t n,
-                         const int32_t *c_col, const T *c_val, int32_t *out_rp,
-                         int32_t *out_col, T *out_val, int32_t *out_nnz) {
-  int32_t *keep = nullptr;
-  int64_t *off = nullptr, *partials = nullptr, *total = nullptr;
+                         const int32_t *c_col, const T *c_val, char *scratch,
+                         int32_t *out_rp, int32_t *out_col, T *out_val, int32_t *out_nnz) {
   const size_t nb = size_t(n > 0 ? n : 1);
-  cudaError_t e = cudaMalloc(reinterpret_cast<void **>(&keep), nb * sizeof(int32_t));
-  if (e == cudaSuccess) e = cudaMalloc(reinterpret_cast<void **>(&off), nb * sizeof(int64_t));
-  if (e == cudaSuccess)
-    e = cudaMalloc(reinterpret_cast<void **>(&partials),
-                   scan_partials_bytes(static_cast<int32_t>(n > 0 ? n : 1)));
-  if (e == cudaSuccess) e = cudaMalloc(reinterpret_cast<void **>(&total), sizeof(int64_t));
+  int32_t *keep = reinterpret_cast<int32_t *>(scratch);
+  char *p = scratch + align256(nb * sizeof(int32_t));
+  int64_t *off = reinterpret_cast<int64_t *>(p);
+  p += align256(nb * sizeof(int64_t));
+  int64_t *partials = reinterpret_cast<int64_t *>(p);
+  p += align256(scan_partials_bytes(static_cast<int32_t>(n > 0 ? n : 1)));
+  int64_t *total = reinterpret_cast<int64_t *>(p);
   int64_t kept = 0;
-  if (e == cudaSuccess) {
-    cudaMemsetAsync(total, 0, sizeof(int64_t), s);
-    if (n > 0) {
-      nonzero_flags_kernel<T><<<flat_grid(n), kFlatThreads, 0, s>>>(n, c_val, keep);
-      launch_scan_i64(static_cast<int32_t>(n), keep, off, partials, total, s);
-    }
-    e = cudaMemcpyAsync(&kept, total, sizeof(int64_t), cudaMemcpyDeviceToHost, s);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
-    if (e == cudaSuccess) {
-      kept_row_ptr_kernel<<<static_cast<unsigned>((int64_t(rows) + kFlatThreads) / kFlatThreads),
-                            kFlatThreads, 0, s>>>(rows, c_rp, off, n, kept, out_rp);
-      if (n > 0)
-        compact_nonzero_kernel<T><<<flat_grid(n), kFlatThreads, 0, s>>>(
-            n, keep, off, c_col, c_val, out_col, out_val);
-      e = cudaStreamSynchronize(s);
-    }
-    if (e == cudaSuccess) e = cudaGetLastError();
+  cudaMemsetAsync(total, 0, sizeof(int64_t), s);
+  if (n > 0) {
+    nonzero_flags_kernel<T><<<flat_grid(n), kFlatThreads, 0, s>>>(n, c_val, keep);
+    launch_scan_i64(static_cast<int32_t>(n), keep, off, partials, total, s);
   }
-  cudaFree(keep);
-  cudaFree(off);
-  cudaFree(partials);
-  cudaFree(total);
+  cudaError_t e = cudaMemcpyAsync(&kept, total, sizeof(int64_t), cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e == cudaSuccess) {
+    kept_row_ptr_kernel<<<static_cast<unsigned>((int64_t(rows) + kFlatThreads) / kFlatThreads),
+                          kFlatThreads, 0, s>>>(rows, c_rp, off, n, kept, out_rp);
+    if (n > 0)
+      compact_nonzero_kernel<T><<<flat_grid(n), kFlatThreads, 0, s>>>(
+          n, keep, off, c_col, c_val, out_col, out_val);
+    e = cudaGetLastError();
+  }
   if (e != cudaSuccess) return typed_status(e);
   *out_nnz = static_cast<int32_t>(kept);
   return RVSP_SUCCESS;
@@ -212,23 +214,30 @@ extern "C" rvsp_status_t rvsp_cuda_typed_numeric(void *stream, int32_t in_dtype,
   return typed_status(cudaGetLastError());
 }
 
+extern "C" size_t rvsp_cuda_drop_zeros_scratch_bytes(int64_t nnz) {
+  return drop_scratch_bytes(nnz);
+}
+
 extern "C" rvsp_status_t rvsp_cuda_drop_zeros(void *stream, int32_t out_dtype, int32_t rows,
                                               const int32_t *c_row_ptr, int64_t nnz,
                                               const int32_t *c_col_idx, const void *c_values,
+                                              void *scratch, size_t scratch_bytes,
                                               int32_t *out_row_ptr, int32_t *out_col_idx,
                                               void *out_values, int32_t *out_nnz) {
   if (!c_row_ptr || !c_col_idx || !c_values || !out_row_ptr || !out_col_idx || !out_values ||
-      !out_nnz)
+      !out_nnz || !scratch)
     return RVSP_ERROR_NULL_POINTER;
   if (rows < 0 || nnz < 0 || nnz > int64_t(INT32_MAX)) return RVSP_ERROR_INVALID_ARGUMENT;
+  if (scratch_bytes < drop_scratch_bytes(nnz)) return RVSP_ERROR_INVALID_ARGUMENT;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
+  char *sc = static_cast<char *>(scratch);
   if (out_dtype == RVSP_DTYPE_FP64)
     return drop_zeros<double>(s, rows, c_row_ptr, nnz, c_col_idx,
-                              static_cast<const double *>(c_values), out_row_ptr, out_col_idx,
-                              static_cast<double *>(out_values), out_nnz);
+                              static_cast<const double *>(c_values), sc, out_row_ptr,
+                              out_col_idx, static_cast<double *>(out_values), out_nnz);
   if (out_dtype == RVSP_DTYPE_INT32)
     return drop_zeros<int32_t>(s, rows, c_row_ptr, nnz, c_col_idx,
-                               static_cast<const int32_t *>(c_values), out_row_ptr,
+                               static_cast<const int32_t *>(c_values), sc, out_row_ptr,
                                out_col_idx, static_cast<int32_t *>(out_values), out_nnz);
   return RVSP_ERROR_UNSUPPORTED_DTYPE;
 }

@@ -22,6 +22,7 @@
  * kernels store only acc != 0.  C gets malloc'd host arrays (owns_data = 1),
  * dtype FP64 or INT32, as the reference wrappers set them.
  */
+#include <pthread.h>
 #include <stdlib.h>
 #include <string.h>
 
@@ -73,34 +74,68 @@ static int canonical(const rvsp_csr_matrix_t *M)
     return rvsp_csr_check(M->rows, M->cols, M->row_ptr, M->col_idx, NULL) == RVSP_CSR_OK;
 }
 
+/* Per-thread device context of the typed one-shot path: a plan, a stream and
+ * grow-only device buffers, kept between calls so repeated products pay no
+ * cudaMalloc / cudaFree; released when the thread exits. */
 typedef struct {
-    void *p[16];
-    int n;
-} dev_list_t;
+    rvsp_cuda_plan_t plan;
+    cudaStream_t stream;
+    rvsp_dbuf_t a_rp, a_ci, a_v, b_rp, b_ci, b_v, c_rp, c_ci, c_v, ws, o_rp, o_ci, o_v, dz;
+} typed_ctx_t;
 
-static cudaError_t dalloc(dev_list_t *l, void **out, size_t bytes)
+static pthread_key_t g_typed_key;
+static pthread_once_t g_typed_once = PTHREAD_ONCE_INIT;
+
+static void typed_ctx_free(void *p)
 {
-    if (l->n >= 16)
-        return cudaErrorMemoryAllocation;
-    cudaError_t e = cudaMalloc(out, bytes ? bytes : 1);
-    if (e == cudaSuccess)
-        l->p[l->n++] = *out;
-    return e;
+    typed_ctx_t *c = (typed_ctx_t *)p;
+    if (!c)
+        return;
+    if (c->stream)
+        cudaStreamSynchronize(c->stream);
+    rvsp_cuda_plan_destroy(c->plan);
+    rvsp_dbuf_t *bufs[] = {&c->a_rp, &c->a_ci, &c->a_v, &c->b_rp, &c->b_ci, &c->b_v, &c->c_rp,
+                           &c->c_ci, &c->c_v, &c->ws, &c->o_rp, &c->o_ci, &c->o_v, &c->dz};
+    for (size_t i = 0; i < sizeof(bufs) / sizeof(bufs[0]); i++)
+        rvsp_dbuf_release(bufs[i]);
+    if (c->stream)
+        cudaStreamDestroy(c->stream);
+    free(c);
 }
 
-static void dfree_all(dev_list_t *l)
+static void typed_key_init(void) { pthread_key_create(&g_typed_key, typed_ctx_free); }
+
+static rvsp_status_t typed_ctx(typed_ctx_t **out)
 {
-    for (int i = 0; i < l->n; i++)
-        cudaFree(l->p[i]);
-    l->n = 0;
+    pthread_once(&g_typed_once, typed_key_init);
+    typed_ctx_t *c = (typed_ctx_t *)pthread_getspecific(g_typed_key);
+    if (!c) {
+        c = (typed_ctx_t *)calloc(1, sizeof(*c));
+        if (!c)
+            return RVSP_ERROR_ALLOCATION_FAILED;
+        rvsp_status_t st = rvsp_cuda_plan_create(&c->plan);
+        if (st != RVSP_SUCCESS) {
+            free(c);
+            return st;
+        }
+        cudaError_t e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+        if (e != cudaSuccess) {
+            rvsp_cuda_plan_destroy(c->plan);
+            free(c);
+            return rvsp_map_cuda(e);
+        }
+        pthread_setspecific(g_typed_key, c);
+    }
+    *out = c;
+    return RVSP_SUCCESS;
 }
 
-static cudaError_t upload(dev_list_t *l, void **out, const void *src, size_t bytes)
+static rvsp_status_t put(rvsp_dbuf_t *b, const void *src, size_t bytes, cudaStream_t s)
 {
-    cudaError_t e = dalloc(l, out, bytes);
-    if (e == cudaSuccess && bytes)
-        e = cudaMemcpy(*out, src, bytes, cudaMemcpyHostToDevice);
-    return e;
+    rvsp_status_t st = rvsp_dbuf_reserve(b, bytes);
+    if (st == RVSP_SUCCESS && bytes)
+        st = rvsp_map_cuda(cudaMemcpyAsync(b->p, src, bytes, cudaMemcpyHostToDevice, s));
+    return st;
 }
 
 rvsp_status_t rvsp_typed_oneshot(const rvsp_csr_matrix_t *A, const rvsp_csr_matrix_t *B,
@@ -116,141 +151,119 @@ rvsp_status_t rvsp_typed_oneshot(const rvsp_csr_matrix_t *A, const rvsp_csr_matr
     const size_t out_sz = f64 ? sizeof(double) : sizeof(int32_t);
     const rvsp_dtype_t out_dtype = f64 ? RVSP_DTYPE_FP64 : RVSP_DTYPE_INT32;
     const int32_t a_nnz = A->row_ptr[A->rows], b_nnz = B->row_ptr[B->rows];
-    if (A->rows == 0) { /* (FP64 only: INT8 requires rows > 0) an empty product */
-        int32_t *rp = (int32_t *)calloc(1, sizeof(int32_t));
-        int32_t *ci = (int32_t *)malloc(sizeof(int32_t));
-        void *v = malloc(out_sz);
-        if (!rp || !ci || !v) {
-            free(rp);
-            free(ci);
-            free(v);
-            return RVSP_ERROR_ALLOCATION_FAILED;
-        }
-        C->rows = 0;
-        C->cols = B->cols;
-        C->nnz = 0;
-        C->row_ptr = rp;
-        C->col_idx = ci;
-        C->values = v;
-        C->dtype = out_dtype;
-        C->format = RVSP_FORMAT_CSR;
-        C->owns_data = 1;
-        return RVSP_SUCCESS;
-    }
-
-    dev_list_t l = {{0}, 0};
-    rvsp_cuda_plan_t plan = NULL;
-    void *a_rp = NULL, *a_ci = NULL, *a_v = NULL, *b_rp = NULL, *b_ci = NULL, *b_v = NULL;
-    void *c_rp = NULL, *c_ci = NULL, *c_v = NULL, *ws = NULL;
-    void *o_rp = NULL, *o_ci = NULL, *o_v = NULL;
+    const size_t rp_b = ((size_t)A->rows + 1) * sizeof(int32_t);
     int32_t *h_rp = NULL, *h_ci = NULL;
     void *h_v = NULL;
-    int64_t nnz = 0;
-    int32_t kept = 0;
-    cudaError_t e = cudaSuccess;
-
-    st = rvsp_cuda_plan_create(&plan);
-    if (st != RVSP_SUCCESS)
-        return st;
-    e = upload(&l, &a_rp, A->row_ptr, ((size_t)A->rows + 1) * sizeof(int32_t));
-    if (e == cudaSuccess) e = upload(&l, &a_ci, A->col_idx, (size_t)a_nnz * sizeof(int32_t));
-    if (e == cudaSuccess) e = upload(&l, &a_v, A->values, (size_t)a_nnz * in_sz);
-    if (e == cudaSuccess) e = upload(&l, &b_rp, B->row_ptr, ((size_t)B->rows + 1) * sizeof(int32_t));
-    if (e == cudaSuccess) e = upload(&l, &b_ci, B->col_idx, (size_t)b_nnz * sizeof(int32_t));
-    if (e == cudaSuccess) e = upload(&l, &b_v, B->values, (size_t)b_nnz * in_sz);
-    if (e == cudaSuccess) e = dalloc(&l, &c_rp, ((size_t)A->rows + 1) * sizeof(int32_t));
-    if (e != cudaSuccess) {
-        st = rvsp_map_cuda(e);
-        goto done;
-    }
-    st = rvsp_cuda_symbolic(plan, NULL, A->rows, B->rows, B->cols, (const int32_t *)a_rp,
-                            (const int32_t *)a_ci, (const int32_t *)b_rp,
-                            (const int32_t *)b_ci, (int32_t *)c_rp, &nnz);
-    if (st != RVSP_SUCCESS)
-        goto done;
-    {
-        /* C's values buffer holds the fill's FP32 scratch values first
-         * (4 bytes an entry; out_sz >= 4), then the typed sums. */
-        const size_t ws_b = rvsp_cuda_numeric_workspace_bytes(plan);
-        e = dalloc(&l, &c_ci, (size_t)nnz * sizeof(int32_t));
-        if (e == cudaSuccess) e = dalloc(&l, &c_v, (size_t)nnz * out_sz);
-        if (e == cudaSuccess && ws_b) e = dalloc(&l, &ws, ws_b);
-        if (e != cudaSuccess) {
-            st = rvsp_map_cuda(e);
+    if (A->rows == 0) { /* (FP64 only: INT8 requires rows > 0) an empty product */
+        h_rp = (int32_t *)calloc(1, sizeof(int32_t));
+        h_ci = (int32_t *)malloc(sizeof(int32_t));
+        h_v = malloc(out_sz);
+        if (!h_rp || !h_ci || !h_v) {
+            st = RVSP_ERROR_ALLOCATION_FAILED;
             goto done;
         }
-        /* The fill's columns do not depend on the values; A's and B's column
-         * arrays stand in for FP32 values of the right length. */
-        st = rvsp_cuda_numeric(plan, NULL, (const int32_t *)a_rp, (const int32_t *)a_ci,
-                               (const float *)a_ci, (const int32_t *)b_rp,
-                               (const int32_t *)b_ci, (const float *)b_ci,
-                               (const int32_t *)c_rp, (int32_t *)c_ci, (float *)c_v, 1, ws,
-                               ws_b);
-        if (st != RVSP_SUCCESS)
-            goto done;
+        goto out;
     }
-    e = cudaMemsetAsync(c_v, 0, (size_t)nnz * out_sz, NULL);
-    if (e != cudaSuccess) {
-        st = rvsp_map_cuda(e);
-        goto done;
+    typed_ctx_t *c = NULL;
+    st = typed_ctx(&c);
+    if (st != RVSP_SUCCESS)
+        return st;
+    cudaStream_t s = c->stream;
+    const int b_is_a = A->row_ptr == B->row_ptr && A->col_idx == B->col_idx &&
+                       A->values == B->values && A->rows == B->rows;
+    st = put(&c->a_rp, A->row_ptr, rp_b, s);
+    if (st == RVSP_SUCCESS) st = put(&c->a_ci, A->col_idx, (size_t)a_nnz * sizeof(int32_t), s);
+    if (st == RVSP_SUCCESS) st = put(&c->a_v, A->values, (size_t)a_nnz * in_sz, s);
+    if (st == RVSP_SUCCESS && !b_is_a) {
+        st = put(&c->b_rp, B->row_ptr, ((size_t)B->rows + 1) * sizeof(int32_t), s);
+        if (st == RVSP_SUCCESS) st = put(&c->b_ci, B->col_idx, (size_t)b_nnz * sizeof(int32_t), s);
+        if (st == RVSP_SUCCESS) st = put(&c->b_v, B->values, (size_t)b_nnz * in_sz, s);
     }
-    st = rvsp_cuda_typed_numeric(NULL, (int32_t)in_dtype, A->rows, (const int32_t *)a_rp,
-                                 (const int32_t *)a_ci, a_v, (const int32_t *)b_rp,
-                                 (const int32_t *)b_ci, b_v, (const int32_t *)c_rp,
-                                 (const int32_t *)c_ci, c_v);
+    if (st == RVSP_SUCCESS) st = rvsp_dbuf_reserve(&c->c_rp, rp_b);
     if (st != RVSP_SUCCESS)
         goto done;
-    e = dalloc(&l, &o_rp, ((size_t)A->rows + 1) * sizeof(int32_t));
-    if (e == cudaSuccess) e = dalloc(&l, &o_ci, (size_t)nnz * sizeof(int32_t));
-    if (e == cudaSuccess) e = dalloc(&l, &o_v, (size_t)nnz * out_sz);
-    if (e != cudaSuccess) {
-        st = rvsp_map_cuda(e);
+    const int32_t *d_brp = (const int32_t *)(b_is_a ? c->a_rp.p : c->b_rp.p);
+    const int32_t *d_bci = (const int32_t *)(b_is_a ? c->a_ci.p : c->b_ci.p);
+    const void *d_bv = b_is_a ? c->a_v.p : c->b_v.p;
+    int64_t nnz = 0;
+    st = rvsp_cuda_symbolic(c->plan, s, A->rows, B->rows, B->cols, (const int32_t *)c->a_rp.p,
+                            (const int32_t *)c->a_ci.p, d_brp, d_bci, (int32_t *)c->c_rp.p,
+                            &nnz);
+    if (st != RVSP_SUCCESS)
         goto done;
-    }
-    st = rvsp_cuda_drop_zeros(NULL, (int32_t)out_dtype, A->rows, (const int32_t *)c_rp, nnz,
-                              (const int32_t *)c_ci, c_v, (int32_t *)o_rp, (int32_t *)o_ci,
-                              o_v, &kept);
+    /* C's values buffer holds the fill's FP32 scratch values first (4 bytes
+     * an entry; out_sz >= 4), then the typed sums. */
+    const size_t ws_b = rvsp_cuda_numeric_workspace_bytes(c->plan);
+    const size_t dz_b = rvsp_cuda_drop_zeros_scratch_bytes(nnz);
+    st = rvsp_dbuf_reserve(&c->c_ci, (size_t)nnz * sizeof(int32_t));
+    if (st == RVSP_SUCCESS) st = rvsp_dbuf_reserve(&c->c_v, (size_t)nnz * out_sz);
+    if (st == RVSP_SUCCESS && ws_b) st = rvsp_dbuf_reserve(&c->ws, ws_b);
+    if (st == RVSP_SUCCESS) st = rvsp_dbuf_reserve(&c->o_rp, rp_b);
+    if (st == RVSP_SUCCESS) st = rvsp_dbuf_reserve(&c->o_ci, (size_t)nnz * sizeof(int32_t));
+    if (st == RVSP_SUCCESS) st = rvsp_dbuf_reserve(&c->o_v, (size_t)nnz * out_sz);
+    if (st == RVSP_SUCCESS) st = rvsp_dbuf_reserve(&c->dz, dz_b);
+    if (st != RVSP_SUCCESS)
+        goto done;
+    /* The fill's columns do not depend on the values; A's and B's column
+     * arrays stand in for FP32 values of the right length. */
+    st = rvsp_cuda_numeric(c->plan, s, (const int32_t *)c->a_rp.p, (const int32_t *)c->a_ci.p,
+                           (const float *)c->a_ci.p, d_brp, d_bci, (const float *)d_bci,
+                           (const int32_t *)c->c_rp.p, (int32_t *)c->c_ci.p,
+                           (float *)c->c_v.p, 1, ws_b ? c->ws.p : NULL, ws_b);
     if (st == RVSP_SUCCESS)
-        st = rvsp_cuda_plan_status(plan, NULL);
+        st = rvsp_map_cuda(cudaMemsetAsync(c->c_v.p, 0, (size_t)nnz * out_sz, s));
+    if (st == RVSP_SUCCESS)
+        st = rvsp_cuda_typed_numeric(s, (int32_t)in_dtype, A->rows, (const int32_t *)c->a_rp.p,
+                                     (const int32_t *)c->a_ci.p, c->a_v.p, d_brp, d_bci, d_bv,
+                                     (const int32_t *)c->c_rp.p, (const int32_t *)c->c_ci.p,
+                                     c->c_v.p);
+    int32_t kept = 0;
+    if (st == RVSP_SUCCESS)
+        st = rvsp_cuda_drop_zeros(s, (int32_t)out_dtype, A->rows, (const int32_t *)c->c_rp.p,
+                                  nnz, (const int32_t *)c->c_ci.p, c->c_v.p, c->dz.p, dz_b,
+                                  (int32_t *)c->o_rp.p, (int32_t *)c->o_ci.p, c->o_v.p, &kept);
+    if (st == RVSP_SUCCESS)
+        st = rvsp_cuda_plan_status(c->plan, s);
     if (st != RVSP_SUCCESS)
         goto done;
     {
         const size_t kn = (size_t)(kept > 0 ? kept : 1);
-        h_rp = (int32_t *)malloc(((size_t)A->rows + 1) * sizeof(int32_t));
+        h_rp = (int32_t *)malloc(rp_b);
         h_ci = (int32_t *)malloc(kn * sizeof(int32_t));
         h_v = malloc(kn * out_sz);
         if (!h_rp || !h_ci || !h_v) {
             st = RVSP_ERROR_ALLOCATION_FAILED;
             goto done;
         }
-        e = cudaMemcpy(h_rp, o_rp, ((size_t)A->rows + 1) * sizeof(int32_t),
-                       cudaMemcpyDeviceToHost);
+        cudaError_t e = cudaMemcpyAsync(h_rp, c->o_rp.p, rp_b, cudaMemcpyDeviceToHost, s);
         if (e == cudaSuccess && kept > 0)
-            e = cudaMemcpy(h_ci, o_ci, (size_t)kept * sizeof(int32_t), cudaMemcpyDeviceToHost);
+            e = cudaMemcpyAsync(h_ci, c->o_ci.p, (size_t)kept * sizeof(int32_t),
+                                cudaMemcpyDeviceToHost, s);
         if (e == cudaSuccess && kept > 0)
-            e = cudaMemcpy(h_v, o_v, (size_t)kept * out_sz, cudaMemcpyDeviceToHost);
+            e = cudaMemcpyAsync(h_v, c->o_v.p, (size_t)kept * out_sz, cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess)
+            e = cudaStreamSynchronize(s);
         if (e != cudaSuccess) {
             st = rvsp_map_cuda(e);
             goto done;
         }
+        C->nnz = kept;
     }
+out:
+    if (A->rows == 0)
+        C->nnz = 0;
     C->rows = A->rows;
     C->cols = B->cols;
-    C->nnz = kept;
     C->row_ptr = h_rp;
     C->col_idx = h_ci;
     C->values = h_v;
     C->dtype = out_dtype;
     C->format = RVSP_FORMAT_CSR;
     C->owns_data = 1;
-    h_rp = NULL;
-    h_ci = NULL;
-    h_v = NULL;
+    return RVSP_SUCCESS;
 done:
     free(h_rp);
     free(h_ci);
     free(h_v);
-    dfree_all(&l);
-    rvsp_cuda_plan_destroy(plan);
     return st;
 }

@@ -96,8 +96,9 @@ SIGNATURES = {
                                     _P(_vp), _P(_vp), _P(_i32)]),
     "rvsp_cuda_typed_numeric": (_int, [_vp, _i32, _i32, _vp, _vp, _vp, _vp, _vp, _vp, _vp,
                                        _vp, _vp]),
-    "rvsp_cuda_drop_zeros": (_int, [_vp, _i32, _i32, _vp, _i64, _vp, _vp, _vp, _vp, _vp,
-                                    _P(_i32)]),
+    "rvsp_cuda_drop_zeros": (_int, [_vp, _i32, _i32, _vp, _i64, _vp, _vp, _vp, _sz, _vp,
+                                    _vp, _vp, _P(_i32)]),
+    "rvsp_cuda_drop_zeros_scratch_bytes": (_sz, [_i64]),
     "rvsp_csr_status_string": (C.c_char_p, [_int]),
     "rvsp_spgemm_buffer_size": (_int, [_i32, _P(_sz)]),
     "rvsp_spgemm_set_memory_space": (_int, [_vp, _int]),
