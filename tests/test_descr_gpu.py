@@ -156,3 +156,30 @@ def _copy_device_to_host(dst: np.ndarray, src_ptr: int, nbytes: int):
     err, = rt.cudaMemcpy(dst.ctypes.data, src_ptr, nbytes,
                          rt.cudaMemcpyKind.cudaMemcpyDeviceToHost)
     assert int(err) == 0
+
+
+def test_device_chain_keeps_c_on_device():
+    # (A B) C with the intermediate product never leaving the device: the
+    # first result (owns_data = 2) is the left operand of the second call
+    lib = L.load()
+    A = gen.uniform_rows(1500, 1200, 9, 31)
+    B = gen.uniform_rows(1200, 1300, 7, 32)
+    Cm = gen.uniform_rows(1300, 900, 5, 33)
+    rp1, ci1, cv1, _ = oracle.spgemm(A, B)
+    AB = CSR(A.rows, B.cols, rp1, ci1, cv1)
+    rp2, ci2, cv2, _ = oracle.spgemm(AB, Cm)
+    dA, dB, dC = DeviceCSR.from_host(A), DeviceCSR.from_host(B), DeviceCSR.from_host(Cm)
+    a, b, c3 = dA.struct(), dB.struct(), dC.struct()
+    ab = L.CsrMatrix()
+    assert lib.rvsp_spgemm_csr_device(C.byref(a), C.byref(b), C.byref(ab), None) == L.SUCCESS
+    abc = L.CsrMatrix()
+    assert lib.rvsp_spgemm_csr_device(C.byref(ab), C.byref(c3), C.byref(abc), None) == L.SUCCESS
+    h_rp = np.zeros(A.rows + 1, np.int32)
+    h_ci = np.zeros(abc.nnz, np.int32)
+    h_cv = np.zeros(abc.nnz, np.float32)
+    for dst, src in ((h_rp, abc.row_ptr), (h_ci, abc.col_idx), (h_cv, abc.values)):
+        _copy_device_to_host(dst, src, dst.nbytes)
+    assert np.array_equal(h_rp, rp2) and np.array_equal(h_ci, ci2)
+    assert np.array_equal(h_cv.view(np.uint32), cv2.view(np.uint32))
+    lib.rvsp_csr_destroy(C.byref(ab))
+    lib.rvsp_csr_destroy(C.byref(abc))
