@@ -172,6 +172,84 @@ merge_numeric_kernel(Operands op, const int32_t *__restrict__ rows, int32_t nrow
   else if (out != out_end) report(status, kDevCountMismatch);
 }
 
+// Outputs a warp can stage in shared memory (24 KB a block of 4 warps).
+constexpr int kStageOut = 768;
+
+// The non-fused numeric pass: the same merge, order and roundings as
+// merge_numeric_kernel, but a warp whose 32 rows have at most kStageOut
+// outputs in all writes them to shared memory first and then copies them to
+// C together, 32 consecutive outputs per step: the rows of a warp are mostly
+// consecutive rows, so the copy writes whole lines instead of 32 scattered
+// words per store.  A warp with more outputs writes them directly.
+template <int K>
+__global__ void __launch_bounds__(kMergeThreads, MergeOccupancy<K, true>::value)
+merge_numeric_fill_kernel(Operands op, const int32_t *__restrict__ rows, int32_t nrows,
+                          const int32_t *__restrict__ c_rp, int32_t *__restrict__ c_col,
+                          float *__restrict__ c_val, bool fill,
+                          int32_t *__restrict__ status) {
+  __shared__ int32_t s_col[kMergeThreads / 32][kStageOut];
+  __shared__ float s_val[kMergeThreads / 32][kStageOut];
+  const int32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int lane = lane_id(), wb = threadIdx.x >> 5;
+  const bool valid = t < nrows;
+  int32_t row = 0;
+  int64_t out0 = 0, out_end = 0;
+  if (valid) {
+    row = row_of(rows, t);
+    out0 = c_rp[row];
+    out_end = c_rp[row + 1];
+  }
+  const int32_t m = static_cast<int32_t>(out_end - out0);  // <= 2048 in these classes
+  const int32_t incl = warp_incl_scan(m);
+  const int32_t total = __shfl_sync(kFull, incl, 31);
+  const int32_t base = incl - m;
+  const bool staged = total <= kStageOut;  // the same in every lane
+  if (valid) {
+    const int32_t p0 = op.a_rp[row];
+    const int32_t k = op.a_rp[row + 1] - p0;
+    Lists<K> L;
+    open_lists<K, true>(op, p0, k, L);
+    int32_t n = 0;
+    for (;;) {
+      const int32_t mn = min_head<K>(L);
+      if (mn == INT_MAX) break;
+      float acc = 0.0f;
+#pragma unroll
+      for (int j = 0; j < K; ++j) {
+        if (L.cur[j] == mn) {
+          acc = __fadd_rn(acc, __fmul_rn(L.a[j], L.curv[j]));
+          advance<K, true>(op, L, j);
+        }
+      }
+      if (n < m) {
+        if (staged) {
+          s_col[wb][base + n] = mn;
+          s_val[wb][base + n] = acc;
+        } else {
+          if (fill) c_col[out0 + n] = mn;
+          c_val[out0 + n] = acc;
+        }
+      }
+      ++n;
+    }
+    if (n != m) report(status, kDevCountMismatch);
+  }
+  if (!staged) return;
+  __syncwarp();
+  for (int32_t e0 = 0; e0 < total; e0 += 32) {
+    const int32_t e = e0 + lane;
+    const bool v = e < total;
+    const int j = warp_owner_of(incl, v ? e : 0);
+    const int64_t dst0 = __shfl_sync(kFull, out0, j);
+    const int32_t b = __shfl_sync(kFull, base, j);
+    if (v) {
+      const int64_t d = dst0 + (e - b);
+      if (fill) c_col[d] = s_col[wb][e];
+      c_val[d] = s_val[wb][e];
+    }
+  }
+}
+
 template <int K>
 void sym(const Operands &op, const int32_t *rows, int32_t nrows, int32_t *counts,
          cudaStream_t s) {
@@ -188,8 +266,8 @@ void num(const Operands &op, const int32_t *rows, int32_t nrows, const int32_t *
     merge_numeric_kernel<K, true><<<grid, kMergeThreads, 0, s>>>(
         op, rows, nrows, c_rp, c_col, c_val, true, status, *fo);
   else
-    merge_numeric_kernel<K, false><<<grid, kMergeThreads, 0, s>>>(
-        op, rows, nrows, c_rp, c_col, c_val, fill, status, FusedOut{});
+    merge_numeric_fill_kernel<K><<<grid, kMergeThreads, 0, s>>>(op, rows, nrows, c_rp, c_col,
+                                                                c_val, fill, status);
 }
 
 }  // namespace
