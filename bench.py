@@ -111,7 +111,9 @@ def committed_traffic(workload: str, phase: str):
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+    """nvidia-smi clocks and throttle reasons sampled every 50 ms; start()
+    returns once the first sample is written, so the timed region that
+    follows is covered."""
 
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
@@ -127,10 +129,16 @@ class ClockSampler:
             self.fh = open(self.path, "w")
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
-                 "--format=csv,noheader,nounits", "-lms", "200"],
+                 "--format=csv,noheader,nounits", "-lms", "50"],
                 stdout=self.fh, stderr=subprocess.DEVNULL)
         except Exception:
             self.proc = None
+            return
+        t0 = time.time()
+        while time.time() - t0 < 5.0 and self.proc.poll() is None:
+            if self.path.exists() and self.path.stat().st_size > 0:
+                break
+            time.sleep(0.02)
 
     def stop(self):
         if self.proc is None:
@@ -855,7 +863,10 @@ def cpu_baseline(A, B, flops, seconds=12.0):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=40)
+    ap.add_argument("--steps", type=int, default=None,
+                    help="timed steps (default: 1500 for the sub-millisecond laplace2d and "
+                         "uniform4096 steps, so the timed region lasts long enough for the "
+                         "clock samples; 40 otherwise; 3 for --impl reference)")
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--workload", default="laplace2d", choices=sorted(WORKLOADS))
     ap.add_argument("--impl", default="ours", choices=("ours", "reference"))
@@ -870,6 +881,11 @@ def main():
                     help="f64 / i8: the FP64 or INT8->INT32 one-shot product of the "
                          "workload's matrices (host arrays in and out)")
     args = ap.parse_args()
+    if args.steps is None:
+        if args.impl == "reference":
+            args.steps = 3  # each step is seconds of CPU work
+        else:
+            args.steps = 1500 if args.workload in ("laplace2d", "uniform4096") else 40
     args.warmup = max(args.warmup, 3)
     world, rank, local = dist_setup()
 
