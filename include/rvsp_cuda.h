@@ -55,6 +55,23 @@ rvsp_status_t rvsp_cuda_symbolic(rvsp_cuda_plan_t plan, void *stream,
  * the reference's host workspace. */
 size_t rvsp_cuda_numeric_workspace_bytes(rvsp_cuda_plan_t plan);
 
+/* rvsp_cuda_symbolic with the canonical-CSR check of A (and of B when
+ * check_b != 0) folded in: the checks (rvsp_cuda_csr_check) are queued
+ * before the row statistics, which read only A's a_nnz entries and B's
+ * b_rows + 1 row pointers whatever the structure holds, and one host round
+ * trip returns both the checks' verdicts and the class sizes.  A structure
+ * that fails either check gives RVSP_ERROR_INVALID_CSR before any pass that
+ * depends on it runs (the plan is left unanalysed).  Otherwise the same
+ * results as rvsp_cuda_symbolic, with one host round trip fewer than
+ * calling the check first.  Synchronizes `stream`. */
+rvsp_status_t rvsp_cuda_symbolic_checked(rvsp_cuda_plan_t plan, void *stream, int32_t a_rows,
+                                         int32_t a_cols, int32_t a_nnz, int32_t b_rows,
+                                         int32_t b_cols, int32_t b_nnz,
+                                         const int32_t *a_row_ptr, const int32_t *a_col_idx,
+                                         const int32_t *b_row_ptr, const int32_t *b_col_idx,
+                                         int check_b, int32_t *c_row_ptr,
+                                         int64_t *c_nnz_out);
+
 /* Replaces rvsp_symbolic_fill (rvsp_spgemm.h:72-79) and
  * rvsp_spgemm_scalar_f32_numeric (rvsp_spgemm.h:93, gustavson_core_f32.inc:
  * 18-64): writes c_values and, when fill != 0, c_col_idx sorted within rows.

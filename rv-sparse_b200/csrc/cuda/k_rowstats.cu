@@ -15,6 +15,23 @@ constexpr int kThreads = 256;
 
 // Adds one to class_count[c] for every lane with take, one atomic per class
 // per warp.
+// A row's entry range, cut to [0, a_nnz] when the bound is known.
+__device__ __forceinline__ void row_range(const Operands &op, int32_t i, int32_t &p0,
+                                          int32_t &p1) {
+  p0 = op.a_rp[i];
+  p1 = op.a_rp[i + 1];
+  if (op.a_nnz >= 0) {
+    p0 = min(max(p0, 0), op.a_nnz);
+    p1 = min(max(p1, p0), op.a_nnz);
+  }
+}
+
+// |B row k|, or 0 for a k outside B when B's row count is known.
+__device__ __forceinline__ int32_t b_len(const Operands &op, int32_t k) {
+  if (op.b_rows >= 0 && (k < 0 || k >= op.b_rows)) return 0;
+  return __ldg(op.b_rp + k + 1) - __ldg(op.b_rp + k);
+}
+
 __device__ __forceinline__ void count_class(int32_t *s_cnt, bool take, int c) {
   const unsigned peers = __match_any_sync(kFull, take ? c : (-1 - lane_id()));
   if (take && (peers & lanemask_lt()) == 0) atomicAdd(&s_cnt[c], __popc(peers));
@@ -33,16 +50,14 @@ rowstats_kernel(Operands op, int64_t *__restrict__ ops, uint8_t *__restrict__ cl
   bool take = false;
   int c = kEmpty_;
   if (i < op.a_rows) {
-    const int32_t p0 = op.a_rp[i], p1 = op.a_rp[i + 1];
+    int32_t p0, p1;
+    row_range(op, i, p0, p1);
     if (p1 - p0 > kLongRowNnz) {
       const int32_t slot = atomicAdd(long_count, 1);
       if (slot < max_long) long_rows[slot] = i;
     } else {
       int64_t s = 0;
-      for (int32_t p = p0; p < p1; ++p) {
-        const int32_t k = __ldg(op.a_col + p);
-        s += __ldg(op.b_rp + k + 1) - __ldg(op.b_rp + k);
-      }
+      for (int32_t p = p0; p < p1; ++p) s += b_len(op, __ldg(op.a_col + p));
       c = classify_row(p1 - p0, s, s < op.b_cols ? s : op.b_cols, op.merge_ok);
       ops[i] = s;
       cls[i] = static_cast<uint8_t>(c);
@@ -69,12 +84,10 @@ rowstats_long_kernel(Operands op, const int32_t *__restrict__ long_rows,
   for (int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; w < n_long;
        w += warps) {
     const int32_t i = long_rows[w];
-    const int32_t p0 = op.a_rp[i], p1 = op.a_rp[i + 1];
+    int32_t p0, p1;
+    row_range(op, i, p0, p1);
     long long s = 0;
-    for (int32_t p = p0 + lane; p < p1; p += 32) {
-      const int32_t k = __ldg(op.a_col + p);
-      s += __ldg(op.b_rp + k + 1) - __ldg(op.b_rp + k);
-    }
+    for (int32_t p = p0 + lane; p < p1; p += 32) s += b_len(op, __ldg(op.a_col + p));
     s = warp_sum64(s);
     if (lane == 0) {
       const int c = classify_row(p1 - p0, s, s < op.b_cols ? s : op.b_cols, op.merge_ok);

@@ -87,6 +87,11 @@ struct Operands {
   // Rows may take the merge classes (set by the plan from its merge policy
   // and the row count; see classify_row).
   bool merge_ok;
+  // When >= 0: A's entry count and B's row count, which bound every index
+  // the row statistics read, so they run safely on structure whose device
+  // check has not finished yet (rvsp_cuda_symbolic_checked).
+  int32_t a_nnz = -1;
+  int32_t b_rows = -1;
 };
 
 // Merge policies of a plan: automatic (merge classes when the matrix has at

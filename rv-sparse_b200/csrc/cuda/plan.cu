@@ -93,6 +93,7 @@ struct rvsp_cuda_plan {
   DevArray<uint32_t> sym_bits;
   DevArray<unsigned long long> check;
   DevArray<int32_t> check_long;  // count + list of the long rows the check met
+  DevArray<int32_t> check_long_b;  // the same for B in rvsp_cuda_symbolic_checked
   int32_t sym_bits_slots = 0;
 
   int32_t *h_misc = nullptr;  // pinned, kMiscWords
@@ -318,10 +319,10 @@ rvsp_status_t rvsp_cuda_plan_create(rvsp_cuda_plan_t *plan) {
   p->num_sms = sms > 0 ? sms : 148;
   cudaError_t e = p->misc.reserve(kMiscWords);
   if (e == cudaSuccess) e = p->total.reserve(1);
-  if (e == cudaSuccess) e = p->check.reserve(1);
+  if (e == cudaSuccess) e = p->check.reserve(2);
   if (e == cudaSuccess) e = cudaMallocHost(reinterpret_cast<void **>(&p->h_misc), kMiscWords * sizeof(int32_t));
   if (e == cudaSuccess) e = cudaMallocHost(reinterpret_cast<void **>(&p->h_total), sizeof(int64_t));
-  if (e == cudaSuccess) e = cudaMallocHost(reinterpret_cast<void **>(&p->h_check), sizeof(unsigned long long));
+  if (e == cudaSuccess) e = cudaMallocHost(reinterpret_cast<void **>(&p->h_check), 2 * sizeof(unsigned long long));
   if (e == cudaSuccess) e = cudaMallocHost(reinterpret_cast<void **>(&p->h_vhash), 2 * sizeof(unsigned long long));
   if (e == cudaSuccess) e = p->vhash.reserve(2);
   if (e == cudaSuccess) e = cudaMemset(p->misc.p, 0, kMiscWords * sizeof(int32_t));
@@ -368,6 +369,7 @@ void rvsp_cuda_plan_destroy(rvsp_cuda_plan_t p) {
   p->sym_bits.release();
   p->check.release();
   p->check_long.release();
+  p->check_long_b.release();
   p->cap.release();
   p->slab_off.release();
   p->slab_col.release();
@@ -384,6 +386,23 @@ void rvsp_cuda_plan_destroy(rvsp_cuda_plan_t p) {
   delete p;
 }
 
+namespace {
+
+// The structure checks rvsp_cuda_symbolic_checked folds into the symbolic
+// pass: A always, B unless it is A.
+struct PreCheck {
+  int32_t a_cols, a_nnz, b_nnz;
+  bool check_b;
+};
+
+rvsp_status_t symbolic_impl(rvsp_cuda_plan_t p, cudaStream_t s, int32_t a_rows,
+                            int32_t b_rows, int32_t b_cols, const int32_t *a_row_ptr,
+                            const int32_t *a_col_idx, const int32_t *b_row_ptr,
+                            const int32_t *b_col_idx, int32_t *c_row_ptr,
+                            int64_t *c_nnz_out, const PreCheck *chk);
+
+}  // namespace
+
 rvsp_status_t rvsp_cuda_symbolic(rvsp_cuda_plan_t p, void *stream, int32_t a_rows,
                                  int32_t b_rows, int32_t b_cols,
                                  const int32_t *a_row_ptr,
@@ -395,7 +414,38 @@ rvsp_status_t rvsp_cuda_symbolic(rvsp_cuda_plan_t p, void *stream, int32_t a_row
       !c_nnz_out)
     return RVSP_ERROR_NULL_POINTER;
   if (a_rows <= 0 || b_rows <= 0 || b_cols <= 0) return RVSP_ERROR_INVALID_ARGUMENT;
-  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  return symbolic_impl(p, static_cast<cudaStream_t>(stream), a_rows, b_rows, b_cols,
+                       a_row_ptr, a_col_idx, b_row_ptr, b_col_idx, c_row_ptr, c_nnz_out,
+                       nullptr);
+}
+
+rvsp_status_t rvsp_cuda_symbolic_checked(rvsp_cuda_plan_t p, void *stream, int32_t a_rows,
+                                         int32_t a_cols, int32_t a_nnz, int32_t b_rows,
+                                         int32_t b_cols, int32_t b_nnz,
+                                         const int32_t *a_row_ptr, const int32_t *a_col_idx,
+                                         const int32_t *b_row_ptr, const int32_t *b_col_idx,
+                                         int check_b, int32_t *c_row_ptr,
+                                         int64_t *c_nnz_out) {
+  if (!p || !a_row_ptr || !a_col_idx || !b_row_ptr || !b_col_idx || !c_row_ptr ||
+      !c_nnz_out)
+    return RVSP_ERROR_NULL_POINTER;
+  if (a_rows <= 0 || b_rows <= 0 || b_cols <= 0 || a_cols < 0 || a_nnz < 0 || b_nnz < 0)
+    return RVSP_ERROR_INVALID_ARGUMENT;
+  // A's columns index B's rows: a column the check lets through is < a_cols,
+  // and the row statistics bound it by b_rows as well.
+  const PreCheck chk{a_cols, a_nnz, b_nnz, check_b != 0};
+  return symbolic_impl(p, static_cast<cudaStream_t>(stream), a_rows, b_rows, b_cols,
+                       a_row_ptr, a_col_idx, b_row_ptr, b_col_idx, c_row_ptr, c_nnz_out,
+                       &chk);
+}
+
+namespace {
+
+rvsp_status_t symbolic_impl(rvsp_cuda_plan_t p, cudaStream_t s, int32_t a_rows,
+                            int32_t b_rows, int32_t b_cols, const int32_t *a_row_ptr,
+                            const int32_t *a_col_idx, const int32_t *b_row_ptr,
+                            const int32_t *b_col_idx, int32_t *c_row_ptr,
+                            int64_t *c_nnz_out, const PreCheck *chk) {
   p->analysed = 0;
   p->rmap_state = 0;
   p->rmap_col = nullptr;
@@ -408,11 +458,35 @@ rvsp_status_t rvsp_cuda_symbolic(rvsp_cuda_plan_t p, void *stream, int32_t a_row
   if (e == cudaSuccess) e = p->rows_num.reserve(n);
   if (e == cudaSuccess) e = p->long_rows.reserve(n);
   if (e == cudaSuccess) e = p->partials.reserve(scan_partials_bytes(a_rows) / sizeof(int64_t));
+  if (e == cudaSuccess && chk)
+    e = p->check_long.reserve(1 + size_t(check_long_rows_cap(a_rows, chk->a_nnz)));
+  if (e == cudaSuccess && chk && chk->check_b)
+    e = p->check_long_b.reserve(1 + size_t(check_long_rows_cap(b_rows, chk->b_nnz)));
   if (e != cudaSuccess) return map_cuda(e);
 
-  const Operands op{a_rows, b_cols, a_row_ptr, a_col_idx, nullptr,
-                    b_row_ptr, b_col_idx, nullptr,
-                    merge_allowed(p->merge_policy, a_rows)};
+  Operands op{a_rows, b_cols, a_row_ptr, a_col_idx, nullptr,
+              b_row_ptr, b_col_idx, nullptr,
+              merge_allowed(p->merge_policy, a_rows)};
+  if (chk) {
+    // Checks of A (and B) run first; the row statistics after them are
+    // bounded (they read nothing outside A's entries and B's row pointers),
+    // and one host round trip brings back both the checks' verdicts and the
+    // class sizes.  Nothing that depends on the structure runs before it.
+    op.a_nnz = chk->a_nnz;
+    op.b_rows = b_rows;
+    cudaMemsetAsync(p->check.p, 0xff, 2 * sizeof(unsigned long long), s);
+    cudaMemsetAsync(p->check_long.p, 0, sizeof(int32_t), s);
+    if (chk->check_b) cudaMemsetAsync(p->check_long_b.p, 0, sizeof(int32_t), s);
+    PhaseScope ph(p, s, RVSP_PHASE_CHECK);
+    launch_csr_check(a_rows, chk->a_cols, a_row_ptr, a_col_idx, chk->a_nnz, p->check.p,
+                     p->check_long.p, s);
+    ph.launches = 2;
+    if (chk->check_b) {
+      launch_csr_check(b_rows, b_cols, b_row_ptr, b_col_idx, chk->b_nnz, p->check.p + 1,
+                       p->check_long_b.p, s);
+      ph.launches += 2;
+    }
+  }
   int32_t *misc = p->misc.p;
   cudaMemsetAsync(misc, 0, kMiscWords * sizeof(int32_t), s);
   {
@@ -425,8 +499,13 @@ rvsp_status_t rvsp_cuda_symbolic(rvsp_cuda_plan_t p, void *stream, int32_t a_row
   }
   cudaMemcpyAsync(p->h_misc, misc, kNumClasses * sizeof(int32_t),
                   cudaMemcpyDeviceToHost, s);
+  if (chk)
+    cudaMemcpyAsync(p->h_check, p->check.p, 2 * sizeof(unsigned long long),
+                    cudaMemcpyDeviceToHost, s);
   e = cudaStreamSynchronize(s);
   if (e != cudaSuccess) return map_cuda(e);
+  if (chk && (p->h_check[0] != ~0ull || (chk->check_b && p->h_check[1] != ~0ull)))
+    return RVSP_ERROR_INVALID_CSR;  // not canonical: nothing more runs on it
   int32_t sym_off[kNumClasses];
   int32_t off = 0;
   for (int c = 0; c < kNumClasses; ++c) {
@@ -501,6 +580,8 @@ rvsp_status_t rvsp_cuda_symbolic(rvsp_cuda_plan_t p, void *stream, int32_t a_row
   *c_nnz_out = total;
   return RVSP_SUCCESS;
 }
+
+}  // namespace
 
 rvsp_status_t rvsp_cuda_learned_symbolic(
     rvsp_cuda_plan_t p, rvsp_mlp_t model, void *stream, int32_t a_rows, int32_t b_rows,

@@ -334,13 +334,17 @@ rvsp_status_t rvsp_spgemm_work_estimation(rvsp_spgemm_descr_t d,
         a_ci = A->col_idx;
         b_rp = B->row_ptr;
         b_ci = B->col_idx;
-        st = rvsp_device_check(d->plan, d->stream, A->rows, A->cols, a_rp, a_ci,
-                               A->nnz, RVSP_REJECT_ALL);
-        if (st == RVSP_SUCCESS && !same_structure(A, B))
-            st = rvsp_device_check(d->plan, d->stream, B->rows, B->cols, b_rp, b_ci,
-                                   B->nnz, RVSP_REJECT_ALL);
-        if (st != RVSP_SUCCESS)
-            return st;
+        /* The plain path folds these checks into its symbolic pass (one host
+         * round trip fewer, rvsp_cuda_symbolic_checked). */
+        if (d->algo == RVSP_SPGEMM_ALGO_CUDA_LEARNED) {
+            st = rvsp_device_check(d->plan, d->stream, A->rows, A->cols, a_rp, a_ci,
+                                   A->nnz, RVSP_REJECT_ALL);
+            if (st == RVSP_SUCCESS && !same_structure(A, B))
+                st = rvsp_device_check(d->plan, d->stream, B->rows, B->cols, b_rp, b_ci,
+                                       B->nnz, RVSP_REJECT_ALL);
+            if (st != RVSP_SUCCESS)
+                return st;
+        }
     }
 
     st = rvsp_dbuf_reserve(&d->c_row_ptr, ((size_t)A->rows + 1) * sizeof(int32_t));
@@ -366,6 +370,11 @@ rvsp_status_t rvsp_spgemm_work_estimation(rvsp_spgemm_descr_t d,
                                         B->cols, a_rp, a_ci, a_v, a_n, b_rp, b_ci, b_v,
                                         b_n, d->capacity_scale,
                                         (int32_t *)d->c_row_ptr.p, &total);
+    } else if (d->mem == RVSP_MEM_DEVICE) {
+        st = rvsp_cuda_symbolic_checked(d->plan, d->stream, A->rows, A->cols, A->nnz,
+                                        B->rows, B->cols, B->nnz, a_rp, a_ci, b_rp, b_ci,
+                                        !same_structure(A, B), (int32_t *)d->c_row_ptr.p,
+                                        &total);
     } else {
         st = rvsp_cuda_symbolic(d->plan, d->stream, A->rows, B->rows, B->cols, a_rp,
                                 a_ci, b_rp, b_ci, (int32_t *)d->c_row_ptr.p, &total);

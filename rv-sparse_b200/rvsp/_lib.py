@@ -94,6 +94,8 @@ SIGNATURES = {
     "rvsp_csr_copy_arrays": (_int, [_P(CsrMatrix), _P(CsrMatrix)]),
     "rvsp_cuda_coo_to_csr": (_int, [_vp, _i32, _i32, _i64, _int, _vp, _vp, _vp, _vp,
                                     _P(_vp), _P(_vp), _P(_i32)]),
+    "rvsp_cuda_symbolic_checked": (_int, [_vp, _vp, _i32, _i32, _i32, _i32, _i32, _i32, _vp,
+                                          _vp, _vp, _vp, _int, _vp, _P(_i64)]),
     "rvsp_cuda_typed_numeric": (_int, [_vp, _i32, _i32, _vp, _vp, _vp, _vp, _vp, _vp, _vp,
                                        _vp, _vp]),
     "rvsp_cuda_drop_zeros": (_int, [_vp, _i32, _i32, _vp, _i64, _vp, _vp, _vp, _sz, _vp,
