@@ -135,6 +135,118 @@ sym_dense_kernel(Operands op, const int32_t *__restrict__ rows, int32_t nrows,
   }
 }
 
+// Optimistic sizing of the W1024 / W2048 rows.  Their class comes from the
+// product count, an upper bound that can be far above the row's distinct
+// columns (a 27-point stencil row: 729 products, 125 columns), and a table of
+// 2048 slots per warp leaves few warps resident.  Such a row first counts in
+// a table of 1 << kOptLog2 slots with at most kOptProbes probes per insert;
+// the count is exact whenever every insert succeeds.  A row whose insert
+// fails (more columns than the table holds, or a probe run that long) is
+// appended to a retry list and counted again at its class size.
+constexpr int kOptLog2 = 9;
+constexpr uint32_t kOptProbes = 32;
+
+__device__ __forceinline__ int hash_insert_bounded(int32_t *keys, int log2t, int32_t col,
+                                                   bool &created) {
+  const uint32_t mask = (1u << log2t) - 1u;
+  uint32_t h = hash_slot(col, log2t);
+  created = false;
+  for (uint32_t probe = 0; probe < kOptProbes; ++probe) {
+    int32_t cur = *reinterpret_cast<volatile int32_t *>(&keys[h]);
+    if (cur == col) return static_cast<int>(h);
+    if (cur == kEmpty) {
+      int32_t prev = atomicCAS(&keys[h], kEmpty, col);
+      if (prev == kEmpty) {
+        created = true;
+        return static_cast<int>(h);
+      }
+      if (prev == col) return static_cast<int>(h);
+    }
+    h = (h + 1u) & mask;
+  }
+  return -1;
+}
+
+__global__ void __launch_bounds__(kWarpsPerBlock * 32)
+sym_warp_hash_try_kernel(Operands op, const int32_t *__restrict__ rows, int32_t nrows,
+                         int32_t *__restrict__ counts, int32_t *__restrict__ retry,
+                         int32_t *__restrict__ retry_n) {
+  constexpr int T = 1 << kOptLog2;
+  __shared__ int32_t s_keys[kWarpsPerBlock][T];
+  int32_t *keys = s_keys[threadIdx.x >> 5];
+  const int64_t w = (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+  if (w >= nrows) return;
+  const int lane = lane_id();
+  fill_words(keys, T, 0xffffffffu, lane, 32);
+  __syncwarp();
+  const int32_t row = row_of(rows, static_cast<int32_t>(w));
+  int cnt = 0;
+  bool bad = false;
+  for_each_product_col(op, op.a_rp[row], op.a_rp[row + 1], 0, 1, [&](int32_t col) {
+    if (bad) return;
+    bool created;
+    if (hash_insert_bounded(keys, kOptLog2, col, created) < 0) bad = true;
+    cnt += created;
+  });
+  cnt = warp_sum(cnt);
+  const bool any_bad = __any_sync(kFull, bad);
+  if (lane == 0) {
+    if (any_bad) retry[atomicAdd(retry_n, 1)] = row;
+    else counts[row] = cnt;
+  }
+}
+
+// The retried rows at their class size: persistent warps over the list,
+// whose length is read on the device.
+template <int LOG2T>
+__global__ void __launch_bounds__(kWarpsPerBlock * 32)
+sym_warp_hash_list_kernel(Operands op, const int32_t *__restrict__ list,
+                          const int32_t *__restrict__ list_n, int32_t *__restrict__ counts,
+                          int32_t *__restrict__ status) {
+  constexpr int T = 1 << LOG2T;
+  extern __shared__ __align__(16) int32_t smem_i32[];
+  int32_t *keys = smem_i32 + (threadIdx.x >> 5) * T;
+  const int lane = lane_id();
+  const int32_t n = *list_n;
+  const int64_t stride = (int64_t(gridDim.x) * blockDim.x) >> 5;
+  for (int64_t w = (int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5; w < n;
+       w += stride) {
+    fill_words(keys, T, 0xffffffffu, lane, 32);
+    __syncwarp();
+    const int32_t row = list[w];
+    int cnt = 0;
+    bool bad = false;
+    for_each_product_col(op, op.a_rp[row], op.a_rp[row + 1], 0, 1, [&](int32_t col) {
+      bool created;
+      if (hash_insert(keys, LOG2T, col, created) < 0) bad = true;
+      cnt += created;
+    });
+    cnt = warp_sum(cnt);
+    if (__any_sync(kFull, bad) && lane == 0) report(status, kDevHashFull);
+    if (lane == 0) counts[row] = cnt;
+    __syncwarp();  // the table is cleared for the warp's next row
+  }
+}
+
+template <int LOG2T>
+void launch_list_hash(const Operands &op, const int32_t *list, const int32_t *list_n,
+                      int32_t max_rows, int32_t *counts, int32_t *status, int num_sms,
+                      cudaStream_t s) {
+  const size_t smem = size_t(kWarpsPerBlock) * (size_t(1) << LOG2T) * sizeof(int32_t);
+  const int threads = kWarpsPerBlock * 32;
+  int per_sm = 1;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, sym_warp_hash_list_kernel<LOG2T>,
+                                                    threads, smem) != cudaSuccess ||
+      per_sm < 1)
+    per_sm = 1;
+  int64_t grid = int64_t(num_sms) * per_sm;
+  const int64_t need = (int64_t(max_rows) + kWarpsPerBlock - 1) / kWarpsPerBlock;
+  if (grid > need) grid = need;
+  if (grid < 1) grid = 1;
+  sym_warp_hash_list_kernel<LOG2T><<<static_cast<unsigned>(grid), threads, smem, s>>>(
+      op, list, list_n, counts, status);
+}
+
 template <int LOG2T>
 void launch_warp_hash(const Operands &op, const int32_t *rows, int32_t nrows,
                       int32_t *counts, int32_t *status, cudaStream_t s) {
@@ -146,6 +258,22 @@ void launch_warp_hash(const Operands &op, const int32_t *rows, int32_t nrows,
 }
 
 }  // namespace
+
+bool symbolic_optimistic_class(int cls) { return cls == kW1024 || cls == kW2048; }
+
+void launch_symbolic_optimistic(int cls, const Operands &op, const int32_t *rows,
+                                int32_t nrows, int32_t *counts, int32_t *retry,
+                                int32_t *retry_n, int32_t *status, int num_sms,
+                                cudaStream_t s) {
+  if (nrows <= 0 || !symbolic_optimistic_class(cls)) return;
+  const int64_t grid = (int64_t(nrows) + kWarpsPerBlock - 1) / kWarpsPerBlock;
+  sym_warp_hash_try_kernel<<<static_cast<unsigned>(grid), kWarpsPerBlock * 32, 0, s>>>(
+      op, rows, nrows, counts, retry, retry_n);
+  if (cls == kW1024)
+    launch_list_hash<10>(op, retry, retry_n, nrows, counts, status, num_sms, s);
+  else
+    launch_list_hash<11>(op, retry, retry_n, nrows, counts, status, num_sms, s);
+}
 
 void launch_symbolic_class(int cls, const Operands &op, const int32_t *rows,
                            int32_t nrows, int32_t *counts, uint32_t *gbitmap,

@@ -177,6 +177,14 @@ void launch_merge_numeric(int cls, const Operands &op, const int32_t *rows,
                           const FusedOut *fo, cudaStream_t s);
 
 // ---- k_symbolic.cu ---------------------------------------------------------
+// W1024 / W2048 rows: counted first in a 512-slot table with bounded probes;
+// rows that do not fit go to retry[] (count at *retry_n, zeroed by the
+// caller, room for nrows) and are counted at their class size.
+bool symbolic_optimistic_class(int cls);
+void launch_symbolic_optimistic(int cls, const Operands &op, const int32_t *rows,
+                                int32_t nrows, int32_t *counts, int32_t *retry,
+                                int32_t *retry_n, int32_t *status, int num_sms,
+                                cudaStream_t s);
 // counts[row] = nnz of output row, for the rows of one class.
 void launch_symbolic_class(int cls, const Operands &op, const int32_t *rows,
                            int32_t nrows, int32_t *counts, uint32_t *gbitmap,

@@ -68,7 +68,8 @@ constexpr int kNumOff = 4 * kNumClasses;
 constexpr int kNumFill = 5 * kNumClasses;
 constexpr int kStatus = 6 * kNumClasses;
 constexpr int kLongCount = 6 * kNumClasses + 1;
-constexpr int kMiscWords = 6 * kNumClasses + 2;
+constexpr int kRetryCount = 6 * kNumClasses + 2;  // two: W1024, W2048 retry lists
+constexpr int kMiscWords = 6 * kNumClasses + 4;
 // A map shared by at least this many rows gets a term table.
 constexpr int32_t kPatMinShare = 16;
 constexpr int kPatCountWords = 4 + kNumClasses;
@@ -529,11 +530,24 @@ rvsp_status_t symbolic_impl(rvsp_cuda_plan_t p, cudaStream_t s, int32_t a_rows,
   }
   {
     PhaseScope ph(p, s, RVSP_PHASE_SYMBOLIC);
+    // W1024 / W2048 rows count optimistically in a small table first; their
+    // retry lists live in long_rows (free once the row statistics are done),
+    // W1024's from 0, W2048's after it.
+    auto launch_class = [&](int c, const int32_t *rows, int32_t nrows) {
+      if (symbolic_optimistic_class(c)) {
+        const int32_t base = c == kW1024 ? 0 : p->sym_count[kW1024];
+        launch_symbolic_optimistic(c, op, rows, nrows, p->counts.p, p->long_rows.p + base,
+                                   misc + kRetryCount + (c == kW1024 ? 0 : 1),
+                                   misc + kStatus, p->num_sms, s);
+        return 2;
+      }
+      launch_symbolic_class(c, op, rows, nrows, p->counts.p, p->sym_bits.p, slots,
+                            misc + kStatus, p->num_sms, s);
+      return 1;
+    };
     const int whole = whole_matrix_class(p->sym_count, a_rows);
     if (whole >= 0) {
-      launch_symbolic_class(whole, op, nullptr, a_rows, p->counts.p, p->sym_bits.p,
-                            slots, misc + kStatus, p->num_sms, s);
-      ph.launches = 1;
+      ph.launches = launch_class(whole, nullptr, a_rows);
     } else {
       launch_class_offsets(misc + kSymCount, misc + kSymOff, s);
       launch_scatter_rows(a_rows, p->cls.p, misc + kSymOff, misc + kSymFill,
@@ -541,10 +555,7 @@ rvsp_status_t symbolic_impl(rvsp_cuda_plan_t p, cudaStream_t s, int32_t a_rows,
       ph.launches = 2;
       for (int c = kEmpty_ + 1; c < kNumClasses; ++c) {
         if (p->sym_count[c] <= 0) continue;
-        launch_symbolic_class(c, op, p->rows_sym.p + sym_off[c],
-                              p->sym_count[c], p->counts.p, p->sym_bits.p, slots,
-                              misc + kStatus, p->num_sms, s);
-        ph.launches += 1;
+        ph.launches += launch_class(c, p->rows_sym.p + sym_off[c], p->sym_count[c]);
       }
     }
   }
