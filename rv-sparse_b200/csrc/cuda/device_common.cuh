@@ -212,11 +212,13 @@ __device__ __forceinline__ void ordered_apply(float *acc, bool valid, int slot,
 }
 
 // Bitonic sort of n (power of two) 64-bit keys in shared memory by one warp.
+// Pair p of a stage with distance j (a power of two) compares i and i + j,
+// i = (p / j) * 2j + p % j, computed as p + (p & -j) (no division).
 __device__ __forceinline__ void warp_bitonic_sort(unsigned long long *s, int n) {
   for (int k = 2; k <= n; k <<= 1) {
     for (int j = k >> 1; j > 0; j >>= 1) {
       for (int p = lane_id(); p < (n >> 1); p += 32) {
-        const int i = ((p / j) * (j << 1)) + (p % j);
+        const int i = p + (p & -j);
         const int l = i + j;
         const unsigned long long x = s[i], y = s[l];
         const bool up = (i & k) == 0;
@@ -235,7 +237,7 @@ __device__ __forceinline__ void block_bitonic_sort(unsigned long long *s, int n)
   for (int k = 2; k <= n; k <<= 1) {
     for (int j = k >> 1; j > 0; j >>= 1) {
       for (int p = threadIdx.x; p < (n >> 1); p += blockDim.x) {
-        const int i = ((p / j) * (j << 1)) + (p % j);
+        const int i = p + (p & -j);
         const int l = i + j;
         const unsigned long long x = s[i], y = s[l];
         const bool up = (i & k) == 0;
