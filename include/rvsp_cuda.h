@@ -40,7 +40,11 @@ void rvsp_cuda_plan_destroy(rvsp_cuda_plan_t plan);
 /* Replaces rvsp_symbolic_count (rvsp_spgemm.h:62-70, rvsp_symbolic.c:13-86):
  * per-row op counts, exact per-row output nnz, exclusive scan into
  * c_row_ptr[0..a_rows] (device) and the int64 total.  ALLOCATION_FAILED when
- * the total exceeds INT32_MAX, as in the reference.  Synchronizes `stream`. */
+ * the total exceeds INT32_MAX, as in the reference.  One host round trip
+ * when every non-empty row falls in the merge classes (at most 16 A
+ * nonzeros and 2048 products; under the automatic merge policy only when A
+ * has at least 32768 rows), two otherwise.
+ * Synchronizes `stream`. */
 rvsp_status_t rvsp_cuda_symbolic(rvsp_cuda_plan_t plan, void *stream,
                                  int32_t a_rows, int32_t b_rows, int32_t b_cols,
                                  const int32_t *a_row_ptr,
@@ -60,10 +64,13 @@ size_t rvsp_cuda_numeric_workspace_bytes(rvsp_cuda_plan_t plan);
  * before the row statistics, which read only A's a_nnz entries and B's
  * b_rows + 1 row pointers whatever the structure holds, and one host round
  * trip returns both the checks' verdicts and the class sizes.  A structure
- * that fails either check gives RVSP_ERROR_INVALID_CSR before any pass that
- * depends on it runs (the plan is left unanalysed).  Otherwise the same
- * results as rvsp_cuda_symbolic, with one host round trip fewer than
- * calling the check first.  Synchronizes `stream`. */
+ * that fails either check gives RVSP_ERROR_INVALID_CSR and no pass that
+ * depends on it does any work: the passes queued before the verdict reaches
+ * the host (the merge rows' count and the scan, when merge classes are on)
+ * read the verdict on the device and return without reading the
+ * structure or writing c_row_ptr; the plan is left unanalysed.  Otherwise
+ * the same results as rvsp_cuda_symbolic, with one host round trip fewer
+ * than calling the check first.  Synchronizes `stream`. */
 rvsp_status_t rvsp_cuda_symbolic_checked(rvsp_cuda_plan_t plan, void *stream, int32_t a_rows,
                                          int32_t a_cols, int32_t a_nnz, int32_t b_rows,
                                          int32_t b_cols, int32_t b_nnz,

@@ -110,12 +110,22 @@ __device__ __forceinline__ int32_t min_head(const Lists<K> &L) {
 }
 
 template <int K>
+constexpr int merge_class_of() {
+  return K == 4 ? kM4 : K == 8 ? kM8 : kM16;
+}
+
+// Rows: rows[0..nrows) (rows == nullptr: rows 0..nrows).  With sel, rows
+// whose sel entry is not this kernel's class are skipped.
+template <int K>
 __global__ void __launch_bounds__(kMergeThreads, MergeOccupancy<K, false>::value)
 merge_symbolic_kernel(Operands op, const int32_t *__restrict__ rows,
-                      int32_t nrows, int32_t *__restrict__ counts) {
+                      int32_t nrows, int32_t *__restrict__ counts,
+                      const uint8_t *__restrict__ sel, CheckGuard guard) {
   const int32_t t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= nrows) return;
   const int32_t row = row_of(rows, t);
+  if (sel && sel[row] != merge_class_of<K>()) return;
+  if (guard.failed()) return;
   const int32_t p0 = op.a_rp[row];
   const int32_t k = op.a_rp[row + 1] - p0;
   Lists<K> L;
@@ -252,9 +262,10 @@ merge_numeric_fill_kernel(Operands op, const int32_t *__restrict__ rows, int32_t
 
 template <int K>
 void sym(const Operands &op, const int32_t *rows, int32_t nrows, int32_t *counts,
-         cudaStream_t s) {
+         cudaStream_t s, const uint8_t *sel = nullptr, CheckGuard guard = CheckGuard()) {
   const int grid = (nrows + kMergeThreads - 1) / kMergeThreads;
-  merge_symbolic_kernel<K><<<grid, kMergeThreads, 0, s>>>(op, rows, nrows, counts);
+  merge_symbolic_kernel<K><<<grid, kMergeThreads, 0, s>>>(op, rows, nrows, counts, sel,
+                                                           guard);
 }
 
 template <int K>
@@ -281,6 +292,14 @@ void launch_merge_symbolic(int cls, const Operands &op, const int32_t *rows,
     case kM16: sym<16>(op, rows, nrows, counts, s); break;
     default: break;
   }
+}
+
+void launch_merge_symbolic_all(const Operands &op, const uint8_t *cls, int32_t a_rows,
+                               int32_t *counts, CheckGuard guard, cudaStream_t s) {
+  if (a_rows <= 0) return;
+  sym<4>(op, nullptr, a_rows, counts, s, cls, guard);
+  sym<8>(op, nullptr, a_rows, counts, s, cls, guard);
+  sym<16>(op, nullptr, a_rows, counts, s, cls, guard);
 }
 
 void launch_merge_numeric(int cls, const Operands &op, const int32_t *rows,

@@ -76,8 +76,10 @@ tile_sum_kernel(int32_t n, const int32_t *__restrict__ counts,
 // when it fits, row_ptr[n].
 __global__ void __launch_bounds__(kThreads)
 partials_scan_kernel(int32_t n, int32_t nt, int64_t *__restrict__ partials,
-                     int64_t *__restrict__ total, int32_t *__restrict__ row_ptr) {
+                     int64_t *__restrict__ total, int32_t *__restrict__ row_ptr,
+                     CheckGuard guard) {
   __shared__ long long s_warp[kThreads / 32];
+  if (guard.failed()) return;
   long long carry = 0;
   for (int32_t b = 0; b < nt; b += kThreads) {
     const int32_t i = b + threadIdx.x;
@@ -100,10 +102,11 @@ tile_apply_kernel(int32_t n, const int32_t *__restrict__ counts,
                   const int32_t *__restrict__ a_rp,
                   const int64_t *__restrict__ partials,
                   int32_t *__restrict__ row_ptr, uint8_t *__restrict__ cls,
-                  int32_t *__restrict__ class_count, bool merge_ok) {
+                  int32_t *__restrict__ class_count, bool merge_ok, CheckGuard guard) {
   __shared__ int32_t s_items[kTile + kTile / 32];
   __shared__ long long s_warp[kThreads / 32];
   __shared__ int32_t s_cnt[kNumClasses];
+  if (guard.failed()) return;
   for (int c = threadIdx.x; c < kNumClasses; c += blockDim.x) s_cnt[c] = 0;
   const int64_t base = static_cast<int64_t>(blockIdx.x) * kTile;
   __syncthreads();
@@ -215,12 +218,13 @@ size_t scan_partials_bytes(int32_t n) {
 void launch_scan_and_class(int32_t n, const int32_t *counts, const int64_t *ops,
                            const int32_t *a_rp, int32_t *row_ptr,
                            int64_t *partials, int64_t *total, uint8_t *cls,
-                           int32_t *class_count, bool merge_ok, cudaStream_t s) {
+                           int32_t *class_count, bool merge_ok, cudaStream_t s,
+                           CheckGuard guard) {
   const int32_t nt = static_cast<int32_t>((static_cast<int64_t>(n) + kTile - 1) / kTile);
   tile_sum_kernel<<<nt, kThreads, 0, s>>>(n, counts, partials);
-  partials_scan_kernel<<<1, kThreads, 0, s>>>(n, nt, partials, total, row_ptr);
+  partials_scan_kernel<<<1, kThreads, 0, s>>>(n, nt, partials, total, row_ptr, guard);
   tile_apply_kernel<<<nt, kThreads, 0, s>>>(n, counts, ops, a_rp, partials, row_ptr,
-                                            cls, class_count, merge_ok);
+                                            cls, class_count, merge_ok, guard);
 }
 
 }  // namespace rvsp

@@ -73,6 +73,7 @@ __host__ __device__ inline int classify_row(int32_t nnz_a, int64_t ops,
 }
 
 inline int class_log2(int cls) { return kWarpHashMinLog2 + (cls - kW64); }
+inline bool is_merge_class(int cls) { return cls == kM4 || cls == kM8 || cls == kM16; }
 
 // Pointers of one product.  A's columns index B's rows.
 struct Operands {
@@ -92,6 +93,22 @@ struct Operands {
   // check has not finished yet (rvsp_cuda_symbolic_checked).
   int32_t a_nnz = -1;
   int32_t b_rows = -1;
+};
+
+// The device-side verdict of CSR checks queued earlier on the same stream:
+// n words at w, each ~0ull when its structure passed.  A pass given a guard
+// that failed returns without reading the structure or writing anything, so
+// it can be queued before the verdict reaches the host.  n == 0: no check.
+struct CheckGuard {
+  const unsigned long long *w = nullptr;
+  int n = 0;
+#ifdef __CUDACC__
+  __device__ __forceinline__ bool failed() const {
+    for (int i = 0; i < n; ++i)
+      if (w[i] != ~0ull) return true;
+    return false;
+  }
+#endif
 };
 
 // Merge policies of a plan: automatic (merge classes when the matrix has at
@@ -133,12 +150,14 @@ void launch_scatter_rows(int32_t n, const uint8_t *cls, const int32_t *class_off
 
 // ---- k_scan.cu -------------------------------------------------------------
 // row_ptr = exclusive scan of counts (n + 1 entries), *total = sum (int64).
-// Also classes every row for the numeric pass (cls, class_count).
+// Also classes every row for the numeric pass (cls, class_count).  With a
+// guard that failed, nothing is written but the tile partials.
 size_t scan_partials_bytes(int32_t n);
 void launch_scan_and_class(int32_t n, const int32_t *counts, const int64_t *ops,
                            const int32_t *a_rp, int32_t *row_ptr,
                            int64_t *partials, int64_t *total, uint8_t *cls,
-                           int32_t *class_count, bool merge_ok, cudaStream_t s);
+                           int32_t *class_count, bool merge_ok, cudaStream_t s,
+                           CheckGuard guard = CheckGuard());
 
 // out[i] = sum of in[0..i) as int64 (n entries), *total = sum of all.
 void launch_scan_i64(int32_t n, const int32_t *in, int64_t *out, int64_t *partials,
@@ -171,6 +190,11 @@ void launch_values_hash(const float *v, int64_t n, unsigned long long salt,
 // values and sorted columns (numeric).
 void launch_merge_symbolic(int cls, const Operands &op, const int32_t *rows,
                            int32_t nrows, int32_t *counts, cudaStream_t s);
+// The symbolic pass of every M4, M8 and M16 row, with no row lists and no
+// host-side class counts: one launch per merge class over all a_rows rows,
+// each thread skipping rows whose cls is another class.  Three launches.
+void launch_merge_symbolic_all(const Operands &op, const uint8_t *cls, int32_t a_rows,
+                               int32_t *counts, CheckGuard guard, cudaStream_t s);
 void launch_merge_numeric(int cls, const Operands &op, const int32_t *rows,
                           int32_t nrows, const int32_t *c_rp, int32_t *c_col,
                           float *c_val, bool fill, int32_t *status,

@@ -14,6 +14,7 @@
 #include <climits>
 #include <cstring>
 #include <new>
+#include <utility>
 #include <vector>
 
 #include "device_common.cuh"
@@ -87,6 +88,9 @@ struct rvsp_cuda_plan {
 
   DevArray<int64_t> ops;
   DevArray<uint8_t> cls;
+  // Numeric classes from the scan queued before the class census (plain
+  // symbolic with merge classes); swapped into cls when that scan is final.
+  DevArray<uint8_t> cls_spec;
   DevArray<int32_t> counts;
   DevArray<int32_t> rows_sym, rows_num, long_rows;
   DevArray<int32_t> misc;
@@ -360,6 +364,7 @@ void rvsp_cuda_plan_destroy(rvsp_cuda_plan_t p) {
   p->pat_rec.release();
   p->ops.release();
   p->cls.release();
+  p->cls_spec.release();
   p->counts.release();
   p->rows_sym.release();
   p->rows_num.release();
@@ -401,6 +406,9 @@ rvsp_status_t symbolic_impl(rvsp_cuda_plan_t p, cudaStream_t s, int32_t a_rows,
                             const int32_t *a_col_idx, const int32_t *b_row_ptr,
                             const int32_t *b_col_idx, int32_t *c_row_ptr,
                             int64_t *c_nnz_out, const PreCheck *chk);
+cudaError_t symbolic_rest(rvsp_cuda_plan *p, cudaStream_t s, const Operands &op,
+                          int32_t a_rows, int32_t b_cols, const int32_t *a_row_ptr,
+                          int32_t *c_row_ptr, const int32_t *sym_off, bool merge_done);
 
 }  // namespace
 
@@ -459,6 +467,7 @@ rvsp_status_t symbolic_impl(rvsp_cuda_plan_t p, cudaStream_t s, int32_t a_rows,
   if (e == cudaSuccess) e = p->rows_num.reserve(n);
   if (e == cudaSuccess) e = p->long_rows.reserve(n);
   if (e == cudaSuccess) e = p->partials.reserve(scan_partials_bytes(a_rows) / sizeof(int64_t));
+  if (e == cudaSuccess && merge_allowed(p->merge_policy, a_rows)) e = p->cls_spec.reserve(n);
   if (e == cudaSuccess && chk)
     e = p->check_long.reserve(1 + size_t(check_long_rows_cap(a_rows, chk->a_nnz)));
   if (e == cudaSuccess && chk && chk->check_b)
@@ -498,23 +507,89 @@ rvsp_status_t symbolic_impl(rvsp_cuda_plan_t p, cudaStream_t s, int32_t a_rows,
                          p->counts.p, misc + kSymCount, p->num_sms, s);
     ph.launches = 2;
   }
-  cudaMemcpyAsync(p->h_misc, misc, kNumClasses * sizeof(int32_t),
-                  cudaMemcpyDeviceToHost, s);
+  // Merge-class rows need no host-side census: their symbolic pass (one
+  // launch per merge class over all rows, each skipping the other classes)
+  // and the scan are queued at once, behind the check verdict, so a product
+  // whose rows are all merge rows takes one host round trip.  When other
+  // classes turn up, their pass and the scan follow the census.  The early
+  // scan writes its numeric classes to cls_spec: the census-driven pass
+  // still needs the symbolic classes in cls.
+  const bool spec = op.merge_ok;
+  CheckGuard guard;
+  if (chk) {
+    guard.w = p->check.p;
+    guard.n = chk->check_b ? 2 : 1;
+  }
+  if (spec) {
+    {
+      PhaseScope ph(p, s, RVSP_PHASE_SYMBOLIC);
+      launch_merge_symbolic_all(op, p->cls.p, a_rows, p->counts.p, guard, s);
+      ph.launches = 3;
+    }
+    {
+      PhaseScope ph(p, s, RVSP_PHASE_SCAN);
+      launch_scan_and_class(a_rows, p->counts.p, p->ops.p, a_row_ptr, c_row_ptr,
+                            p->partials.p, p->total.p, p->cls_spec.p, misc + kNumCount,
+                            op.merge_ok, s, guard);
+      ph.launches = 3;
+    }
+    cudaMemcpyAsync(p->h_misc, misc, kMiscWords * sizeof(int32_t), cudaMemcpyDeviceToHost, s);
+    cudaMemcpyAsync(p->h_total, p->total.p, sizeof(int64_t), cudaMemcpyDeviceToHost, s);
+  } else {
+    cudaMemcpyAsync(p->h_misc, misc, kNumClasses * sizeof(int32_t),
+                    cudaMemcpyDeviceToHost, s);
+  }
   if (chk)
     cudaMemcpyAsync(p->h_check, p->check.p, 2 * sizeof(unsigned long long),
                     cudaMemcpyDeviceToHost, s);
   e = cudaStreamSynchronize(s);
   if (e != cudaSuccess) return map_cuda(e);
   if (chk && (p->h_check[0] != ~0ull || (chk->check_b && p->h_check[1] != ~0ull)))
-    return RVSP_ERROR_INVALID_CSR;  // not canonical: nothing more runs on it
+    return RVSP_ERROR_INVALID_CSR;  // not canonical: nothing ran on it
   int32_t sym_off[kNumClasses];
   int32_t off = 0;
+  bool rest = !spec;  // classes left for the census-driven pass
   for (int c = 0; c < kNumClasses; ++c) {
     p->sym_count[c] = p->h_misc[kSymCount + c];
     sym_off[c] = off;
     if (c != kEmpty_) off += p->sym_count[c];
+    if (c != kEmpty_ && !is_merge_class(c) && p->sym_count[c] > 0) rest = true;
   }
+  if (rest) {
+    e = symbolic_rest(p, s, op, a_rows, b_cols, a_row_ptr, c_row_ptr, sym_off, spec);
+    if (e != cudaSuccess) return map_cuda(e);
+  } else {
+    std::swap(p->cls, p->cls_spec);  // the early scan's numeric classes
+  }
+  if (p->h_misc[kStatus] != kDevOk) {
+    cudaMemsetAsync(misc + kStatus, 0, sizeof(int32_t), s);
+    return RVSP_ERROR_DEVICE;
+  }
+  const int64_t total = *p->h_total;
+  if (total > INT32_MAX) return RVSP_ERROR_ALLOCATION_FAILED;
 
+  finish_numeric_bins(p, a_rows, b_cols, s);
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return map_cuda(e);
+
+  p->learned = 0;
+  p->a_rows = a_rows;
+  p->b_rows = b_rows;
+  p->b_cols = b_cols;
+  p->c_nnz = total;
+  p->analysed = 1;
+  *c_nnz_out = total;
+  return RVSP_SUCCESS;
+}
+
+// The symbolic pass of the rows the census found outside the merge classes
+// (all rows when merge_done is false), then the scan again, and the host
+// copy of the counters and the total (one more round trip).
+cudaError_t symbolic_rest(rvsp_cuda_plan *p, cudaStream_t s, const Operands &op,
+                          int32_t a_rows, int32_t b_cols, const int32_t *a_row_ptr,
+                          int32_t *c_row_ptr, const int32_t *sym_off, bool merge_done) {
+  int32_t *misc = p->misc.p;
+  cudaError_t e = cudaSuccess;
   // Global bitmaps for dense symbolic rows when B is too wide for shared memory.
   const size_t bits_bytes = dense_slot_bits_bytes(b_cols);
   int32_t slots = 0;
@@ -523,7 +598,7 @@ rvsp_status_t symbolic_impl(rvsp_cuda_plan_t p, cudaStream_t s, int32_t a_rows,
     const size_t words = bits_bytes / sizeof(uint32_t) * size_t(slots);
     if (words > p->sym_bits.cap) {
       e = p->sym_bits.reserve(words);
-      if (e != cudaSuccess) return map_cuda(e);
+      if (e != cudaSuccess) return e;
       cudaMemsetAsync(p->sym_bits.p, 0, words * sizeof(uint32_t), s);
     }
     p->sym_bits_slots = slots;
@@ -545,6 +620,8 @@ rvsp_status_t symbolic_impl(rvsp_cuda_plan_t p, cudaStream_t s, int32_t a_rows,
                             misc + kStatus, p->num_sms, s);
       return 1;
     };
+    // whole >= 0 is never a merge class here when merge_done (a class
+    // outside them is non-empty).
     const int whole = whole_matrix_class(p->sym_count, a_rows);
     if (whole >= 0) {
       ph.launches = launch_class(whole, nullptr, a_rows);
@@ -554,11 +631,13 @@ rvsp_status_t symbolic_impl(rvsp_cuda_plan_t p, cudaStream_t s, int32_t a_rows,
                           p->rows_sym.p, s);
       ph.launches = 2;
       for (int c = kEmpty_ + 1; c < kNumClasses; ++c) {
-        if (p->sym_count[c] <= 0) continue;
+        if (p->sym_count[c] <= 0 || (merge_done && is_merge_class(c))) continue;
         ph.launches += launch_class(c, p->rows_sym.p + sym_off[c], p->sym_count[c]);
       }
     }
   }
+  if (merge_done)  // the first scan counted numeric classes already
+    cudaMemsetAsync(misc + kNumCount, 0, kNumClasses * sizeof(int32_t), s);
   {
     PhaseScope ph(p, s, RVSP_PHASE_SCAN);
     launch_scan_and_class(a_rows, p->counts.p, p->ops.p, a_row_ptr, c_row_ptr,
@@ -569,27 +648,7 @@ rvsp_status_t symbolic_impl(rvsp_cuda_plan_t p, cudaStream_t s, int32_t a_rows,
   cudaMemcpyAsync(p->h_misc + kNumCount, misc + kNumCount,
                   (kMiscWords - kNumCount) * sizeof(int32_t), cudaMemcpyDeviceToHost, s);
   cudaMemcpyAsync(p->h_total, p->total.p, sizeof(int64_t), cudaMemcpyDeviceToHost, s);
-  e = cudaStreamSynchronize(s);
-  if (e != cudaSuccess) return map_cuda(e);
-  if (p->h_misc[kStatus] != kDevOk) {
-    cudaMemsetAsync(misc + kStatus, 0, sizeof(int32_t), s);
-    return RVSP_ERROR_DEVICE;
-  }
-  const int64_t total = *p->h_total;
-  if (total > INT32_MAX) return RVSP_ERROR_ALLOCATION_FAILED;
-
-  finish_numeric_bins(p, a_rows, b_cols, s);
-  e = cudaGetLastError();
-  if (e != cudaSuccess) return map_cuda(e);
-
-  p->learned = 0;
-  p->a_rows = a_rows;
-  p->b_rows = b_rows;
-  p->b_cols = b_cols;
-  p->c_nnz = total;
-  p->analysed = 1;
-  *c_nnz_out = total;
-  return RVSP_SUCCESS;
+  return cudaStreamSynchronize(s);
 }
 
 }  // namespace

@@ -252,6 +252,57 @@ def test_invalid_csr_rejected():
         assert e.value.status == L.ERROR_INVALID_CSR, mutate
 
 
+def test_checked_symbolic_merge_rows():
+    # With merge classes on (>= 32768 rows) the checked symbolic pass queues
+    # the merge rows' count and the scan before the check's verdict reaches
+    # the host: a valid structure gives the oracle's row_ptr, with and without
+    # warp-class rows beside the merge rows; a structure that fails the check
+    # gives INVALID_CSR and the caller's row_ptr is left untouched.  The
+    # mutations keep every index in range.
+    import ctypes as C
+    import torch
+    lib = L.load()
+    n = 40000
+    plan = C.c_void_p()
+    L.check(lib.rvsp_cuda_plan_create(C.byref(plan)), "plan_create")
+    try:
+        B = gen.random_csr(n, n, 41, mean_len=4.0, empty_frac=0.1)
+        db = [torch.from_numpy(x).cuda() for x in (B.row_ptr, B.col_idx)]
+        plain = gen.random_csr(n, n, 42, mean_len=5.0, empty_frac=0.1)
+        mixed = gen.random_csr(n, n, 43, mean_len=5.0, empty_frac=0.1, heavy_rows=40,
+                               heavy_len=300)
+        cases = [("valid", plain), ("valid+warp rows", mixed)]
+        for mutate in ("unsorted", "dup", "rowptr"):
+            X = plain.copy()
+            r = next(i for i in range(1000, n) if X.row_ptr[i + 1] - X.row_ptr[i] >= 2)
+            p = X.row_ptr[r]
+            if mutate == "unsorted":
+                X.col_idx[p], X.col_idx[p + 1] = X.col_idx[p + 1], X.col_idx[p]
+            elif mutate == "dup":
+                X.col_idx[p + 1] = X.col_idx[p]
+            else:
+                X.row_ptr[r] = X.row_ptr[r + 1] + 1
+            cases.append((mutate, X))
+        for what, X in cases:
+            da = [torch.from_numpy(x).cuda() for x in (X.row_ptr, X.col_idx)]
+            c_rp = torch.full((n + 1,), -7, dtype=torch.int32, device="cuda")
+            total = C.c_int64(-1)
+            st = lib.rvsp_cuda_symbolic_checked(
+                plan, C.c_void_p(0), n, X.cols, X.nnz, B.rows, B.cols, B.nnz,
+                da[0].data_ptr(), da[1].data_ptr(), db[0].data_ptr(), db[1].data_ptr(), 1,
+                c_rp.data_ptr(), C.byref(total))
+            if what.startswith("valid"):
+                assert st == L.SUCCESS, what
+                rp, ci, _, _ = oracle.spgemm(X, B)
+                assert total.value == ci.size, what
+                assert np.array_equal(c_rp.cpu().numpy(), rp.astype(np.int32)), what
+            else:
+                assert st == L.ERROR_INVALID_CSR, what
+                assert bool((c_rp == -7).all()), what
+    finally:
+        lib.rvsp_cuda_plan_destroy(plan)
+
+
 def test_device_check_long_rows_matches_oracle():
     # Rows over 256 entries are checked by a warp each: the (code, first bad
     # row) pair must still be the reference's, for violations at chunk
