@@ -10,6 +10,14 @@ ranks, each rank takes whole panels (no data crosses GPUs inside a product;
 every rank holds all of B) and the only exchange is one all-gather of each
 panel's nnz, from which every rank knows where its rows sit in the global
 C.row_ptr.
+
+Exchanges (torch.distributed, NCCL on GPUs, gloo on CPU):
+  broadcast_csr   B from one rank to all, once: its sizes, then row_ptr,
+                  col_idx and values (four broadcasts);
+  panel_offsets   one all-reduce of a per-panel nnz vector in which each
+                  rank fills its own panels (every panel has one owner), so
+                  it carries exactly the all-gather of the panels' nnz; its
+                  exclusive scan places each panel in the global C.
 """
 from __future__ import annotations
 
@@ -80,3 +88,53 @@ def global_row_ptr(bounds: list[tuple[int, int]], panel_row_ptrs: dict) -> np.nd
         out[r0 + 1:r1 + 1] = base + rp[1:]
         base += int(rp[-1])
     return out
+
+
+def broadcast_csr(M, src: int = 0, device="cpu", group=None):
+    """Every rank's copy of one CSR (B of a sharded product), sent once from
+    rank src.  M is the matrix on rank src (a CSR) and is ignored elsewhere.
+    Returns a DeviceCSR whose tensors live on `device` (the rank's GPU under
+    NCCL, "cpu" under gloo)."""
+    import torch
+    import torch.distributed as dist
+
+    from .api import DeviceCSR
+    rank = dist.get_rank(group)
+    meta = torch.zeros(3, dtype=torch.int64, device=device)
+    if rank == src:
+        meta[0], meta[1], meta[2] = int(M.rows), int(M.cols), int(M.nnz)
+    dist.broadcast(meta, src, group=group)
+    rows, cols, nnz = (int(x) for x in meta.tolist())
+    if rank == src:
+        rp = torch.from_numpy(np.ascontiguousarray(M.row_ptr, np.int32)).to(device)
+        ci = torch.from_numpy(np.ascontiguousarray(M.col_idx, np.int32)).to(device)
+        v = torch.from_numpy(np.ascontiguousarray(M.values, np.float32)).to(device)
+    else:
+        rp = torch.empty(rows + 1, dtype=torch.int32, device=device)
+        ci = torch.empty(nnz, dtype=torch.int32, device=device)
+        v = torch.empty(nnz, dtype=torch.float32, device=device)
+    for t in (rp, ci, v):
+        if t.numel():  # every rank knows the sizes, so all skip alike
+            dist.broadcast(t, src, group=group)
+    return DeviceCSR(rows, cols, rp, ci, v)
+
+
+def panel_offsets(n_panels: int, local_nnz: dict, device="cpu", group=None) -> np.ndarray:
+    """Start of every panel's entries in the whole C: int64, n_panels + 1
+    entries, the last one nnz(C).  local_nnz maps this rank's panel indices
+    to their nnz; every panel must belong to exactly one rank."""
+    import torch
+    import torch.distributed as dist
+    t = torch.zeros(max(n_panels, 1), dtype=torch.int64, device=device)
+    for i, n in local_nnz.items():
+        t[int(i)] = int(n)
+    dist.all_reduce(t, group=group)
+    out = np.zeros(n_panels + 1, np.int64)
+    np.cumsum(t.cpu().numpy()[:n_panels], out=out[1:])
+    return out
+
+
+def rows_in_global_row_ptr(panel_row_ptr, offset: int) -> np.ndarray:
+    """A panel's row_ptr placed in the whole C: entries r0 + 1 .. r1 of the
+    global C.row_ptr for the panel's rows [r0, r1) (int64)."""
+    return offset + np.asarray(panel_row_ptr, np.int64)[1:]
