@@ -19,7 +19,12 @@ flushed by a 256 MiB write between steps, max over ranks); `e2e` is the same
 metric through the public C API in host memory space (pinned host buffers,
 host<->device copies inside the timed region); `roofline` is for the
 dominant kernel phase, timed with CUDA events on its own launch stream;
-`cpu_baseline` is the reference scalar backend on this host's cores.
+`cpu_baseline` is the reference scalar backend on this host's cores, and
+its `check` (and the line's `correct`) says whether the GPU's C of the last
+timed step is bit-identical to the reference's product of the same operands
+(one product; every 16th of a batch; the last panel), as the reference
+bench records `correct` for every timed run.  `correct` is null when the
+CPU leg is skipped (--no-cpu-baseline, or more than one rank).
 
 Multi-GPU (torchrun): every rank computes the full workload on its own GPU
 (weak scaling: rows of C are independent and no data crosses GPUs).
@@ -304,6 +309,35 @@ def run_mtx(args, world, rank, local):
         cv, _, kind = run_mtx_reference(argparse.Namespace(warmup=0, steps=1))
         cpu = {"value": cv, "unit": MTX_UNIT, "cores": 1, "kind": kind,
                "sample": "one read of the same file by the reference reader"}
+        # check: the same text through rvsp_csr_parse_mtx into host arrays
+        # against the reference reader's CSR, bit for bit
+        sys.path.insert(0, str(ROOT))
+        from oracle import oracle
+        if kind == "reference":
+            with tempfile.TemporaryDirectory() as tmp:
+                path = Path(tmp) / "laplace.mtx"
+                path.write_bytes(text)
+                want = oracle.ref_mtx_to_csr(path)
+        else:
+            want = oracle.mtx_to_csr(text)[2:]
+        m = L.CsrMatrix()
+        L.check(lib.rvsp_csr_parse_mtx(text, len(text), L.MEM_HOST, C.byref(m)), "parse_mtx")
+        n_got = int(m.nnz)
+
+        def take(ptr, ctype, n, dtype):
+            if n == 0:
+                return np.zeros(0, dtype)
+            return np.ctypeslib.as_array(C.cast(ptr, C.POINTER(ctype)), shape=(n,)).copy()
+        got = (take(m.row_ptr, C.c_int32, int(m.rows) + 1, np.int32),
+               take(m.col_idx, C.c_int32, n_got, np.int32),
+               take(m.values, C.c_float, n_got, np.float32))
+        lib.rvsp_csr_destroy(C.byref(m))
+        same = (want is not None and np.array_equal(got[0], want[0])
+                and np.array_equal(got[1], want[1])
+                and np.array_equal(got[2].view(np.uint32),
+                                   np.ascontiguousarray(want[2], np.float32).view(np.uint32)))
+        cpu["check"] = {"bit_exact": bool(same), "mismatched": 0 if same else 1,
+                        "against": f"{kind}: the reader's CSR of the same text"}
     line = {"metric": MTX_METRIC, "value": value, "unit": MTX_UNIT, "n_gpus": 1,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * el / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
@@ -320,7 +354,8 @@ def run_mtx(args, world, rank, local):
                          if peak_kind == "measured" else "fallback 6.65 TB/s",
                          "traffic": None, "algorithmic_bytes_per_launch": alg},
             "clocks": clocks, "e2e": e2e, "gpu_launches": 11 * args.steps,
-            "cpu_baseline": cpu}
+            "cpu_baseline": cpu,
+            "correct": cpu["check"]["bit_exact"] if cpu else None}
     print(json.dumps(line), flush=True)
     return 0
 
@@ -370,11 +405,15 @@ def run_typed(args, world, rank, local):
     cpu = None
     if not args.no_cpu_baseline and oracle.ref_available():
         t0 = time.perf_counter()
-        st = oracle.ref_spgemm_typed(ta, tb, args.dtype)[0]
+        st, rrp, rci, rcv = oracle.ref_spgemm_typed(ta, tb, args.dtype)
         t = time.perf_counter() - t0
         if st == 0:
+            same = (np.array_equal(rp, rrp) and np.array_equal(ci, rci)
+                    and cv.dtype == rcv.dtype and cv.tobytes() == rcv.tobytes())
             cpu = {"value": flops / t / 1e9, "unit": UNIT, "cores": 1, "kind": "reference",
-                   "sample": "one product by the reference's legacy scalar kernel"}
+                   "sample": "one product by the reference's legacy scalar kernel",
+                   "check": {"bit_exact": bool(same), "mismatched": 0 if same else 1,
+                             "against": "reference: the product of the last timed step"}}
     in_b = sum(x[2].nbytes + x[3].nbytes + x[4].nbytes for x in ((ta, tb) if tb is not ta else (ta,)))
     out_b = rp.nbytes + ci.nbytes + cv.nbytes
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 1, "steps": args.steps,
@@ -390,7 +429,8 @@ def run_typed(args, world, rank, local):
                     "d2h_bytes_per_step": int(out_b),
                     "api": "rvsp_spgemm_csr {RVSP_BACKEND_CUDA, " +
                            ("FP64, FP64}" if args.dtype == "f64" else "INT8, INT32}")},
-            "gpu_launches": None, "cpu_baseline": cpu}
+            "gpu_launches": None, "cpu_baseline": cpu,
+            "correct": cpu["check"]["bit_exact"] if cpu else None}
     print(json.dumps(line), flush=True)
     return 0
 
@@ -556,6 +596,15 @@ def run_batch(args, world, rank, local):
     peak, peak_kind = measured_peaks()
     achieved = alg_bytes / (ms_per_step * 1e-3) / 1e9
 
+    # Every 16th product's operands in the last timed step and its C, for the
+    # reference check in the CPU baseline leg.
+    check_set = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        last = pools[(args.steps - 1) % 2]
+        check_set = [(prods[i][0].with_values(last[i][0].cpu().numpy()),
+                      prods[i][1].with_values(last[i][1].cpu().numpy()), b.result(i))
+                     for i in range(0, len(prods), 16)]
+
     # End to end: host memory space, pinned operands; each step uploads every
     # value (inside compute) and copies every C_i back (row_ptr, col_idx,
     # values) into one pinned buffer sized for the largest product.
@@ -612,6 +661,9 @@ def run_batch(args, world, rank, local):
                "cores": threads, "kind": "reference" if oracle.ref_available() else "port",
                "sample": f"first {len(done)} of {len(prods)} products (one-shot each, "
                          f"one per thread) on {threads} threads in {el:.1f} s"}
+        cpu["check"] = reference_check(check_set, f"{len(check_set)} of {len(prods)} "
+                                       "products (every 16th) of the last timed step")
+        check_set = None
 
     b.close()
     if rank == 0:
@@ -644,6 +696,7 @@ def run_batch(args, world, rank, local):
                          "algorithmic_bytes_per_launch": alg_bytes},
             "clocks": clocks, "e2e": e2e, "gpu_launches": stats["graph_nodes"],
             "cpu_baseline": cpu,
+            "correct": cpu["check"]["bit_exact"] if cpu else None,
         }
         print(json.dumps(line), flush=True)
     if pg:
@@ -745,6 +798,14 @@ def run_panels(args, world, rank, local):
         total_ms = float(t.item())
     ms_per_step = total_ms / args.steps
     value = flops_all * args.steps / (total_ms * 1e-3) / 1e9
+    # The last panel's C stays in dC after the last step: its operands and C
+    # for the reference check in the CPU baseline leg.
+    check_set = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline and panels:
+        P, n = panels[-1], nnz[-1]
+        gC = DeviceCSR(P.rows, A.cols, dC.row_ptr[:P.rows + 1], dC.col_idx[:max(n, 1)],
+                       dC.values[:max(n, 1)]).to_host(n)
+        check_set = [(P, A, gC)]
     phases = {}
     for d in descs:
         for k, (ms, nl) in d.phase_times(reset=True).items():
@@ -814,6 +875,9 @@ def run_panels(args, world, rank, local):
                "cores": threads, "kind": "reference" if oracle.ref_available() else "port",
                "sample": f"{len(done)} panels of 256 rows spread over the matrix, one-shot "
                          f"each, on {threads} threads in {el:.1f} s"}
+        if check_set:
+            cpu["check"] = reference_check(check_set, "the last panel of the last timed step")
+            check_set = None
 
     for d in descs:
         d.close()
@@ -841,6 +905,7 @@ def run_panels(args, world, rank, local):
                          "traffic": committed_traffic(args.workload, dom),
                          "algorithmic_bytes_per_launch": alg_bytes},
             "clocks": clocks, "e2e": e2e, "gpu_launches": launches, "cpu_baseline": cpu,
+            "correct": cpu["check"]["bit_exact"] if cpu and "check" in cpu else None,
         }
         print(json.dumps(line), flush=True)
     if pg:
@@ -849,15 +914,46 @@ def run_panels(args, world, rank, local):
     return 0
 
 
-def cpu_baseline(A, B, flops, seconds=12.0):
+def same_csr(got, rp, ci, cv) -> bool:
+    """Bit-identical structure and values (values compared as bit patterns)."""
+    return (np.array_equal(got.row_ptr, rp) and np.array_equal(got.col_idx, ci)
+            and np.array_equal(got.values.view(np.uint32), cv.view(np.uint32)))
+
+
+def cpu_baseline(A, B, flops, seconds=12.0, check=None):
+    """The reference library timed on all host cores.  check = (A, B, C): the
+    operands of the GPU's last timed step and the C it wrote; the reference
+    computes that product once more and `check.bit_exact` says whether the
+    GPU's C is bit-identical to it (the reference bench's `correct` column)."""
     sys.path.insert(0, str(ROOT))
     from oracle import oracle
     threads = os.cpu_count() or 1
     runs, el = oracle.time_reference_oneshot(A, B, seconds=seconds, threads=threads,
                                              max_runs=400)
-    return {"value": flops * runs / el / 1e9, "unit": UNIT, "cores": threads,
-            "kind": "reference" if oracle.ref_available() else "port",
-            "sample": f"{runs} full one-shot products on {threads} threads in {el:.1f} s"}
+    kind = "reference" if oracle.ref_available() else "port"
+    out = {"value": flops * runs / el / 1e9, "unit": UNIT, "cores": threads, "kind": kind,
+           "sample": f"{runs} full one-shot products on {threads} threads in {el:.1f} s"}
+    if check is not None:
+        out["check"] = reference_check([check], "one product of the last timed step")
+    return out
+
+
+def reference_check(items, what: str) -> dict:
+    """items: (A, B, C) triples, C the GPU's product; each is recomputed by
+    the reference library (the oracle port when the library is absent) and
+    compared bit for bit."""
+    sys.path.insert(0, str(ROOT))
+    from oracle import oracle
+    ref = oracle.ref_available()
+    bad = 0
+    for cA, cB, gC in items:
+        if ref:
+            st, rp, ci, cv = oracle.ref_spgemm(cA, cB)
+        else:
+            st, (rp, ci, cv, _) = 0, oracle.spgemm(cA, cB)
+        bad += 0 if st == 0 and same_csr(gC, rp, ci, cv) else 1
+    return {"bit_exact": bad == 0, "mismatched": bad,
+            "against": f"{'reference' if ref else 'port'}: {what}"}
 
 
 def main():
@@ -1020,6 +1116,14 @@ def main():
     launches = int(sum(v[1] for v in phases.values()))
     traffic = committed_traffic(args.workload, dom)
 
+    # The last timed step's operands and result, for the reference check in
+    # the CPU baseline leg (in the reuse steps A's values, and B's when B is
+    # A, are the last perturbation).
+    check = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        A_last = A.with_values(dA.values.cpu().numpy())
+        check = (A_last, A_last if B is A else B, dC.to_host(c_nnz))
+
     # End to end through the public API, host memory space, pinned buffers.
     e2e = None
     if rank == 0 or world > 1:
@@ -1071,7 +1175,8 @@ def main():
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu = cpu_baseline(A, B, flops)
+        cpu = cpu_baseline(A, B, flops, check=check)
+        check = None
 
     d.close()
     if rank == 0:
@@ -1107,6 +1212,7 @@ def main():
                          "algorithmic_bytes_per_launch": alg_bytes},
             "clocks": clocks, "e2e": e2e, "gpu_launches": launches,
             "cpu_baseline": cpu,
+            "correct": cpu["check"]["bit_exact"] if cpu and "check" in cpu else None,
         }
         print(json.dumps(line), flush=True)
     if pg:
