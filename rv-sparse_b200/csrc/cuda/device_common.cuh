@@ -232,6 +232,47 @@ __device__ __forceinline__ void warp_bitonic_sort(unsigned long long *s, int n) 
   }
 }
 
+// Bitonic sort of 32 R 64-bit keys held in registers by one warp: element
+// e = 32 r + lane is v[r] of that lane.  Stages with distance j < 32 pair
+// lanes (shuffle; the lane with bit j clear holds the lower index and keeps
+// the minimum in an ascending block, the maximum in a descending one);
+// stages with j >= 32 pair registers r and r | j/32 inside a lane.  No
+// shared memory.
+template <int R>
+__device__ __forceinline__ void warp_bitonic_sort_regs(unsigned long long (&v)[R]) {
+  constexpr int N = 32 * R;
+  const int lane = lane_id();
+#pragma unroll
+  for (int k = 2; k <= N; k <<= 1) {
+#pragma unroll
+    for (int j = k >> 1; j > 0; j >>= 1) {
+      if (j >= 32) {
+        const int jr = j >> 5;
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+          if (r & jr) continue;  // r holds the pair's lower index
+          const bool up = ((r * 32 + lane) & k) == 0;
+          const unsigned long long x = v[r], y = v[r | jr];
+          if ((x > y) == up) {
+            v[r] = y;
+            v[r | jr] = x;
+          }
+        }
+      } else {
+        const bool lower = (lane & j) == 0;
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+          const bool up = ((r * 32 + lane) & k) == 0;
+          const unsigned long long y = __shfl_xor_sync(kFull, v[r], j);
+          const unsigned long long lo = v[r] < y ? v[r] : y;
+          const unsigned long long hi = v[r] < y ? y : v[r];
+          v[r] = lower == up ? lo : hi;
+        }
+      }
+    }
+  }
+}
+
 // Same, by a whole block (n power of two).
 __device__ __forceinline__ void block_bitonic_sort(unsigned long long *s, int n) {
   for (int k = 2; k <= n; k <<= 1) {

@@ -19,8 +19,8 @@
 //           memory that each row leaves zeroed.
 //
 // Fill mode emits columns sorted: hash classes compact their (col, value)
-// pairs and bitonic-sort them; the dense class walks its column bitmap in
-// order.  Reuse mode (columns already in C) maps column -> position through
+// pairs and bitonic-sort them (in registers up to 128 pairs a warp, else in
+// shared memory); the dense class walks its column bitmap in order.  Reuse mode (columns already in C) maps column -> position through
 // a hash of C's row and writes the values coalesced.
 #include <climits>
 
@@ -120,9 +120,42 @@ __device__ __forceinline__ void mark_overflow(const FusedOut &fo, int32_t row) {
   fo.ovf_rows[atomicAdd(fo.ovf_count, 1)] = row;
 }
 
+// Writes a row's kept (column, value) pairs, compacted in sbuf, sorted by
+// column: up to 32 R of them are sorted in registers (no shared-memory
+// traffic, which bounds this kernel) and the first `out` go to C from out0,
+// 32 consecutive entries per store.
+template <int R>
+__device__ __forceinline__ void write_sorted_regs(const unsigned long long *sbuf, int kept,
+                                                  int out, int64_t out0, int32_t *c_col,
+                                                  float *c_val) {
+  const int lane = lane_id();
+  unsigned long long v[R];
+#pragma unroll
+  for (int r = 0; r < R; ++r) {
+    const int e = r * 32 + lane;
+    v[r] = e < kept ? sbuf[e] : ~0ull;
+  }
+  warp_bitonic_sort_regs<R>(v);
+#pragma unroll
+  for (int r = 0; r < R; ++r) {
+    const int e = r * 32 + lane;
+    if (e < out) {
+      c_col[out0 + e] = packed_col(v[r]);
+      c_val[out0 + e] = packed_val(v[r]);
+    }
+  }
+}
+
+// Blocks per SM the fill kernel asks the compiler to fit: 16 (32 registers)
+// for W64, W128 and non-fused W256 rows, which fit 16 blocks by shared memory
+// too and need no spill at 32 registers; 12 (up to 42) for the others.
+constexpr int fill_min_blocks(int log2t, bool fused) {
+  return log2t <= 7 || (log2t == 8 && !fused) ? 16 : 12;
+}
+
 // Shared memory per warp: sbuf[T/2] u64 | keys[T] i32 | vals[T] f32 = 12 T bytes.
 template <int LOG2T, bool kFused>
-__global__ void __launch_bounds__(kWarpsPerBlock * 32)
+__global__ void __launch_bounds__(kWarpsPerBlock * 32, fill_min_blocks(LOG2T, kFused))
 num_warp_fill_kernel(Operands op, const int64_t *__restrict__ ops,
                      const int32_t *__restrict__ rows, int32_t nrows,
                      const int32_t *__restrict__ c_rp, int32_t *__restrict__ c_col,
@@ -201,16 +234,25 @@ num_warp_fill_kernel(Operands op, const int64_t *__restrict__ ops,
     n += __popc(msk);
   }
   const int kept = n < H ? n : H;
-  int npow = 1;
-  while (npow < kept) npow <<= 1;
-  for (int e = kept + lane; e < npow; e += 32) sbuf[e] = ~0ull;
-  __syncwarp();
-  warp_bitonic_sort(sbuf, npow);
   const int out = kept < m ? kept : m;
-  for (int e = lane; e < out; e += 32) {
-    const unsigned long long x = sbuf[e];
-    c_col[out0 + e] = packed_col(x);
-    c_val[out0 + e] = packed_val(x);
+  __syncwarp();
+  if (kept <= 32) {
+    write_sorted_regs<1>(sbuf, kept, out, out0, c_col, c_val);
+  } else if (H >= 64 && kept <= 64) {
+    write_sorted_regs<2>(sbuf, kept, out, out0, c_col, c_val);
+  } else if (H >= 128 && kept <= 128) {
+    write_sorted_regs<4>(sbuf, kept, out, out0, c_col, c_val);
+  } else {
+    int npow = 1;
+    while (npow < kept) npow <<= 1;
+    for (int e = kept + lane; e < npow; e += 32) sbuf[e] = ~0ull;
+    __syncwarp();
+    warp_bitonic_sort(sbuf, npow);
+    for (int e = lane; e < out; e += 32) {
+      const unsigned long long x = sbuf[e];
+      c_col[out0 + e] = packed_col(x);
+      c_val[out0 + e] = packed_val(x);
+    }
   }
   const bool any_bad = __any_sync(kFull, bad);
   if (lane == 0) {
