@@ -195,6 +195,23 @@ def test_long_a_rows():
     check_against_oracle(A, B, "long A rows")
 
 
+def test_nnz_beyond_int32_is_allocation_failed():
+    # nnz(C) = 65536 x 32768 = 2^31 > INT32_MAX from 98,304 stored entries:
+    # every A row selects the one full B row.  The reference's symbolic pass
+    # returns ALLOCATION_FAILED on the int64 total (rvsp_symbolic.c:69-72);
+    # so must the one-shot call and work_estimation here.
+    n, w = 65536, 32768
+    A = CSR(n, 1, np.arange(n + 1), np.zeros(n), np.ones(n, np.float32))
+    B = CSR(1, w, np.array([0, w]), np.arange(w), np.ones(w, np.float32))
+    with pytest.raises(L.RvspError) as e:
+        spgemm_csr(A, B)
+    assert e.value.status == L.ERROR_ALLOCATION_FAILED
+    with Descriptor() as d:
+        with pytest.raises(L.RvspError) as e:
+            d.work_estimation(A, B)
+        assert e.value.status == L.ERROR_ALLOCATION_FAILED
+
+
 def test_edge_cases():
     one = np.ones(1, np.float32)
     # empty A
