@@ -70,7 +70,9 @@ size_t rvsp_cuda_numeric_workspace_bytes(rvsp_cuda_plan_t plan);
  * read the verdict on the device and return without reading the
  * structure or writing c_row_ptr; the plan is left unanalysed.  Otherwise
  * the same results as rvsp_cuda_symbolic, with one host round trip fewer
- * than calling the check first.  Synchronizes `stream`. */
+ * than calling the check first.  INVALID_ARGUMENT when a_cols != b_rows (as
+ * the reference's shape check, spgemm_descr.c:185-188).  Synchronizes
+ * `stream`. */
 rvsp_status_t rvsp_cuda_symbolic_checked(rvsp_cuda_plan_t plan, void *stream, int32_t a_rows,
                                          int32_t a_cols, int32_t a_nnz, int32_t b_rows,
                                          int32_t b_cols, int32_t b_nnz,

@@ -440,8 +440,10 @@ rvsp_status_t rvsp_cuda_symbolic_checked(rvsp_cuda_plan_t p, void *stream, int32
     return RVSP_ERROR_NULL_POINTER;
   if (a_rows <= 0 || b_rows <= 0 || b_cols <= 0 || a_cols < 0 || a_nnz < 0 || b_nnz < 0)
     return RVSP_ERROR_INVALID_ARGUMENT;
-  // A's columns index B's rows: a column the check lets through is < a_cols,
-  // and the row statistics bound it by b_rows as well.
+  // A's columns index B's rows: a column the check lets through is < a_cols
+  // = b_rows, so every pass after the verdict reads B's row pointers in
+  // bounds (the row statistics bound it by b_rows as well).
+  if (a_cols != b_rows) return RVSP_ERROR_INVALID_ARGUMENT;
   const PreCheck chk{a_cols, a_nnz, b_nnz, check_b != 0};
   return symbolic_impl(p, static_cast<cudaStream_t>(stream), a_rows, b_rows, b_cols,
                        a_row_ptr, a_col_idx, b_row_ptr, b_col_idx, c_row_ptr, c_nnz_out,

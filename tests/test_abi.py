@@ -205,3 +205,25 @@ def test_oneshot_argument_errors(golden_fixtures):
     assert lib.rvsp_spgemm_csr(C.byref(badm), C.byref(b), C.byref(c),
                                C.byref(cuda)) == L.ERROR_INVALID_CSR
     assert not c.row_ptr and c.nnz == 0 and c.owns_data == 0
+
+
+def test_checked_symbolic_argument_errors():
+    # Argument checks of rvsp_cuda_symbolic_checked come before any use of the
+    # plan or the arrays, so stand-in non-null pointers never get read here.
+    lib = L.load()
+    p = C.c_void_p(16)  # never dereferenced: every call below fails its checks
+    arr = C.c_void_p(64)
+    total = C.c_int64(0)
+
+    def call(a_rows, a_cols, a_nnz, b_rows, b_cols, b_nnz, plan=p, c_rp=arr):
+        return lib.rvsp_cuda_symbolic_checked(plan, None, a_rows, a_cols, a_nnz, b_rows,
+                                              b_cols, b_nnz, arr, arr, arr, arr, 1, c_rp,
+                                              C.byref(total))
+    assert call(4, 3, 5, 3, 2, 4, plan=None) == L.ERROR_NULL_POINTER
+    assert call(4, 3, 5, 3, 2, 4, c_rp=None) == L.ERROR_NULL_POINTER
+    assert call(0, 3, 5, 3, 2, 4) == L.ERROR_INVALID_ARGUMENT
+    assert call(4, 3, -1, 3, 2, 4) == L.ERROR_INVALID_ARGUMENT
+    # A's columns must be B's rows: more would index B's row pointers past
+    # their end once the check has passed
+    assert call(4, 5, 5, 3, 2, 4) == L.ERROR_INVALID_ARGUMENT
+    assert call(4, 2, 5, 3, 2, 4) == L.ERROR_INVALID_ARGUMENT
