@@ -138,7 +138,7 @@ rvsp_status_t rvsp_spgemm_batch_create(rvsp_spgemm_batch_t *batch)
     if (batch == NULL)
         return RVSP_ERROR_NULL_POINTER;
     *batch = NULL;
-    struct rvsp_spgemm_batch *b = (struct rvsp_spgemm_batch *)calloc(1, sizeof(*b));
+    struct rvsp_spgemm_batch *b = (struct rvsp_spgemm_batch *)rvsp_calloc(1, sizeof(*b));
     if (b == NULL)
         return RVSP_ERROR_ALLOCATION_FAILED;
     b->mem = RVSP_MEM_HOST;
@@ -237,11 +237,11 @@ rvsp_status_t rvsp_spgemm_batch_add(rvsp_spgemm_batch_t b, const rvsp_csr_matrix
         return RVSP_ERROR_INVALID_ARGUMENT;
     if (b->count == b->cap) {
         const int32_t cap = b->cap ? 2 * b->cap : 64;
-        rvsp_csr_matrix_t *na = (rvsp_csr_matrix_t *)realloc(b->A, (size_t)cap * sizeof(*na));
+        rvsp_csr_matrix_t *na = (rvsp_csr_matrix_t *)rvsp_realloc(b->A, (size_t)cap * sizeof(*na));
         if (na == NULL)
             return RVSP_ERROR_ALLOCATION_FAILED;
         b->A = na;
-        rvsp_csr_matrix_t *nb = (rvsp_csr_matrix_t *)realloc(b->B, (size_t)cap * sizeof(*nb));
+        rvsp_csr_matrix_t *nb = (rvsp_csr_matrix_t *)rvsp_realloc(b->B, (size_t)cap * sizeof(*nb));
         if (nb == NULL)
             return RVSP_ERROR_ALLOCATION_FAILED;
         b->B = nb;
@@ -294,7 +294,7 @@ static rvsp_status_t stage_host_operands(rvsp_spgemm_batch_t b)
         st = rvsp_dbuf_reserve(&b->raw_f32, (size_t)(n_f32 > 0 ? n_f32 : 1) * sizeof(float));
     if (st != RVSP_SUCCESS)
         return st;
-    b->raw_val_off = (int64_t *)malloc((size_t)(uint32_t)b->count * 2 * sizeof(int64_t));
+    b->raw_val_off = (int64_t *)rvsp_malloc((size_t)(uint32_t)b->count * 2 * sizeof(int64_t));
     if (b->raw_val_off == NULL)
         return RVSP_ERROR_ALLOCATION_FAILED;
     int32_t *i32 = (int32_t *)b->raw_i32.p;
@@ -371,8 +371,8 @@ static rvsp_status_t take_error(rvsp_spgemm_batch_t b)
 static rvsp_status_t form_groups(rvsp_spgemm_batch_t b)
 {
     const size_t n = (size_t)(uint32_t)b->count;
-    b->groups = (batch_group_t *)calloc(n, sizeof(batch_group_t));
-    b->group_of = (int32_t *)malloc(n * sizeof(int32_t));
+    b->groups = (batch_group_t *)rvsp_calloc(n, sizeof(batch_group_t));
+    b->group_of = (int32_t *)rvsp_malloc(n * sizeof(int32_t));
     if (b->groups == NULL || b->group_of == NULL)
         return RVSP_ERROR_ALLOCATION_FAILED;
     int32_t ng = 0;
@@ -409,7 +409,7 @@ static rvsp_status_t form_groups(rvsp_spgemm_batch_t b)
 static rvsp_status_t pack_group(rvsp_spgemm_batch_t b, batch_group_t *g)
 {
     rvsp_cuda_batch_offset_t *off =
-        (rvsp_cuda_batch_offset_t *)malloc((size_t)(uint32_t)g->count * sizeof(*off));
+        (rvsp_cuda_batch_offset_t *)rvsp_malloc((size_t)(uint32_t)g->count * sizeof(*off));
     if (off == NULL)
         return RVSP_ERROR_ALLOCATION_FAILED;
     int32_t ar = 0, an = 0, br = 0, bn = 0;
@@ -588,9 +588,9 @@ static rvsp_status_t autotune_policy(rvsp_spgemm_batch_t b)
 static rvsp_status_t build_views(rvsp_spgemm_batch_t b)
 {
     const size_t n = (size_t)(uint32_t)b->count;
-    b->crp_off = (int64_t *)malloc(n * sizeof(int64_t));
-    b->base = (int32_t *)malloc(n * sizeof(int32_t));
-    b->nnz = (int32_t *)malloc(n * sizeof(int32_t));
+    b->crp_off = (int64_t *)rvsp_malloc(n * sizeof(int64_t));
+    b->base = (int32_t *)rvsp_malloc(n * sizeof(int32_t));
+    b->nnz = (int32_t *)rvsp_malloc(n * sizeof(int32_t));
     if (b->crp_off == NULL || b->base == NULL || b->nnz == NULL)
         return RVSP_ERROR_ALLOCATION_FAILED;
     int64_t rows = 0;
@@ -644,8 +644,8 @@ rvsp_status_t rvsp_spgemm_batch_work_estimation(rvsp_spgemm_batch_t b,
     if (st != RVSP_SUCCESS)
         return st;
     const size_t n = (size_t)(uint32_t)b->count;
-    b->h_items = (rvsp_cuda_batch_item_t *)calloc(n, sizeof(rvsp_cuda_batch_item_t));
-    b->h_ops = (int64_t *)calloc(n, sizeof(int64_t));
+    b->h_items = (rvsp_cuda_batch_item_t *)rvsp_calloc(n, sizeof(rvsp_cuda_batch_item_t));
+    b->h_ops = (int64_t *)rvsp_calloc(n, sizeof(int64_t));
     if (b->h_items == NULL || b->h_ops == NULL)
         return RVSP_ERROR_ALLOCATION_FAILED;
     for (int32_t i = 0; i < b->count; i++) {

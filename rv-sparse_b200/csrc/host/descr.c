@@ -63,7 +63,7 @@ rvsp_status_t rvsp_spgemm_descr_create(rvsp_spgemm_descr_t *descr)
         return RVSP_ERROR_NULL_POINTER;
     *descr = NULL;
     struct rvsp_spgemm_descr *d =
-        (struct rvsp_spgemm_descr *)calloc(1, sizeof(*d));
+        (struct rvsp_spgemm_descr *)rvsp_calloc(1, sizeof(*d));
     if (d == NULL)
         return RVSP_ERROR_ALLOCATION_FAILED;
     d->algo = RVSP_SPGEMM_ALGO_DEFAULT;
@@ -537,10 +537,10 @@ rvsp_status_t rvsp_spgemm_multiply(rvsp_spgemm_descr_t d, const rvsp_csr_matrix_
     out.format = RVSP_FORMAT_CSR;
     if (d->mem == RVSP_MEM_HOST) {
         out.owns_data = 1;
-        out.row_ptr = (int32_t *)malloc(rp_bytes);
-        out.col_idx = (int32_t *)malloc(alloc * sizeof(int32_t));
-        out.values = malloc(alloc * sizeof(float));
-        void *ws = malloc(ws_bytes > 0 ? ws_bytes : 1);
+        out.row_ptr = (int32_t *)rvsp_malloc(rp_bytes);
+        out.col_idx = (int32_t *)rvsp_malloc(alloc * sizeof(int32_t));
+        out.values = rvsp_malloc(alloc * sizeof(float));
+        void *ws = rvsp_malloc(ws_bytes > 0 ? ws_bytes : 1);
         if (!out.row_ptr || !out.col_idx || !out.values || !ws)
             st = RVSP_ERROR_ALLOCATION_FAILED;
         else

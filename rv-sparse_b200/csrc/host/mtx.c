@@ -304,9 +304,9 @@ static rvsp_status_t finish(int32_t M, int32_t N, int64_t n, int symmetric, cons
         c_val = NULL;
     } else {
         const size_t cn = (size_t)(nnz > 0 ? nnz : 1);
-        int32_t *h_rp = (int32_t *)malloc(((size_t)M + 1) * sizeof(int32_t));
-        int32_t *h_col = (int32_t *)malloc(cn * sizeof(int32_t));
-        float *h_val = (float *)malloc(cn * sizeof(float));
+        int32_t *h_rp = (int32_t *)rvsp_malloc(((size_t)M + 1) * sizeof(int32_t));
+        int32_t *h_col = (int32_t *)rvsp_malloc(cn * sizeof(int32_t));
+        float *h_val = (float *)rvsp_malloc(cn * sizeof(float));
         if (!h_rp || !h_col || !h_val) {
             free(h_rp);
             free(h_col);
@@ -348,10 +348,11 @@ rvsp_status_t rvsp_csr_parse_mtx(const char *text, size_t len, rvsp_memory_space
 {
     if (!text || !out)
         return RVSP_ERROR_NULL_POINTER;
+    memset(out, 0, sizeof(*out)); /* every failure leaves out empty */
     if (space != RVSP_MEM_HOST && space != RVSP_MEM_DEVICE)
         return RVSP_ERROR_INVALID_ARGUMENT;
     /* a NUL-terminated copy: strtol / strtof must not run past the text */
-    char *t = (char *)malloc(len + 1);
+    char *t = (char *)rvsp_malloc(len + 1);
     if (!t)
         return RVSP_ERROR_ALLOCATION_FAILED;
     memcpy(t, text, len);
@@ -378,9 +379,9 @@ rvsp_status_t rvsp_csr_parse_mtx(const char *text, size_t len, rvsp_memory_space
     if (limit > fit)
         limit = fit;
     const size_t nb = (size_t)(limit > 0 ? limit : 1);
-    int32_t *row = (int32_t *)malloc(nb * sizeof(int32_t));
-    int32_t *col = (int32_t *)malloc(nb * sizeof(int32_t));
-    float *val = (float *)malloc(nb * sizeof(float));
+    int32_t *row = (int32_t *)rvsp_malloc(nb * sizeof(int32_t));
+    int32_t *col = (int32_t *)rvsp_malloc(nb * sizeof(int32_t));
+    float *val = (float *)rvsp_malloc(nb * sizeof(float));
     if (!row || !col || !val) {
         st = RVSP_ERROR_ALLOCATION_FAILED;
     } else {
@@ -399,6 +400,7 @@ rvsp_status_t rvsp_csr_read_mtx(const char *path, rvsp_memory_space_t space,
 {
     if (!path || !out)
         return RVSP_ERROR_NULL_POINTER;
+    memset(out, 0, sizeof(*out)); /* every failure leaves out empty */
     FILE *f = fopen(path, "rb");
     if (!f)
         return RVSP_ERROR_INVALID_ARGUMENT;
@@ -411,7 +413,7 @@ rvsp_status_t rvsp_csr_read_mtx(const char *path, rvsp_memory_space_t space,
         fclose(f);
         return RVSP_ERROR_INVALID_ARGUMENT;
     }
-    char *t = (char *)malloc((size_t)size + 1);
+    char *t = (char *)rvsp_malloc((size_t)size + 1);
     if (!t) {
         fclose(f);
         return RVSP_ERROR_ALLOCATION_FAILED;

@@ -22,6 +22,12 @@ typedef struct {
     size_t cap;
 } rvsp_dbuf_t;
 
+/* Host allocations of the library (alloc.c): malloc / calloc / realloc with
+ * the failure hook of rvsp_debug.h; release with free(). */
+void *rvsp_malloc(size_t n);
+void *rvsp_calloc(size_t n, size_t size);
+void *rvsp_realloc(void *p, size_t n);
+
 rvsp_status_t rvsp_dbuf_reserve(rvsp_dbuf_t *b, size_t bytes);
 void rvsp_dbuf_release(rvsp_dbuf_t *b);
 

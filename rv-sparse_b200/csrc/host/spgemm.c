@@ -61,7 +61,7 @@ static rvsp_status_t get_ctx(oneshot_ctx_t **out)
     pthread_once(&g_ctx_once, ctx_key_init);
     oneshot_ctx_t *c = (oneshot_ctx_t *)pthread_getspecific(g_ctx_key);
     if (!c) {
-        c = (oneshot_ctx_t *)calloc(1, sizeof(*c));
+        c = (oneshot_ctx_t *)rvsp_calloc(1, sizeof(*c));
         if (!c)
             return RVSP_ERROR_ALLOCATION_FAILED;
         rvsp_status_t st = rvsp_cuda_plan_create(&c->plan);
@@ -200,9 +200,9 @@ static rvsp_status_t oneshot_host(const rvsp_csr_matrix_t *A, const rvsp_csr_mat
         return st;
 
     const size_t alloc = (size_t)(c_nnz > 0 ? c_nnz : 1);
-    int32_t *rp = (int32_t *)malloc(((size_t)A->rows + 1) * sizeof(int32_t));
-    int32_t *ci = (int32_t *)malloc(alloc * sizeof(int32_t));
-    float *cv = (float *)malloc(alloc * sizeof(float));
+    int32_t *rp = (int32_t *)rvsp_malloc(((size_t)A->rows + 1) * sizeof(int32_t));
+    int32_t *ci = (int32_t *)rvsp_malloc(alloc * sizeof(int32_t));
+    float *cv = (float *)rvsp_malloc(alloc * sizeof(float));
     if (!rp || !ci || !cv) {
         free(rp);
         free(ci);

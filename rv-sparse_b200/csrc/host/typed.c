@@ -110,7 +110,7 @@ static rvsp_status_t typed_ctx(typed_ctx_t **out)
     pthread_once(&g_typed_once, typed_key_init);
     typed_ctx_t *c = (typed_ctx_t *)pthread_getspecific(g_typed_key);
     if (!c) {
-        c = (typed_ctx_t *)calloc(1, sizeof(*c));
+        c = (typed_ctx_t *)rvsp_calloc(1, sizeof(*c));
         if (!c)
             return RVSP_ERROR_ALLOCATION_FAILED;
         rvsp_status_t st = rvsp_cuda_plan_create(&c->plan);
@@ -155,9 +155,9 @@ rvsp_status_t rvsp_typed_oneshot(const rvsp_csr_matrix_t *A, const rvsp_csr_matr
     int32_t *h_rp = NULL, *h_ci = NULL;
     void *h_v = NULL;
     if (A->rows == 0) { /* (FP64 only: INT8 requires rows > 0) an empty product */
-        h_rp = (int32_t *)calloc(1, sizeof(int32_t));
-        h_ci = (int32_t *)malloc(sizeof(int32_t));
-        h_v = malloc(out_sz);
+        h_rp = (int32_t *)rvsp_calloc(1, sizeof(int32_t));
+        h_ci = (int32_t *)rvsp_malloc(sizeof(int32_t));
+        h_v = rvsp_malloc(out_sz);
         if (!h_rp || !h_ci || !h_v) {
             st = RVSP_ERROR_ALLOCATION_FAILED;
             goto done;
@@ -228,9 +228,9 @@ rvsp_status_t rvsp_typed_oneshot(const rvsp_csr_matrix_t *A, const rvsp_csr_matr
         goto done;
     {
         const size_t kn = (size_t)(kept > 0 ? kept : 1);
-        h_rp = (int32_t *)malloc(rp_b);
-        h_ci = (int32_t *)malloc(kn * sizeof(int32_t));
-        h_v = malloc(kn * out_sz);
+        h_rp = (int32_t *)rvsp_malloc(rp_b);
+        h_ci = (int32_t *)rvsp_malloc(kn * sizeof(int32_t));
+        h_v = rvsp_malloc(kn * out_sz);
         if (!h_rp || !h_ci || !h_v) {
             st = RVSP_ERROR_ALLOCATION_FAILED;
             goto done;

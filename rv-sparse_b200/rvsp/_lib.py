@@ -92,6 +92,8 @@ SIGNATURES = {
     "rvsp_csr_read_mtx": (_int, [C.c_char_p, _int, _P(CsrMatrix)]),
     "rvsp_csr_parse_mtx": (_int, [C.c_char_p, C.c_size_t, _int, _P(CsrMatrix)]),
     "rvsp_csr_copy_arrays": (_int, [_P(CsrMatrix), _P(CsrMatrix)]),
+    "rvsp_debug_fail_host_alloc": (None, [_i32]),
+    "rvsp_debug_host_allocs": (_i64, []),
     "rvsp_cuda_coo_to_csr": (_int, [_vp, _i32, _i32, _i64, _int, _vp, _vp, _vp, _vp,
                                     _P(_vp), _P(_vp), _P(_i32)]),
     "rvsp_cuda_symbolic_checked": (_int, [_vp, _vp, _i32, _i32, _i32, _i32, _i32, _i32, _vp,
