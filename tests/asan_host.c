@@ -3,9 +3,10 @@
  * build of the library (make -C rv-sparse_b200 asan) and run by
  * tests/test_asan_host.py with leak detection on.  It drives the host C
  * layer through the calls that need no GPU to reach their error paths:
- * argument errors, the Matrix Market reader, the one-shot, descriptor and
- * batch entry points up to their first device step, and every host
- * allocation of the reader failed in turn (rvsp_debug.h).  Exit 0 when every
+ * argument errors, the Matrix Market reader, the one-shot (FP32, FP64,
+ * INT8 -> INT32), descriptor and batch entry points up to their first device
+ * step, and every host allocation of the reader and of the one-shot failed in
+ * turn (rvsp_debug.h).  Exit 0 when every
  * status is the expected one; AddressSanitizer exits non-zero on a memory
  * error or a leak.  With a GPU present the device steps succeed instead, and
  * the driver frees what they return.
@@ -61,6 +62,32 @@ static void walk_parse(rvsp_memory_space_t space)
         st = rvsp_csr_parse_mtx(kText, sizeof(kText) - 1, space, &m);
         EXPECT(st == RVSP_ERROR_ALLOCATION_FAILED, "parse_mtx injected failure");
         EXPECT(empty(&m), "parse_mtx output empty after failure");
+    }
+    rvsp_debug_fail_host_alloc(-1);
+}
+
+/* Every host allocation of one one-shot product failed in turn: each must
+ * return ALLOCATION_FAILED with C left empty (the reference nulls C on any
+ * failure, spgemm.c:117-130). */
+static void walk_oneshot(const rvsp_csr_matrix_t *A, const rvsp_csr_matrix_t *B,
+                         const rvsp_spgemm_options_t *opts, const char *what)
+{
+    rvsp_csr_matrix_t C;
+    memset(&C, 0, sizeof(C));
+    const int64_t before = rvsp_debug_host_allocs();
+    rvsp_status_t st = rvsp_spgemm_csr(A, B, &C, opts);
+    const int64_t n = rvsp_debug_host_allocs() - before;
+    EXPECT(device_outcome(st), what);
+    if (st == RVSP_SUCCESS)
+        rvsp_csr_destroy(&C);
+    for (int64_t k = 0; k < n; k++) {
+        memset(&C, 0, sizeof(C));
+        rvsp_debug_fail_host_alloc((int32_t)k);
+        st = rvsp_spgemm_csr(A, B, &C, opts);
+        EXPECT(st == RVSP_ERROR_ALLOCATION_FAILED, what);
+        EXPECT(empty(&C), what);
+        if (st == RVSP_SUCCESS)
+            rvsp_csr_destroy(&C);
     }
     rvsp_debug_fail_host_alloc(-1);
 }
@@ -136,6 +163,24 @@ int main(void)
             EXPECT(rvsp_spgemm_batch_add(b, &A, &B, NULL) == RVSP_SUCCESS, "batch_add");
         rvsp_spgemm_batch_destroy(b);
     }
+
+    /* the one-shot in its three value types, every host allocation failed */
+    walk_oneshot(&A, &B, NULL, "oneshot fp32 walk");
+    double av64[] = {1.0, 2.0, 3.0}, bv64[] = {4.0, 5.0, 6.0, 7.0};
+    int8_t av8[] = {1, 2, 3}, bv8[] = {4, 5, 6, 7};
+    rvsp_csr_matrix_t A64, B64, A8, B8;
+    EXPECT(rvsp_csr_create(&A64, 2, 3, 3, arp, aci, av64, RVSP_DTYPE_FP64) == RVSP_SUCCESS,
+           "csr_create A64");
+    EXPECT(rvsp_csr_create(&B64, 3, 2, 4, brp, bci, bv64, RVSP_DTYPE_FP64) == RVSP_SUCCESS,
+           "csr_create B64");
+    EXPECT(rvsp_csr_create(&A8, 2, 3, 3, arp, aci, av8, RVSP_DTYPE_INT8) == RVSP_SUCCESS,
+           "csr_create A8");
+    EXPECT(rvsp_csr_create(&B8, 3, 2, 4, brp, bci, bv8, RVSP_DTYPE_INT8) == RVSP_SUCCESS,
+           "csr_create B8");
+    const rvsp_spgemm_options_t o64 = {RVSP_BACKEND_CUDA, RVSP_DTYPE_FP64, RVSP_DTYPE_FP64};
+    const rvsp_spgemm_options_t o8 = {RVSP_BACKEND_CUDA, RVSP_DTYPE_INT8, RVSP_DTYPE_INT32};
+    walk_oneshot(&A64, &B64, &o64, "oneshot fp64 walk");
+    walk_oneshot(&A8, &B8, &o8, "oneshot int8 walk");
 
     walk_parse(RVSP_MEM_HOST);
     walk_parse(RVSP_MEM_DEVICE);
