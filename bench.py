@@ -5,7 +5,12 @@
   python bench.py --impl reference ...      # the reference scalar CPU backend
 
 A step is one pass of the hot path over the workload's input:
-  laplace2d   (default) C = A x A, A the 2D 5-point Laplacian on 1024^2
+  stencil3d_job  (default) the 128^3 27-point stencil's whole job: C = A x A
+              by the learned path (work_estimation + compute), then 50
+              numeric-only computes with A's values perturbed by
+              U[-0.01, 0.01]; plain and learned products and the repeat are
+              also reported alone (run_job).
+  laplace2d   C = A x A, A the 2D 5-point Laplacian on 1024^2
               (n = 1,048,576, nnz = 5,238,784): one full product
               (work_estimation + compute) with A resident in HBM.
   uniform4096 C = A x B, 4096^2, exactly 16 nnz/row (A seed S, B seed S+1).
@@ -50,6 +55,9 @@ UNIT = "GFLOP/s"
 FALLBACK_HBM_GBS = 6650.0
 
 WORKLOADS = {
+    "stencil3d_job": ("3D 27-point stencil 128^3 (n=2,097,152, nnz=55,742,968), C=A*A: the "
+                      "first product (learned binning, fused single pass) then 50 numeric-only "
+                      "descriptor repeats with A's values perturbed by U[-0.01,0.01]"),
     "laplace2d": "2D 5-point Laplacian 1024x1024 (n=1,048,576, nnz=5,238,784), C=A*A, full product",
     "uniform4096": "4096x4096, exactly 16 nnz/row uniform columns, values U[-1,1], C=A*B, full product",
     "stencil3d": "3D 27-point stencil 128^3 (n=2,097,152, nnz=55,742,968), C=A*A, full product",
@@ -461,6 +469,25 @@ def run_reference(args, world, rank):
         value = fl / el / 1e9
         sample = (f"{args.steps * threads} of the {len(prods)} products, one per thread "
                   f"({args.steps} steps x {threads} threads)")
+    elif args.workload == "stencil3d_job":
+        # each step: the job's first product + JOB_CPU_REPEATS numeric-only
+        # repeats (two perturbed value sets alternating), rows of A cut into
+        # one panel per thread
+        from rvsp import gen
+        A = gen.stencil_3d_27(args.grid)
+        flops = 2.0 * float(intermediate_products(A, A).sum())
+        sets = job_value_sets_host(A, 2, args.seed + 2)
+        cpu_sets = [(sets[r % 2], sets[r % 2]) for r in range(JOB_CPU_REPEATS)]
+        fl, el = 0.0, 0.0
+        for i in range(args.warmup + args.steps):
+            t = oracle.time_reference_job(A, A, cpu_sets, threads)
+            if i >= args.warmup:
+                fl += (1 + JOB_CPU_REPEATS) * flops
+                el += t
+        value = fl / el / 1e9
+        sample = (f"per step the job's first product + {JOB_CPU_REPEATS} of its "
+                  f"{args.repeats} numeric-only repeats, rows of A cut into {threads} "
+                  f"panels, one per thread ({args.steps} steps)")
     elif args.workload == "rmat20_panels":
         # C does not fit the reference (nnz(C) ~9e9 > INT32_MAX): each step
         # times `threads` panels of 256 rows spread over the matrix, one per
@@ -914,6 +941,326 @@ def run_panels(args, world, rank, local):
     return 0
 
 
+JOB_REPEATS = 50     # numeric-only repeats of the stencil job
+JOB_CPU_REPEATS = 8  # repeats in the reference's bounded sample of the job
+
+
+def panel_rows(ops: np.ndarray, world: int, rank: int):
+    """Rank's contiguous row range [r0, r1) when the rows are cut into
+    `world` panels of about equal op count (rows of C are independent)."""
+    if world <= 1:
+        return 0, int(ops.size)
+    cum = np.concatenate([[0], np.cumsum(ops, dtype=np.int64)])
+    cuts = [int(np.searchsorted(cum, cum[-1] * k / world)) for k in range(world + 1)]
+    cuts[0], cuts[-1] = 0, int(ops.size)
+    for k in range(1, world + 1):
+        cuts[k] = max(cuts[k], cuts[k - 1])
+    return cuts[rank], cuts[rank + 1]
+
+
+def job_value_sets_host(A, n: int, seed: int):
+    """n host copies of A's values perturbed by U[-0.01, 0.01] (seeded)."""
+    rng = np.random.default_rng(seed)
+    return [(A.values + rng.uniform(-0.01, 0.01, A.nnz)).astype(np.float32) for _ in range(n)]
+
+
+def run_job(args, world, rank, local):
+    """stencil3d_job (default): the 128^3 27-point stencil's whole job.  A
+    step is C = A x A through the descriptor API in device memory space --
+    work_estimation + compute on the learned path (fused single pass, or the
+    plain two-pass path with --path plain) -- then JOB_REPEATS numeric-only
+    computes into the same C, each with A's values (B is A) perturbed by
+    U[-0.01, 0.01] (pre-drawn on the device, one array per repeat).  The
+    first numeric-only compute builds the reuse structures (map, term
+    tables, row tiles) inside the step.  value = (1 + JOB_REPEATS) products'
+    flops per step time.  Beside it, timed separately on the same inputs:
+    the plain and the learned full products alone, and the numeric-only
+    repeat alone (read from the job's own per-compute events).  With N ranks
+    the rows of A are cut into N panels of equal op count (each rank holds all
+    of B and runs the job on its panel): strong scaling."""
+    import torch
+    import rvsp
+    from rvsp import CSR, Descriptor, DeviceCSR, gen, intermediate_products
+    from rvsp import _lib as L
+    from rvsp.learn import RowModel, weights_for
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    torch.cuda.set_stream(torch.cuda.Stream(dev))
+    stream = torch.cuda.current_stream(dev)
+    pg = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=dev)
+        pg = dist
+    R = args.repeats
+    A = gen.stencil_3d_27(args.grid)
+    ops = intermediate_products(A, A)
+    flops_all = 2.0 * float(ops.sum())
+    r0, r1 = panel_rows(ops, world, rank)
+    p0, p1 = int(A.row_ptr[r0]), int(A.row_ptr[r1])
+    P = A if world == 1 else A.row_panel(r0, r1)
+    my_flops = 2.0 * float(ops[r0:r1].sum())
+    dA = DeviceCSR.from_host(A, dev)
+    dP = dA if world == 1 else DeviceCSR.from_host(P, dev)
+    gen_t = torch.Generator(device=dev)
+    gen_t.manual_seed(args.seed)
+    vals = [dA.values + (torch.rand(A.nnz, generator=gen_t, device=dev) * 0.02 - 0.01)
+            for _ in range(R)]
+    views_b = [DeviceCSR(A.rows, A.cols, dA.row_ptr, dA.col_idx, v) for v in vals]
+    views_p = views_b if world == 1 else [
+        DeviceCSR(P.rows, P.cols, dP.row_ptr, dP.col_idx, v[p0:p1]) for v in vals]
+    torch.cuda.synchronize(dev)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    model_file = weights_for("stencil3d")
+    model = RowModel(path=model_file)
+
+    def make_descr(algo, memory=L.MEM_DEVICE, **kw):
+        dd = Descriptor(algo=algo, memory=memory, **kw)
+        if algo == L.ALGO_CUDA_LEARNED:
+            dd.set_model(model)
+        return dd
+
+    algo = L.ALGO_CUDA_LEARNED if args.path == "learned" else L.ALGO_CUDA_PLAIN
+    d = make_descr(algo, stream=stream, profiling=True)
+    ws_bytes, c_nnz = d.work_estimation(dP, dA)
+    dC = DeviceCSR.empty(P.rows, A.cols, c_nnz, dev)
+    ws = torch.zeros(max(ws_bytes, 1), dtype=torch.uint8, device=dev)
+    alg_bytes = rvsp.algorithmic_bytes(P, A, c_nnz)
+
+    def job(ev=None):
+        d.work_estimation(dP, dA)
+        d.compute(dP, dA, dC, ws)
+        if ev is not None:
+            ev[0].record(stream)
+        for r in range(R):
+            d.compute(views_p[r], views_b[r], dC, ws)
+            if ev is not None:
+                ev[r + 1].record(stream)
+
+    sampler = ClockSampler(local)
+    sampler.start()
+    for _ in range(args.warmup):
+        flush.zero_()
+        job()
+    torch.cuda.synchronize(dev)
+    d.synchronize()
+    d.phase_times(reset=True)
+    if pg:
+        pg.barrier()
+    torch.cuda.synchronize(dev)
+    E = torch.cuda.Event
+    starts = [E(enable_timing=True) for _ in range(args.steps)]
+    evs = [[E(enable_timing=True) for _ in range(R + 1)] for _ in range(args.steps)]
+    for i in range(args.steps):
+        flush.zero_()
+        starts[i].record(stream)
+        job(evs[i])
+    torch.cuda.synchronize(dev)
+    d.synchronize()
+    if pg:
+        pg.barrier()
+    clocks = sampler.stop()
+    step_ms = [starts[i].elapsed_time(evs[i][R]) for i in range(args.steps)]
+    first_ms = [starts[i].elapsed_time(evs[i][0]) for i in range(args.steps)]
+    rep_ms = [[evs[i][r].elapsed_time(evs[i][r + 1]) for r in range(R)]
+              for i in range(args.steps)]
+    phases = d.phase_times(reset=True)
+    total_ms = float(sum(step_ms))
+    if pg:
+        t = torch.tensor([total_ms], device=dev)
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        total_ms = float(t.item())
+    ms_per_step = total_ms / args.steps
+    value = (1 + R) * flops_all * args.steps / (total_ms * 1e-3) / 1e9
+    steady = [x for row in rep_ms for x in row[1:]]
+    repeat_ms = float(np.median(steady)) if steady else float(np.mean([r[0] for r in rep_ms]))
+    prep_ms = float(np.mean([r[0] for r in rep_ms])) - repeat_ms
+    peak, peak_kind = measured_peaks()
+    peak_src = (f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured"
+                else "fallback 6.65 TB/s")
+    repeat_gbs = alg_bytes / (repeat_ms * 1e-3) / 1e9
+    tiled = d.tiled_rows()
+    overflow = d.overflow_rows()
+    per_step = {k: v[0] / args.steps for k, v in phases.items() if v[1]}
+    launches = int(sum(v[1] for v in phases.values()) / args.steps)
+    last_vals = vals[R - 1]
+
+    # The full products alone, plain and learned, on the unperturbed values.
+    def product_ms(pa, keep):
+        dd = make_descr(pa, stream=stream)
+        wsb, n = dd.work_estimation(dP, dA)
+        cc = DeviceCSR.empty(P.rows, A.cols, n, dev)
+        w = torch.zeros(max(wsb, 1), dtype=torch.uint8, device=dev)
+        for _ in range(args.warmup):
+            flush.zero_()
+            dd.work_estimation(dP, dA)
+            dd.compute(dP, dA, cc, w)
+        torch.cuda.synchronize(dev)
+        if pg:
+            pg.barrier()
+        es = [(E(enable_timing=True), E(enable_timing=True)) for _ in range(args.steps)]
+        for i in range(args.steps):
+            flush.zero_()
+            es[i][0].record(stream)
+            dd.work_estimation(dP, dA)
+            dd.compute(dP, dA, cc, w)
+            es[i][1].record(stream)
+        torch.cuda.synchronize(dev)
+        dd.synchronize()
+        ms = float(sum(a.elapsed_time(b) for a, b in es)) / args.steps
+        if pg:
+            t = torch.tensor([ms], device=dev)
+            pg.all_reduce(t, op=pg.ReduceOp.MAX)
+            ms = float(t.item())
+        host = cc.to_host(n) if keep else None
+        dd.close()
+        del cc
+        return ms, host
+    keep = rank == 0 and world == 1 and not args.no_cpu_baseline
+    plain_ms, plain_c = product_ms(L.ALGO_CUDA_PLAIN, keep)
+    learned_ms, learned_c = product_ms(L.ALGO_CUDA_LEARNED, keep)
+    job_c = dC.to_host(c_nnz) if keep else None
+    last_host = last_vals.cpu().numpy() if keep else None
+    d.close()
+
+    # End to end through the public C API in host memory space: pinned host
+    # operands, the job's first product and every repeat with host values
+    # (two pinned perturbed arrays, alternating), C copied back each compute.
+    e2e = None
+    if args.e2e_steps > 0:
+        def pinned(x):
+            return torch.from_numpy(np.ascontiguousarray(x)).pin_memory().numpy()
+        hA = CSR(A.rows, A.cols, pinned(A.row_ptr), pinned(A.col_idx), pinned(A.values))
+        hP = hA if world == 1 else CSR(P.rows, P.cols, pinned(P.row_ptr), pinned(P.col_idx),
+                                       pinned(P.values))
+        hv = [pinned(v) for v in job_value_sets_host(A, 2, args.seed + 1)]
+        hvb = [hA.with_values(v) for v in hv]
+        hvp = hvb if world == 1 else [hP.with_values(v[p0:p1]) for v in hv]
+        n = max(c_nnz, 1)
+        hC = CSR(P.rows, A.cols, pinned(np.zeros(P.rows + 1, np.int32)),
+                 pinned(np.zeros(n, np.int32)), pinned(np.zeros(n, np.float32)))
+        hws = np.zeros(256, np.uint8)
+        he = make_descr(algo, memory=L.MEM_HOST)
+
+        def e2e_step():
+            he.work_estimation(hP, hA)
+            he.compute(hP, hA, hC, hws)
+            for r in range(R):
+                he.compute(hvp[r % 2], hvb[r % 2], hC, hws)
+        e2e_step()
+        torch.cuda.synchronize(dev)
+        if pg:
+            pg.barrier()
+        t0 = time.perf_counter()
+        for _ in range(args.e2e_steps):
+            e2e_step()
+        torch.cuda.synchronize(dev)
+        el = time.perf_counter() - t0
+        if pg:
+            t = torch.tensor([el], device=dev)
+            pg.all_reduce(t, op=pg.ReduceOp.MAX)
+            el = float(t.item())
+        h2d = P.nbytes() + (0 if world == 1 else A.nbytes()) + R * (
+            P.values.nbytes + (0 if world == 1 else A.values.nbytes))
+        d2h = (4 * (P.rows + 1) + 8 * c_nnz) + R * (4 * (P.rows + 1) + 4 * c_nnz)
+        e2e = {"value": (1 + R) * flops_all * args.e2e_steps / el / 1e9, "unit": UNIT,
+               "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+               "steps": args.e2e_steps,
+               "api": "rvsp_spgemm_work_estimation + rvsp_spgemm_compute, then "
+                      f"{R} numeric-only rvsp_spgemm_compute, host memory space"}
+        he.close()
+        del hA, hP, hv, hvb, hvp, hC
+
+    cpu, checks = None, None
+    if keep:
+        sys.path.insert(0, str(ROOT))
+        from oracle import oracle
+        threads = os.cpu_count() or 1
+        sets = job_value_sets_host(A, 2, args.seed + 2)
+        cpu_sets = [(sets[r % 2], sets[r % 2]) for r in range(JOB_CPU_REPEATS)]
+        el = oracle.time_reference_job(A, A, cpu_sets, threads)
+        kind = "reference" if oracle.ref_available() else "port"
+        cpu = {"value": (1 + JOB_CPU_REPEATS) * flops_all / el / 1e9, "unit": UNIT,
+               "cores": threads, "kind": kind,
+               "sample": f"the job with {JOB_CPU_REPEATS} of its {R} numeric-only repeats "
+                         f"(first product + {JOB_CPU_REPEATS} repeats, two perturbed value "
+                         f"sets alternating), rows of A cut into {threads} panels, one per "
+                         f"thread, in {el:.1f} s"}
+        # Bit-exact checks of every measured path against the reference
+        # library's descriptor: its first compute (unperturbed values) for the
+        # plain and learned products, and a numeric-only compute with the last
+        # repeat's values for the job's C.
+        if oracle.ref_available():
+            st, rp, ci, first, last = oracle.ref_job(A, A, [(last_host, last_host)])
+        else:
+            rp, ci, first, _ = oracle.spgemm(A, A)
+            last = oracle.numeric_f32(A.with_values(last_host), A.with_values(last_host),
+                                      rp, ci)
+            st = 0
+        checks = {}
+        for name, got, want in (("plain", plain_c, first), ("learned", learned_c, first),
+                                ("job", job_c, last)):
+            checks[name] = bool(st == 0 and same_csr(got, rp, ci, want))
+        cpu["check"] = {"bit_exact": all(checks.values()),
+                        "mismatched": sum(not v for v in checks.values()),
+                        "paths": checks,
+                        "against": f"{kind}: descriptor first compute (plain, learned) and a "
+                                   "numeric-only compute with the last repeat's values (job)"}
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
+            "higher_is_better": True, "scaling": "strong" if world > 1 else "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "stencil3d_job", "description": WORKLOADS["stencil3d_job"],
+                       "path": args.path, "model": model_file.name, "grid": args.grid,
+                       "rows": A.rows, "nnz_a": A.nnz, "nnz_c": int(c_nnz) if world == 1 else None,
+                       "products": int(ops.sum()), "repeats": R, "seed": args.seed,
+                       "flops_per_product": flops_all,
+                       "algorithmic_bytes_per_product": rvsp.algorithmic_bytes(A, A, c_nnz)
+                       if world == 1 else None,
+                       "l2": "flushed between steps (256 MiB write outside the step events); "
+                             "every repeat reads its own 223 MB value array",
+                       "parallelism": f"row panels over {world} GPUs" if world > 1
+                       else "single GPU",
+                       "overflow_rows": overflow, "tiled_rows": tiled},
+            "hbm_frac": (1 + R) * alg_bytes / (ms_per_step * 1e-3) / 1e9 / peak,
+            "job": {"first_product_ms": float(np.mean(first_ms)),
+                    "reuse_prep_ms": prep_ms, "repeat_ms": repeat_ms,
+                    "repeat_gflops": my_flops / (repeat_ms * 1e-3) / 1e9,
+                    "repeat_hbm_frac": repeat_gbs / peak},
+            "plain": {"product_ms": plain_ms,
+                      "gflops": flops_all / (plain_ms * 1e-3) / 1e9},
+            "learned": {"product_ms": learned_ms,
+                        "gflops": flops_all / (learned_ms * 1e-3) / 1e9},
+            "learned_vs_plain": plain_ms / learned_ms,
+            "job_vs_plain_job": ((plain_ms + prep_ms + R * repeat_ms) /
+                                 (float(np.mean(first_ms)) + prep_ms + R * repeat_ms)),
+            "phase_ms_per_step": per_step,
+            "roofline": {"bound": "hbm",
+                         "kernel": "numeric-only repeat (tile_numeric_kernel, with "
+                                   "pat_numeric_kernel and map_numeric for the rows no tile "
+                                   "takes)",
+                         "achieved": repeat_gbs, "peak": peak, "unit": "GB/s",
+                         "frac": repeat_gbs / peak, "peak_source": peak_src,
+                         "traffic": committed_traffic("stencil3d_job", "repeat"),
+                         "traffic_source": "committed: profiles/traffic.json (ncu capture "
+                                           "named there), not measured in this run",
+                         "algorithmic_bytes_per_launch": alg_bytes},
+            "clocks": clocks, "e2e": e2e, "gpu_launches": launches,
+            "cpu_baseline": cpu,
+            "correct": cpu["check"]["bit_exact"] if cpu else None,
+        }
+        print(json.dumps(line), flush=True)
+    if pg:
+        pg.barrier()
+        pg.destroy_process_group()
+    return 0
+
+
 def same_csr(got, rp, ci, cv) -> bool:
     """Bit-identical structure and values (values compared as bit patterns)."""
     return (np.array_equal(got.row_ptr, rp) and np.array_equal(got.col_idx, ci)
@@ -956,6 +1303,19 @@ def reference_check(items, what: str) -> dict:
             "against": f"{'reference' if ref else 'port'}: {what}"}
 
 
+def launch_ranks(n: int) -> int:
+    """--gpus N without a launcher: run this same command as N ranks (one per
+    GPU) under torch.distributed.run on 127.0.0.1, and return its status."""
+    import socket
+    with socket.socket() as sk:
+        sk.bind(("127.0.0.1", 0))
+        port = sk.getsockname()[1]
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1",
+           f"--nproc-per-node={n}", "--master-addr=127.0.0.1", f"--master-port={port}",
+           str(Path(__file__).resolve())] + sys.argv[1:]
+    return subprocess.call(cmd)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -964,15 +1324,21 @@ def main():
                          "uniform4096 steps, so the timed region lasts long enough for the "
                          "clock samples; 40 otherwise; 3 for --impl reference)")
     ap.add_argument("--warmup", type=int, default=5)
-    ap.add_argument("--workload", default="laplace2d", choices=sorted(WORKLOADS))
+    ap.add_argument("--workload", default="stencil3d_job", choices=sorted(WORKLOADS))
     ap.add_argument("--impl", default="ours", choices=("ours", "reference"))
-    ap.add_argument("--path", default="plain", choices=("plain", "learned"),
-                    help="plain GPU Gustavson, or the learned (MLP-binned, fused) path")
+    ap.add_argument("--path", default=None, choices=("plain", "learned"),
+                    help="plain GPU Gustavson, or the learned (MLP-binned, fused) path "
+                         "(default: learned for stencil3d_job, plain otherwise)")
+    ap.add_argument("--repeats", type=int, default=JOB_REPEATS,
+                    help="stencil3d_job: numeric-only repeats per job")
+    ap.add_argument("--seed", type=int, default=11,
+                    help="stencil3d_job: seed of the value perturbations")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--grid", type=int, default=128,
                     help="stencil workloads: grid edge (128 is the benchmark; smaller "
                          "grids are for profiler captures)")
-    ap.add_argument("--e2e-steps", type=int, default=10)
+    ap.add_argument("--e2e-steps", type=int, default=None,
+                    help="end-to-end steps (default 2 for stencil3d_job, 10 otherwise)")
     ap.add_argument("--dtype", default="f32", choices=("f32", "f64", "i8"),
                     help="f64 / i8: the FP64 or INT8->INT32 one-shot product of the "
                          "workload's matrices (host arrays in and out)")
@@ -980,9 +1346,18 @@ def main():
     if args.steps is None:
         if args.impl == "reference":
             args.steps = 3  # each step is seconds of CPU work
+        elif args.workload == "stencil3d_job":
+            args.steps = 10
         else:
             args.steps = 1500 if args.workload in ("laplace2d", "uniform4096") else 40
+    if args.path is None:
+        args.path = "learned" if args.workload == "stencil3d_job" else "plain"
+    if args.e2e_steps is None:
+        args.e2e_steps = 2 if args.workload == "stencil3d_job" else 10
+    args.repeats = max(args.repeats, 1)
     args.warmup = max(args.warmup, 3)
+    if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
+        return launch_ranks(args.gpus)
     world, rank, local = dist_setup()
 
     if args.impl == "reference" and args.workload == "mtx_ingest":
@@ -1010,6 +1385,8 @@ def main():
         return run_batch(args, world, rank, local)
     if args.workload == "rmat20_panels":
         return run_panels(args, world, rank, local)
+    if args.workload == "stencil3d_job":
+        return run_job(args, world, rank, local)
 
     import torch
     import rvsp

@@ -201,6 +201,14 @@ rvsp_status_t rvsp_spgemm_set_capacity_scale(rvsp_spgemm_descr_t descr, float sc
  * eligible.  Refused after work_estimation. */
 rvsp_status_t rvsp_spgemm_set_merge_policy(rvsp_spgemm_descr_t descr, int32_t policy);
 
+/* Row tiles for numeric-only computes (see rvsp_cuda_plan_set_row_tiles):
+ * 1 (default) or 0.  Values are identical either way; allowed at any time. */
+rvsp_status_t rvsp_spgemm_set_row_tiles(rvsp_spgemm_descr_t descr, int32_t enable);
+
+/* Rows the row tiles compute in numeric-only computes (after the first
+ * numeric-only compute on the current structure; 0 before). */
+rvsp_status_t rvsp_spgemm_get_tiled_rows(rvsp_spgemm_descr_t descr, int32_t *n_out);
+
 /* Rows the last learned work_estimation redid with the plain path. */
 rvsp_status_t rvsp_spgemm_get_overflow_rows(rvsp_spgemm_descr_t descr, int32_t *n_out);
 

@@ -208,6 +208,19 @@ int32_t rvsp_cuda_plan_overflow_rows(rvsp_cuda_plan_t plan);
  * and 2 to time both accumulators on the same rows. */
 rvsp_status_t rvsp_cuda_plan_set_merge_policy(rvsp_cuda_plan_t plan, int32_t policy);
 
+/* Row tiles for numeric-only repeats (1, the default) or not (0).  The GPU
+ * form of the reference's numeric-only compute (spgemm_descr.c:330-349) for
+ * runs of consecutive rows that share one term pattern: a warp computes 32
+ * such rows at once, one per lane (k_tile.cu).  0 keeps every such row on the
+ * warp-per-row table kernel; the values are the same either way.  Enabling
+ * after the reuse structures were built without tiles rebuilds them on the
+ * next numeric-only call. */
+rvsp_status_t rvsp_cuda_plan_set_row_tiles(rvsp_cuda_plan_t plan, int32_t enable);
+
+/* Rows the row tiles of the current reuse structures compute (0 when there
+ * are none or tiles are off). */
+int32_t rvsp_cuda_plan_tiled_rows(rvsp_cuda_plan_t plan);
+
 /* Size of the library's fixed device scratch for rvsp_cuda_numeric_noalloc,
  * and the widest B it accepts (one float accumulator per B column). */
 #define RVSP_NOALLOC_SCRATCH_BYTES (16u << 20)
@@ -217,21 +230,27 @@ rvsp_status_t rvsp_cuda_plan_set_merge_policy(rvsp_cuda_plan_t plan, int32_t pol
  * CPU scalar backend takes a caller-allocated workspace, and every other
  * numeric entry point here takes a caller-allocated device workspace.  This
  * one is for callers that cannot call cudaMalloc when they need C's values:
- * code running under CUDA graph capture, memory pools that forbid re-entrant
- * allocation, and latency-bound loops that must not take allocation locks.
+ * memory pools and allocators that forbid re-entrant allocation from inside
+ * their own callbacks, and latency-bound loops that must not take the
+ * driver's allocation locks.
  *
  * Computes c_values for a structure (c_row_ptr, c_col_idx) that a symbolic
- * pass already produced for this sparsity pattern; all pointers are device
- * pointers, the caller passes every input and output.  Values are
- * bit-identical to rvsp_cuda_numeric's.  Scratch is a fixed 16 MiB device
- * array inside the library (held by every GPU that loads it until the
- * process exits).  The first call on each device, with that device current,
- * looks that array's address up; make it before any stream capture.  Each
- * call clears the scratch it uses and is asynchronous on `stream`.  All calls
- * share the one array: calls that overlap on the GPU (different streams or
- * host threads) race, so serialise them.  b_cols > RVSP_NOALLOC_MAX_B_COLS
- * (4,194,304) is rejected with RVSP_ERROR_INVALID_ARGUMENT before any device
- * work; NULL pointers give RVSP_ERROR_NULL_POINTER. */
+ * pass already produced for exactly this A and B; all pointers are device
+ * pointers, the caller passes every input and output.  A and B must be
+ * canonical CSR (as rvsp_cuda_csr_check accepts): column indices are
+ * range-checked and skipped when out of range, row pointers are not, and a
+ * B row that repeats a column races.  Values are bit-identical to
+ * rvsp_cuda_numeric's.  Scratch is a fixed 16 MiB device array inside the
+ * library (held by every GPU that loads it until the process exits).  The
+ * first call on each device, with that device current, looks that array's
+ * address up; make it before any stream capture.  Each call clears the
+ * scratch it uses and is asynchronous on `stream`.  All calls share the one
+ * array: calls that overlap on the GPU (different streams or host threads)
+ * race, so serialise them.  a_rows == 0 or b_cols == 0 (an empty product)
+ * returns RVSP_SUCCESS with no device work; a negative size, or
+ * b_cols > RVSP_NOALLOC_MAX_B_COLS (4,194,304), is rejected with
+ * RVSP_ERROR_INVALID_ARGUMENT before any device work; NULL pointers give
+ * RVSP_ERROR_NULL_POINTER. */
 rvsp_status_t rvsp_cuda_numeric_noalloc(void *stream, int32_t a_rows,
                                         int32_t b_rows, int32_t b_cols,
                                         const int32_t *a_row_ptr,

@@ -390,6 +390,89 @@ def time_reference_batch(products, seconds: float = 10.0, threads: int = 1):
     return sorted(done), time.perf_counter() - t0
 
 
+def ref_job(A, B, value_sets=(), keep_first=True, keep_all=False):
+    """The reference descriptor's job (spgemm_descr.c:66-380):
+    work_estimation(A, B), compute into a caller-owned C (fill + numeric),
+    then one numeric-only compute per (a_values, b_values) in value_sets into
+    the same C.  Returns (status, row_ptr, col_idx, values after the first
+    compute or None, values after the last compute); with keep_all the last
+    item is the list of the values after every numeric-only compute."""
+    lib = ref()
+    keep = []
+    a, b = _ref_struct(A, keep), _ref_struct(B, keep)
+    d = C.c_void_p()
+    assert lib.rvsp_spgemm_descr_create(C.byref(d)) == 0
+    try:
+        ws_b, nnz = C.c_size_t(), C.c_int32()
+        st = lib.rvsp_spgemm_work_estimation(d, C.byref(a), C.byref(b), C.byref(ws_b),
+                                             C.byref(nnz))
+        if st != 0:
+            return st, None, None, None, None
+        n = nnz.value
+        rp = np.zeros(A.rows + 1, np.int32)
+        ci = np.zeros(max(n, 1), np.int32)
+        cv = np.zeros(max(n, 1), np.float32)
+        ws = np.zeros(max(int(ws_b.value), 1), np.uint8)
+        c = _RefCsr()
+        c.rows, c.cols, c.nnz = A.rows, B.cols, n
+        c.row_ptr, c.col_idx, c.values = rp.ctypes.data, ci.ctypes.data, cv.ctypes.data
+        c.dtype, c.format, c.owns_data = 3, 0, 0
+        st = lib.rvsp_spgemm_compute(d, C.byref(a), C.byref(b), C.byref(c), ws.ctypes.data)
+        if st != 0:
+            return st, None, None, None, None
+        first = cv[:n].copy() if keep_first else None
+        every = []
+        for av, bv in value_sets:
+            av = np.ascontiguousarray(av, np.float32)
+            bv = np.ascontiguousarray(bv, np.float32)
+            keep += [av, bv]
+            a.values, b.values = av.ctypes.data, bv.ctypes.data
+            st = lib.rvsp_spgemm_compute(d, C.byref(a), C.byref(b), C.byref(c),
+                                         ws.ctypes.data)
+            if st != 0:
+                return st, None, None, None, None
+            if keep_all:
+                every.append(cv[:n].copy())
+        return 0, rp, ci[:n], first, (every if keep_all else cv[:n])
+    finally:
+        lib.rvsp_spgemm_descr_destroy(d)
+
+
+def time_reference_job(A, B, value_sets, threads: int):
+    """The reference's descriptor job on host cores, the rows of A shared out
+    as `threads` row panels (each panel times B is a product of its own; the
+    panels together are the whole product): each thread runs
+    work_estimation + compute + one numeric-only compute per entry of
+    value_sets ((A values, B values) of the whole matrices) on its panel.
+    Returns elapsed seconds (all threads)."""
+    import threading
+    use_ref = ref_available()
+    bounds = np.linspace(0, A.rows, threads + 1).astype(int)
+
+    def worker(t):
+        r0, r1 = int(bounds[t]), int(bounds[t + 1])
+        if r1 <= r0:
+            return
+        P = A.row_panel(r0, r1)
+        p0, p1 = int(A.row_ptr[r0]), int(A.row_ptr[r1])
+        sets = [(av[p0:p1], bv) for av, bv in value_sets]
+        if use_ref:
+            ref_job(P, B, sets, keep_first=False)
+        else:
+            rp, ci, _ = symbolic(P, B)
+            numeric_f32(P, B, rp, ci)
+            for av, bv in sets:
+                numeric_f32(P.with_values(av), B.with_values(bv), rp, ci)
+
+    t0 = time.perf_counter()
+    ths = [threading.Thread(target=worker, args=(t,)) for t in range(threads)]
+    for th in ths:
+        th.start()
+    for th in ths:
+        th.join()
+    return time.perf_counter() - t0
+
+
 # ---- FP64 and INT8 -> INT32 products (legacy scalar kernels) ----------------
 
 _TYPED = {"f64": (np.float64, np.float64, 4, 4), "i8": (np.int8, np.int32, 0, 1)}

@@ -2,22 +2,22 @@
 // allocate device memory.
 //
 // Who needs it.  Some callers may not call cudaMalloc at the moment they want
-// values computed: code running while a CUDA graph is being captured (where a
-// cudaMalloc/cudaFree would break or serialise the capture), allocators and
-// memory pools that forbid re-entrant allocation from inside their own
-// callbacks, and real-time loops that must not take the driver's allocation
-// locks.  Every other numeric entry point here needs a caller-provided device
-// workspace for its dense accumulators; this one needs none.
+// values computed: memory pools and allocators that forbid re-entrant
+// allocation from inside their own callbacks, and real-time loops that must
+// not take the driver's allocation locks.  Every other numeric entry point
+// here needs a caller-provided device workspace for its dense accumulators;
+// this one needs none.
 //
 // How.  The dense accumulators live in one file-scope device array of
 // kScratchBytes (16 MiB), which every GPU that loads the library keeps until
 // the process exits.  Host code cannot use the array's name as a device
 // address, so the first call on each device (with that device current) looks
 // the address up with cudaGetSymbolAddress and caches it; make that first
-// call before any stream capture begins.  Each call then clears the part of
-// the array it uses (cudaMemsetAsync, no allocation) and launches one kernel.
-// All calls share the array: calls whose kernels overlap on the GPU (other
-// streams, other host threads) race and must be serialised by the caller.
+// call before any stream capture begins.  Each call then
+// clears the part of the array it uses (cudaMemsetAsync, no allocation) and
+// launches one kernel.  All calls share the array: calls whose kernels
+// overlap on the GPU (other streams, other host threads) race and must be
+// serialised by the caller.
 //
 // What it computes.  C's values for a structure (c_row_ptr, c_col_idx)
 // already produced by the symbolic pass for this sparsity pattern, with the
@@ -80,9 +80,12 @@ rvsp_status_t scratch_of_current_device(float **ptr, int *sms) {
   return RVSP_SUCCESS;
 }
 
-// One block per row (grid-stride).  Indices outside B's shape are skipped,
-// never dereferenced, so a malformed structure cannot reach past the arrays
-// named by the shapes.
+// One block per row (grid-stride).  Column indices are range-checked (A's
+// against b_rows, B's and C's against b_cols) and an out-of-range one is
+// skipped; row pointers are not checked, so the operands must be canonical
+// CSR (as rvsp_cuda_csr_check accepts).  After each row the block zeroes
+// every accumulator its B rows touched, so a C structure that misses a
+// column of the product leaves only that entry wrong.
 __global__ void __launch_bounds__(kThreads)
 noalloc_numeric_kernel(rvsp::Operands op, int32_t b_rows,
                        const int32_t *__restrict__ c_rp,
@@ -118,15 +121,22 @@ noalloc_numeric_kernel(rvsp::Operands op, int32_t b_rows,
         __syncthreads();
       }
     }
-    // Drain in C's column order and leave the accumulator zeroed.
+    // Drain in C's column order.
     for (int32_t e = c_rp[row] + threadIdx.x; e < c_rp[row + 1]; e += blockDim.x) {
       const int32_t col = __ldg(c_col + e);
-      float v = 0.0f;
-      if (static_cast<uint32_t>(col) < static_cast<uint32_t>(op.b_cols)) {
-        v = acc[col];
-        acc[col] = 0.0f;
+      c_val[e] = static_cast<uint32_t>(col) < static_cast<uint32_t>(op.b_cols) ? acc[col]
+                                                                            : 0.0f;
+    }
+    __syncthreads();
+    // Leave the accumulator zeroed at every column this row touched.
+    for (int32_t p = p0; p < p1; ++p) {
+      const int32_t k = __ldg(op.a_col + p);
+      if (static_cast<uint32_t>(k) >= static_cast<uint32_t>(b_rows)) continue;
+      const int32_t bbeg = __ldg(op.b_rp + k), len = __ldg(op.b_rp + k + 1) - bbeg;
+      for (int32_t e = threadIdx.x; e < len; e += blockDim.x) {
+        const int32_t col = __ldg(op.b_col + bbeg + e);
+        if (static_cast<uint32_t>(col) < static_cast<uint32_t>(op.b_cols)) acc[col] = 0.0f;
       }
-      c_val[e] = v;
     }
     __syncthreads();
   }
@@ -142,7 +152,9 @@ extern "C" rvsp_status_t rvsp_cuda_numeric_noalloc(
   if (!a_row_ptr || !a_col_idx || !a_values || !b_row_ptr || !b_col_idx ||
       !b_values || !c_row_ptr || !c_col_idx || !c_values)
     return RVSP_ERROR_NULL_POINTER;
-  if (a_rows <= 0 || b_rows <= 0 || b_cols <= 0) return RVSP_ERROR_INVALID_ARGUMENT;
+  if (a_rows < 0 || b_rows < 0 || b_cols < 0) return RVSP_ERROR_INVALID_ARGUMENT;
+  // An empty product (no rows of A, or no columns of B) has no values.
+  if (a_rows == 0 || b_cols == 0) return RVSP_SUCCESS;
   // One accumulator of b_cols floats must fit the fixed scratch.
   if (static_cast<size_t>(b_cols) > RVSP_NOALLOC_MAX_B_COLS)
     return RVSP_ERROR_INVALID_ARGUMENT;

@@ -207,8 +207,9 @@ pat_build_kernel(const int32_t *__restrict__ pat_canon, const int32_t *__restric
 // Splits one class's rows: a row whose canonical row has a table, and whose
 // own A row has the canonical's length and B row lengths (the records name
 // A nonzeros and B entries, not just positions), goes to the table list
-// (pat_rows, pat_ids; count at *pat_n); the rest to res_rows (count
-// *res_n), which keep the map path.
+// (pat_rows, pat_ids; count at *pat_n, and pid_of_row[row] = id when
+// pid_of_row is given); the rest to res_rows (count *res_n), which keep the
+// map path.
 __global__ void __launch_bounds__(256)
 pat_split_kernel(const int32_t *__restrict__ rows, int32_t nrows,
                  const int32_t *__restrict__ canon, const int32_t *__restrict__ pat_of,
@@ -216,7 +217,7 @@ pat_split_kernel(const int32_t *__restrict__ rows, int32_t nrows,
                  const int32_t *__restrict__ a_col, const int32_t *__restrict__ b_rp,
                  int32_t *__restrict__ pat_rows, int32_t *__restrict__ pat_ids,
                  int32_t *__restrict__ pat_n, int32_t *__restrict__ res_rows,
-                 int32_t *__restrict__ res_n) {
+                 int32_t *__restrict__ res_n, int32_t *__restrict__ pid_of_row) {
   const int32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   const int lane = lane_id();
   const bool valid = i < nrows;
@@ -253,6 +254,7 @@ pat_split_kernel(const int32_t *__restrict__ rows, int32_t nrows,
       const int32_t at = base + __popc(to_pat & below);
       pat_rows[at] = row;
       pat_ids[at] = pid;
+      if (pid_of_row) pid_of_row[row] = pid;
     }
   }
   if (to_res) {
@@ -351,11 +353,11 @@ void launch_pat_split(const int32_t *rows, int32_t nrows, const int32_t *canon,
                       const int32_t *pat_of, const int32_t *psteps, const int32_t *a_rp,
                       const int32_t *a_col, const int32_t *b_rp, int32_t *pat_rows,
                       int32_t *pat_ids, int32_t *pat_n, int32_t *res_rows, int32_t *res_n,
-                      cudaStream_t s) {
+                      int32_t *pid_of_row, cudaStream_t s) {
   if (nrows <= 0) return;
   pat_split_kernel<<<(nrows + 255) / 256, 256, 0, s>>>(rows, nrows, canon, pat_of, psteps,
                                                         a_rp, a_col, b_rp, pat_rows, pat_ids,
-                                                        pat_n, res_rows, res_n);
+                                                        pat_n, res_rows, res_n, pid_of_row);
 }
 
 void launch_pat_numeric(const Operands &op, const int64_t *ops, const int32_t *pat_rows,

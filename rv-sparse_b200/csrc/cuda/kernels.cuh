@@ -285,18 +285,50 @@ void launch_pat_build(int32_t npat, const int32_t *pat_canon, const int32_t *a_r
                       const int32_t *pat_cap, uint32_t *rec, int32_t *psteps,
                       cudaStream_t s);
 // Split a class's rows into table rows (pat_rows / pat_ids, appended at
-// *pat_n) and the rest (res_rows, appended at *res_n).
+// *pat_n; pid_of_row[row] = id when pid_of_row is not null) and the rest
+// (res_rows, appended at *res_n).
 void launch_pat_split(const int32_t *rows, int32_t nrows, const int32_t *canon,
                       const int32_t *pat_of, const int32_t *psteps, const int32_t *a_rp,
                       const int32_t *a_col, const int32_t *b_rp, int32_t *pat_rows,
                       int32_t *pat_ids, int32_t *pat_n, int32_t *res_rows, int32_t *res_n,
-                      cudaStream_t s);
+                      int32_t *pid_of_row, cudaStream_t s);
 // Values of the n table rows (structure in C); max_ops / max_out: the
 // maxima the select step found.
 void launch_pat_numeric(const Operands &op, const int64_t *ops, const int32_t *pat_rows,
                         const int32_t *pat_ids, int32_t n, const int32_t *c_rp, float *c_val,
                         const int64_t *pat_off, const int32_t *psteps, const uint32_t *rec,
                         int32_t max_ops, int32_t max_out, cudaStream_t s);
+
+// ---- k_tile.cu -------------------------------------------------------------
+// Row tiles of the table rows (see k_tile.cu).  Warps per block of the tile
+// kernel; uint16 entries per pattern in
+// the tile tables (tab has npat * tile_tab_stride() entries).
+constexpr int kTileKernelWarps = 2;
+int32_t tile_tab_stride();
+// Per pattern: its table, B row lengths (lens[id * 32 + j]) and desc[id] =
+// (na, m, ops, 0), or na = -1 when the pattern is not tiled.
+void launch_tile_tab(int32_t npat, const int32_t *pat_canon, const int32_t *psteps,
+                     const int32_t *a_rp, const int32_t *a_col, const int32_t *b_rp,
+                     const int32_t *c_rp, const int64_t *moff, const uint16_t *map,
+                     uint16_t *tab, uint16_t *lens, int4 *desc, cudaStream_t s);
+// Tiles of the n rows (pid_of_row: pattern of each table row, -1 for the
+// others): tiles[*ntiles] = (first row, lane mask, pattern, 0); the table rows
+// no tile takes go to lo_rows / lo_ids (count *lo_n).  maxima (3 words,
+// zeroed by the caller): stage floats, A segment entries and C row the tile
+// kernel must hold.
+void launch_tile_build(int32_t n, const int32_t *pid_of_row, const int4 *desc,
+                       const uint16_t *lens, const int32_t *a_rp, const int32_t *a_col,
+                       const int32_t *b_rp, const int32_t *c_rp, int4 *tiles, int32_t *ntiles,
+                       int32_t *lo_rows, int32_t *lo_ids, int32_t *lo_n, int32_t *maxima,
+                       cudaStream_t s);
+// Shared memory one warp of the tile kernel needs for those maxima.
+size_t tile_smem_per_warp(int32_t stage_need, int32_t a_seg, int32_t max_out,
+                          int32_t *acc_rows, int32_t *work_floats, int32_t *stage_cap);
+// Values of the tiled rows (structure in C).
+void launch_tile_numeric(const Operands &op, int32_t b_nnz, const int4 *tiles, int32_t ntiles,
+                         const int4 *desc, const uint16_t *lens, const uint16_t *tab,
+                         const int32_t *c_rp, float *c_val, int32_t stage_need, int32_t a_seg,
+                         int32_t max_out, cudaStream_t s);
 
 // ---- k_check.cu ------------------------------------------------------------
 // *result (initialised to ~0ull) receives min over bad rows of

@@ -157,6 +157,16 @@ struct rvsp_cuda_plan {
   int32_t pat_max_ops = 0, pat_max_out = 0;
   DevArray<int64_t> pat_off;
   DevArray<uint32_t> pat_rec;
+  // Row tiles of the table rows (k_tile.cu): per pattern its tile table,
+  // B row lengths and shape; per row its pattern; the tiles and the table
+  // rows left to the warp-per-row kernel (tile_lo_rows / tile_lo_ids).
+  int tiles_enabled = 1;
+  int tile_ready = 0;
+  int32_t n_tiles = 0, n_tile_lo = 0;
+  int32_t tile_stage = 0, tile_aseg = 0, tile_max_out = 0, tile_b_nnz = 0;
+  DevArray<uint16_t> tile_tab, tile_lens;
+  DevArray<int4> tile_desc, tiles;
+  DevArray<int32_t> tile_pid, tile_lo_rows, tile_lo_ids, tile_counts;
   const int32_t *rmap_col = nullptr;
   int rmap_state = 0;
   int64_t rmap_entries = 0;
@@ -362,6 +372,14 @@ void rvsp_cuda_plan_destroy(rvsp_cuda_plan_t p) {
   p->pat_counts.release();
   p->pat_off.release();
   p->pat_rec.release();
+  p->tile_tab.release();
+  p->tile_lens.release();
+  p->tile_desc.release();
+  p->tiles.release();
+  p->tile_pid.release();
+  p->tile_lo_rows.release();
+  p->tile_lo_ids.release();
+  p->tile_counts.release();
   p->ops.release();
   p->cls.release();
   p->cls_spec.release();
@@ -862,6 +880,23 @@ rvsp_status_t rvsp_cuda_plan_set_merge_policy(rvsp_cuda_plan_t p, int32_t policy
   return RVSP_SUCCESS;
 }
 
+rvsp_status_t rvsp_cuda_plan_set_row_tiles(rvsp_cuda_plan_t p, int32_t enable) {
+  if (!p) return RVSP_ERROR_NULL_POINTER;
+  if (enable != 0 && enable != 1) return RVSP_ERROR_INVALID_ARGUMENT;
+  if (enable && !p->tiles_enabled) {
+    // tiles were never built for the current reuse map: build it again
+    p->rmap_state = 0;
+    p->rmap_col = nullptr;
+  }
+  p->tiles_enabled = enable;
+  return RVSP_SUCCESS;
+}
+
+int32_t rvsp_cuda_plan_tiled_rows(rvsp_cuda_plan_t p) {
+  if (!p || !p->tile_ready || !p->tiles_enabled) return 0;
+  return p->n_pat_rows - p->n_tile_lo;
+}
+
 int32_t rvsp_cuda_plan_overflow_rows(rvsp_cuda_plan_t p) {
   return (p && p->analysed && p->learned) ? p->n_ovf : 0;
 }
@@ -875,6 +910,58 @@ namespace {
 // The reuse map may take at most this much device memory (and a quarter of
 // what is free).
 constexpr size_t kReuseMapMaxBytes = size_t(24) << 30;
+
+// The tile tables may take at most this much device memory.
+constexpr size_t kTileTablesMaxBytes = size_t(256) << 20;
+constexpr int kTileCountWords = 8;  // ntiles, leftovers, 3 maxima, spare
+
+// Row tiles of the table rows (k_tile.cu): the per-pattern tile tables, then
+// tiles over chunks of 32 consecutive rows and the leftover list.  Leaves
+// tile_ready 0 (every table row on the warp-per-row kernel) when nothing is
+// tiled or the tile kernel's shared memory would not fit.  Synchronizes `s`.
+cudaError_t build_row_tiles(rvsp_cuda_plan *p, cudaStream_t s, const Operands &op,
+                            const int32_t *c_rp, int32_t npat) {
+  const size_t n = static_cast<size_t>(p->a_rows);
+  const size_t tab_entries = size_t(npat) * size_t(tile_tab_stride());
+  if (p->tile_tab.reserve(tab_entries) != cudaSuccess ||
+      p->tile_lens.reserve(size_t(npat) * 32) != cudaSuccess ||
+      p->tile_desc.reserve(size_t(npat)) != cudaSuccess ||
+      p->tiles.reserve((n + 31) / 32) != cudaSuccess ||
+      p->tile_lo_rows.reserve(n) != cudaSuccess || p->tile_lo_ids.reserve(n) != cudaSuccess ||
+      p->tile_counts.reserve(kTileCountWords) != cudaSuccess) {
+    cudaGetLastError();
+    return cudaSuccess;
+  }
+  int32_t b_nnz = 0;
+  cudaError_t e = cudaMemcpyAsync(&b_nnz, op.b_rp + p->b_rows, sizeof(int32_t),
+                                  cudaMemcpyDeviceToHost, s);
+  if (e != cudaSuccess) return e;
+  cudaMemsetAsync(p->tile_counts.p, 0, kTileCountWords * sizeof(int32_t), s);
+  launch_tile_tab(npat, p->pat_canon.p, p->pat_steps.p, op.a_rp, op.a_col, op.b_rp, c_rp,
+                  p->rmap_off.p, p->rmap.p, p->tile_tab.p, p->tile_lens.p, p->tile_desc.p, s);
+  launch_tile_build(p->a_rows, p->tile_pid.p, p->tile_desc.p, p->tile_lens.p, op.a_rp,
+                    op.a_col, op.b_rp, c_rp, p->tiles.p, p->tile_counts.p,
+                    p->tile_lo_rows.p, p->tile_lo_ids.p, p->tile_counts.p + 1,
+                    p->tile_counts.p + 2, s);
+  int32_t h[kTileCountWords] = {};
+  e = cudaMemcpyAsync(h, p->tile_counts.p, sizeof(h), cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) return e;
+  if (h[0] <= 0) return cudaSuccess;
+  int32_t acc_rows = 0, work = 0, stage_cap = 0;
+  const size_t per_warp = tile_smem_per_warp(h[2], h[3], h[4], &acc_rows, &work, &stage_cap);
+  int dev_max = 0;
+  cudaDeviceGetAttribute(&dev_max, cudaDevAttrMaxSharedMemoryPerBlockOptin, p->device);
+  if (per_warp * kTileKernelWarps > size_t(dev_max)) return cudaSuccess;
+  p->n_tiles = h[0];
+  p->n_tile_lo = h[1];
+  p->tile_stage = h[2];
+  p->tile_aseg = h[3];
+  p->tile_max_out = h[4];
+  p->tile_b_nnz = b_nnz;
+  p->tile_ready = 1;
+  return cudaSuccess;
+}
 
 // Builds the reuse map of the W<T> rows for the structure in c_col (written
 // by an earlier fill).  Leaves rmap_state -1 when the map does not apply:
@@ -932,6 +1019,13 @@ cudaError_t build_term_tables(rvsp_cuda_plan *p, cudaStream_t s, const Operands 
   }
   launch_pat_build(npat, p->pat_canon.p, op.a_rp, op.a_col, op.b_rp, c_rp, p->rmap_off.p,
                    p->rmap.p, p->pat_off.p, p->pat_cap.p, p->pat_rec.p, p->pat_steps.p, s);
+  // per-row pattern ids for the row tiles (skipped when they do not fit)
+  const size_t tab_entries = size_t(npat) * size_t(tile_tab_stride());
+  const bool tiles_fit = p->tiles_enabled &&
+                         tab_entries * sizeof(uint16_t) <= kTileTablesMaxBytes &&
+                         p->tile_pid.reserve(n) == cudaSuccess;
+  if (!tiles_fit) cudaGetLastError();
+  if (tiles_fit) cudaMemsetAsync(p->tile_pid.p, 0xff, n * sizeof(int32_t), s);
   int32_t off = 0;
   for (int c = kEmpty_ + 1; c < kNumClasses; ++c) {
     p->res_off[c] = off;
@@ -941,7 +1035,7 @@ cudaError_t build_term_tables(rvsp_cuda_plan *p, cudaStream_t s, const Operands 
                      whole ? p->a_rows : p->num_count[c], p->rmap_canon.p, p->pat_of.p,
                      p->pat_steps.p, op.a_rp, op.a_col, op.b_rp, p->pat_rows.p,
                      p->pat_ids.p, p->pat_counts.p + 1, p->res_rows.p + off,
-                     p->pat_counts.p + 2 + c, s);
+                     p->pat_counts.p + 2 + c, tiles_fit ? p->tile_pid.p : nullptr, s);
     off += whole ? p->a_rows : p->num_count[c];
   }
   int32_t h[kPatCountWords] = {};
@@ -954,6 +1048,11 @@ cudaError_t build_term_tables(rvsp_cuda_plan *p, cudaStream_t s, const Operands 
   p->pat_max_ops = h[2 + kNumClasses];
   p->pat_max_out = h[3 + kNumClasses];
   p->pat_ready = 1;
+  p->tile_ready = 0;
+  if (tiles_fit && p->n_pat_rows > 0) {
+    e = build_row_tiles(p, s, op, c_rp, npat);
+    if (e != cudaSuccess) return e;
+  }
   return cudaSuccess;
 }
 
@@ -1151,10 +1250,23 @@ rvsp_status_t rvsp_cuda_numeric(rvsp_cuda_plan_t p, void *stream,
   {
     PhaseScope ph(p, s, RVSP_PHASE_NUMERIC);
     if (use_map && p->pat_ready && p->n_pat_rows > 0) {
-      launch_pat_numeric(op, p->ops.p, p->pat_rows.p, p->pat_ids.p, p->n_pat_rows,
-                         c_row_ptr, c_values, p->pat_off.p, p->pat_steps.p, p->pat_rec.p,
-                         p->pat_max_ops, p->pat_max_out, s);
-      ph.launches += 1;
+      if (p->tile_ready && p->tiles_enabled) {
+        launch_tile_numeric(op, p->tile_b_nnz, p->tiles.p, p->n_tiles, p->tile_desc.p,
+                            p->tile_lens.p, p->tile_tab.p, c_row_ptr, c_values, p->tile_stage,
+                            p->tile_aseg, p->tile_max_out, s);
+        ph.launches += 1;
+        if (p->n_tile_lo > 0) {
+          launch_pat_numeric(op, p->ops.p, p->tile_lo_rows.p, p->tile_lo_ids.p, p->n_tile_lo,
+                             c_row_ptr, c_values, p->pat_off.p, p->pat_steps.p, p->pat_rec.p,
+                             p->pat_max_ops, p->pat_max_out, s);
+          ph.launches += 1;
+        }
+      } else {
+        launch_pat_numeric(op, p->ops.p, p->pat_rows.p, p->pat_ids.p, p->n_pat_rows,
+                           c_row_ptr, c_values, p->pat_off.p, p->pat_steps.p, p->pat_rec.p,
+                           p->pat_max_ops, p->pat_max_out, s);
+        ph.launches += 1;
+      }
     }
     for (int c = kEmpty_ + 1; c < kNumClasses; ++c) {
       if (p->num_count[c] <= 0) continue;

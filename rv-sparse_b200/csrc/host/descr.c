@@ -36,6 +36,7 @@ struct rvsp_spgemm_descr {
     rvsp_mlp_t model;      /* learned algorithm only; not owned */
     float capacity_scale;  /* learned algorithm only */
     int32_t merge_policy;
+    int32_t row_tiles;
 
     int32_t c_nnz;
     rvsp_dbuf_t c_row_ptr; /* analysed row pointers, device, a_rows + 1 */
@@ -69,6 +70,7 @@ rvsp_status_t rvsp_spgemm_descr_create(rvsp_spgemm_descr_t *descr)
     d->algo = RVSP_SPGEMM_ALGO_DEFAULT;
     d->mem = RVSP_MEM_HOST;
     d->capacity_scale = 1.15f;
+    d->row_tiles = 1;
     *descr = d;
     return RVSP_SUCCESS;
 }
@@ -100,6 +102,24 @@ rvsp_status_t rvsp_spgemm_set_merge_policy(rvsp_spgemm_descr_t d, int32_t policy
     if (d->estimated || policy < 0 || policy > 2)
         return RVSP_ERROR_INVALID_ARGUMENT;
     d->merge_policy = policy;
+    return RVSP_SUCCESS;
+}
+
+rvsp_status_t rvsp_spgemm_set_row_tiles(rvsp_spgemm_descr_t d, int32_t enable)
+{
+    if (d == NULL)
+        return RVSP_ERROR_NULL_POINTER;
+    if (enable != 0 && enable != 1)
+        return RVSP_ERROR_INVALID_ARGUMENT;
+    d->row_tiles = enable;
+    return d->plan ? rvsp_cuda_plan_set_row_tiles(d->plan, enable) : RVSP_SUCCESS;
+}
+
+rvsp_status_t rvsp_spgemm_get_tiled_rows(rvsp_spgemm_descr_t d, int32_t *n_out)
+{
+    if (d == NULL || n_out == NULL)
+        return RVSP_ERROR_NULL_POINTER;
+    *n_out = d->plan ? rvsp_cuda_plan_tiled_rows(d->plan) : 0;
     return RVSP_SUCCESS;
 }
 
@@ -229,6 +249,9 @@ static rvsp_status_t ensure_device(rvsp_spgemm_descr_t d)
     }
     if (!d->user_stream)
         d->stream = d->own_stream;
+    rvsp_status_t st = rvsp_cuda_plan_set_row_tiles(d->plan, d->row_tiles);
+    if (st != RVSP_SUCCESS)
+        return st;
     return rvsp_cuda_plan_set_merge_policy(d->plan, d->merge_policy);
 }
 

@@ -295,6 +295,15 @@ class Descriptor:
     def set_merge_policy(self, policy: int):
         L.check(self.lib.rvsp_spgemm_set_merge_policy(self.h, policy), "set_merge_policy")
 
+    def set_row_tiles(self, enable: bool):
+        """Row tiles for numeric-only computes (on by default)."""
+        L.check(self.lib.rvsp_spgemm_set_row_tiles(self.h, int(bool(enable))), "set_row_tiles")
+
+    def tiled_rows(self) -> int:
+        n = C.c_int32()
+        L.check(self.lib.rvsp_spgemm_get_tiled_rows(self.h, C.byref(n)), "tiled_rows")
+        return n.value
+
     def overflow_rows(self) -> int:
         n = C.c_int32()
         L.check(self.lib.rvsp_spgemm_get_overflow_rows(self.h, C.byref(n)), "overflow_rows")

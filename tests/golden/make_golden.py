@@ -15,6 +15,7 @@ The GPU tests only read the committed outputs.
 from __future__ import annotations
 
 import argparse
+import os
 import json
 import re
 import sys
@@ -95,7 +96,10 @@ def make_random():
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref-root", default="/root/reference")
+    ap.add_argument("--ref-root", default=os.environ.get(
+        "RVSP_REFERENCE_ROOT", str(Path(__file__).resolve().parents[3] / "reference")),
+        help="the reference tree (default: RVSP_REFERENCE_ROOT, else a checkout named "
+             "'reference' beside this repository)")
     args = ap.parse_args()
     here = Path(__file__).resolve().parent
     fx = parse_fixtures(Path(args.ref_root) / "tests" / "csr_fixtures.h")

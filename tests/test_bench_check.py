@@ -57,3 +57,47 @@ def test_signed_zero_differs():
     flipped = CSR(1, 1, rp, ci, np.array([-0.0], np.float32))
     assert bench.same_csr(CSR(1, 1, rp, ci, cv), rp, ci, cv)
     assert not bench.same_csr(flipped, rp, ci, cv)
+
+
+def test_panel_rows_cover_every_row_once_by_op_count():
+    # the stencil job's row panels: contiguous, disjoint, covering all rows,
+    # each near 1/N of the op count (the rows of C are independent)
+    from rvsp import intermediate_products
+    A = gen.stencil_3d_27(20)
+    ops = intermediate_products(A, A)
+    for world in (1, 2, 3, 8):
+        cuts = [bench.panel_rows(ops, world, r) for r in range(world)]
+        assert cuts[0][0] == 0 and cuts[-1][1] == A.rows
+        for (a0, a1), (b0, b1) in zip(cuts, cuts[1:]):
+            assert a1 == b0 and a0 <= a1
+        shares = [int(ops[r0:r1].sum()) for r0, r1 in cuts]
+        assert sum(shares) == int(ops.sum())
+        assert max(shares) - min(shares) <= 2 * int(ops.max())
+
+
+def test_job_value_sets_are_seeded_perturbations():
+    A = gen.stencil_3d_27(6)
+    s1 = bench.job_value_sets_host(A, 2, 5)
+    s2 = bench.job_value_sets_host(A, 2, 5)
+    for a, b in zip(s1, s2):
+        assert np.array_equal(a, b)
+        assert a.dtype == np.float32
+        assert np.all(np.abs(a - A.values) <= 0.0100001)
+    assert not np.array_equal(s1[0], s1[1])
+
+
+def test_reference_job_matches_the_restatement():
+    # the reference descriptor job the bench checks against: first compute,
+    # then numeric-only computes with new values, against the oracle
+    A = gen.stencil_3d_27(8)
+    sets = bench.job_value_sets_host(A, 2, 9)
+    st, rp, ci, first, every = oracle.ref_job(A, A, [(v, v) for v in sets], keep_all=True) \
+        if oracle.ref_available() else (0, *oracle.spgemm(A, A)[:3], None)
+    assert st == 0
+    want_rp, want_ci, want_cv, _ = oracle.spgemm(A, A)
+    assert np.array_equal(rp, want_rp) and np.array_equal(ci, want_ci)
+    assert np.array_equal(first.view(np.uint32), want_cv.view(np.uint32))
+    if every is not None:
+        for v, got in zip(sets, every):
+            A2 = A.with_values(v)
+            assert np.array_equal(got.view(np.uint32), oracle.spgemm(A2, A2)[2].view(np.uint32))
