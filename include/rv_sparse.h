@@ -209,6 +209,14 @@ rvsp_status_t rvsp_spgemm_set_row_tiles(rvsp_spgemm_descr_t descr, int32_t enabl
  * numeric-only compute on the current structure; 0 before). */
 rvsp_status_t rvsp_spgemm_get_tiled_rows(rvsp_spgemm_descr_t descr, int32_t *n_out);
 
+/* Shift classes in work_estimation (see rvsp_cuda_plan_set_shift_classes):
+ * 1 (default) or 0.  Results are identical either way. */
+rvsp_status_t rvsp_spgemm_set_shift_classes(rvsp_spgemm_descr_t descr, int32_t enable);
+
+/* Rows of the last work_estimation that took their structure from a shift
+ * class. */
+rvsp_status_t rvsp_spgemm_get_shift_rows(rvsp_spgemm_descr_t descr, int32_t *n_out);
+
 /* Rows the last learned work_estimation redid with the plain path. */
 rvsp_status_t rvsp_spgemm_get_overflow_rows(rvsp_spgemm_descr_t descr, int32_t *n_out);
 

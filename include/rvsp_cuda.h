@@ -221,6 +221,24 @@ rvsp_status_t rvsp_cuda_plan_set_row_tiles(rvsp_cuda_plan_t plan, int32_t enable
  * are none or tiles are off). */
 int32_t rvsp_cuda_plan_tiled_rows(rvsp_cuda_plan_t plan);
 
+/* Shift classes in the analysis (1, the default) or not (0).  The GPU form of
+ * rvsp_symbolic_count + rvsp_symbolic_fill (rvsp_symbolic.c:13-137) for rows
+ * that are exact translates of another row (banded and stencil matrices):
+ * such a row's A nonzeros sit at the same offsets from it as the other row's,
+ * over B rows whose columns sit at the same offsets from their own index
+ * (checked entry by entry).  Its count, columns (moved by the row distance)
+ * and term table come from the canonical row, so it skips the symbolic pass
+ * and the fill (k_shift.cu).  Matrices of at least 4096 rows run a probe of
+ * 2048 rows on the device, and the analysis only when at least half of them
+ * have a translate among the others; the learned analysis hands such
+ * matrices to it.  Values are identical either way.  Applies from the next
+ * analysis. */
+rvsp_status_t rvsp_cuda_plan_set_shift_classes(rvsp_cuda_plan_t plan, int32_t enable);
+
+/* Rows of the last analysis that took their structure from a shift class (0
+ * when none did). */
+int32_t rvsp_cuda_plan_shift_rows(rvsp_cuda_plan_t plan);
+
 /* Size of the library's fixed device scratch for rvsp_cuda_numeric_noalloc,
  * and the widest B it accepts (one float accumulator per B column). */
 #define RVSP_NOALLOC_SCRATCH_BYTES (16u << 20)

@@ -99,6 +99,10 @@ pat_build_kernel(const int32_t *__restrict__ pat_canon, const int32_t *__restric
   const int32_t row = pat_canon[id];
   const int32_t p0 = a_rp[row], na = a_rp[row + 1] - p0;
   const int32_t m = c_rp[row + 1] - c_rp[row];
+  if (na > kPatMaxA || m > kPatMaxOut) {  // does not fit the tables
+    if (tid == 0) psteps[id] = -1;
+    return;
+  }
   const int64_t base = moff[row];
   uint32_t *const tab = rec + pat_off[id];
   for (int q = tid; q < m; q += kPatBuildThreads) cnt[q] = 0;
@@ -321,7 +325,7 @@ pat_numeric_kernel(const int32_t *__restrict__ a_rp, const int32_t *__restrict__
     }
   }
   __syncwarp();
-  const int32_t cs = c_rp[row], m = c_rp[row + 1] - cs;
+  const int32_t cs = c_rp[row], m = min(c_rp[row + 1] - cs, out_cap);
   for (int32_t q = lane; q < m; q += 32) c_val[cs + q] = outv[q];
 }
 

@@ -102,7 +102,8 @@ tile_apply_kernel(int32_t n, const int32_t *__restrict__ counts,
                   const int32_t *__restrict__ a_rp,
                   const int64_t *__restrict__ partials,
                   int32_t *__restrict__ row_ptr, uint8_t *__restrict__ cls,
-                  int32_t *__restrict__ class_count, bool merge_ok, CheckGuard guard) {
+                  int32_t *__restrict__ class_count, bool merge_ok, CheckGuard guard,
+                  const int32_t *__restrict__ skip) {
   __shared__ int32_t s_items[kTile + kTile / 32];
   __shared__ long long s_warp[kThreads / 32];
   __shared__ int32_t s_cnt[kNumClasses];
@@ -120,7 +121,8 @@ tile_apply_kernel(int32_t n, const int32_t *__restrict__ counts,
     int c = kEmpty_;
     if (i < n) {
       m = counts[i];
-      c = classify_row(a_rp[i + 1] - a_rp[i], ops[i], m, merge_ok);
+      c = (skip && skip[i] >= 0) ? kEmpty_
+                                 : classify_row(a_rp[i + 1] - a_rp[i], ops[i], m, merge_ok);
       cls[i] = static_cast<uint8_t>(c);
     }
     s_items[skew(idx)] = m;
@@ -219,12 +221,12 @@ void launch_scan_and_class(int32_t n, const int32_t *counts, const int64_t *ops,
                            const int32_t *a_rp, int32_t *row_ptr,
                            int64_t *partials, int64_t *total, uint8_t *cls,
                            int32_t *class_count, bool merge_ok, cudaStream_t s,
-                           CheckGuard guard) {
+                           CheckGuard guard, const int32_t *skip) {
   const int32_t nt = static_cast<int32_t>((static_cast<int64_t>(n) + kTile - 1) / kTile);
   tile_sum_kernel<<<nt, kThreads, 0, s>>>(n, counts, partials);
   partials_scan_kernel<<<1, kThreads, 0, s>>>(n, nt, partials, total, row_ptr, guard);
   tile_apply_kernel<<<nt, kThreads, 0, s>>>(n, counts, ops, a_rp, partials, row_ptr,
-                                            cls, class_count, merge_ok, guard);
+                                            cls, class_count, merge_ok, guard, skip);
 }
 
 }  // namespace rvsp

@@ -1,0 +1,608 @@
+// Shift classes: rows of C that are exact translates of another row.
+//
+// For a banded or stencil matrix most rows of C = A x B look alike: row i's
+// A nonzeros sit at the same offsets from i as row r's at offsets from r, and
+// each selects a B row whose columns sit at the same offsets from its own
+// index as the matching B row of r.  Then C's row i is C's row r moved by
+// i - r: the same count, columns + (i - r), and the same position of every
+// product in the row (so the same term table, k_tile.cu / k_pattern.cu).
+//
+// Classes are found in two levels, each by a 64-bit key, a hash table that
+// keeps the smallest row per key, and an entry-by-entry check against that
+// row (a row that fails the check stays in a class of its own, so nothing
+// rests on the hash):
+//
+//   B rows: key(len, (column - k) at each position e); bcls[k] = the
+//           smallest B row with the same translated columns, else k;
+//   rows:   key(nA, (A column - i, bcls of that B row) at each position j);
+//           rcls[i] = the smallest row with the same translated A row over
+//           the same B classes, else i.
+//
+// A class of at least min_share rows whose canonical row fits a term table
+// (at most 32 A nonzeros, 1024 products and kShiftMaxOut outputs) is a
+// pattern: its other rows (members) skip the symbolic pass and the fill,
+// take their count from the canonical row, their columns by translation, and
+// their values from the term tables built on the canonical row's map.  Every
+// value is still summed in ascending A-nonzero order from +0.0f with
+// separately rounded products and sums (the reference's order,
+// gustavson_core_f32.inc:31-62), so results are bit-identical to the plain
+// path.
+//
+// Whether to look at all is decided on the device: a probe keys rows spread
+// over A and one block sorts the keys; the analysis runs when at least half
+// of them have a translate among the others.  Every pass after the probe
+// reads that flag (*on) and returns at once when it is 0, so the plan queues
+// them without a host round trip.
+#include <climits>
+
+#include "device_common.cuh"
+#include "kernels.cuh"
+
+namespace rvsp {
+
+namespace {
+
+constexpr int kShiftMaxA = 32;
+constexpr int kShiftMaxOps = 1024;
+constexpr int kShiftMaxOut = 512;    // C entries of a pattern (the term tables' limit)
+constexpr int kShiftSamples = 2048;  // rows the probe keys
+constexpr int kThreads = 256;
+
+__device__ __forceinline__ unsigned long long mix64(unsigned long long z) {
+  z = (z ^ (z >> 31)) * 0x7FB5D329728EA185ull;
+  z = (z ^ (z >> 27)) * 0x81DADEF4BC2DD44Dull;
+  return z ^ (z >> 33);
+}
+
+__device__ __forceinline__ unsigned long long warp_xor64(unsigned long long h) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) h ^= __shfl_xor_sync(kFull, h, o);
+  return h;
+}
+
+// Key of B row k (warp-wide; every lane returns it).  Never 0.
+__device__ __forceinline__ unsigned long long brow_key(const int32_t *__restrict__ b_rp,
+                                                       const int32_t *__restrict__ b_col,
+                                                       int32_t k, int lane) {
+  const int32_t b0 = __ldg(b_rp + k), len = __ldg(b_rp + k + 1) - b0;
+  unsigned long long h = 0;
+  for (int32_t e = lane; e < len; e += 32) {
+    const uint32_t off = static_cast<uint32_t>(__ldg(b_col + b0 + e) - k);
+    h ^= mix64((static_cast<unsigned long long>(e) << 32) | off);
+  }
+  h = warp_xor64(h);
+  return mix64(h ^ (static_cast<unsigned long long>(len) * 0x9E3779B97F4A7C15ull)) | 1ull;
+}
+
+// Row key from per-position terms (lane j < na contributes its A nonzero j).
+__device__ __forceinline__ unsigned long long row_key(int32_t na, int lane, int32_t d,
+                                                      unsigned long long cls_word) {
+  unsigned long long h = 0;
+  if (lane < na)
+    h = mix64((static_cast<unsigned long long>(lane) << 32) | static_cast<uint32_t>(d)) ^
+        mix64(cls_word * 0xD6E8FEB86659FD93ull + static_cast<unsigned long long>(lane));
+  h = warp_xor64(h);
+  return mix64(h ^ (static_cast<unsigned long long>(na) * 0xA0761D6478BD642Full)) | 1ull;
+}
+
+__device__ __forceinline__ uint32_t key_slot(unsigned long long key, unsigned long long mask) {
+  return static_cast<uint32_t>((key * 0x9E3779B97F4A7C15ull) >> 32) & static_cast<uint32_t>(mask);
+}
+
+// A row that may join a pattern: 1..32 A nonzeros and at most 1024 products.
+__device__ __forceinline__ bool shiftable(int32_t na, int64_t ops) {
+  return na > 0 && na <= kShiftMaxA && ops > 0 && ops <= kShiftMaxOps;
+}
+
+// Probe: keys of `samples` rows spread over A, computed directly (B keys on
+// the fly).  Warp per sampled row.  Reads nothing when the structure check
+// queued before it failed.
+__global__ void __launch_bounds__(kThreads)
+shift_probe_kernel(Operands op, int32_t samples, unsigned long long *__restrict__ keys,
+                   CheckGuard guard) {
+  const int32_t w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (w >= samples) return;
+  const int lane = lane_id();
+  if (guard.failed()) {
+    if (lane == 0) keys[w] = 0;
+    return;
+  }
+  const int32_t i = static_cast<int32_t>((static_cast<int64_t>(w) * op.a_rows) / samples);
+  const int32_t p0 = op.a_rp[i], na = op.a_rp[i + 1] - p0;
+  if (na <= 0 || na > kShiftMaxA) {
+    if (lane == 0) keys[w] = 0;
+    return;
+  }
+  int32_t k = 0;
+  if (lane < na) k = __ldg(op.a_col + p0 + lane);
+  unsigned long long mine = 0;
+  for (int32_t j = 0; j < na; ++j) {
+    const int32_t kj = __shfl_sync(kFull, k, j);
+    const unsigned long long bk = brow_key(op.b_rp, op.b_col, kj, lane);
+    if (lane == j) mine = bk;
+  }
+  const unsigned long long key = row_key(na, lane, k - i, mine);
+  if (lane == 0) keys[w] = key;
+}
+
+// The decision: sorts the probe's keys (one block) and sets *on when at
+// least half of the sampled rows share their key with another sampled row.
+// *on stays 0 when the structure check failed.
+__global__ void __launch_bounds__(1024)
+shift_decide_kernel(const unsigned long long *__restrict__ keys, int32_t samples,
+                    int32_t *__restrict__ on, CheckGuard guard) {
+  __shared__ unsigned long long sk[kShiftSamples];
+  __shared__ int32_t dup;
+  const int tid = threadIdx.x;
+  if (tid == 0) {
+    *on = 0;
+    dup = 0;
+  }
+  if (guard.failed()) return;
+  for (int t = tid; t < kShiftSamples; t += blockDim.x)
+    sk[t] = t < samples ? keys[t] : ~0ull;
+  __syncthreads();
+  block_bitonic_sort(sk, kShiftSamples);
+  int mine = 0;
+  for (int t = tid; t < samples; t += blockDim.x) {
+    const unsigned long long v = sk[t];
+    const bool shared = v != 0ull && v != ~0ull &&
+                        ((t > 0 && sk[t - 1] == v) || (t + 1 < samples && sk[t + 1] == v));
+    mine += shared ? 1 : 0;
+  }
+  mine = warp_sum(mine);
+  if (lane_id() == 0 && mine) atomicAdd(&dup, mine);
+  __syncthreads();
+  if (tid == 0) *on = 2 * dup >= samples ? 1 : 0;
+}
+
+// Gated fills.
+__global__ void __launch_bounds__(kThreads)
+shift_fill64_kernel(const int32_t *__restrict__ on, unsigned long long *__restrict__ p, size_t n,
+                    unsigned long long v) {
+  if (!*on) return;
+  for (size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+       i += size_t(gridDim.x) * blockDim.x)
+    p[i] = v;
+}
+__global__ void __launch_bounds__(kThreads)
+shift_fill32_kernel(const int32_t *__restrict__ on, int32_t *__restrict__ p, size_t n,
+                    int32_t v) {
+  if (!*on) return;
+  for (size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+       i += size_t(gridDim.x) * blockDim.x)
+    p[i] = v;
+}
+
+// B row keys: warp per B row.
+__global__ void __launch_bounds__(kThreads)
+shift_bkey_kernel(const int32_t *__restrict__ on, int32_t b_rows,
+                  const int32_t *__restrict__ b_rp, const int32_t *__restrict__ b_col,
+                  unsigned long long *__restrict__ bkey) {
+  if (!*on) return;
+  const int32_t k = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (k >= b_rows) return;
+  const unsigned long long key = brow_key(b_rp, b_col, k, lane_id());
+  if (lane_id() == 0) bkey[k] = key;
+}
+
+// Inserts every nonzero key into the table (tkey zeroed, trow INT_MAX), the
+// slot keeping the smallest row of its key.  Lanes with equal keys make one
+// insert (the lowest lane, which holds the smallest row).  The probe loop is
+// bounded by the table size (at least twice the keys, so it never fills).
+__global__ void __launch_bounds__(kThreads)
+shift_insert_kernel(const int32_t *__restrict__ on, int32_t n,
+                    const unsigned long long *__restrict__ keys,
+                    unsigned long long *__restrict__ tkey, int32_t *__restrict__ trow,
+                    unsigned long long mask) {
+  if (!*on) return;
+  const int32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  const unsigned long long key = i < n ? keys[i] : 0ull;
+  const unsigned peers = __match_any_sync(kFull, key);
+  if (key == 0ull || (peers & lanemask_lt()) != 0u) return;
+  uint32_t s = key_slot(key, mask);
+  for (unsigned long long t = 0; t <= mask; ++t) {
+    const unsigned long long prev = atomicCAS(tkey + s, 0ull, key);
+    if (prev == 0ull || prev == key) {
+      atomicMin(trow + s, i);
+      return;
+    }
+    s = (s + 1) & static_cast<uint32_t>(mask);
+  }
+}
+
+// The table's row for key; -1 if not found.
+__device__ __forceinline__ int32_t lookup(unsigned long long key,
+                                          const unsigned long long *__restrict__ tkey,
+                                          const int32_t *__restrict__ trow,
+                                          unsigned long long mask) {
+  uint32_t s = key_slot(key, mask);
+  for (unsigned long long t = 0; t <= mask; ++t) {
+    const unsigned long long v = tkey[s];
+    if (v == key) return trow[s];
+    if (v == 0ull) return -1;
+    s = (s + 1) & static_cast<uint32_t>(mask);
+  }
+  return -1;
+}
+
+// bcls[k]: the smallest B row with k's translated columns (checked entry by
+// entry), else k.  Warp per B row.
+__global__ void __launch_bounds__(kThreads)
+shift_bresolve_kernel(const int32_t *__restrict__ on, int32_t b_rows,
+                      const unsigned long long *__restrict__ bkey,
+                      const unsigned long long *__restrict__ tkey,
+                      const int32_t *__restrict__ trow, unsigned long long mask,
+                      const int32_t *__restrict__ b_rp, const int32_t *__restrict__ b_col,
+                      int32_t *__restrict__ bcls) {
+  if (!*on) return;
+  const int32_t k = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (k >= b_rows) return;
+  const int lane = lane_id();
+  const int32_t c = lookup(bkey[k], tkey, trow, mask);
+  bool ok = c >= 0 && c < b_rows;
+  if (ok && c != k) {
+    const int32_t k0 = __ldg(b_rp + k), len = __ldg(b_rp + k + 1) - k0;
+    const int32_t c0 = __ldg(b_rp + c), lc = __ldg(b_rp + c + 1) - c0;
+    bool same = len == lc;
+    for (int32_t e = lane; same && e < len; e += 32)
+      same = (__ldg(b_col + k0 + e) - k) == (__ldg(b_col + c0 + e) - c);
+    ok = __all_sync(kFull, same);
+  }
+  if (lane == 0) bcls[k] = ok ? c : k;
+}
+
+// Row keys: warp per row; 0 for a row that cannot join a pattern.
+__global__ void __launch_bounds__(kThreads)
+shift_rkey_kernel(const int32_t *__restrict__ on, int32_t a_rows,
+                  const int32_t *__restrict__ a_rp, const int32_t *__restrict__ a_col,
+                  const int64_t *__restrict__ ops, const int32_t *__restrict__ bcls,
+                  unsigned long long *__restrict__ rkey) {
+  if (!*on) return;
+  const int32_t i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (i >= a_rows) return;
+  const int lane = lane_id();
+  const int32_t p0 = a_rp[i], na = a_rp[i + 1] - p0;
+  if (!shiftable(na, ops[i])) {
+    if (lane == 0) rkey[i] = 0ull;
+    return;
+  }
+  int32_t k = 0, bc = 0;
+  if (lane < na) {
+    k = __ldg(a_col + p0 + lane);
+    bc = __ldg(bcls + k);
+  }
+  const unsigned long long key = row_key(na, lane, k - i, static_cast<uint32_t>(bc));
+  if (lane == 0) rkey[i] = key;
+}
+
+// rcls[i]: the smallest row with i's translated A row over the same B
+// classes (checked entry by entry), else i.  Warp per row.
+__global__ void __launch_bounds__(kThreads)
+shift_rresolve_kernel(const int32_t *__restrict__ on, int32_t a_rows,
+                      const unsigned long long *__restrict__ rkey,
+                      const unsigned long long *__restrict__ tkey,
+                      const int32_t *__restrict__ trow, unsigned long long mask,
+                      const int32_t *__restrict__ a_rp, const int32_t *__restrict__ a_col,
+                      const int32_t *__restrict__ bcls, int32_t *__restrict__ rcls) {
+  if (!*on) return;
+  const int32_t i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (i >= a_rows) return;
+  const int lane = lane_id();
+  const unsigned long long key = rkey[i];
+  const int32_t c = key ? lookup(key, tkey, trow, mask) : -1;
+  bool ok = c >= 0 && c < a_rows && c != i;
+  if (ok) {
+    const int32_t pi = a_rp[i], na = a_rp[i + 1] - pi;
+    const int32_t pc = a_rp[c], nc = a_rp[c + 1] - pc;
+    bool same = na == nc && na <= kShiftMaxA;
+    if (same && lane < na) {
+      const int32_t ki = __ldg(a_col + pi + lane), kc = __ldg(a_col + pc + lane);
+      same = (ki - i) == (kc - c) && __ldg(bcls + ki) == __ldg(bcls + kc);
+    }
+    ok = __all_sync(kFull, same);
+  }
+  if (lane == 0) rcls[i] = ok ? c : i;
+}
+
+// share[c] += rows whose class is c (other than c); warp-aggregated.
+__global__ void __launch_bounds__(kThreads)
+shift_share_kernel(const int32_t *__restrict__ on, int32_t n, const int32_t *__restrict__ rcls,
+                   int32_t *__restrict__ share) {
+  if (!*on) return;
+  const int32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int32_t c = i < n ? rcls[i] : -1;
+  const bool member = i < n && c != i;
+  const unsigned peers = __match_any_sync(kFull, member ? c : -1 - lane_id());
+  if (member && (peers & lanemask_lt()) == 0u) atomicAdd(share + c, __popc(peers));
+}
+
+// Candidates: a canonical row shared by at least min_share - 1 others gets
+// an id (pat_of[c], pat_canon[id]) and its table capacity (the warp-per-row
+// table kernel's record count, k_pattern.cu: (2 ceil(ops/32) + nA) * 32).
+__global__ void __launch_bounds__(kThreads)
+shift_pat_kernel(const int32_t *__restrict__ on, int32_t n, const int32_t *__restrict__ rcls,
+                 const int32_t *__restrict__ share, int32_t min_share,
+                 const int32_t *__restrict__ a_rp, const int64_t *__restrict__ ops,
+                 int32_t *__restrict__ pat_of, int32_t *__restrict__ pat_canon,
+                 int32_t *__restrict__ pat_cap, int32_t *__restrict__ npat, int32_t cap_pat) {
+  if (!*on) return;
+  const int32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  pat_of[i] = -1;
+  if (rcls[i] != i || share[i] + 1 < min_share) return;
+  const int32_t id = atomicAdd(npat, 1);
+  if (id >= cap_pat) return;  // cannot happen: cap_pat >= n / min_share + 1
+  pat_of[i] = id;
+  pat_canon[id] = i;
+  const int32_t tiles = static_cast<int32_t>((ops[i] + 31) / 32);
+  pat_cap[id] = (2 * tiles + (a_rp[i + 1] - a_rp[i])) * 32;
+}
+
+// The output count of each candidate's canonical row (distinct columns of
+// its at most 1024 products: one block sort), and whether the pattern is
+// kept: at most kShiftMaxOut outputs, which the term tables hold.  Blocks
+// stride over the candidates; pat_m[id] = count, or -1 when dropped.
+__global__ void __launch_bounds__(1024)
+shift_canon_count_kernel(const int32_t *__restrict__ on, const int32_t *__restrict__ npat,
+                         int32_t cap_pat, const int32_t *__restrict__ pat_canon,
+                         const int32_t *__restrict__ a_rp, const int32_t *__restrict__ a_col,
+                         const int32_t *__restrict__ b_rp, const int32_t *__restrict__ b_col,
+                         int32_t *__restrict__ pat_m) {
+  __shared__ unsigned long long cols[kShiftMaxOps];
+  __shared__ int32_t bstart[kShiftMaxA + 1];
+  __shared__ int32_t s_m;
+  if (!*on) return;
+  const int32_t np = min(*npat, cap_pat);
+  const int tid = threadIdx.x;
+  for (int32_t id = blockIdx.x; id < np; id += gridDim.x) {
+    const int32_t row = pat_canon[id];
+    const int32_t p0 = a_rp[row], na = a_rp[row + 1] - p0;
+    if (tid == 0) {
+      int32_t run = 0;
+      for (int32_t j = 0; j < na; ++j) {
+        bstart[j] = run;
+        const int32_t k = a_col[p0 + j];
+        run += b_rp[k + 1] - b_rp[k];
+      }
+      bstart[na] = run;
+      s_m = 0;
+    }
+    __syncthreads();
+    const int32_t ops = bstart[na];
+    for (int32_t t = tid; t < kShiftMaxOps; t += blockDim.x) {
+      unsigned long long v = ~0ull;
+      if (t < ops) {
+        int32_t j = 0;
+        while (j + 1 < na && bstart[j + 1] <= t) ++j;
+        const int32_t k = a_col[p0 + j];
+        v = static_cast<unsigned long long>(
+            static_cast<uint32_t>(b_col[b_rp[k] + t - bstart[j]]));
+      }
+      cols[t] = v;
+    }
+    __syncthreads();
+    block_bitonic_sort(cols, kShiftMaxOps);
+    int mine = 0;
+    for (int32_t t = tid; t < ops; t += blockDim.x)
+      mine += (t == 0 || cols[t] != cols[t - 1]) ? 1 : 0;
+    mine = warp_sum(mine);
+    if (lane_id() == 0 && mine) atomicAdd(&s_m, mine);
+    __syncthreads();
+    if (tid == 0) pat_m[id] = s_m <= kShiftMaxOut ? s_m : -1;
+    __syncthreads();
+  }
+}
+
+// Members: pid_of_row[i] = pattern of a member row (else -1; every row -1
+// when *on is 0), its symbolic class set to empty (it skips the symbolic
+// pass); *members counts them.
+__global__ void __launch_bounds__(kThreads)
+shift_members_kernel(const int32_t *__restrict__ on, int32_t n, const int32_t *__restrict__ rcls,
+                     const int32_t *__restrict__ pat_of, const int32_t *__restrict__ pat_m,
+                     int32_t *__restrict__ pid_of_row, uint8_t *__restrict__ cls,
+                     int32_t *__restrict__ members) {
+  const int32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  const bool live = *on != 0;
+  bool m = false;
+  if (i < n) {
+    int32_t pid = -1;
+    if (live) {
+      const int32_t c = rcls[i];
+      pid = c != i ? pat_of[c] : -1;
+      if (pid >= 0 && pat_m[pid] < 0) pid = -1;
+    }
+    pid_of_row[i] = pid;
+    if (pid >= 0) {
+      cls[i] = static_cast<uint8_t>(kEmpty_);
+      m = true;
+    }
+  }
+  const unsigned b = __ballot_sync(kFull, m);
+  if (b && lane_id() == 0) atomicAdd(members, __popc(b));
+}
+
+// Class census of cls (class_count zeroed before).
+__global__ void __launch_bounds__(kThreads)
+shift_census_kernel(const int32_t *__restrict__ on, int32_t n, const uint8_t *__restrict__ cls,
+                    int32_t *__restrict__ class_count) {
+  __shared__ int32_t s_cnt[kNumClasses];
+  if (!*on) return;
+  for (int c = threadIdx.x; c < kNumClasses; c += blockDim.x) s_cnt[c] = 0;
+  __syncthreads();
+  const int32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int c = i < n ? cls[i] : -1;
+  const unsigned peers = __match_any_sync(kFull, c);
+  if (c >= 0 && (peers & lanemask_lt()) == 0u) atomicAdd(&s_cnt[c], __popc(peers));
+  __syncthreads();
+  for (int k = threadIdx.x; k < kNumClasses; k += blockDim.x)
+    if (s_cnt[k]) atomicAdd(class_count + k, s_cnt[k]);
+}
+
+// counts[i] = counts[canonical] for member rows.
+__global__ void __launch_bounds__(kThreads)
+shift_copy_counts_kernel(const int32_t *__restrict__ on, int32_t n,
+                         const int32_t *__restrict__ pid_of_row,
+                         const int32_t *__restrict__ rcls, int32_t *__restrict__ counts) {
+  if (!*on) return;
+  const int32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n || pid_of_row[i] < 0) return;
+  counts[i] = counts[rcls[i]];
+}
+
+// Member rows' columns: the canonical row's, moved by i - c.  Warp per row.
+__global__ void __launch_bounds__(kThreads)
+shift_fill_kernel(int32_t n, const int32_t *__restrict__ pid_of_row,
+                  const int32_t *__restrict__ rcls, const int32_t *__restrict__ c_rp,
+                  int32_t *__restrict__ c_col) {
+  const int32_t i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (i >= n || pid_of_row[i] < 0) return;
+  const int32_t c = rcls[i];
+  const int32_t cs = c_rp[i], cc = c_rp[c], m = c_rp[i + 1] - cs;
+  const int32_t d = i - c;
+  for (int32_t e = lane_id(); e < m; e += 32) c_col[cs + e] = __ldg(c_col + cc + e) + d;
+}
+
+// Map of each pattern's canonical row: for product t in flattened order
+// (A nonzero j, then B position e), its position in C's sorted row, by
+// binary search; 0xffff when the column is missing (C is not this product's).
+// moff[canonical row] = id * kShiftMaxOps.  Warp per pattern.
+__global__ void __launch_bounds__(kThreads)
+shift_canon_map_kernel(int32_t npat, const int32_t *__restrict__ pat_canon,
+                       const int32_t *__restrict__ a_rp, const int32_t *__restrict__ a_col,
+                       const int32_t *__restrict__ b_rp, const int32_t *__restrict__ b_col,
+                       const int32_t *__restrict__ c_rp, const int32_t *__restrict__ c_col,
+                       int64_t *__restrict__ moff, uint16_t *__restrict__ map) {
+  const int32_t id = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (id >= npat) return;
+  const int lane = lane_id();
+  const int32_t row = pat_canon[id];
+  const int32_t p0 = a_rp[row], na = a_rp[row + 1] - p0;
+  const int32_t cs = c_rp[row], m = c_rp[row + 1] - cs;
+  const int64_t base = int64_t(id) * kShiftMaxOps;
+  if (lane == 0) moff[row] = base;
+  int32_t t0 = 0;
+  for (int32_t j = 0; j < na; ++j) {
+    const int32_t k = __ldg(a_col + p0 + j);
+    const int32_t b0 = __ldg(b_rp + k), len = __ldg(b_rp + k + 1) - b0;
+    for (int32_t e = lane; e < len && t0 + e < kShiftMaxOps; e += 32) {
+      const int32_t col = __ldg(b_col + b0 + e);
+      int32_t lo = 0, hi = m;
+      while (lo < hi) {
+        const int32_t mid = (lo + hi) >> 1;
+        if (__ldg(c_col + cs + mid) < col) lo = mid + 1;
+        else hi = mid;
+      }
+      const bool found = lo < m && __ldg(c_col + cs + lo) == col;
+      map[base + t0 + e] = found ? static_cast<uint16_t>(lo) : uint16_t(0xffff);
+    }
+    t0 += len;
+  }
+}
+
+// Largest products (rounded up to 32) and outputs over the kept patterns
+// (out[0], out[1], zeroed by the caller).
+__global__ void __launch_bounds__(kThreads)
+shift_maxima_kernel(int32_t npat, const int32_t *__restrict__ pat_canon,
+                    const int32_t *__restrict__ pat_m, const int64_t *__restrict__ ops,
+                    int32_t *__restrict__ out) {
+  const int32_t id = blockIdx.x * blockDim.x + threadIdx.x;
+  if (id >= npat || pat_m[id] < 0) return;
+  atomicMax(out, static_cast<int32_t>((ops[pat_canon[id]] + 31) / 32) * 32);
+  atomicMax(out + 1, pat_m[id]);
+}
+
+unsigned grid_warps(int64_t warps) {
+  return static_cast<unsigned>((warps * 32 + kThreads - 1) / kThreads);
+}
+unsigned grid_threads(int64_t n) {
+  return static_cast<unsigned>((n + kThreads - 1) / kThreads);
+}
+unsigned grid_fill(size_t n) {
+  const size_t b = (n + kThreads - 1) / kThreads;
+  return static_cast<unsigned>(b < 4096 ? (b ? b : 1) : 4096);
+}
+
+}  // namespace
+
+int32_t shift_max_ops() { return kShiftMaxOps; }
+int32_t shift_samples() { return kShiftSamples; }
+
+void launch_shift_decide(const Operands &op, unsigned long long *keys, int32_t *on,
+                         CheckGuard guard, cudaStream_t s) {
+  const int32_t samples = op.a_rows < kShiftSamples ? op.a_rows : kShiftSamples;
+  shift_probe_kernel<<<grid_warps(samples), kThreads, 0, s>>>(op, samples, keys, guard);
+  shift_decide_kernel<<<1, 1024, 0, s>>>(keys, samples, on, guard);
+}
+
+void launch_shift_classes(const int32_t *on, const Operands &op, int32_t b_rows,
+                          const int64_t *ops, unsigned long long *bkey,
+                          unsigned long long *rkey, unsigned long long *tkey, int32_t *trow,
+                          size_t tcap, int32_t *bcls, int32_t *rcls, cudaStream_t s) {
+  const unsigned long long mask = tcap - 1;
+  // B classes
+  shift_fill64_kernel<<<grid_fill(tcap), kThreads, 0, s>>>(on, tkey, tcap, 0ull);
+  shift_fill32_kernel<<<grid_fill(tcap), kThreads, 0, s>>>(on, trow, tcap, INT_MAX);
+  shift_bkey_kernel<<<grid_warps(b_rows), kThreads, 0, s>>>(on, b_rows, op.b_rp, op.b_col,
+                                                            bkey);
+  shift_insert_kernel<<<grid_threads(b_rows), kThreads, 0, s>>>(on, b_rows, bkey, tkey, trow,
+                                                                mask);
+  shift_bresolve_kernel<<<grid_warps(b_rows), kThreads, 0, s>>>(on, b_rows, bkey, tkey, trow,
+                                                                mask, op.b_rp, op.b_col, bcls);
+  // row classes
+  shift_fill64_kernel<<<grid_fill(tcap), kThreads, 0, s>>>(on, tkey, tcap, 0ull);
+  shift_fill32_kernel<<<grid_fill(tcap), kThreads, 0, s>>>(on, trow, tcap, INT_MAX);
+  shift_rkey_kernel<<<grid_warps(op.a_rows), kThreads, 0, s>>>(on, op.a_rows, op.a_rp,
+                                                               op.a_col, ops, bcls, rkey);
+  shift_insert_kernel<<<grid_threads(op.a_rows), kThreads, 0, s>>>(on, op.a_rows, rkey, tkey,
+                                                                   trow, mask);
+  shift_rresolve_kernel<<<grid_warps(op.a_rows), kThreads, 0, s>>>(
+      on, op.a_rows, rkey, tkey, trow, mask, op.a_rp, op.a_col, bcls, rcls);
+}
+
+void launch_shift_patterns(const int32_t *on, const Operands &op, const int32_t *rcls,
+                           int32_t *share, int32_t min_share, const int64_t *ops,
+                           int32_t *pat_of, int32_t *pat_canon, int32_t *pat_cap,
+                           int32_t *pat_m, int32_t *npat, int32_t cap_pat,
+                           int32_t *pid_of_row, uint8_t *cls, int32_t *members,
+                           int32_t *class_count, int num_sms, cudaStream_t s) {
+  const int32_t n = op.a_rows;
+  shift_fill32_kernel<<<grid_fill(size_t(n)), kThreads, 0, s>>>(on, share, size_t(n), 0);
+  shift_share_kernel<<<grid_threads(n), kThreads, 0, s>>>(on, n, rcls, share);
+  shift_pat_kernel<<<grid_threads(n), kThreads, 0, s>>>(on, n, rcls, share, min_share, op.a_rp,
+                                                        ops, pat_of, pat_canon, pat_cap, npat,
+                                                        cap_pat);
+  shift_canon_count_kernel<<<num_sms, 1024, 0, s>>>(on, npat, cap_pat, pat_canon, op.a_rp,
+                                                    op.a_col, op.b_rp, op.b_col, pat_m);
+  shift_members_kernel<<<grid_threads(n), kThreads, 0, s>>>(on, n, rcls, pat_of, pat_m,
+                                                            pid_of_row, cls, members);
+  shift_fill32_kernel<<<1, kThreads, 0, s>>>(on, class_count, kNumClasses, 0);
+  shift_census_kernel<<<grid_threads(n), kThreads, 0, s>>>(on, n, cls, class_count);
+}
+
+void launch_shift_copy_counts(const int32_t *on, int32_t n, const int32_t *pid_of_row,
+                              const int32_t *rcls, int32_t *counts, cudaStream_t s) {
+  shift_copy_counts_kernel<<<grid_threads(n), kThreads, 0, s>>>(on, n, pid_of_row, rcls,
+                                                                counts);
+}
+
+void launch_shift_fill(int32_t n, const int32_t *pid_of_row, const int32_t *rcls,
+                       const int32_t *c_rp, int32_t *c_col, cudaStream_t s) {
+  shift_fill_kernel<<<grid_warps(n), kThreads, 0, s>>>(n, pid_of_row, rcls, c_rp, c_col);
+}
+
+void launch_shift_canon_map(int32_t npat, const int32_t *pat_canon, const Operands &op,
+                            const int32_t *c_rp, const int32_t *c_col, int64_t *moff,
+                            uint16_t *map, cudaStream_t s) {
+  if (npat <= 0) return;
+  shift_canon_map_kernel<<<grid_warps(npat), kThreads, 0, s>>>(
+      npat, pat_canon, op.a_rp, op.a_col, op.b_rp, op.b_col, c_rp, c_col, moff, map);
+}
+
+void launch_pat_maxima(int32_t npat, const int32_t *pat_canon, const int32_t *pat_m,
+                       const int64_t *ops, int32_t *out, cudaStream_t s) {
+  if (npat <= 0) return;
+  shift_maxima_kernel<<<grid_threads(npat), kThreads, 0, s>>>(npat, pat_canon, pat_m, ops, out);
+}
+
+}  // namespace rvsp

@@ -364,9 +364,33 @@ tile_numeric_kernel(const int32_t *__restrict__ a_rp, const int32_t *__restrict_
   }
 }
 
+// rows / ids: every row with pid_of_row[row] >= 0, in chunk order.
+__global__ void __launch_bounds__(256)
+tile_list_kernel(int32_t n, const int32_t *__restrict__ pid_of_row, int32_t *__restrict__ rows,
+                 int32_t *__restrict__ ids, int32_t *__restrict__ count) {
+  const int32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int32_t pid = i < n ? pid_of_row[i] : -1;
+  const unsigned b = __ballot_sync(kFull, pid >= 0);
+  if (!b) return;
+  int32_t base = 0;
+  if (lane_id() == 0) base = atomicAdd(count, __popc(b));
+  base = __shfl_sync(kFull, base, 0);
+  if (pid >= 0) {
+    const int32_t at = base + __popc(b & lanemask_lt());
+    rows[at] = i;
+    ids[at] = pid;
+  }
+}
+
 }  // namespace
 
 int32_t tile_tab_stride() { return kTileTabStride; }
+
+void launch_tile_list(int32_t n, const int32_t *pid_of_row, int32_t *rows, int32_t *ids,
+                      int32_t *count, cudaStream_t s) {
+  if (n <= 0) return;
+  tile_list_kernel<<<(n + 255) / 256, 256, 0, s>>>(n, pid_of_row, rows, ids, count);
+}
 
 void launch_tile_tab(int32_t npat, const int32_t *pat_canon, const int32_t *psteps,
                      const int32_t *a_rp, const int32_t *a_col, const int32_t *b_rp,

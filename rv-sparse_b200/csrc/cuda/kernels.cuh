@@ -150,14 +150,15 @@ void launch_scatter_rows(int32_t n, const uint8_t *cls, const int32_t *class_off
 
 // ---- k_scan.cu -------------------------------------------------------------
 // row_ptr = exclusive scan of counts (n + 1 entries), *total = sum (int64).
-// Also classes every row for the numeric pass (cls, class_count).  With a
-// guard that failed, nothing is written but the tile partials.
+// Also classes every row for the numeric pass (cls, class_count); rows with
+// skip[row] >= 0 (the shift-class members) are classed empty.  With a guard
+// that failed, nothing is written but the tile partials.
 size_t scan_partials_bytes(int32_t n);
 void launch_scan_and_class(int32_t n, const int32_t *counts, const int64_t *ops,
                            const int32_t *a_rp, int32_t *row_ptr,
                            int64_t *partials, int64_t *total, uint8_t *cls,
                            int32_t *class_count, bool merge_ok, cudaStream_t s,
-                           CheckGuard guard = CheckGuard());
+                           CheckGuard guard = CheckGuard(), const int32_t *skip = nullptr);
 
 // out[i] = sum of in[0..i) as int64 (n entries), *total = sum of all.
 void launch_scan_i64(int32_t n, const int32_t *in, int64_t *out, int64_t *partials,
@@ -321,6 +322,10 @@ void launch_tile_build(int32_t n, const int32_t *pid_of_row, const int4 *desc,
                        const int32_t *b_rp, const int32_t *c_rp, int4 *tiles, int32_t *ntiles,
                        int32_t *lo_rows, int32_t *lo_ids, int32_t *lo_n, int32_t *maxima,
                        cudaStream_t s);
+// rows / ids (count at *count, zeroed by the caller): every row with
+// pid_of_row[row] >= 0 and its pattern.
+void launch_tile_list(int32_t n, const int32_t *pid_of_row, int32_t *rows, int32_t *ids,
+                      int32_t *count, cudaStream_t s);
 // Shared memory one warp of the tile kernel needs for those maxima.
 size_t tile_smem_per_warp(int32_t stage_need, int32_t a_seg, int32_t max_out,
                           int32_t *acc_rows, int32_t *work_floats, int32_t *stage_cap);
@@ -329,6 +334,49 @@ void launch_tile_numeric(const Operands &op, int32_t b_nnz, const int4 *tiles, i
                          const int4 *desc, const uint16_t *lens, const uint16_t *tab,
                          const int32_t *c_rp, float *c_val, int32_t stage_need, int32_t a_seg,
                          int32_t max_out, cudaStream_t s);
+
+// ---- k_shift.cu ------------------------------------------------------------
+// Shift classes (see k_shift.cu).  Every pass but the probe is gated by the
+// device flag *on, which the probe's decision sets, so the plan queues them
+// without a host round trip.
+int32_t shift_max_ops();
+int32_t shift_samples();
+// Keys of up to shift_samples() rows spread over A (keys: that many words)
+// and the decision *on (1: at least half of them share their key).
+void launch_shift_decide(const Operands &op, unsigned long long *keys, int32_t *on,
+                         CheckGuard guard, cudaStream_t s);
+// bcls[b_rows], rcls[a_rows]: the class (smallest verified translate) of
+// every B row and row; bkey / rkey / tkey / trow scratch, tcap a power of two
+// >= 2 max(a_rows, b_rows).
+void launch_shift_classes(const int32_t *on, const Operands &op, int32_t b_rows,
+                          const int64_t *ops, unsigned long long *bkey,
+                          unsigned long long *rkey, unsigned long long *tkey, int32_t *trow,
+                          size_t tcap, int32_t *bcls, int32_t *rcls, cudaStream_t s);
+// Patterns (classes of at least min_share rows whose canonical row has at
+// most 512 outputs): pat_of[row] / pat_canon / pat_cap / pat_m (-1: dropped)
+// / *npat (zeroed by the caller); members: pid_of_row[row] = their pattern
+// (else -1; all -1 when *on is 0), cls[row] = empty, *members += count;
+// class_count = the census of cls afterwards.
+void launch_shift_patterns(const int32_t *on, const Operands &op, const int32_t *rcls,
+                           int32_t *share, int32_t min_share, const int64_t *ops,
+                           int32_t *pat_of, int32_t *pat_canon, int32_t *pat_cap,
+                           int32_t *pat_m, int32_t *npat, int32_t cap_pat,
+                           int32_t *pid_of_row, uint8_t *cls, int32_t *members,
+                           int32_t *class_count, int num_sms, cudaStream_t s);
+// counts[member] = counts[its canonical row].
+void launch_shift_copy_counts(const int32_t *on, int32_t n, const int32_t *pid_of_row,
+                              const int32_t *rcls, int32_t *counts, cudaStream_t s);
+// Member rows' columns: the canonical row's moved by the row distance.
+void launch_shift_fill(int32_t n, const int32_t *pid_of_row, const int32_t *rcls,
+                       const int32_t *c_rp, int32_t *c_col, cudaStream_t s);
+// Maps of the canonical rows (moff[canonical] = id * shift_max_ops()).
+void launch_shift_canon_map(int32_t npat, const int32_t *pat_canon, const Operands &op,
+                            const int32_t *c_rp, const int32_t *c_col, int64_t *moff,
+                            uint16_t *map, cudaStream_t s);
+// out[0] = largest products (rounded up to 32), out[1] = largest C row over
+// the patterns with pat_m >= 0 (out zeroed by the caller).
+void launch_pat_maxima(int32_t npat, const int32_t *pat_canon, const int32_t *pat_m,
+                       const int64_t *ops, int32_t *out, cudaStream_t s);
 
 // ---- k_check.cu ------------------------------------------------------------
 // *result (initialised to ~0ull) receives min over bad rows of

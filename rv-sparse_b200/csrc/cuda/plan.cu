@@ -70,12 +70,42 @@ constexpr int kNumFill = 5 * kNumClasses;
 constexpr int kStatus = 6 * kNumClasses;
 constexpr int kLongCount = 6 * kNumClasses + 1;
 constexpr int kRetryCount = 6 * kNumClasses + 2;  // two: W1024, W2048 retry lists
-constexpr int kMiscWords = 6 * kNumClasses + 4;
+constexpr int kShiftMembers = 6 * kNumClasses + 4;  // shift-class member rows
+constexpr int kShiftNpat = 6 * kNumClasses + 5;     // shift-class pattern candidates
+constexpr int kMiscWords = 6 * kNumClasses + 6;
 // A map shared by at least this many rows gets a term table.
 constexpr int32_t kPatMinShare = 16;
 constexpr int kPatCountWords = 4 + kNumClasses;
 
 }  // namespace
+
+namespace rvsp {
+// Row tiles over one set of term-table patterns (k_tile.cu): per pattern its
+// tile table, B row lengths and shape; per row its pattern (pid, -1 for rows
+// outside the set); the tiles and the pattern rows left to the warp-per-row
+// table kernel (lo_rows / lo_ids); for the shift classes also every pattern
+// row (all_rows / all_ids, for when tiles are off).
+struct TileBuild {
+  int ready = 0;
+  int32_t n_tiles = 0, n_lo = 0, stage = 0, aseg = 0, max_out = 0, b_nnz = 0;
+  DevArray<uint16_t> tab, lens;
+  DevArray<int4> desc, tiles;
+  DevArray<int32_t> pid, lo_rows, lo_ids, counts, all_rows, all_ids;
+  void release() {
+    tab.release();
+    lens.release();
+    desc.release();
+    tiles.release();
+    pid.release();
+    lo_rows.release();
+    lo_ids.release();
+    counts.release();
+    all_rows.release();
+    all_ids.release();
+    ready = 0;
+  }
+};
+}  // namespace rvsp
 
 struct rvsp_cuda_plan {
   int device = 0;
@@ -157,16 +187,26 @@ struct rvsp_cuda_plan {
   int32_t pat_max_ops = 0, pat_max_out = 0;
   DevArray<int64_t> pat_off;
   DevArray<uint32_t> pat_rec;
-  // Row tiles of the table rows (k_tile.cu): per pattern its tile table,
-  // B row lengths and shape; per row its pattern; the tiles and the table
-  // rows left to the warp-per-row kernel (tile_lo_rows / tile_lo_ids).
+  // Row tiles of the table rows of shared maps (k_tile.cu).
   int tiles_enabled = 1;
-  int tile_ready = 0;
-  int32_t n_tiles = 0, n_tile_lo = 0;
-  int32_t tile_stage = 0, tile_aseg = 0, tile_max_out = 0, tile_b_nnz = 0;
-  DevArray<uint16_t> tile_tab, tile_lens;
-  DevArray<int4> tile_desc, tiles;
-  DevArray<int32_t> tile_pid, tile_lo_rows, tile_lo_ids, tile_counts;
+  TileBuild rt;
+  // Shift classes (k_shift.cu): rows that are translates of a canonical row.
+  // The probe sets the device flag sh_on; shift_active when the current
+  // analysis has member rows (pattern in st.pid).  Their patterns' term
+  // tables (sh_*) and row tiles (st) are built from the canonical rows' maps
+  // on the first numeric call (shift_tables 1, or -1 when that failed).
+  int shift_enabled = 1;
+  int shift_active = 0;
+  int shift_tables = 0;
+  int32_t shift_members = 0, shift_npat = 0, shift_cap_pat = 0;
+  int32_t sh_max_ops = 0, sh_max_out = 0;
+  DevArray<int32_t> sh_on, sh_trow, sh_bcls, sh_rcls, sh_share, sh_pat_of, sh_pat_canon,
+      sh_pat_cap, sh_pat_m, sh_steps, sh_counts;
+  DevArray<unsigned long long> sh_probe, sh_bkey, sh_rkey, sh_tkey;
+  DevArray<int64_t> sh_moff, sh_pat_off;
+  DevArray<uint16_t> sh_map;
+  DevArray<uint32_t> sh_rec;
+  TileBuild st;
   const int32_t *rmap_col = nullptr;
   int rmap_state = 0;
   int64_t rmap_entries = 0;
@@ -262,7 +302,7 @@ void finish_numeric_bins(rvsp_cuda_plan *p, int32_t a_rows, int32_t b_cols,
     p->num_off[c] = off;
     if (c != kEmpty_) off += p->num_count[c];
   }
-  p->num_whole = whole_matrix_class(p->num_count, a_rows);
+  p->num_whole = p->shift_active ? -1 : whole_matrix_class(p->num_count, a_rows);
   if (p->num_whole < 0) {
     PhaseScope ph(p, s, RVSP_PHASE_SCAN);
     launch_class_offsets(misc + kNumCount, misc + kNumOff, s);
@@ -372,14 +412,17 @@ void rvsp_cuda_plan_destroy(rvsp_cuda_plan_t p) {
   p->pat_counts.release();
   p->pat_off.release();
   p->pat_rec.release();
-  p->tile_tab.release();
-  p->tile_lens.release();
-  p->tile_desc.release();
-  p->tiles.release();
-  p->tile_pid.release();
-  p->tile_lo_rows.release();
-  p->tile_lo_ids.release();
-  p->tile_counts.release();
+  p->rt.release();
+  p->st.release();
+  for (auto *a : {&p->sh_on, &p->sh_trow, &p->sh_bcls, &p->sh_rcls, &p->sh_share,
+                  &p->sh_pat_of, &p->sh_pat_canon, &p->sh_pat_cap, &p->sh_pat_m,
+                  &p->sh_steps, &p->sh_counts})
+    a->release();
+  for (auto *a : {&p->sh_probe, &p->sh_bkey, &p->sh_rkey, &p->sh_tkey}) a->release();
+  p->sh_moff.release();
+  p->sh_pat_off.release();
+  p->sh_map.release();
+  p->sh_rec.release();
   p->ops.release();
   p->cls.release();
   p->cls_spec.release();
@@ -411,6 +454,35 @@ void rvsp_cuda_plan_destroy(rvsp_cuda_plan_t p) {
 }
 
 namespace {
+
+// Matrices of at least this many rows run the shift-class probe.
+constexpr int32_t kShiftMinRows = 4096;
+
+// Scratch of the shift-class analysis (k_shift.cu).  The key table is a
+// power of two of at least twice the rows; a larger one kept from before is
+// used whole.
+cudaError_t reserve_shift(rvsp_cuda_plan *p, int32_t a_rows, int32_t b_rows) {
+  const size_t n = static_cast<size_t>(a_rows), nb = static_cast<size_t>(b_rows);
+  size_t tcap = 64;
+  while (tcap < 2 * (n > nb ? n : nb)) tcap <<= 1;
+  p->shift_cap_pat = static_cast<int32_t>(n / kPatMinShare + 1);
+  const size_t cp = static_cast<size_t>(p->shift_cap_pat);
+  cudaError_t e = p->sh_on.reserve(1);
+  if (e == cudaSuccess) e = p->sh_probe.reserve(size_t(shift_samples()));
+  if (e == cudaSuccess) e = p->sh_bkey.reserve(nb);
+  if (e == cudaSuccess) e = p->sh_rkey.reserve(n);
+  if (e == cudaSuccess) e = p->sh_tkey.reserve(tcap);
+  if (e == cudaSuccess) e = p->sh_trow.reserve(p->sh_tkey.cap);
+  if (e == cudaSuccess) e = p->sh_bcls.reserve(nb);
+  if (e == cudaSuccess) e = p->sh_rcls.reserve(n);
+  if (e == cudaSuccess) e = p->sh_share.reserve(n);
+  if (e == cudaSuccess) e = p->sh_pat_of.reserve(n);
+  if (e == cudaSuccess) e = p->st.pid.reserve(n);
+  if (e == cudaSuccess) e = p->sh_pat_canon.reserve(cp);
+  if (e == cudaSuccess) e = p->sh_pat_cap.reserve(cp);
+  if (e == cudaSuccess) e = p->sh_pat_m.reserve(cp);
+  return e;
+}
 
 // The structure checks rvsp_cuda_symbolic_checked folds into the symbolic
 // pass: A always, B unless it is A.
@@ -519,6 +591,18 @@ rvsp_status_t symbolic_impl(rvsp_cuda_plan_t p, cudaStream_t s, int32_t a_rows,
   }
   int32_t *misc = p->misc.p;
   cudaMemsetAsync(misc, 0, kMiscWords * sizeof(int32_t), s);
+  CheckGuard guard;
+  if (chk) {
+    guard.w = p->check.p;
+    guard.n = chk->check_b ? 2 : 1;
+  }
+  p->shift_active = 0;
+  p->shift_tables = 0;
+  p->shift_members = 0;
+  p->shift_npat = 0;
+  const bool shift = p->shift_enabled && a_rows >= kShiftMinRows &&
+                     reserve_shift(p, a_rows, b_rows) == cudaSuccess;
+  if (!shift) cudaGetLastError();
   {
     PhaseScope ph(p, s, RVSP_PHASE_ROWSTATS);
     launch_rowstats(op, p->ops.p, p->cls.p, p->counts.p, misc + kSymCount,
@@ -526,7 +610,22 @@ rvsp_status_t symbolic_impl(rvsp_cuda_plan_t p, cudaStream_t s, int32_t a_rows,
     launch_rowstats_long(op, p->long_rows.p, misc + kLongCount, p->ops.p, p->cls.p,
                          p->counts.p, misc + kSymCount, p->num_sms, s);
     ph.launches = 2;
+    if (shift) {
+      // Shift classes: the probe decides on the device; every pass after it
+      // is gated by that decision, so no host round trip is added.  Member
+      // rows leave the symbolic classes (census recounted).
+      launch_shift_decide(op, p->sh_probe.p, p->sh_on.p, guard, s);
+      launch_shift_classes(p->sh_on.p, op, b_rows, p->ops.p, p->sh_bkey.p, p->sh_rkey.p,
+                           p->sh_tkey.p, p->sh_trow.p, p->sh_tkey.cap, p->sh_bcls.p,
+                           p->sh_rcls.p, s);
+      launch_shift_patterns(p->sh_on.p, op, p->sh_rcls.p, p->sh_share.p, kPatMinShare,
+                            p->ops.p, p->sh_pat_of.p, p->sh_pat_canon.p, p->sh_pat_cap.p,
+                            p->sh_pat_m.p, misc + kShiftNpat, p->shift_cap_pat, p->st.pid.p,
+                            p->cls.p, misc + kShiftMembers, misc + kSymCount, p->num_sms, s);
+      ph.launches += 20;
+    }
   }
+  const int32_t *skip = shift ? p->st.pid.p : nullptr;
   // Merge-class rows need no host-side census: their symbolic pass (one
   // launch per merge class over all rows, each skipping the other classes)
   // and the scan are queued at once, behind the check verdict, so a product
@@ -535,11 +634,6 @@ rvsp_status_t symbolic_impl(rvsp_cuda_plan_t p, cudaStream_t s, int32_t a_rows,
   // scan writes its numeric classes to cls_spec: the census-driven pass
   // still needs the symbolic classes in cls.
   const bool spec = op.merge_ok;
-  CheckGuard guard;
-  if (chk) {
-    guard.w = p->check.p;
-    guard.n = chk->check_b ? 2 : 1;
-  }
   if (spec) {
     {
       PhaseScope ph(p, s, RVSP_PHASE_SYMBOLIC);
@@ -548,16 +642,17 @@ rvsp_status_t symbolic_impl(rvsp_cuda_plan_t p, cudaStream_t s, int32_t a_rows,
     }
     {
       PhaseScope ph(p, s, RVSP_PHASE_SCAN);
+      if (shift)
+        launch_shift_copy_counts(p->sh_on.p, a_rows, p->st.pid.p, p->sh_rcls.p, p->counts.p, s);
       launch_scan_and_class(a_rows, p->counts.p, p->ops.p, a_row_ptr, c_row_ptr,
                             p->partials.p, p->total.p, p->cls_spec.p, misc + kNumCount,
-                            op.merge_ok, s, guard);
-      ph.launches = 3;
+                            op.merge_ok, s, guard, skip);
+      ph.launches = shift ? 4 : 3;
     }
     cudaMemcpyAsync(p->h_misc, misc, kMiscWords * sizeof(int32_t), cudaMemcpyDeviceToHost, s);
     cudaMemcpyAsync(p->h_total, p->total.p, sizeof(int64_t), cudaMemcpyDeviceToHost, s);
   } else {
-    cudaMemcpyAsync(p->h_misc, misc, kNumClasses * sizeof(int32_t),
-                    cudaMemcpyDeviceToHost, s);
+    cudaMemcpyAsync(p->h_misc, misc, kMiscWords * sizeof(int32_t), cudaMemcpyDeviceToHost, s);
   }
   if (chk)
     cudaMemcpyAsync(p->h_check, p->check.p, 2 * sizeof(unsigned long long),
@@ -566,6 +661,12 @@ rvsp_status_t symbolic_impl(rvsp_cuda_plan_t p, cudaStream_t s, int32_t a_rows,
   if (e != cudaSuccess) return map_cuda(e);
   if (chk && (p->h_check[0] != ~0ull || (chk->check_b && p->h_check[1] != ~0ull)))
     return RVSP_ERROR_INVALID_CSR;  // not canonical: nothing ran on it
+  if (shift) {
+    p->shift_members = p->h_misc[kShiftMembers];
+    p->shift_npat = p->h_misc[kShiftNpat] < p->shift_cap_pat ? p->h_misc[kShiftNpat]
+                                                              : p->shift_cap_pat;
+    p->shift_active = p->shift_members > 0;
+  }
   int32_t sym_off[kNumClasses];
   int32_t off = 0;
   bool rest = !spec;  // classes left for the census-driven pass
@@ -642,7 +743,7 @@ cudaError_t symbolic_rest(rvsp_cuda_plan *p, cudaStream_t s, const Operands &op,
     };
     // whole >= 0 is never a merge class here when merge_done (a class
     // outside them is non-empty).
-    const int whole = whole_matrix_class(p->sym_count, a_rows);
+    const int whole = p->shift_active ? -1 : whole_matrix_class(p->sym_count, a_rows);
     if (whole >= 0) {
       ph.launches = launch_class(whole, nullptr, a_rows);
     } else {
@@ -660,10 +761,16 @@ cudaError_t symbolic_rest(rvsp_cuda_plan *p, cudaStream_t s, const Operands &op,
     cudaMemsetAsync(misc + kNumCount, 0, kNumClasses * sizeof(int32_t), s);
   {
     PhaseScope ph(p, s, RVSP_PHASE_SCAN);
+    const int32_t *skip = nullptr;
+    if (p->shift_active) {
+      launch_shift_copy_counts(p->sh_on.p, a_rows, p->st.pid.p, p->sh_rcls.p, p->counts.p, s);
+      skip = p->st.pid.p;
+    }
     launch_scan_and_class(a_rows, p->counts.p, p->ops.p, a_row_ptr, c_row_ptr,
                           p->partials.p,
-                          p->total.p, p->cls.p, misc + kNumCount, op.merge_ok, s);
-    ph.launches = 3;
+                          p->total.p, p->cls.p, misc + kNumCount, op.merge_ok, s,
+                          CheckGuard(), skip);
+    ph.launches = skip ? 4 : 3;
   }
   cudaMemcpyAsync(p->h_misc + kNumCount, misc + kNumCount,
                   (kMiscWords - kNumCount) * sizeof(int32_t), cudaMemcpyDeviceToHost, s);
@@ -690,6 +797,28 @@ rvsp_status_t rvsp_cuda_learned_symbolic(
   p->learned = 0;
   p->rmap_state = 0;
   p->rmap_col = nullptr;
+  p->shift_active = 0;
+  p->shift_tables = 0;
+  p->shift_members = 0;
+  if (p->shift_enabled && a_rows >= kShiftMinRows) {
+    // Rows that are translates of a few canonical rows need no prediction:
+    // their structure comes from the canonical rows.  When the probe finds
+    // them common, the analysis is the shift-class one (symbolic_impl).
+    if (reserve_shift(p, a_rows, b_rows) == cudaSuccess) {
+      const Operands pop{a_rows, b_cols, a_row_ptr, a_col_idx, nullptr,
+                         b_row_ptr, b_col_idx, nullptr, false};
+      launch_shift_decide(pop, p->sh_probe.p, p->sh_on.p, CheckGuard(), s);
+      cudaError_t e = cudaMemcpyAsync(p->h_misc, p->sh_on.p, sizeof(int32_t),
+                                      cudaMemcpyDeviceToHost, s);
+      if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+      if (e != cudaSuccess) return map_cuda(e);
+      if (p->h_misc[0])
+        return symbolic_impl(p, s, a_rows, b_rows, b_cols, a_row_ptr, a_col_idx, b_row_ptr,
+                             b_col_idx, c_row_ptr, c_nnz_out, nullptr);
+    } else {
+      cudaGetLastError();
+    }
+  }
   const size_t n = static_cast<size_t>(a_rows);
   cudaError_t e = p->ops.reserve(n);
   if (e == cudaSuccess) e = p->cls.reserve(n);
@@ -892,9 +1021,24 @@ rvsp_status_t rvsp_cuda_plan_set_row_tiles(rvsp_cuda_plan_t p, int32_t enable) {
   return RVSP_SUCCESS;
 }
 
+rvsp_status_t rvsp_cuda_plan_set_shift_classes(rvsp_cuda_plan_t p, int32_t enable) {
+  if (!p) return RVSP_ERROR_NULL_POINTER;
+  if (enable != 0 && enable != 1) return RVSP_ERROR_INVALID_ARGUMENT;
+  p->shift_enabled = enable;
+  return RVSP_SUCCESS;
+}
+
+int32_t rvsp_cuda_plan_shift_rows(rvsp_cuda_plan_t p) {
+  return (p && p->analysed && p->shift_active) ? p->shift_members : 0;
+}
+
 int32_t rvsp_cuda_plan_tiled_rows(rvsp_cuda_plan_t p) {
-  if (!p || !p->tile_ready || !p->tiles_enabled) return 0;
-  return p->n_pat_rows - p->n_tile_lo;
+  if (!p || !p->tiles_enabled) return 0;
+  int32_t n = 0;
+  if (p->rmap_state == 1 && p->pat_ready && p->rt.ready) n += p->n_pat_rows - p->rt.n_lo;
+  if (p->shift_active && p->shift_tables == 1 && p->st.ready)
+    n += p->shift_members - p->st.n_lo;
+  return n;
 }
 
 int32_t rvsp_cuda_plan_overflow_rows(rvsp_cuda_plan_t p) {
@@ -913,53 +1057,66 @@ constexpr size_t kReuseMapMaxBytes = size_t(24) << 30;
 
 // The tile tables may take at most this much device memory.
 constexpr size_t kTileTablesMaxBytes = size_t(256) << 20;
-constexpr int kTileCountWords = 8;  // ntiles, leftovers, 3 maxima, spare
+constexpr int kTileCountWords = 8;  // ntiles, leftovers, 3 maxima, list count, spare
 
-// Row tiles of the table rows (k_tile.cu): the per-pattern tile tables, then
-// tiles over chunks of 32 consecutive rows and the leftover list.  Leaves
-// tile_ready 0 (every table row on the warp-per-row kernel) when nothing is
-// tiled or the tile kernel's shared memory would not fit.  Synchronizes `s`.
+// Row tiles of a set of table patterns (k_tile.cu): the per-pattern tile
+// tables (from each pattern's canonical row map: moff[row], map), then tiles
+// over chunks of 32 consecutive rows of tb.pid (the pattern of each row, -1
+// elsewhere, filled by the caller) and the leftover list.  Leaves tb.ready 0
+// (every pattern row on the warp-per-row kernel) when nothing is tiled.
+// With `required` (the shift classes, whose rows have no other path) a
+// failed allocation is an error, and the list of every pattern row is built
+// too.  Synchronizes `s`.
 cudaError_t build_row_tiles(rvsp_cuda_plan *p, cudaStream_t s, const Operands &op,
-                            const int32_t *c_rp, int32_t npat) {
+                            const int32_t *c_rp, int32_t npat, const int32_t *pat_canon,
+                            const int32_t *psteps, const int64_t *moff, const uint16_t *map,
+                            TileBuild &tb, bool required = false) {
+  tb.ready = 0;
+  tb.n_lo = 0;
   const size_t n = static_cast<size_t>(p->a_rows);
   const size_t tab_entries = size_t(npat) * size_t(tile_tab_stride());
-  if (p->tile_tab.reserve(tab_entries) != cudaSuccess ||
-      p->tile_lens.reserve(size_t(npat) * 32) != cudaSuccess ||
-      p->tile_desc.reserve(size_t(npat)) != cudaSuccess ||
-      p->tiles.reserve((n + 31) / 32) != cudaSuccess ||
-      p->tile_lo_rows.reserve(n) != cudaSuccess || p->tile_lo_ids.reserve(n) != cudaSuccess ||
-      p->tile_counts.reserve(kTileCountWords) != cudaSuccess) {
-    cudaGetLastError();
-    return cudaSuccess;
+  if (tb.tab.reserve(tab_entries) != cudaSuccess ||
+      tb.lens.reserve(size_t(npat) * 32) != cudaSuccess ||
+      tb.desc.reserve(size_t(npat)) != cudaSuccess ||
+      tb.tiles.reserve((n + 31) / 32) != cudaSuccess ||
+      tb.lo_rows.reserve(n) != cudaSuccess || tb.lo_ids.reserve(n) != cudaSuccess ||
+      tb.counts.reserve(kTileCountWords) != cudaSuccess ||
+      (required && (tb.all_rows.reserve(n) != cudaSuccess ||
+                    tb.all_ids.reserve(n) != cudaSuccess))) {
+    const cudaError_t err = cudaGetLastError();
+    return required ? err : cudaSuccess;
   }
   int32_t b_nnz = 0;
   cudaError_t e = cudaMemcpyAsync(&b_nnz, op.b_rp + p->b_rows, sizeof(int32_t),
                                   cudaMemcpyDeviceToHost, s);
   if (e != cudaSuccess) return e;
-  cudaMemsetAsync(p->tile_counts.p, 0, kTileCountWords * sizeof(int32_t), s);
-  launch_tile_tab(npat, p->pat_canon.p, p->pat_steps.p, op.a_rp, op.a_col, op.b_rp, c_rp,
-                  p->rmap_off.p, p->rmap.p, p->tile_tab.p, p->tile_lens.p, p->tile_desc.p, s);
-  launch_tile_build(p->a_rows, p->tile_pid.p, p->tile_desc.p, p->tile_lens.p, op.a_rp,
-                    op.a_col, op.b_rp, c_rp, p->tiles.p, p->tile_counts.p,
-                    p->tile_lo_rows.p, p->tile_lo_ids.p, p->tile_counts.p + 1,
-                    p->tile_counts.p + 2, s);
+  cudaMemsetAsync(tb.counts.p, 0, kTileCountWords * sizeof(int32_t), s);
+  if (required)
+    launch_tile_list(p->a_rows, tb.pid.p, tb.all_rows.p, tb.all_ids.p, tb.counts.p + 5, s);
+  launch_tile_tab(npat, pat_canon, psteps, op.a_rp, op.a_col, op.b_rp, c_rp, moff, map,
+                  tb.tab.p, tb.lens.p, tb.desc.p, s);
+  launch_tile_build(p->a_rows, tb.pid.p, tb.desc.p, tb.lens.p, op.a_rp, op.a_col, op.b_rp,
+                    c_rp, tb.tiles.p, tb.counts.p, tb.lo_rows.p, tb.lo_ids.p,
+                    tb.counts.p + 1, tb.counts.p + 2, s);
   int32_t h[kTileCountWords] = {};
-  e = cudaMemcpyAsync(h, p->tile_counts.p, sizeof(h), cudaMemcpyDeviceToHost, s);
+  e = cudaMemcpyAsync(h, tb.counts.p, sizeof(h), cudaMemcpyDeviceToHost, s);
   if (e == cudaSuccess) e = cudaStreamSynchronize(s);
   if (e != cudaSuccess) return e;
+  tb.n_lo = h[1];
   if (h[0] <= 0) return cudaSuccess;
   int32_t acc_rows = 0, work = 0, stage_cap = 0;
   const size_t per_warp = tile_smem_per_warp(h[2], h[3], h[4], &acc_rows, &work, &stage_cap);
   int dev_max = 0;
   cudaDeviceGetAttribute(&dev_max, cudaDevAttrMaxSharedMemoryPerBlockOptin, p->device);
-  if (per_warp * kTileKernelWarps > size_t(dev_max)) return cudaSuccess;
-  p->n_tiles = h[0];
-  p->n_tile_lo = h[1];
-  p->tile_stage = h[2];
-  p->tile_aseg = h[3];
-  p->tile_max_out = h[4];
-  p->tile_b_nnz = b_nnz;
-  p->tile_ready = 1;
+  // (cannot happen: the tile limits keep one block under 140 KB)
+  if (per_warp * kTileKernelWarps > size_t(dev_max))
+    return required ? cudaErrorInvalidValue : cudaSuccess;
+  tb.n_tiles = h[0];
+  tb.stage = h[2];
+  tb.aseg = h[3];
+  tb.max_out = h[4];
+  tb.b_nnz = b_nnz;
+  tb.ready = 1;
   return cudaSuccess;
 }
 
@@ -1023,9 +1180,9 @@ cudaError_t build_term_tables(rvsp_cuda_plan *p, cudaStream_t s, const Operands 
   const size_t tab_entries = size_t(npat) * size_t(tile_tab_stride());
   const bool tiles_fit = p->tiles_enabled &&
                          tab_entries * sizeof(uint16_t) <= kTileTablesMaxBytes &&
-                         p->tile_pid.reserve(n) == cudaSuccess;
+                         p->rt.pid.reserve(n) == cudaSuccess;
   if (!tiles_fit) cudaGetLastError();
-  if (tiles_fit) cudaMemsetAsync(p->tile_pid.p, 0xff, n * sizeof(int32_t), s);
+  if (tiles_fit) cudaMemsetAsync(p->rt.pid.p, 0xff, n * sizeof(int32_t), s);
   int32_t off = 0;
   for (int c = kEmpty_ + 1; c < kNumClasses; ++c) {
     p->res_off[c] = off;
@@ -1035,7 +1192,7 @@ cudaError_t build_term_tables(rvsp_cuda_plan *p, cudaStream_t s, const Operands 
                      whole ? p->a_rows : p->num_count[c], p->rmap_canon.p, p->pat_of.p,
                      p->pat_steps.p, op.a_rp, op.a_col, op.b_rp, p->pat_rows.p,
                      p->pat_ids.p, p->pat_counts.p + 1, p->res_rows.p + off,
-                     p->pat_counts.p + 2 + c, tiles_fit ? p->tile_pid.p : nullptr, s);
+                     p->pat_counts.p + 2 + c, tiles_fit ? p->rt.pid.p : nullptr, s);
     off += whole ? p->a_rows : p->num_count[c];
   }
   int32_t h[kPatCountWords] = {};
@@ -1048,12 +1205,82 @@ cudaError_t build_term_tables(rvsp_cuda_plan *p, cudaStream_t s, const Operands 
   p->pat_max_ops = h[2 + kNumClasses];
   p->pat_max_out = h[3 + kNumClasses];
   p->pat_ready = 1;
-  p->tile_ready = 0;
+  p->rt.ready = 0;
   if (tiles_fit && p->n_pat_rows > 0) {
-    e = build_row_tiles(p, s, op, c_rp, npat);
+    e = build_row_tiles(p, s, op, c_rp, npat, p->pat_canon.p, p->pat_steps.p, p->rmap_off.p,
+                        p->rmap.p, p->rt);
     if (e != cudaSuccess) return e;
   }
   return cudaSuccess;
+}
+
+// Term tables and row tiles of the shift-class patterns, from the canonical
+// rows' structure in C (c_rp, c_col): their maps (binary search in C's row),
+// the warp-per-row tables (k_pattern.cu) and the row tiles of the member
+// rows (k_tile.cu).  Every member row is then in a tile or on the leftover
+// list.  Synchronizes `s`.
+cudaError_t build_shift_tables(rvsp_cuda_plan *p, cudaStream_t s, const Operands &op,
+                               const int32_t *c_rp, const int32_t *c_col) {
+  p->shift_tables = -1;
+  const int32_t npat = p->shift_npat;
+  if (npat <= 0) return cudaErrorInvalidValue;
+  const size_t n = static_cast<size_t>(p->a_rows);
+  cudaError_t e = p->sh_moff.reserve(n);
+  if (e == cudaSuccess) e = p->sh_map.reserve(size_t(npat) * size_t(shift_max_ops()));
+  if (e == cudaSuccess) e = p->sh_pat_off.reserve(size_t(npat));
+  if (e == cudaSuccess) e = p->sh_steps.reserve(size_t(npat));
+  if (e == cudaSuccess) e = p->sh_counts.reserve(4);
+  if (e != cudaSuccess) return e;
+  launch_shift_canon_map(npat, p->sh_pat_canon.p, op, c_rp, c_col, p->sh_moff.p, p->sh_map.p,
+                         s);
+  launch_scan_i64(npat, p->sh_pat_cap.p, p->sh_pat_off.p, p->partials.p, p->total.p, s);
+  cudaMemsetAsync(p->sh_counts.p, 0, 4 * sizeof(int32_t), s);
+  launch_pat_maxima(npat, p->sh_pat_canon.p, p->sh_pat_m.p, p->ops.p, p->sh_counts.p, s);
+  int64_t records = 0;
+  int32_t maxima[4] = {};
+  e = cudaMemcpyAsync(&records, p->total.p, sizeof(int64_t), cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(maxima, p->sh_counts.p, sizeof(maxima), cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) return e;
+  e = p->sh_rec.reserve(size_t(records > 0 ? records : 1));
+  if (e != cudaSuccess) return e;
+  launch_pat_build(npat, p->sh_pat_canon.p, op.a_rp, op.a_col, op.b_rp, c_rp, p->sh_moff.p,
+                   p->sh_map.p, p->sh_pat_off.p, p->sh_pat_cap.p, p->sh_rec.p, p->sh_steps.p,
+                   s);
+  p->sh_max_ops = maxima[0];
+  p->sh_max_out = maxima[1];
+  e = build_row_tiles(p, s, op, c_rp, npat, p->sh_pat_canon.p, p->sh_steps.p, p->sh_moff.p,
+                      p->sh_map.p, p->st, true);
+  if (e != cudaSuccess) return e;
+  p->shift_tables = 1;
+  return cudaSuccess;
+}
+
+// Values of the shift-class member rows (tables built): row tiles, then the
+// members no tile took through the warp-per-row table kernel; every member
+// through that kernel when tiles are off.
+int launch_shift_numeric(rvsp_cuda_plan *p, cudaStream_t s, const Operands &op,
+                         const int32_t *c_rp, float *c_val) {
+  int launches = 0;
+  if (p->st.ready && p->tiles_enabled) {
+    launch_tile_numeric(op, p->st.b_nnz, p->st.tiles.p, p->st.n_tiles, p->st.desc.p,
+                        p->st.lens.p, p->st.tab.p, c_rp, c_val, p->st.stage, p->st.aseg,
+                        p->st.max_out, s);
+    ++launches;
+    if (p->st.n_lo > 0) {
+      launch_pat_numeric(op, p->ops.p, p->st.lo_rows.p, p->st.lo_ids.p, p->st.n_lo, c_rp,
+                         c_val, p->sh_pat_off.p, p->sh_steps.p, p->sh_rec.p, p->sh_max_ops,
+                         p->sh_max_out, s);
+      ++launches;
+    }
+  } else {
+    launch_pat_numeric(op, p->ops.p, p->st.all_rows.p, p->st.all_ids.p, p->shift_members,
+                       c_rp, c_val, p->sh_pat_off.p, p->sh_steps.p, p->sh_rec.p,
+                       p->sh_max_ops, p->sh_max_out, s);
+    ++launches;
+  }
+  return launches;
 }
 
 cudaError_t build_reuse_map(rvsp_cuda_plan *p, cudaStream_t s, const Operands &op,
@@ -1250,13 +1477,13 @@ rvsp_status_t rvsp_cuda_numeric(rvsp_cuda_plan_t p, void *stream,
   {
     PhaseScope ph(p, s, RVSP_PHASE_NUMERIC);
     if (use_map && p->pat_ready && p->n_pat_rows > 0) {
-      if (p->tile_ready && p->tiles_enabled) {
-        launch_tile_numeric(op, p->tile_b_nnz, p->tiles.p, p->n_tiles, p->tile_desc.p,
-                            p->tile_lens.p, p->tile_tab.p, c_row_ptr, c_values, p->tile_stage,
-                            p->tile_aseg, p->tile_max_out, s);
+      if (p->rt.ready && p->tiles_enabled) {
+        launch_tile_numeric(op, p->rt.b_nnz, p->rt.tiles.p, p->rt.n_tiles, p->rt.desc.p,
+                            p->rt.lens.p, p->rt.tab.p, c_row_ptr, c_values, p->rt.stage,
+                            p->rt.aseg, p->rt.max_out, s);
         ph.launches += 1;
-        if (p->n_tile_lo > 0) {
-          launch_pat_numeric(op, p->ops.p, p->tile_lo_rows.p, p->tile_lo_ids.p, p->n_tile_lo,
+        if (p->rt.n_lo > 0) {
+          launch_pat_numeric(op, p->ops.p, p->rt.lo_rows.p, p->rt.lo_ids.p, p->rt.n_lo,
                              c_row_ptr, c_values, p->pat_off.p, p->pat_steps.p, p->pat_rec.p,
                              p->pat_max_ops, p->pat_max_out, s);
           ph.launches += 1;
@@ -1287,6 +1514,25 @@ rvsp_status_t rvsp_cuda_numeric(rvsp_cuda_plan_t p, void *stream,
                              p->misc.p + kStatus, p->num_sms, s);
       ph.launches += 1;
     }
+  }
+  if (p->shift_active) {
+    // Shift-class members: columns by translation of their canonical rows
+    // (filled above), values from the canonical rows' term tables.
+    if (fill) {
+      PhaseScope ph(p, s, RVSP_PHASE_NUMERIC);
+      launch_shift_fill(p->a_rows, p->st.pid.p, p->sh_rcls.p, c_row_ptr, c_col_idx, s);
+      ph.launches = 1;
+    }
+    if (p->shift_tables == 0) {
+      cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+      if (cudaStreamIsCapturing(s, &cap) != cudaSuccess || cap != cudaStreamCaptureStatusNone)
+        return RVSP_ERROR_INVALID_ARGUMENT;  // building synchronizes: not under capture
+      const cudaError_t e = build_shift_tables(p, s, op, c_row_ptr, c_col_idx);
+      if (e != cudaSuccess) return map_cuda(e);
+    }
+    if (p->shift_tables != 1) return RVSP_ERROR_DEVICE;
+    PhaseScope ph(p, s, RVSP_PHASE_NUMERIC);
+    ph.launches = launch_shift_numeric(p, s, op, c_row_ptr, c_values);
   }
   return map_cuda(cudaGetLastError());
 }

@@ -37,6 +37,7 @@ struct rvsp_spgemm_descr {
     float capacity_scale;  /* learned algorithm only */
     int32_t merge_policy;
     int32_t row_tiles;
+    int32_t shift_classes;
 
     int32_t c_nnz;
     rvsp_dbuf_t c_row_ptr; /* analysed row pointers, device, a_rows + 1 */
@@ -71,6 +72,7 @@ rvsp_status_t rvsp_spgemm_descr_create(rvsp_spgemm_descr_t *descr)
     d->mem = RVSP_MEM_HOST;
     d->capacity_scale = 1.15f;
     d->row_tiles = 1;
+    d->shift_classes = 1;
     *descr = d;
     return RVSP_SUCCESS;
 }
@@ -113,6 +115,24 @@ rvsp_status_t rvsp_spgemm_set_row_tiles(rvsp_spgemm_descr_t d, int32_t enable)
         return RVSP_ERROR_INVALID_ARGUMENT;
     d->row_tiles = enable;
     return d->plan ? rvsp_cuda_plan_set_row_tiles(d->plan, enable) : RVSP_SUCCESS;
+}
+
+rvsp_status_t rvsp_spgemm_set_shift_classes(rvsp_spgemm_descr_t d, int32_t enable)
+{
+    if (d == NULL)
+        return RVSP_ERROR_NULL_POINTER;
+    if (enable != 0 && enable != 1)
+        return RVSP_ERROR_INVALID_ARGUMENT;
+    d->shift_classes = enable;
+    return d->plan ? rvsp_cuda_plan_set_shift_classes(d->plan, enable) : RVSP_SUCCESS;
+}
+
+rvsp_status_t rvsp_spgemm_get_shift_rows(rvsp_spgemm_descr_t d, int32_t *n_out)
+{
+    if (d == NULL || n_out == NULL)
+        return RVSP_ERROR_NULL_POINTER;
+    *n_out = d->plan ? rvsp_cuda_plan_shift_rows(d->plan) : 0;
+    return RVSP_SUCCESS;
 }
 
 rvsp_status_t rvsp_spgemm_get_tiled_rows(rvsp_spgemm_descr_t d, int32_t *n_out)
@@ -250,6 +270,8 @@ static rvsp_status_t ensure_device(rvsp_spgemm_descr_t d)
     if (!d->user_stream)
         d->stream = d->own_stream;
     rvsp_status_t st = rvsp_cuda_plan_set_row_tiles(d->plan, d->row_tiles);
+    if (st == RVSP_SUCCESS)
+        st = rvsp_cuda_plan_set_shift_classes(d->plan, d->shift_classes);
     if (st != RVSP_SUCCESS)
         return st;
     return rvsp_cuda_plan_set_merge_policy(d->plan, d->merge_policy);

@@ -151,6 +151,10 @@ SIGNATURES = {
     "rvsp_spgemm_get_tiled_rows": (_int, [_vp, _P(_i32)]),
     "rvsp_cuda_plan_set_row_tiles": (_int, [_vp, _i32]),
     "rvsp_cuda_plan_tiled_rows": (_i32, [_vp]),
+    "rvsp_cuda_plan_set_shift_classes": (_int, [_vp, _i32]),
+    "rvsp_cuda_plan_shift_rows": (_i32, [_vp]),
+    "rvsp_spgemm_set_shift_classes": (_int, [_vp, _i32]),
+    "rvsp_spgemm_get_shift_rows": (_int, [_vp, _P(_i32)]),
     "rvsp_spgemm_set_model": (_int, [_vp, _vp]),
     "rvsp_spgemm_set_capacity_scale": (_int, [_vp, C.c_float]),
     "rvsp_spgemm_get_overflow_rows": (_int, [_vp, _P(_i32)]),

@@ -299,6 +299,16 @@ class Descriptor:
         """Row tiles for numeric-only computes (on by default)."""
         L.check(self.lib.rvsp_spgemm_set_row_tiles(self.h, int(bool(enable))), "set_row_tiles")
 
+    def set_shift_classes(self, enable: bool):
+        """Shift classes in work_estimation (on by default)."""
+        L.check(self.lib.rvsp_spgemm_set_shift_classes(self.h, int(bool(enable))),
+                "set_shift_classes")
+
+    def shift_rows(self) -> int:
+        n = C.c_int32()
+        L.check(self.lib.rvsp_spgemm_get_shift_rows(self.h, C.byref(n)), "shift_rows")
+        return n.value
+
     def tiled_rows(self) -> int:
         n = C.c_int32()
         L.check(self.lib.rvsp_spgemm_get_tiled_rows(self.h, C.byref(n)), "tiled_rows")
