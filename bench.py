@@ -620,6 +620,7 @@ def run_batch(args, world, rank, local):
     ms_per_step = total_ms / args.steps
     value = world * flops * args.steps / (total_ms * 1e-3) / 1e9
     stats = b.stats()
+    tuning = b.tuning()
     peak, peak_kind = measured_peaks()
     achieved = alg_bytes / (ms_per_step * 1e-3) / 1e9
 
@@ -642,7 +643,9 @@ def run_batch(args, world, rank, local):
         hprods = [(CSR(A.rows, A.cols, pinned(A.row_ptr), pinned(A.col_idx), pinned(A.values)),
                    CSR(B.rows, B.cols, pinned(B.row_ptr), pinned(B.col_idx), pinned(B.values)))
                   for A, B in prods]
-        hb = Batch(memory=L.MEM_HOST, merge_policy=stats["merge_policy"])
+        hb = Batch(memory=L.MEM_HOST, merge_policy=stats["merge_policy"],
+                   persistent=(tuning["persistent_merge_rows"],
+                               tuning["persistent_blocks_per_sm"]))
         for A, B in hprods:
             hb.add(A, B)
         hb.work_estimation()
@@ -708,6 +711,7 @@ def run_batch(args, world, rank, local):
                        "flops_per_step": flops, "algorithmic_bytes_per_step": alg_bytes,
                        "groups": stats["groups"],
                        "merge_policy_autotuned": stats["merge_policy"],
+                       "numeric_shape_autotuned": tuning,
                        "graph_nodes": stats["graph_nodes"],
                        "analysis_ms": analysis_ms, "first_fill_ms": fill_ms,
                        "first_product_gflops": flops / ((analysis_ms + fill_ms) * 1e-3) / 1e9,

@@ -264,7 +264,9 @@ rvsp_status_t rvsp_spgemm_csr_device(const rvsp_csr_matrix_t *A,
  * replayed after.  Results are bit-identical to computing each product on
  * its own.  With autotune on, work_estimation times the merge-accumulator
  * policies (automatic, never, always) on the batch's own rows and keeps the
- * fastest. */
+ * fastest, then times the numeric-only pass as one launch per row class and
+ * as the persistent pass (rvsp_cuda_plan_set_persistent) with several bin
+ * sizes and occupancies, and keeps the fastest shape. */
 typedef struct rvsp_spgemm_batch *rvsp_spgemm_batch_t;
 
 rvsp_status_t rvsp_spgemm_batch_create(rvsp_spgemm_batch_t *batch);
@@ -276,6 +278,20 @@ rvsp_status_t rvsp_spgemm_batch_set_memory_space(rvsp_spgemm_batch_t batch,
 rvsp_status_t rvsp_spgemm_batch_set_stream(rvsp_spgemm_batch_t batch, void *stream);
 rvsp_status_t rvsp_spgemm_batch_set_autotune(rvsp_spgemm_batch_t batch, int enable);
 rvsp_status_t rvsp_spgemm_batch_set_merge_policy(rvsp_spgemm_batch_t batch, int32_t policy);
+/* Numeric-only shape of the batch's repeats (see rvsp_cuda_plan_set_persistent):
+ * merge_rows 0 for one launch per row class, else merge rows per bin of the
+ * persistent pass (a multiple of 32, at most 256), with blocks_per_sm 1..4.
+ * Before work_estimation; autotune overrides it. */
+rvsp_status_t rvsp_spgemm_batch_set_persistent(rvsp_spgemm_batch_t batch, int32_t merge_rows,
+                                               int32_t blocks_per_sm);
+/* The tuning in use: merge policy, persistent merge rows (0: per-class
+ * launches) and blocks per SM; with autotune, the numeric-only milliseconds
+ * of each shape tried (shape_ms_out: at least 8 floats, in the order
+ * per-class, 128x2, 256x2, 256x1, 64x4) and their count.  NULL outputs are
+ * skipped. */
+rvsp_status_t rvsp_spgemm_batch_get_tuning(rvsp_spgemm_batch_t batch, int32_t *merge_policy_out,
+                                           int32_t *merge_rows_out, int32_t *blocks_out,
+                                           float *shape_ms_out, int32_t *n_shapes_out);
 /* Largest op count of one group (default INT32_MAX; smaller values split a
  * batch into more groups). */
 rvsp_status_t rvsp_spgemm_batch_set_group_ops(rvsp_spgemm_batch_t batch, int64_t max_ops);

@@ -221,6 +221,18 @@ rvsp_status_t rvsp_cuda_plan_set_row_tiles(rvsp_cuda_plan_t plan, int32_t enable
  * are none or tiles are off). */
 int32_t rvsp_cuda_plan_tiled_rows(rvsp_cuda_plan_t plan);
 
+/* Persistent numeric-only pass (k_persist.cu): merge_rows > 0 (a multiple
+ * of 32, at most 256) runs the numeric-only computes' merge-class and
+ * map-class rows in one launch of blocks_per_sm (1..4) blocks per SM that
+ * pull row bins (merge_rows merge rows, or 8 map rows, each) from a global
+ * queue, heaviest class first; 0 (the default) keeps one launch per row
+ * class.  The GPU form of the reference's numeric-only compute loop over rows
+ * (spgemm_descr.c:330-349, gustavson_core_f32.inc:31-62); values are
+ * identical either way.  The batch autotuner (rvsp_spgemm_batch_set_autotune)
+ * times both. */
+rvsp_status_t rvsp_cuda_plan_set_persistent(rvsp_cuda_plan_t plan, int32_t merge_rows,
+                                           int32_t blocks_per_sm);
+
 /* Shift classes in the analysis (1, the default) or not (0).  The GPU form of
  * rvsp_symbolic_count + rvsp_symbolic_fill (rvsp_symbolic.c:13-137) for rows
  * that are exact translates of another row (banded and stencil matrices):

@@ -19,12 +19,12 @@
 
 #include "device_common.cuh"
 #include "kernels.cuh"
+#include "map_walk.cuh"
 
 namespace rvsp {
 
 namespace {
 
-constexpr int kMapSteppingMinAvgLen = 16;  // same rule as the plain walkers
 
 __global__ void __launch_bounds__(256)
 map_ops_kernel(const int32_t *__restrict__ rows, int32_t nrows,
@@ -202,62 +202,7 @@ map_numeric_kernel(Operands op, const int64_t *__restrict__ ops,
   float *acc = smem_f32 + size_t(threadIdx.x >> 5) * H;
   const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   if (w >= nrows) return;
-  const int lane = lane_id();
-  const int32_t row = row_of(rows, w);
-  const int32_t cs = c_rp[row];
-  const int m = c_rp[row + 1] - cs;
-  for (int e = lane; e < m; e += 32) acc[e] = 0.0f;
-  __syncwarp();
-  const int64_t base = moff[row];
-  const int32_t p0 = op.a_rp[row], p1 = op.a_rp[row + 1];
-  const bool stepping =
-      ops[row] >= static_cast<int64_t>(kMapSteppingMinAvgLen) * (p1 - p0);
-  bool bad = false;
-  int64_t run = 0;
-  for (int32_t p = p0; p < p1; p += 32) {
-    const AChunk c = load_chunk(op.a_col, op.a_val, op.b_rp, p + lane, p1, true);
-    if (stepping) {
-      const int cnt = min(32, p1 - p);
-      for (int jj = 0; jj < cnt; ++jj) {
-        const int len = __shfl_sync(kFull, c.len, jj);
-        const int bbeg = __shfl_sync(kFull, c.bbeg, jj);
-        const float a = __shfl_sync(kFull, c.a, jj);
-        const int64_t k0 = base + run + __shfl_sync(kFull, c.incl - c.len, jj);
-        for (int e = lane; e < len; e += 32) {
-          const int pos = __ldg(map + k0 + e);
-          const float term = __fmul_rn(a, __ldg(op.b_val + bbeg + e));
-          if (pos < m) acc[pos] = __fadd_rn(acc[pos], term);
-          else bad = true;
-        }
-        __syncwarp();
-      }
-    } else {
-      for (int t0 = 0; t0 < c.total; t0 += 32) {
-        const int t = t0 + lane;
-        bool v = t < c.total;
-        const int j = warp_owner_of(c.incl, v ? t : 0);
-        const int excl = __shfl_sync(kFull, c.incl - c.len, j);
-        const int bbeg = __shfl_sync(kFull, c.bbeg, j);
-        const float a = __shfl_sync(kFull, c.a, j);
-        int pos = 0;
-        float term = 0.0f;
-        if (v) {
-          pos = __ldg(map + base + run + t);
-          if (pos >= m) {
-            bad = true;
-            v = false;
-          } else {
-            term = __fmul_rn(a, __ldg(op.b_val + bbeg + (t - excl)));
-          }
-        }
-        ordered_apply(acc, v, pos, term);
-      }
-    }
-    run += c.total;
-  }
-  __syncwarp();
-  for (int e = lane; e < m; e += 32) c_val[cs + e] = acc[e];
-  if (__any_sync(kFull, bad) && lane == 0) report(status, kDevKeyMissing);
+  map_numeric_row(op, ops, row_of(rows, w), c_rp, c_val, moff, map, status, acc, lane_id());
 }
 
 template <int LOG2T>

@@ -335,6 +335,29 @@ void launch_tile_numeric(const Operands &op, int32_t b_nnz, const int4 *tiles, i
                          const int32_t *c_rp, float *c_val, int32_t stage_need, int32_t a_seg,
                          int32_t max_out, cudaStream_t s);
 
+// ---- k_persist.cu ----------------------------------------------------------
+// One persistent launch for the numeric-only pass of the merge and map rows
+// of a plan (see k_persist.cu): the rows of each class cut into items of
+// per_item rows, numbered from item0; segments heaviest class first.
+constexpr int kPersistThreads = 256;
+struct PersistSeg {
+  const int32_t *rows;  // the class's row list (nullptr: rows 0.. in order)
+  int32_t cls, count, per_item, item0;
+};
+struct PersistPlan {
+  PersistSeg seg[kNumClasses];
+  int32_t nseg = 0, n_items = 0;
+};
+// Classes the persistent kernel takes (merge and map classes).
+bool persist_class(int cls);
+// head: one int the launch clears first; max_map_out: the largest C row of
+// the map classes in the plan (their accumulators).
+void launch_persist_numeric(const Operands &op, const int64_t *ops, const PersistPlan &pp,
+                            int32_t *head, const int32_t *c_rp, float *c_val,
+                            const int64_t *moff, const uint16_t *map, int32_t *status,
+                            int32_t max_map_out, int blocks_per_sm, int num_sms,
+                            cudaStream_t s);
+
 // ---- k_shift.cu ------------------------------------------------------------
 // Shift classes (see k_shift.cu).  Every pass but the probe is gated by the
 // device flag *on, which the probe's decision sets, so the plan queues them

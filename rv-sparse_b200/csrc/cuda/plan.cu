@@ -195,6 +195,10 @@ struct rvsp_cuda_plan {
   // analysis has member rows (pattern in st.pid).  Their patterns' term
   // tables (sh_*) and row tiles (st) are built from the canonical rows' maps
   // on the first numeric call (shift_tables 1, or -1 when that failed).
+  // Persistent numeric-only pass (k_persist.cu): merge rows per item (0: off)
+  // and blocks per SM.
+  int32_t persist_merge_rows = 0, persist_blocks = 2;
+  DevArray<int32_t> persist_head;
   int shift_enabled = 1;
   int shift_active = 0;
   int shift_tables = 0;
@@ -414,6 +418,7 @@ void rvsp_cuda_plan_destroy(rvsp_cuda_plan_t p) {
   p->pat_rec.release();
   p->rt.release();
   p->st.release();
+  p->persist_head.release();
   for (auto *a : {&p->sh_on, &p->sh_trow, &p->sh_bcls, &p->sh_rcls, &p->sh_share,
                   &p->sh_pat_of, &p->sh_pat_canon, &p->sh_pat_cap, &p->sh_pat_m,
                   &p->sh_steps, &p->sh_counts})
@@ -1021,6 +1026,17 @@ rvsp_status_t rvsp_cuda_plan_set_row_tiles(rvsp_cuda_plan_t p, int32_t enable) {
   return RVSP_SUCCESS;
 }
 
+rvsp_status_t rvsp_cuda_plan_set_persistent(rvsp_cuda_plan_t p, int32_t merge_rows,
+                                           int32_t blocks_per_sm) {
+  if (!p) return RVSP_ERROR_NULL_POINTER;
+  if (merge_rows < 0 || merge_rows > kPersistThreads || merge_rows % 32 != 0 ||
+      blocks_per_sm < 1 || blocks_per_sm > 4)
+    return RVSP_ERROR_INVALID_ARGUMENT;
+  p->persist_merge_rows = merge_rows;
+  p->persist_blocks = blocks_per_sm;
+  return RVSP_SUCCESS;
+}
+
 rvsp_status_t rvsp_cuda_plan_set_shift_classes(rvsp_cuda_plan_t p, int32_t enable) {
   if (!p) return RVSP_ERROR_NULL_POINTER;
   if (enable != 0 && enable != 1) return RVSP_ERROR_INVALID_ARGUMENT;
@@ -1495,8 +1511,43 @@ rvsp_status_t rvsp_cuda_numeric(rvsp_cuda_plan_t p, void *stream,
         ph.launches += 1;
       }
     }
+    // Persistent pass: the merge and map rows in one launch over a queue of
+    // row bins, heaviest class first.
+    const bool persist = use_map && p->persist_merge_rows > 0 &&
+                         p->persist_head.reserve(1) == cudaSuccess;
+    if (persist) {
+      PersistPlan pp;
+      int32_t max_out = 0;
+      const int order[] = {kW2048, kW1024, kW512, kW256, kW128, kW64, kM16, kM8, kM4};
+      for (int c : order) {
+        if (p->num_count[c] <= 0) continue;
+        const bool whole = c == p->num_whole;
+        PersistSeg g;
+        g.cls = c;
+        if (map_class(c) && p->pat_ready) {
+          g.rows = p->res_rows.p + p->res_off[c];
+          g.count = p->res_count[c];
+        } else {
+          g.rows = whole ? nullptr : p->rows_num.p + p->num_off[c];
+          g.count = whole ? p->a_rows : p->num_count[c];
+        }
+        if (g.count <= 0) continue;
+        g.per_item = map_class(c) ? kPersistThreads / 32 : p->persist_merge_rows;
+        g.item0 = pp.n_items;
+        pp.seg[pp.nseg++] = g;
+        pp.n_items += (g.count + g.per_item - 1) / g.per_item;
+        if (map_class(c) && max_out == 0) max_out = 1 << (class_log2(c) - 1);
+      }
+      launch_persist_numeric(op, p->ops.p, pp, p->persist_head.p, c_row_ptr, c_values,
+                             p->rmap_off.p, p->rmap.p, p->misc.p + kStatus, max_out,
+                             p->persist_blocks, p->num_sms, s);
+      ph.launches += 2;
+    } else {
+      cudaGetLastError();
+    }
     for (int c = kEmpty_ + 1; c < kNumClasses; ++c) {
       if (p->num_count[c] <= 0) continue;
+      if (persist && persist_class(c)) continue;
       const bool whole = c == p->num_whole;
       const int32_t *rows = whole ? nullptr : p->rows_num.p + p->num_off[c];
       const int32_t nrows = whole ? p->a_rows : p->num_count[c];

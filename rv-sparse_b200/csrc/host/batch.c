@@ -48,6 +48,9 @@ struct rvsp_spgemm_batch {
     int user_stream;
     int autotune;
     int32_t merge_policy;
+    int32_t persist_rows, persist_blocks; /* persistent numeric-only pass */
+    float tuned_ms[8];                    /* autotuner timings (see get_tuning) */
+    int32_t n_tuned;
     int64_t group_ops;
 
     int32_t count, cap;
@@ -198,6 +201,39 @@ rvsp_status_t rvsp_spgemm_batch_set_autotune(rvsp_spgemm_batch_t b, int enable)
     if (b == NULL)
         return RVSP_ERROR_NULL_POINTER;
     b->autotune = enable != 0;
+    return RVSP_SUCCESS;
+}
+
+rvsp_status_t rvsp_spgemm_batch_set_persistent(rvsp_spgemm_batch_t b, int32_t merge_rows,
+                                               int32_t blocks_per_sm)
+{
+    if (b == NULL)
+        return RVSP_ERROR_NULL_POINTER;
+    if (merge_rows < 0 || merge_rows > 256 || merge_rows % 32 != 0 || blocks_per_sm < 1 ||
+        blocks_per_sm > 4 || b->estimated)
+        return RVSP_ERROR_INVALID_ARGUMENT;
+    b->persist_rows = merge_rows;
+    b->persist_blocks = blocks_per_sm;
+    return RVSP_SUCCESS;
+}
+
+rvsp_status_t rvsp_spgemm_batch_get_tuning(rvsp_spgemm_batch_t b, int32_t *merge_policy_out,
+                                           int32_t *merge_rows_out, int32_t *blocks_out,
+                                           float *shape_ms_out, int32_t *n_shapes_out)
+{
+    if (b == NULL)
+        return RVSP_ERROR_NULL_POINTER;
+    if (merge_policy_out)
+        *merge_policy_out = b->merge_policy;
+    if (merge_rows_out)
+        *merge_rows_out = b->persist_rows;
+    if (blocks_out)
+        *blocks_out = b->persist_blocks > 0 ? b->persist_blocks : 2;
+    if (shape_ms_out)
+        for (int32_t i = 0; i < b->n_tuned; i++)
+            shape_ms_out[i] = b->tuned_ms[i];
+    if (n_shapes_out)
+        *n_shapes_out = b->n_tuned;
     return RVSP_SUCCESS;
 }
 
@@ -548,6 +584,15 @@ static rvsp_status_t time_numeric(rvsp_spgemm_batch_t b, float *ms_out)
     return st;
 }
 
+static rvsp_status_t set_persistent_all(rvsp_spgemm_batch_t b)
+{
+    rvsp_status_t st = RVSP_SUCCESS;
+    for (int32_t k = 0; k < b->ngroups && st == RVSP_SUCCESS; k++)
+        st = rvsp_cuda_plan_set_persistent(b->groups[k].plan, b->persist_rows,
+                                           b->persist_blocks > 0 ? b->persist_blocks : 2);
+    return st;
+}
+
 static rvsp_status_t analyse_all(rvsp_spgemm_batch_t b)
 {
     rvsp_status_t st = RVSP_SUCCESS;
@@ -556,7 +601,62 @@ static rvsp_status_t analyse_all(rvsp_spgemm_batch_t b)
         if (st == RVSP_SUCCESS)
             st = analyse_group(b, &b->groups[k]);
     }
+    if (st == RVSP_SUCCESS)
+        st = set_persistent_all(b);
     return st;
+}
+
+/* Builds every group's reuse map for the structure of the last fill. */
+static rvsp_status_t prepare_reuse_all(rvsp_spgemm_batch_t b)
+{
+    rvsp_status_t st = RVSP_SUCCESS;
+    for (int32_t k = 0; k < b->ngroups && st == RVSP_SUCCESS; k++) {
+        const batch_group_t *g = &b->groups[k];
+        st = rvsp_cuda_plan_prepare_reuse(g->plan, b->stream, (const int32_t *)g->a_rp.p,
+                                          (const int32_t *)g->a_ci.p,
+                                          (const int32_t *)g->b_rp.p,
+                                          (const int32_t *)g->b_ci.p,
+                                          (const int32_t *)g->c_rp.p,
+                                          (const int32_t *)g->c_ci.p, NULL);
+    }
+    return st;
+}
+
+/* The numeric-only shapes the autotuner times: one launch per row class,
+ * then the persistent pass with merge rows per bin x blocks per SM. */
+static const int32_t kTuneShapes[][2] = {{0, 2}, {128, 2}, {256, 2}, {256, 1}, {64, 4}};
+#define N_TUNE_SHAPES ((int32_t)(sizeof(kTuneShapes) / sizeof(kTuneShapes[0])))
+
+/* Times each shape on the analysed batch (one fill, reuse maps built, then
+ * numeric-only passes) and keeps the fastest. */
+static rvsp_status_t autotune_shape(rvsp_spgemm_batch_t b)
+{
+    rvsp_status_t st = run_groups(b, 1);
+    if (st == RVSP_SUCCESS)
+        st = prepare_reuse_all(b);
+    int32_t best = -1;
+    float best_ms = 0.0f;
+    b->n_tuned = 0;
+    for (int32_t i = 0; i < N_TUNE_SHAPES && st == RVSP_SUCCESS; i++) {
+        b->persist_rows = kTuneShapes[i][0];
+        b->persist_blocks = kTuneShapes[i][1];
+        st = set_persistent_all(b);
+        float ms = 0.0f;
+        if (st == RVSP_SUCCESS)
+            st = time_numeric(b, &ms);
+        if (st == RVSP_SUCCESS) {
+            b->tuned_ms[b->n_tuned++] = ms;
+            if (best < 0 || ms < best_ms) {
+                best = i;
+                best_ms = ms;
+            }
+        }
+    }
+    if (st != RVSP_SUCCESS)
+        return st;
+    b->persist_rows = kTuneShapes[best][0];
+    b->persist_blocks = kTuneShapes[best][1];
+    return set_persistent_all(b);
 }
 
 /* The autotuner: tries each merge policy on the batch (symbolic + one fill
@@ -581,7 +681,10 @@ static rvsp_status_t autotune_policy(rvsp_spgemm_batch_t b)
         }
     }
     b->merge_policy = best;
-    return best == 2 ? RVSP_SUCCESS : analyse_all(b);
+    rvsp_status_t st = best == 2 ? RVSP_SUCCESS : analyse_all(b);
+    if (st == RVSP_SUCCESS)
+        st = autotune_shape(b);
+    return st;
 }
 
 /* Per-product views of the groups' C: rebased row pointers, bases, nnz. */
@@ -730,15 +833,8 @@ rvsp_status_t rvsp_spgemm_batch_compute(rvsp_spgemm_batch_t b)
     if (!b->filled) {
         st = run_groups(b, 1);
         /* The repeats are captured, so build each group's reuse map now. */
-        for (int32_t k = 0; k < b->ngroups && st == RVSP_SUCCESS; k++) {
-            const batch_group_t *g = &b->groups[k];
-            st = rvsp_cuda_plan_prepare_reuse(g->plan, b->stream, (const int32_t *)g->a_rp.p,
-                                              (const int32_t *)g->a_ci.p,
-                                              (const int32_t *)g->b_rp.p,
-                                              (const int32_t *)g->b_ci.p,
-                                              (const int32_t *)g->c_rp.p,
-                                              (const int32_t *)g->c_ci.p, NULL);
-        }
+        if (st == RVSP_SUCCESS)
+            st = prepare_reuse_all(b);
         if (st == RVSP_SUCCESS)
             b->filled = 1;
         return st;

@@ -154,6 +154,10 @@ SIGNATURES = {
     "rvsp_cuda_plan_set_shift_classes": (_int, [_vp, _i32]),
     "rvsp_cuda_plan_shift_rows": (_i32, [_vp]),
     "rvsp_spgemm_set_shift_classes": (_int, [_vp, _i32]),
+    "rvsp_cuda_plan_set_persistent": (_int, [_vp, _i32, _i32]),
+    "rvsp_spgemm_batch_set_persistent": (_int, [_vp, _i32, _i32]),
+    "rvsp_spgemm_batch_get_tuning": (_int, [_vp, _P(_i32), _P(_i32), _P(_i32),
+                                            _P(C.c_float), _P(_i32)]),
     "rvsp_spgemm_get_shift_rows": (_int, [_vp, _P(_i32)]),
     "rvsp_spgemm_set_model": (_int, [_vp, _vp]),
     "rvsp_spgemm_set_capacity_scale": (_int, [_vp, C.c_float]),

@@ -382,7 +382,8 @@ class Batch:
     computes (numeric-only repeats), never their structure."""
 
     def __init__(self, memory: int = L.MEM_HOST, stream=None, autotune: bool = False,
-                 merge_policy: int | None = None, group_ops: int | None = None):
+                 merge_policy: int | None = None, group_ops: int | None = None,
+                 persistent: tuple | None = None):
         self.lib = L.load()
         self.h = C.c_void_p()
         L.check(self.lib.rvsp_spgemm_batch_create(C.byref(self.h)), "batch_create")
@@ -401,6 +402,9 @@ class Batch:
         if group_ops is not None:
             L.check(self.lib.rvsp_spgemm_batch_set_group_ops(self.h, group_ops),
                     "batch_set_group_ops")
+        if persistent is not None:  # (merge rows per bin, blocks per SM)
+            L.check(self.lib.rvsp_spgemm_batch_set_persistent(self.h, *persistent),
+                    "batch_set_persistent")
         self.memory = memory
         self.operands = []
         self.total_nnz = None
@@ -461,6 +465,19 @@ class Batch:
                 "batch_get_stats")
         return {"groups": g.value, "ops": ops.value, "merge_policy": pol.value,
                 "graph_nodes": nodes.value}
+
+    def tuning(self):
+        """Merge policy, persistent shape and (autotuned) the timed shapes."""
+        pol, rows, blocks, n = C.c_int32(), C.c_int32(), C.c_int32(), C.c_int32()
+        ms = (C.c_float * 8)()
+        L.check(self.lib.rvsp_spgemm_batch_get_tuning(self.h, C.byref(pol), C.byref(rows),
+                                                      C.byref(blocks), ms, C.byref(n)),
+                "batch_get_tuning")
+        shapes = ["per-class", "persistent 128x2", "persistent 256x2", "persistent 256x1",
+                  "persistent 64x4"]
+        return {"merge_policy": pol.value, "persistent_merge_rows": rows.value,
+                "persistent_blocks_per_sm": blocks.value,
+                "shape_ms": {shapes[i]: float(ms[i]) for i in range(n.value)}}
 
     def close(self):
         if self.h:

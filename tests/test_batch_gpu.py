@@ -136,3 +136,47 @@ def test_batch_errors():
     with Batch() as b:
         with pytest.raises(L.RvspError):
             b.work_estimation()  # empty batch
+
+
+@pytest.mark.parametrize("shape", [(128, 2), (256, 1), (64, 4)])
+def test_batch_persistent_pass(shape):
+    # numeric-only repeats through the persistent kernel (one launch pulling
+    # row bins from a global queue), captured and replayed: bit-exact
+    prods = uneven_products(count=24, seed=41)
+    rng = np.random.default_rng(6)
+    with Batch(persistent=shape) as b:
+        for A, B in prods:
+            b.add(A, B)
+        b.work_estimation()
+        b.compute()
+        for rep in range(3):
+            for A, B in prods:
+                redraw(A, rng)
+                redraw(B, rng)
+            b.compute()
+            for i, (A, B) in enumerate(prods):
+                assert_exact(b.result(i), A, B, f"product {i} repeat {rep}")
+        t = b.tuning()
+        assert t["persistent_merge_rows"] == shape[0]
+        assert t["persistent_blocks_per_sm"] == shape[1]
+
+
+def test_batch_autotune_times_every_shape():
+    prods = uneven_products(count=16, seed=43)
+    rng = np.random.default_rng(8)
+    with Batch(autotune=True) as b:
+        for A, B in prods:
+            b.add(A, B)
+        b.work_estimation()
+        t = b.tuning()
+        assert len(t["shape_ms"]) == 5 and all(v > 0 for v in t["shape_ms"].values())
+        best = min(t["shape_ms"], key=t["shape_ms"].get)
+        assert (t["persistent_merge_rows"] == 0) == (best == "per-class")
+        b.compute()
+        for rep in range(2):
+            for A, B in prods:
+                redraw(A, rng)
+                redraw(B, rng)
+            b.compute()
+        for i, (A, B) in enumerate(prods):
+            assert_exact(b.result(i), A, B, f"product {i}")
