@@ -209,6 +209,10 @@ rvsp_status_t rvsp_spgemm_set_row_tiles(rvsp_spgemm_descr_t descr, int32_t enabl
  * numeric-only compute on the current structure; 0 before). */
 rvsp_status_t rvsp_spgemm_get_tiled_rows(rvsp_spgemm_descr_t descr, int32_t *n_out);
 
+/* Pattern kernels for the row tiles (see rvsp_cuda_plan_set_pattern_kernels):
+ * 1 (default) or 0.  Results are identical either way. */
+rvsp_status_t rvsp_spgemm_set_pattern_kernels(rvsp_spgemm_descr_t descr, int32_t enable);
+
 /* Shift classes in work_estimation (see rvsp_cuda_plan_set_shift_classes):
  * 1 (default) or 0.  Results are identical either way. */
 rvsp_status_t rvsp_spgemm_set_shift_classes(rvsp_spgemm_descr_t descr, int32_t enable);

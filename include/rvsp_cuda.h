@@ -233,6 +233,25 @@ int32_t rvsp_cuda_plan_tiled_rows(rvsp_cuda_plan_t plan);
 rvsp_status_t rvsp_cuda_plan_set_persistent(rvsp_cuda_plan_t plan, int32_t merge_rows,
                                            int32_t blocks_per_sm);
 
+/* Pattern kernels (1, the default) or not (0).  When row tiles are built,
+ * the (at most four) patterns with at least 128 tiles get a kernel written
+ * for that pattern and compiled at run time with NVRTC (k_jit.cu): each lane
+ * keeps its row's outputs in registers, so a product is a shared load, a
+ * multiply and an add.  Values are identical to the table kernel's (same
+ * order, separately rounded products and sums).  Without NVRTC in the
+ * process, or if a compile fails, the pattern stays on the table kernel.
+ * Kernels are cached for the life of the process.  Changing the setting
+ * rebuilds the tiles on the next numeric-only call. */
+rvsp_status_t rvsp_cuda_plan_set_pattern_kernels(rvsp_cuda_plan_t plan, int32_t enable);
+
+/* Rows (32 per tile, the tiles' masks not subtracted) the pattern kernels
+ * of the current reuse structures take. */
+int32_t rvsp_cuda_plan_pattern_kernel_rows(rvsp_cuda_plan_t plan);
+
+/* Pattern kernels compiled in this process so far and the milliseconds the
+ * compiles took (NULL outputs are skipped). */
+void rvsp_cuda_pattern_kernel_stats(int32_t *compiles, double *compile_ms);
+
 /* Shift classes in the analysis (1, the default) or not (0).  The GPU form of
  * rvsp_symbolic_count + rvsp_symbolic_fill (rvsp_symbolic.c:13-137) for rows
  * that are exact translates of another row (banded and stencil matrices):

@@ -55,6 +55,7 @@ constexpr int kTileMinRows = 8;         // rows of one pattern that make a tile
 constexpr int kTileStageMax = 4096;     // floats in one stage buffer
 constexpr int kTileASegMax = 2048;      // A entries of one chunk
 constexpr int kTileMaxOut = 256;        // C entries of a tiled row
+constexpr int kTileStages = 2;          // B spans in flight per warp (ring)
 // uint16 entries of one pattern's table: at most kPatMaxOps (1024) products
 // plus 7 padding entries per A nonzero, rounded to a multiple of 8
 constexpr int kTileTabStride = 1280;
@@ -235,8 +236,8 @@ __device__ __forceinline__ int32_t stage_span(float *dst, const float *__restric
 
 // Values of the tiled rows: warp per tile.  Shared memory per warp:
 // acc[(acc_rows) * 33] floats, then a work area of work_floats floats that
-// first holds the chunk's A segment (columns, then values) and then the two
-// stage buffers of stage_cap floats each.
+// first holds the chunk's A segment (columns, then values) and then the
+// kTileStages stage buffers of stage_cap floats each.
 __global__ void __launch_bounds__(kTileKernelWarps * 32)
 tile_numeric_kernel(const int32_t *__restrict__ a_rp, const int32_t *__restrict__ a_col,
                     const float *__restrict__ a_val, const int32_t *__restrict__ b_rp,
@@ -259,6 +260,7 @@ tile_numeric_kernel(const int32_t *__restrict__ a_rp, const int32_t *__restrict_
   const unsigned mask = static_cast<unsigned>(tile.y);
   const int32_t pid = tile.z;
   const int4 d = desc[pid];
+  if (d.w != 0) return;  // a pattern kernel (k_jit.cu) takes these tiles
   const int32_t na = d.x, m = d.y;
   const bool active = (mask >> lane) & 1u;
   const int32_t row = row0 + lane;
@@ -306,33 +308,39 @@ tile_numeric_kernel(const int32_t *__restrict__ a_rp, const int32_t *__restrict_
   __syncwarp();  // the work area becomes the stage buffers
 
   const uint4 *const tq = reinterpret_cast<const uint4 *>(tab + size_t(pid) * kTileTabStride);
-  float *const stage0 = work;
-  float *const stage1 = work + stage_cap;
-  int32_t c0_cur = 0;
-  {
-    const int32_t l0 = __shfl_sync(kFull, len, 0);
-    const int32_t lo = __reduce_min_sync(kFull, active ? rp[0] : INT_MAX);
-    const int32_t hi = __reduce_max_sync(kFull, active ? rp[0] + l0 : INT_MIN);
-    c0_cur = stage_span(stage0, b_val, lo, hi, b_nnz, aligned16, lane);
+  // A ring of kTileStages stage buffers: the B span of A nonzero j + S - 1 is
+  // requested while j is computed, so S - 1 spans are always in flight.
+  // Every iteration commits one cp.async group (empty past the row's end),
+  // so waiting for all but the newest S - 1 groups means span j is in.
+  int32_t c0s[kTileStages];
+#pragma unroll
+  for (int j = 0; j < kTileStages - 1; ++j) {
+    c0s[j] = 0;
+    if (j < kTileMaxA && j < na) {
+      const int32_t lj = __shfl_sync(kFull, len, j);
+      const int32_t lo = __reduce_min_sync(kFull, active ? rp[j] : INT_MAX);
+      const int32_t hi = __reduce_max_sync(kFull, active ? rp[j] + lj : INT_MIN);
+      c0s[j] = stage_span(work + j * stage_cap, b_val, lo, hi, b_nnz, aligned16, lane);
+    }
     cp_async_commit();
   }
 #pragma unroll
   for (int j = 0; j < kTileMaxA; ++j) {
     if (j >= na) break;
-    int32_t c0_next = 0;
-    if (j + 1 < na) {
-      const int32_t ln = __shfl_sync(kFull, len, j + 1);
-      const int32_t lo = __reduce_min_sync(kFull, active ? rp[j + 1] : INT_MAX);
-      const int32_t hi = __reduce_max_sync(kFull, active ? rp[j + 1] + ln : INT_MIN);
-      c0_next = stage_span((j & 1) ? stage0 : stage1, b_val, lo, hi, b_nnz, aligned16, lane);
-      cp_async_commit();
-      cp_async_wait<1>();
-    } else {
-      cp_async_wait<0>();
+    constexpr int kS = kTileStages;
+    const int jn = j + kS - 1;
+    if (jn < kTileMaxA && jn < na) {
+      const int32_t ln = __shfl_sync(kFull, len, jn);
+      const int32_t lo = __reduce_min_sync(kFull, active ? rp[jn] : INT_MAX);
+      const int32_t hi = __reduce_max_sync(kFull, active ? rp[jn] + ln : INT_MIN);
+      c0s[jn % kS] =
+          stage_span(work + (jn % kS) * stage_cap, b_val, lo, hi, b_nnz, aligned16, lane);
     }
+    cp_async_commit();
+    cp_async_wait<kS - 1>();
     __syncwarp();
-    const float *st = (j & 1) ? stage1 : stage0;
-    const int32_t bl = active ? rp[j] - c0_cur : 0;
+    const float *st = work + (j % kS) * stage_cap;
+    const int32_t bl = active ? rp[j] - c0s[j % kS] : 0;
     const float aj = av[j];
     const int32_t lj = __shfl_sync(kFull, len, j);
     const uint4 *tj = tq + (__shfl_sync(kFull, jo, j) >> 3);
@@ -354,8 +362,8 @@ tile_numeric_kernel(const int32_t *__restrict__ a_rp, const int32_t *__restrict_
       for (int i = 0; i < 8; ++i) accl[(u[i] & 0x7fffu) * 33] = __fadd_rn(v[i], b[i]);
     }
     __syncwarp();  // every lane is done with this buffer before it is refilled
-    c0_cur = c0_next;
   }
+  cp_async_wait<0>();  // (only empty groups can be left)
   // C: each row's m values, lanes over positions (coalesced)
   for (int r = 0; r < 32; ++r) {
     const int32_t base = __shfl_sync(kFull, cs, r);
@@ -418,7 +426,8 @@ size_t tile_smem_per_warp(int32_t stage_need, int32_t a_seg, int32_t max_out,
                           int32_t *acc_rows, int32_t *work_floats, int32_t *stage_cap) {
   *acc_rows = max_out + 1;
   *stage_cap = (stage_need + 3) & ~3;
-  const int32_t work = 2 * *stage_cap > 2 * a_seg ? 2 * *stage_cap : 2 * a_seg;
+  const int32_t work = kTileStages * *stage_cap > 2 * a_seg ? kTileStages * *stage_cap
+                                                            : 2 * a_seg;
   *work_floats = (work + 3) & ~3;
   const int32_t acc_floats = (*acc_rows * 33 + 3) & ~3;
   return size_t(acc_floats + *work_floats) * sizeof(float);

@@ -3,6 +3,7 @@
 
 #include <cstddef>
 #include <cstdint>
+#include <vector>
 #include <cuda_runtime.h>
 
 struct rvsp_mlp;
@@ -357,6 +358,26 @@ void launch_persist_numeric(const Operands &op, const int64_t *ops, const Persis
                             const int64_t *moff, const uint16_t *map, int32_t *status,
                             int32_t max_map_out, int blocks_per_sm, int num_sms,
                             cudaStream_t s);
+
+// ---- k_jit.cu --------------------------------------------------------------
+// Pattern kernels (see k_jit.cu): *kernel_out = a kernel compiled for one
+// pattern (na A nonzeros, B row lengths len[j], slot[t] = output position of
+// flattened product t, m outputs); returns 0 when NVRTC is missing or the
+// compile failed.  Kernels are cached for the process.
+int jit_pattern_kernel(int na, const int *len, const std::vector<int> &slot, int m,
+                       void **kernel_out);
+void jit_stats(int32_t *compiles, double *ms);
+// out[*n] = the tiles of pattern pid (*n zeroed by the caller).
+void launch_tile_select(const int4 *tiles, int32_t ntiles, int32_t pid, int4 *out, int32_t *n,
+                        cudaStream_t s);
+// Marks pattern pid's tiles for the table kernel to skip (desc[pid].w = 1).
+void launch_mark_pattern(int4 *desc, int32_t pid, cudaStream_t s);
+// One launch of a pattern kernel over its tiles; work_floats per warp holds
+// the A segment, two stage buffers of stage_cap floats, and 32 x 33 floats.
+cudaError_t launch_pattern_kernel(void *kernel, const Operands &op, int32_t b_nnz,
+                                  const int4 *tiles, int32_t ntiles, const int32_t *c_rp,
+                                  float *c_val, int32_t stage_cap, int32_t work_floats,
+                                  cudaStream_t s);
 
 // ---- k_shift.cu ------------------------------------------------------------
 // Shift classes (see k_shift.cu).  Every pass but the probe is gated by the

@@ -11,6 +11,7 @@
 // per non-empty numeric class with no host round trip.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <climits>
 #include <cstring>
 #include <new>
@@ -85,7 +86,13 @@ namespace rvsp {
 // outside the set); the tiles and the pattern rows left to the warp-per-row
 // table kernel (lo_rows / lo_ids); for the shift classes also every pattern
 // row (all_rows / all_ids, for when tiles are off).
+struct JitPattern {
+  void *kernel = nullptr;
+  DevArray<int4> tiles;
+  int32_t n = 0;
+};
 struct TileBuild {
+  std::vector<JitPattern> jit;  // patterns with their own kernel (k_jit.cu)
   int ready = 0;
   int32_t n_tiles = 0, n_lo = 0, stage = 0, aseg = 0, max_out = 0, b_nnz = 0;
   DevArray<uint16_t> tab, lens;
@@ -102,6 +109,8 @@ struct TileBuild {
     counts.release();
     all_rows.release();
     all_ids.release();
+    for (auto &j : jit) j.tiles.release();
+    jit.clear();
     ready = 0;
   }
 };
@@ -189,6 +198,7 @@ struct rvsp_cuda_plan {
   DevArray<uint32_t> pat_rec;
   // Row tiles of the table rows of shared maps (k_tile.cu).
   int tiles_enabled = 1;
+  int pattern_kernels = 1;  // compile kernels for the largest patterns (k_jit.cu)
   TileBuild rt;
   // Shift classes (k_shift.cu): rows that are translates of a canonical row.
   // The probe sets the device flag sh_on; shift_active when the current
@@ -1037,6 +1047,33 @@ rvsp_status_t rvsp_cuda_plan_set_persistent(rvsp_cuda_plan_t p, int32_t merge_ro
   return RVSP_SUCCESS;
 }
 
+rvsp_status_t rvsp_cuda_plan_set_pattern_kernels(rvsp_cuda_plan_t p, int32_t enable) {
+  if (!p) return RVSP_ERROR_NULL_POINTER;
+  if (enable != 0 && enable != 1) return RVSP_ERROR_INVALID_ARGUMENT;
+  if (enable != p->pattern_kernels) {
+    // the tiles are built with or without pattern kernels: rebuild them
+    p->rmap_state = 0;
+    p->rmap_col = nullptr;
+    if (p->shift_tables == 1) p->shift_tables = 0;
+  }
+  p->pattern_kernels = enable;
+  return RVSP_SUCCESS;
+}
+
+int32_t rvsp_cuda_plan_pattern_kernel_rows(rvsp_cuda_plan_t p) {
+  if (!p || !p->tiles_enabled) return 0;
+  int32_t n = 0;
+  if (p->rmap_state == 1 && p->pat_ready && p->rt.ready)
+    for (const auto &j : p->rt.jit) n += 32 * j.n;
+  if (p->shift_active && p->shift_tables == 1 && p->st.ready)
+    for (const auto &j : p->st.jit) n += 32 * j.n;
+  return n;
+}
+
+void rvsp_cuda_pattern_kernel_stats(int32_t *compiles, double *compile_ms) {
+  jit_stats(compiles, compile_ms);
+}
+
 rvsp_status_t rvsp_cuda_plan_set_shift_classes(rvsp_cuda_plan_t p, int32_t enable) {
   if (!p) return RVSP_ERROR_NULL_POINTER;
   if (enable != 0 && enable != 1) return RVSP_ERROR_INVALID_ARGUMENT;
@@ -1073,6 +1110,80 @@ constexpr size_t kReuseMapMaxBytes = size_t(24) << 30;
 
 // The tile tables may take at most this much device memory.
 constexpr size_t kTileTablesMaxBytes = size_t(256) << 20;
+// Patterns with at least this many tiles (of 32 rows) get a compiled kernel,
+// the kJitMaxPatterns largest of them.
+constexpr int32_t kJitMinTiles = 128;
+constexpr int kJitMaxPatterns = 4;
+
+// Work area of one warp of a pattern kernel (k_jit.cu), in floats.
+int32_t pattern_work_floats(const TileBuild &tb) {
+  int32_t stage_cap = (tb.stage + 3) & ~3;
+  int32_t w = 2 * stage_cap;
+  if (2 * tb.aseg > w) w = 2 * tb.aseg;
+  if (32 * 33 > w) w = 32 * 33;
+  return (w + 3) & ~3;
+}
+
+// Compiled kernels for the patterns that cover the most tiles: the tile list
+// is read back once, each chosen pattern's table is turned into CUDA source
+// (k_jit.cu), and its tiles are listed for its kernel and marked so the
+// table kernel skips them.  A pattern whose compile fails stays on the table
+// kernel.  Synchronizes `s`.
+cudaError_t build_pattern_kernels(rvsp_cuda_plan *p, cudaStream_t s, int32_t npat,
+                                  TileBuild &tb) {
+  for (auto &j : tb.jit) j.tiles.release();
+  tb.jit.clear();
+  std::vector<int4> tiles(static_cast<size_t>(tb.n_tiles));
+  cudaError_t e = cudaMemcpyAsync(tiles.data(), tb.tiles.p, tiles.size() * sizeof(int4),
+                                  cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) return e;
+  std::vector<int32_t> count(static_cast<size_t>(npat), 0);
+  for (const int4 &t : tiles)
+    if (t.z >= 0 && t.z < npat) ++count[size_t(t.z)];
+  std::vector<int32_t> order;
+  for (int32_t id = 0; id < npat; ++id)
+    if (count[size_t(id)] >= kJitMinTiles) order.push_back(id);
+  std::sort(order.begin(), order.end(),
+            [&](int32_t a, int32_t b) { return count[size_t(a)] > count[size_t(b)]; });
+  if (order.size() > size_t(kJitMaxPatterns)) order.resize(size_t(kJitMaxPatterns));
+  const int32_t stride = tile_tab_stride();
+  for (int32_t id : order) {
+    int4 d;
+    uint16_t lens[32];
+    std::vector<uint16_t> tab(static_cast<size_t>(stride));
+    e = cudaMemcpyAsync(&d, tb.desc.p + id, sizeof(int4), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(lens, tb.lens.p + size_t(id) * 32, sizeof(lens),
+                          cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(tab.data(), tb.tab.p + size_t(id) * stride,
+                          tab.size() * sizeof(uint16_t), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return e;
+    if (d.x <= 0 || d.x > 32 || d.y <= 0) continue;
+    int len[32];
+    std::vector<int> slot;
+    int32_t off = 0;
+    for (int j = 0; j < d.x; ++j) {
+      len[j] = lens[j];
+      for (int ee = 0; ee < len[j]; ++ee) slot.push_back(tab[size_t(off + ee)] & 0x7fff);
+      off += (len[j] + 7) & ~7;
+    }
+    JitPattern jp;
+    if (!jit_pattern_kernel(d.x, len, slot, d.y, &jp.kernel)) continue;
+    if (jp.tiles.reserve(size_t(count[size_t(id)])) != cudaSuccess) {
+      cudaGetLastError();
+      continue;
+    }
+    cudaMemsetAsync(tb.counts.p + 6, 0, sizeof(int32_t), s);
+    launch_tile_select(tb.tiles.p, tb.n_tiles, id, jp.tiles.p, tb.counts.p + 6, s);
+    launch_mark_pattern(tb.desc.p, id, s);
+    jp.n = count[size_t(id)];
+    tb.jit.push_back(std::move(jp));
+  }
+  return cudaGetLastError();
+}
 constexpr int kTileCountWords = 8;  // ntiles, leftovers, 3 maxima, list count, spare
 
 // Row tiles of a set of table patterns (k_tile.cu): the per-pattern tile
@@ -1133,6 +1244,7 @@ cudaError_t build_row_tiles(rvsp_cuda_plan *p, cudaStream_t s, const Operands &o
   tb.max_out = h[4];
   tb.b_nnz = b_nnz;
   tb.ready = 1;
+  if (p->pattern_kernels) return build_pattern_kernels(p, s, npat, tb);
   return cudaSuccess;
 }
 
@@ -1273,6 +1385,16 @@ cudaError_t build_shift_tables(rvsp_cuda_plan *p, cudaStream_t s, const Operands
   return cudaSuccess;
 }
 
+// The pattern kernels of a tile set (k_jit.cu); returns the launches.
+int launch_pattern_kernels(const TileBuild &tb, const Operands &op, const int32_t *c_rp,
+                           float *c_val, cudaStream_t s) {
+  const int32_t wf = pattern_work_floats(tb);
+  const int32_t stage_cap = (tb.stage + 3) & ~3;
+  for (const auto &j : tb.jit)
+    launch_pattern_kernel(j.kernel, op, tb.b_nnz, j.tiles.p, j.n, c_rp, c_val, stage_cap, wf, s);
+  return static_cast<int>(tb.jit.size());
+}
+
 // Values of the shift-class member rows (tables built): row tiles, then the
 // members no tile took through the warp-per-row table kernel; every member
 // through that kernel when tiles are off.
@@ -1283,7 +1405,7 @@ int launch_shift_numeric(rvsp_cuda_plan *p, cudaStream_t s, const Operands &op,
     launch_tile_numeric(op, p->st.b_nnz, p->st.tiles.p, p->st.n_tiles, p->st.desc.p,
                         p->st.lens.p, p->st.tab.p, c_rp, c_val, p->st.stage, p->st.aseg,
                         p->st.max_out, s);
-    ++launches;
+    launches += 1 + launch_pattern_kernels(p->st, op, c_rp, c_val, s);
     if (p->st.n_lo > 0) {
       launch_pat_numeric(op, p->ops.p, p->st.lo_rows.p, p->st.lo_ids.p, p->st.n_lo, c_rp,
                          c_val, p->sh_pat_off.p, p->sh_steps.p, p->sh_rec.p, p->sh_max_ops,
@@ -1497,7 +1619,7 @@ rvsp_status_t rvsp_cuda_numeric(rvsp_cuda_plan_t p, void *stream,
         launch_tile_numeric(op, p->rt.b_nnz, p->rt.tiles.p, p->rt.n_tiles, p->rt.desc.p,
                             p->rt.lens.p, p->rt.tab.p, c_row_ptr, c_values, p->rt.stage,
                             p->rt.aseg, p->rt.max_out, s);
-        ph.launches += 1;
+        ph.launches += 1 + launch_pattern_kernels(p->rt, op, c_row_ptr, c_values, s);
         if (p->rt.n_lo > 0) {
           launch_pat_numeric(op, p->ops.p, p->rt.lo_rows.p, p->rt.lo_ids.p, p->rt.n_lo,
                              c_row_ptr, c_values, p->pat_off.p, p->pat_steps.p, p->pat_rec.p,

@@ -38,6 +38,7 @@ struct rvsp_spgemm_descr {
     int32_t merge_policy;
     int32_t row_tiles;
     int32_t shift_classes;
+    int32_t pattern_kernels;
 
     int32_t c_nnz;
     rvsp_dbuf_t c_row_ptr; /* analysed row pointers, device, a_rows + 1 */
@@ -73,6 +74,7 @@ rvsp_status_t rvsp_spgemm_descr_create(rvsp_spgemm_descr_t *descr)
     d->capacity_scale = 1.15f;
     d->row_tiles = 1;
     d->shift_classes = 1;
+    d->pattern_kernels = 1;
     *descr = d;
     return RVSP_SUCCESS;
 }
@@ -125,6 +127,16 @@ rvsp_status_t rvsp_spgemm_set_shift_classes(rvsp_spgemm_descr_t d, int32_t enabl
         return RVSP_ERROR_INVALID_ARGUMENT;
     d->shift_classes = enable;
     return d->plan ? rvsp_cuda_plan_set_shift_classes(d->plan, enable) : RVSP_SUCCESS;
+}
+
+rvsp_status_t rvsp_spgemm_set_pattern_kernels(rvsp_spgemm_descr_t d, int32_t enable)
+{
+    if (d == NULL)
+        return RVSP_ERROR_NULL_POINTER;
+    if (enable != 0 && enable != 1)
+        return RVSP_ERROR_INVALID_ARGUMENT;
+    d->pattern_kernels = enable;
+    return d->plan ? rvsp_cuda_plan_set_pattern_kernels(d->plan, enable) : RVSP_SUCCESS;
 }
 
 rvsp_status_t rvsp_spgemm_get_shift_rows(rvsp_spgemm_descr_t d, int32_t *n_out)
@@ -272,6 +284,8 @@ static rvsp_status_t ensure_device(rvsp_spgemm_descr_t d)
     rvsp_status_t st = rvsp_cuda_plan_set_row_tiles(d->plan, d->row_tiles);
     if (st == RVSP_SUCCESS)
         st = rvsp_cuda_plan_set_shift_classes(d->plan, d->shift_classes);
+    if (st == RVSP_SUCCESS)
+        st = rvsp_cuda_plan_set_pattern_kernels(d->plan, d->pattern_kernels);
     if (st != RVSP_SUCCESS)
         return st;
     return rvsp_cuda_plan_set_merge_policy(d->plan, d->merge_policy);

@@ -155,6 +155,10 @@ SIGNATURES = {
     "rvsp_cuda_plan_shift_rows": (_i32, [_vp]),
     "rvsp_spgemm_set_shift_classes": (_int, [_vp, _i32]),
     "rvsp_cuda_plan_set_persistent": (_int, [_vp, _i32, _i32]),
+    "rvsp_cuda_plan_set_pattern_kernels": (_int, [_vp, _i32]),
+    "rvsp_cuda_plan_pattern_kernel_rows": (_i32, [_vp]),
+    "rvsp_cuda_pattern_kernel_stats": (None, [_P(_i32), _P(C.c_double)]),
+    "rvsp_spgemm_set_pattern_kernels": (_int, [_vp, _i32]),
     "rvsp_spgemm_batch_set_persistent": (_int, [_vp, _i32, _i32]),
     "rvsp_spgemm_batch_get_tuning": (_int, [_vp, _P(_i32), _P(_i32), _P(_i32),
                                             _P(C.c_float), _P(_i32)]),

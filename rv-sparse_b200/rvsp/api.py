@@ -299,6 +299,11 @@ class Descriptor:
         """Row tiles for numeric-only computes (on by default)."""
         L.check(self.lib.rvsp_spgemm_set_row_tiles(self.h, int(bool(enable))), "set_row_tiles")
 
+    def set_pattern_kernels(self, enable: bool):
+        """Compiled kernels for the largest row-tile patterns (on by default)."""
+        L.check(self.lib.rvsp_spgemm_set_pattern_kernels(self.h, int(bool(enable))),
+                "set_pattern_kernels")
+
     def set_shift_classes(self, enable: bool):
         """Shift classes in work_estimation (on by default)."""
         L.check(self.lib.rvsp_spgemm_set_shift_classes(self.h, int(bool(enable))),

@@ -130,6 +130,9 @@ def test_reuse_map_implicit_on_stencil():
     dA = DeviceCSR.from_host(A)
     plan = C.c_void_p()
     L.check(lib.rvsp_cuda_plan_create(C.byref(plan)), "plan_create")
+    # the reuse map itself: shift classes off (with them, the translated rows
+    # never reach the map)
+    L.check(lib.rvsp_cuda_plan_set_shift_classes(plan, 0), "set_shift_classes")
     try:
         rp, n = _symbolic(lib, plan, dA, dA)
         ci = torch.zeros(n, dtype=torch.int32, device="cuda")

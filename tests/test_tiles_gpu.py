@@ -62,7 +62,8 @@ def _bits(x):
     return np.ascontiguousarray(x, np.float32).view(np.uint32)
 
 
-def _repeats(A, B, seeds, tiles=True, min_tiled=1, same_ab=False):
+def _repeats(A, B, seeds, tiles=True, min_tiled=1, same_ab=False, pattern_kernels=True,
+             min_jit=0):
     """Fill once, then numeric-only repeats with new A values (and B's when B
     is A); every repeat against the oracle.  Returns the tiled row count and
     the last C values."""
@@ -73,6 +74,8 @@ def _repeats(A, B, seeds, tiles=True, min_tiled=1, same_ab=False):
     plan = _Plan(lib)
     try:
         L.check(lib.rvsp_cuda_plan_set_row_tiles(plan.h, 1 if tiles else 0), "set_row_tiles")
+        L.check(lib.rvsp_cuda_plan_set_pattern_kernels(plan.h, 1 if pattern_kernels else 0),
+                "set_pattern_kernels")
         rp, n = plan.symbolic(dA, dB)
         ci = torch.zeros(max(n, 1), dtype=torch.int32, device="cuda")
         cv = torch.zeros(max(n, 1), dtype=torch.float32, device="cuda")
@@ -94,6 +97,8 @@ def _repeats(A, B, seeds, tiles=True, min_tiled=1, same_ab=False):
                 f"{int((_bits(got) != _bits(want_cv)).sum())} values differ"
             last = got
         tiled = lib.rvsp_cuda_plan_tiled_rows(plan.h)
+        jit = lib.rvsp_cuda_plan_pattern_kernel_rows(plan.h)
+        assert jit >= min_jit if pattern_kernels else jit == 0
         if tiles:
             assert tiled >= min_tiled
         else:
@@ -204,3 +209,42 @@ def test_descriptor_row_tiles_switch():
     assert np.array_equal(_bits(outs[0]), _bits(outs[1]))
     A2 = A.with_values(scaled)
     assert np.array_equal(_bits(outs[0]), _bits(oracle.spgemm(A2, A2)[2]))
+
+
+@pytest.mark.parametrize("shift", [0, 1])
+def test_pattern_kernels_match_table_kernel(shift):
+    # the largest pattern of a 24^3 stencil gets a kernel compiled for it
+    # (registers for the outputs); its values equal the table kernel's and
+    # the oracle's, with the shift classes on (members) and off (shared maps)
+    import torch
+    lib = L.load()
+    A = gen.stencil_3d_27(24)
+    outs = []
+    for jit in (True, False):
+        dA = DeviceCSR.from_host(A)
+        plan = _Plan(lib)
+        try:
+            L.check(lib.rvsp_cuda_plan_set_shift_classes(plan.h, shift), "set_shift_classes")
+            L.check(lib.rvsp_cuda_plan_set_pattern_kernels(plan.h, int(jit)),
+                    "set_pattern_kernels")
+            rp, n = plan.symbolic(dA, dA)
+            ci = torch.zeros(n, dtype=torch.int32, device="cuda")
+            cv = torch.zeros(n, dtype=torch.float32, device="cuda")
+            plan.numeric(dA, dA, rp, ci, cv, 1)
+            rng = np.random.default_rng(17)
+            vals = (A.values + rng.uniform(-0.01, 0.01, A.nnz)).astype(np.float32)
+            dA.values.copy_(torch.from_numpy(vals))
+            torch.cuda.synchronize()
+            cv.fill_(float("nan"))
+            plan.numeric(dA, dA, rp, ci, cv, 0)
+            rows = lib.rvsp_cuda_plan_pattern_kernel_rows(plan.h)
+            assert (rows > 0) == jit, rows
+            outs.append(cv.cpu().numpy())
+            A2 = A.with_values(vals)
+            assert np.array_equal(_bits(outs[-1]), _bits(oracle.spgemm(A2, A2)[2]))
+        finally:
+            plan.close()
+    assert np.array_equal(_bits(outs[0]), _bits(outs[1]))
+    compiles, ms = C.c_int32(), C.c_double()
+    lib.rvsp_cuda_pattern_kernel_stats(C.byref(compiles), C.byref(ms))
+    assert compiles.value >= 1
