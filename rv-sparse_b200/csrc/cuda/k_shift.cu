@@ -202,10 +202,20 @@ shift_insert_kernel(const int32_t *__restrict__ on, int32_t n,
   if (key == 0ull || (peers & lanemask_lt()) != 0u) return;
   uint32_t s = key_slot(key, mask);
   for (unsigned long long t = 0; t <= mask; ++t) {
-    const unsigned long long prev = atomicCAS(tkey + s, 0ull, key);
-    if (prev == 0ull || prev == key) {
-      atomicMin(trow + s, i);
+    // A slot that already holds the key with a row no larger than i needs
+    // no atomics: most rows of a stencil share one key, and most of them
+    // arrive after a smaller row of it.
+    const unsigned long long seen = *reinterpret_cast<volatile unsigned long long *>(tkey + s);
+    if (seen == key) {
+      if (*reinterpret_cast<volatile int32_t *>(trow + s) > i) atomicMin(trow + s, i);
       return;
+    }
+    if (seen == 0ull) {
+      const unsigned long long prev = atomicCAS(tkey + s, 0ull, key);
+      if (prev == 0ull || prev == key) {
+        atomicMin(trow + s, i);
+        return;
+      }
     }
     s = (s + 1) & static_cast<uint32_t>(mask);
   }
@@ -309,12 +319,25 @@ shift_rresolve_kernel(const int32_t *__restrict__ on, int32_t a_rows,
 __global__ void __launch_bounds__(kThreads)
 shift_share_kernel(const int32_t *__restrict__ on, int32_t n, const int32_t *__restrict__ rcls,
                    int32_t *__restrict__ share) {
+  __shared__ int32_t s_c, s_n;
   if (!*on) return;
   const int32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   const int32_t c = i < n ? rcls[i] : -1;
   const bool member = i < n && c != i;
-  const unsigned peers = __match_any_sync(kFull, member ? c : -1 - lane_id());
-  if (member && (peers & lanemask_lt()) == 0u) atomicAdd(share + c, __popc(peers));
+  // the block's first row's class is counted in shared memory (a stencil
+  // block is mostly one class), the others warp-aggregated
+  if (threadIdx.x == 0) {
+    s_c = member ? c : -1;
+    s_n = 0;
+  }
+  __syncthreads();
+  const bool local = member && c == s_c;
+  const unsigned peers = __match_any_sync(kFull, member && !local ? c : -1 - lane_id());
+  if (member && !local && (peers & lanemask_lt()) == 0u) atomicAdd(share + c, __popc(peers));
+  const unsigned lb = __ballot_sync(kFull, local);
+  if (lb && lane_id() == 0) atomicAdd(&s_n, __popc(lb));
+  __syncthreads();
+  if (threadIdx.x == 0 && s_n) atomicAdd(share + s_c, s_n);
 }
 
 // Candidates: a canonical row shared by at least min_share - 1 others gets
