@@ -29,6 +29,7 @@ enum DevStatus : int32_t {
   kDevKeyMissing = 2,     // numeric reuse looked up a column not in C's row
   kDevCountMismatch = 3,  // a row produced a different nnz than analysed
   kDevBadClass = 4,
+  kDevWaitTimeout = 5,    // a bounded wait on a copy ran out
 };
 
 __device__ __forceinline__ int lane_id() { return threadIdx.x & 31; }

@@ -9,33 +9,56 @@
 // lengths and every product's position are constants -- and compiles it with
 // NVRTC for the GPU in use.  Each lane keeps its row's outputs in registers
 // (c0 ... c{m-1}, named statically), so a product is one shared load of b, a
-// multiply and an add:
+// multiply and an add.  One warp takes one tile (up to 32 consecutive rows of
+// the pattern, one per lane):
 //
-//   for each A nonzero j (ascending, unrolled): stage the lanes' B span (as in
-//   k_tile.cu, two buffers, cp.async);  c[q(j,e)] = fl(c[q(j,e)] + fl(a_j * b))
-//   for every entry e of B row k_j (unrolled, q(j,e) a constant);
+//   A segment: the tile's A values and, per A nonzero, the start of its B row
+//   (b_rp[a_col]) into shared memory;
+//   the A nonzeros are cut into groups whose B spans overlap (in a stencil
+//   the three x-neighbours of a row read B rows one apart, so the tile's
+//   three spans share all but two rows; the grouping is chosen when the
+//   kernel is built, from the largest union span over the pattern's tiles);
+//   per group, the union of the lanes' B rows is one contiguous range of B
+//   values, copied into shared memory by one bulk copy (cp.async.bulk, the
+//   copy engine; its completion is counted on an mbarrier), one group ahead
+//   of the arithmetic (two buffers);
+//   for each A nonzero j of the group (ascending) and entry e of B row k_j:
+//     c[q(j,e)] = fl(c[q(j,e)] + fl(a_j * b[k_j][e]))   (q a constant)
 //
-// and the rows go to C through shared memory in coalesced chunks of 32
-// positions.  Accumulators start from a run-time +0.0f (a kernel argument,
-// so no compiler can fold 0 + p to p: +0 + -0 must give +0) and every
-// product and sum is rounded separately (__fmul_rn, __fadd_rn, -fmad=false),
-// in ascending A-nonzero order: the reference's order and rounding
-// (gustavson_core_f32.inc:31-62, accum_scalar_f32.c:20-71), so values equal
-// the table kernel's bit for bit.
+// and the outputs go to C through shared memory: when the tile's rows are
+// one run of consecutive rows, their C rows are one contiguous block (equal
+// lengths), which is written by one bulk store (plain stores for the ends
+// outside whole 16-byte units); otherwise row by row, coalesced.  Accumulators start from a
+// run-time +0.0f (a kernel argument, so no compiler can fold 0 + p to p:
+// +0 + -0 must give +0) and every product and sum is rounded separately
+// (__fmul_rn, __fadd_rn, -fmad=false), in ascending A-nonzero order: the
+// reference's order and rounding (gustavson_core_f32.inc:31-62,
+// accum_scalar_f32.c:20-71), so values equal the table kernel's bit for bit.
+//
+// A bulk copy moves whole 16-byte units: the range is widened to the units
+// that hold its first and last B values.  Every unit read holds at least one
+// B value of the range, so no copy reads outside the pages of B's values,
+// and the B index of the first staged float is recorded per buffer.  Each
+// wait on an mbarrier is bounded (about a second of clock cycles); a wait
+// that runs out makes the warp wait, again bounded, for the copies it has in
+// flight, record kDevWaitTimeout in the status word and return.
 //
 // NVRTC is opened at run time (dlopen of libnvrtc.so.12); without it, or if
-// a compile fails, the pattern stays on the table kernel.  Compiled kernels
-// are kept for the life of the process, keyed by their source text, so a
-// pattern is compiled once per process.
+// a compile fails, the pattern stays on the table kernel.  The patterns of
+// one structure compile side by side, one host thread each.  Compiled
+// kernels are kept for the life of the process, keyed by their source text,
+// so a pattern is compiled once per process.
 #include <cuda_runtime.h>
 #include <dlfcn.h>
 #include <nvrtc.h>
 
 #include <chrono>
+#include <climits>
 #include <cstdio>
 #include <map>
 #include <mutex>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "device_common.cuh"
@@ -83,180 +106,329 @@ bool open_nvrtc() {
 }
 
 // ---- the generated source ---------------------------------------------------
+// The helpers of every pattern kernel: mbarrier init / bounded wait, the
+// bulk copies of a B range and of a tile's record and A values, the bulk
+// store of a C block.
 const char *kPrelude = R"(
 typedef unsigned int u32;
+typedef unsigned long long u64;
+typedef unsigned short u16;
 #define FULL 0xffffffffu
-__device__ __forceinline__ void cpa16(float *s, const float *g) {
-  const u32 a = (u32)__cvta_generic_to_shared(s);
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(a), "l"(g) : "memory");
+__device__ __forceinline__ u32 saddr(const void *p) { return (u32)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void bar_init(u32 bar) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(bar) : "memory");
 }
-__device__ __forceinline__ void cpa4(float *s, const float *g) {
-  const u32 a = (u32)__cvta_generic_to_shared(s);
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(a), "l"(g) : "memory");
+__device__ __forceinline__ bool bar_try(u32 bar, u32 ph) {
+  u32 ok;
+  asm volatile("{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+               " selp.u32 %0, 1, 0, p;\n}\n" : "=r"(ok) : "r"(bar), "r"(ph) : "memory");
+  return ok != 0u;
 }
-__device__ __forceinline__ void cpa_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-__device__ __forceinline__ void cpa_wait1() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
-__device__ __forceinline__ void cpa_wait0() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
-// B values [lo, hi) into dst; returns the B index dst[0] stands for.
-__device__ __forceinline__ int stage_span(float *dst, const float *__restrict__ b_val, int lo,
-                                          int hi, int b_nnz, bool al, int lane) {
-  if (al) {
-    const int c0 = lo & ~3;
-    const int chunks = (hi - c0 + 3) >> 2;
-    for (int c = lane; c < chunks; c += 32) {
-      const int g = c0 + 4 * c;
-      if (g + 4 <= b_nnz) cpa16(dst + 4 * c, b_val + g);
-      else for (int x = g; x < hi; ++x) cpa4(dst + (x - c0), b_val + x);
-    }
-    return c0;
+// Waits for phase ph of the mbarrier; false after about 2^31 clock cycles.
+__device__ __forceinline__ bool bar_wait(u32 bar, u32 ph) {
+  if (bar_try(bar, ph)) return true;
+  const long long t0 = clock64();
+  while (!bar_try(bar, ph))
+    if (clock64() - t0 > (1ll << 31)) return false;
+  return true;
+}
+__device__ __forceinline__ void bulk_load(void *dst, u64 src, u32 bytes, u32 bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes"
+               " [%0], [%1], %2, [%3];\n"
+               ::"r"(saddr(dst)), "l"(src), "r"(bytes), "r"(bar) : "memory");
+}
+__device__ __forceinline__ void expect(u32 bar, u32 bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n"
+               ::"r"(bar), "r"(bytes) : "memory");
+}
+// Lane 0 copies B values [lo, hi) (widened to whole 16-byte units) to dst,
+// completing on bar.  Returns the position in dst of B value lo.
+__device__ __forceinline__ int stage(float *dst, const float *b_val, int lo, int hi, u32 bar,
+                                     int lane) {
+  const u64 g0 = (u64)(b_val + lo);
+  if (lane == 0) {
+    const u64 a0 = g0 & ~15ull;
+    const u64 a1 = ((u64)(b_val + hi) + 15ull) & ~15ull;
+    expect(bar, (u32)(a1 - a0));
+    bulk_load(dst, a0, (u32)(a1 - a0), bar);
   }
-  for (int x = lo + lane; x < hi; x += 32) cpa4(dst + (x - lo), b_val + x);
-  return lo;
+  return (int)((g0 & 15ull) >> 2);
+}
+// Lane 0 copies a tile's record (rwords words of prog) to dst and its A
+// values a_val[r.x, r.x + r.y) (widened to 16-byte units) after it,
+// completing on bar.
+__device__ __forceinline__ void stage_tile(float *dst, const int *prog, int rwords, int2 r,
+                                           int tile, const float *a_val, u32 bar, int lane) {
+  if (lane == 0) {
+    const u64 a0 = (u64)(a_val + r.x) & ~15ull;
+    const u64 a1 = ((u64)(a_val + r.x + r.y) + 15ull) & ~15ull;
+    const u32 rb = (u32)rwords * 4u, ab = r.y > 0 ? (u32)(a1 - a0) : 0u;
+    expect(bar, rb + ab);
+    bulk_load(dst, (u64)(prog + (size_t)tile * rwords), rb, bar);
+    if (ab) bulk_load(dst + rwords, a0, ab, bar);
+  }
+}
+__device__ __forceinline__ void store_block(float *g, const float *s, int bytes) {
+  asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;\n"
+               ::"l"(g), "r"(saddr(s)), "r"(bytes) : "memory");
+  asm volatile("cp.async.bulk.commit_group;\n" ::: "memory");
+  asm volatile("cp.async.bulk.wait_group.read 0;\n" ::: "memory");
 }
 )";
 
+// Registers of a pattern kernel with m outputs: the m accumulators and
+// about 19 for addresses and staged b values in flight, then raised to the
+// most that keeps as many warps per scheduler (a quarter of the SM's 64K
+// registers, allocated in units of 256 per warp): 168 at m = 125, 3 warps.
+int pattern_regs(int m) {
+  int r = (m + 19 + 7) & ~7;
+  r = r < 64 ? 64 : r > 255 ? 255 : r;
+  const int per_sched = 16384 / (((r * 32) + 255) & ~255);
+  int up = (16384 / per_sched / 32) & ~7;
+  return up > 255 ? 255 : up < r ? r : up;
+}
+
+// Words of a tile record (see jit_record_words).
+int record_words(int na, int ngroups) { return (4 + 2 * ngroups + 16 + 16 * na + 3) & ~3; }
+
 // Source of the kernel for one pattern: na A nonzeros with B row lengths
-// len[j], slot[t] the output position of flattened product t, m outputs.
-std::string pattern_source(int na, const int *len, const std::vector<int> &slot, int m) {
+// len[j], slot[t] the output position of flattened product t (in j, e
+// order), m outputs, and the groups of A nonzeros staged together
+// ([first, end) ranges over j, in order, covering every j with len > 0).
+//
+// The kernel is persistent: warp w takes tiles w, w + 2 * gridDim.x, ...
+// Per warp, shared memory holds two tile buffers (record + A values) around
+// two B stage buffers: [tile 0 | stage 0 | stage 1 | tile 1].  While a tile
+// is computed, the next tile's record and A values are copied into the other
+// tile buffer; the outputs of a tile go out through its own tile buffer and
+// the stage buffers (one contiguous region either way), 16 rows at a time.
+std::string pattern_source(int na, const int *len, const std::vector<int> &slot, int m,
+                           const std::vector<std::pair<int, int>> &groups) {
   std::string s(kPrelude);
   char buf[1024];
-  s += "extern \"C\" __global__ void __launch_bounds__(64)\n"
-       "rvsp_pattern_tiles(const int4 *__restrict__ tiles, int ntiles,\n"
-       "    const int *__restrict__ a_rp, const int *__restrict__ a_col,\n"
-       "    const float *__restrict__ a_val, const int *__restrict__ b_rp,\n"
-       "    const float *__restrict__ b_val, int b_nnz, const int *__restrict__ c_rp,\n"
-       "    float *__restrict__ c_val, int stage_cap, int work_floats, float zero) {\n"
+  const int ms = (m & 1) ? m : m + 1;  // odd row stride: conflict-free stores
+  const int ng = static_cast<int>(groups.size());
+  const int rw = record_words(na, ng);
+  const int aoff_w = 4 + 2 * ng, d_w = aoff_w + 16;
+  const int mid = ng > 1 ? 1 : 0;  // the next tile's copies go out with group mid's
+  std::vector<int> t_of(size_t(na) + 1, 0);
+  for (int j = 0; j < na; ++j) t_of[size_t(j) + 1] = t_of[size_t(j)] + len[j];
+  snprintf(buf, sizeof(buf), "#define RW %d\n#define M %d\n#define MS %d\n", rw, m, ms);
+  s += buf;
+  snprintf(buf, sizeof(buf), "extern \"C\" __global__ void __maxnreg__(%d)\n", pattern_regs(m));
+  s += buf;
+  s += "rvsp_pattern_tiles(const int *__restrict__ prog, const int2 *__restrict__ arange,\n"
+       "    int ntiles, const float *__restrict__ a_val, const float *__restrict__ b_val,\n"
+       "    const int *__restrict__ c_rp, float *__restrict__ c_val, int stage_cap,\n"
+       "    int abuf_floats, int work_floats, float zero, int *__restrict__ status) {\n"
        "  extern __shared__ __align__(16) float sm[];\n"
+       "  __shared__ __align__(8) u64 bars[8];\n"
        "  const int wib = threadIdx.x >> 5, lane = threadIdx.x & 31;\n"
        "  float *const work = sm + wib * work_floats;\n"
-       "  const int w = blockIdx.x * 2 + wib;\n"
-       "  if (w >= ntiles) return;\n"
-       "  const int4 t = tiles[w];\n"
-       "  const int row0 = t.x;\n"
-       "  const u32 mask = (u32)t.y;\n"
-       "  const bool active = (mask >> lane) & 1u;\n"
-       "  const int row = row0 + lane;\n"
-       "  const bool al = (((unsigned long long)b_val) & 15ull) == 0;\n"
-       "  const int seg0 = a_rp[row0];\n"
-       "  int my_p = 0, cs = 0;\n"
-       "  if (active) { my_p = a_rp[row] - seg0; cs = c_rp[row]; }\n"
-       "  const int seg = a_rp[__reduce_max_sync(FULL, active ? row : row0) + 1] - seg0;\n"
-       "  {\n"
-       "    int *scol = (int *)work; float *sval = work + seg;\n"
-       "    for (int i = lane; i < seg; i += 32) {\n"
-       "      scol[i] = __ldg(a_col + seg0 + i); sval[i] = __ldg(a_val + seg0 + i);\n"
+       "  float *const sb0 = work + abuf_floats;\n"
+       "  float *const sb1 = sb0 + stage_cap;\n"
+       "  float *const tb1 = sb1 + stage_cap;\n"
+       "  const int stride = gridDim.x * 2;\n"
+       "  int tile = blockIdx.x * 2 + wib;\n"
+       "  if (tile >= ntiles) return;\n"
+       "  const u32 bar0 = saddr(&bars[4 * wib]), bar1 = bar0 + 8u;\n"
+       "  const u32 bara0 = bar0 + 16u, bara1 = bar0 + 24u;\n"
+       "  if (lane == 0) {\n"
+       "    bar_init(bar0); bar_init(bar1); bar_init(bara0); bar_init(bara1);\n"
+       "    asm volatile(\"fence.mbarrier_init.release.cluster;\\n\" ::: \"memory\");\n"
+       "  }\n"
+       "  __syncwarp();\n"
+       "  u32 pb0 = 0u, pb1 = 0u, pa0 = 0u, pa1 = 0u;\n"
+       "  stage_tile(work, prog, RW, __ldg(arange + tile), tile, a_val, bara0, lane);\n"
+       "  for (int it = 0; tile < ntiles; ++it, tile += stride) {\n"
+       "    const bool odd = (it & 1) != 0;\n"
+       "    float *const ab = odd ? tb1 : work;\n"
+       "    float *const nb = odd ? work : tb1;\n"
+       "    float *const region = odd ? sb0 : work;\n"
+       "    const u32 bara = odd ? bara1 : bara0, barn = odd ? bara0 : bara1;\n"
+       "    const u32 pa = odd ? pa1 : pa0, pn = odd ? pa0 : pa1;\n"
+       "    const int nxt = tile + stride;\n"
+       "    const int2 nr = nxt < ntiles ? __ldg(arange + nxt) : make_int2(0, 0);\n"
+       "    if (!__all_sync(FULL, bar_wait(bara, pa))) {\n"
+       "      bar_wait(bara, pa);\n"
+       "      if (lane == 0) atomicCAS(status, 0, 5);\n"
+       "      return;\n"
+       "    }\n"
+       "    if (odd) pa1 ^= 1u; else pa0 ^= 1u;\n"
+       "    const int *const rec = (const int *)ab;\n"
+       "    const int row0 = rec[0];\n"
+       "    const u32 mask = (u32)rec[1];\n"
+       "    const bool active = ((mask >> lane) & 1u) != 0u;\n"
+       "    const int cs = active ? __ldg(c_rp + row0 + lane) : 0;\n"
+       "    const float *const sa = ab + RW + (int)(((u64)(a_val + rec[2]) & 15ull) >> 2) +\n"
+       "                            (int)((const u16 *)(rec + ";
+  snprintf(buf, sizeof(buf), "%d))[lane];\n    const u16 *const dd = (const u16 *)(rec + %d) + lane;\n",
+           aoff_w, d_w);
+  s += buf;
+  for (int q = 0; q < m; ++q) {
+    snprintf(buf, sizeof(buf), "    float c%d = zero;\n", q);
+    s += buf;
+  }
+  s += "    int cb0 = stage(sb0, b_val, rec[4], rec[5], bar0, lane), cb1 = 0;\n";
+  for (int g = 0; g < ng; ++g) {
+    const int b = g & 1;
+    if (g + 1 < ng) {
+      snprintf(buf, sizeof(buf),
+               "    cb%d = stage(sb%d, b_val, rec[%d], rec[%d], bar%d, lane);\n",
+               (g + 1) & 1, (g + 1) & 1, 4 + 2 * (g + 1), 5 + 2 * (g + 1), (g + 1) & 1);
+      s += buf;
+    }
+    if (g == mid) s += "    if (nxt < ntiles) stage_tile(nb, prog, RW, nr, nxt, a_val, barn, lane);\n";
+    // bounded wait; on a timeout wait (bounded) for the copies still out
+    snprintf(buf, sizeof(buf), "    if (!__all_sync(FULL, bar_wait(bar%d, pb%d))) {\n", b, b);
+    s += buf;
+    snprintf(buf, sizeof(buf), "      bar_wait(bar%d, pb%d);\n", b, b);
+    s += buf;
+    if (g + 1 < ng) {
+      snprintf(buf, sizeof(buf), "      bar_wait(bar%d, pb%d);\n", (g + 1) & 1, (g + 1) & 1);
+      s += buf;
+    }
+    if (g >= mid) s += "      if (nxt < ntiles) bar_wait(barn, pn);\n";
+    s += "      if (lane == 0) atomicCAS(status, 0, 5);\n      return;\n    }\n";
+    snprintf(buf, sizeof(buf), "    pb%d ^= 1u;\n    {\n      const float *const sbb = sb%d + cb%d;\n",
+             b, b, b);
+    s += buf;
+    for (int j = groups[size_t(g)].first; j < groups[size_t(g)].second; ++j) {
+      if (len[j] == 0) continue;
+      snprintf(buf, sizeof(buf),
+               "      {\n        const float a = sa[%d];\n"
+               "        const float *const st = sbb + dd[%d];\n",
+               j, j * 32);
+      s += buf;
+      for (int e = 0; e < len[j]; ++e) {
+        const int q = slot[size_t(t_of[size_t(j)] + e)];
+        snprintf(buf, sizeof(buf), "        c%d = __fadd_rn(c%d, __fmul_rn(a, st[%d]));\n", q,
+                 q, e);
+        s += buf;
+      }
+      s += "      }\n";
+    }
+    s += "    }\n    __syncwarp();\n";
+  }
+  // outputs, 16 rows at a time: the active lanes' rows in lane order at
+  // region[sh + (rank - base) * MS]; when the active lanes are one run of
+  // consecutive rows their C rows are one block (equal lengths), aligned by
+  // sh and written by one bulk store
+  snprintf(buf, sizeof(buf),
+           "    const int first = __ffs(mask) - 1, nact = __popc(mask);\n"
+           "    const bool contig = %s (mask >> first) == (nact == 32 ? FULL : (1u << nact) - 1u);\n"
+           "    const int rank = __popc(mask & ((1u << lane) - 1u));\n"
+           "    const int cs0 = __shfl_sync(FULL, cs, first);\n"
+           "    for (int base = 0; base < nact; base += 16) {\n"
+           "      const int cnt = nact - base < 16 ? nact - base : 16;\n"
+           "      const int sh = contig ? (int)(((u64)(c_val + cs0 + base * M) & 15ull) >> 2) : 0;\n"
+           "      if (active && rank >= base && rank < base + 16) {\n"
+           "        float *const o = region + sh + (rank - base) * MS;\n",
+           ms == m ? "" : "false &&");
+  s += buf;
+  for (int q = 0; q < m; ++q) {
+    snprintf(buf, sizeof(buf), "        o[%d] = c%d;\n", q, q);
+    s += buf;
+  }
+  s += "      }\n"
+       "      if (contig) {\n"
+       "        asm volatile(\"fence.proxy.async.shared::cta;\\n\" ::: \"memory\");\n"
+       "        __syncwarp();\n"
+       "        float *const g = c_val + cs0 + base * M;\n"
+       "        const int total = cnt * M;\n"
+       "        const int head = min((4 - sh) & 3, total);\n"
+       "        const int body = (total - head) & ~3;\n"
+       "        if (lane < head) g[lane] = region[sh + lane];\n"
+       "        if (head + body + lane < total) g[head + body + lane] = region[sh + head + body + lane];\n"
+       "        if (lane == 0 && body > 0) store_block(g + head, region + sh + head, body * 4);\n"
+       "      } else {\n"
+       "        __syncwarp();\n"
+       "        int k = 0;\n"
+       "        for (u32 mm = mask; mm; mm &= mm - 1u, ++k) {\n"
+       "          const int cb = __shfl_sync(FULL, cs, __ffs(mm) - 1);\n"
+       "          if (k >= base && k < base + 16) {\n"
+       "            const float *const src = region + (k - base) * MS;\n"
+       "            for (int q = lane; q < M; q += 32) c_val[cb + q] = src[q];\n"
+       "          }\n"
+       "        }\n"
+       "      }\n"
+       "      __syncwarp();\n"
        "    }\n"
        "  }\n"
-       "  __syncwarp();\n";
-  snprintf(buf, sizeof(buf), "  float av[%d]; int rp[%d];\n", na, na);
-  s += buf;
-  snprintf(buf, sizeof(buf),
-           "  {\n    const int *scol = (const int *)work; const float *sval = work + seg;\n"
-           "#pragma unroll\n    for (int j = 0; j < %d; ++j) {\n"
-           "      av[j] = 0.0f; rp[j] = 0;\n"
-           "      if (active) { av[j] = sval[my_p + j]; rp[j] = __ldg(b_rp + scol[my_p + j]); }\n"
-           "    }\n  }\n  __syncwarp();\n",
-           na);
-  s += buf;
-  // accumulators
-  for (int q = 0; q < m; ++q) {
-    snprintf(buf, sizeof(buf), "  float c%d = zero;\n", q);
-    s += buf;
-  }
-  s += "  int cb0 = 0, cb1 = 0;\n";
-  snprintf(buf, sizeof(buf),
-           "  { const int lo = __reduce_min_sync(FULL, active ? rp[0] : 0x7fffffff);\n"
-           "    const int hi = __reduce_max_sync(FULL, active ? rp[0] + %d : (int)0x80000000);\n"
-           "    cb0 = stage_span(work, b_val, lo, hi, b_nnz, al, lane); cpa_commit(); }\n",
-           len[0]);
-  s += buf;
-  int t0 = 0;
-  for (int j = 0; j < na; ++j) {
-    s += "  {\n";
-    if (j + 1 < na) {
-      snprintf(buf, sizeof(buf),
-               "    const int lo = __reduce_min_sync(FULL, active ? rp[%d] : 0x7fffffff);\n"
-               "    const int hi = __reduce_max_sync(FULL, active ? rp[%d] + %d : (int)0x80000000);\n"
-               "    cb%d = stage_span(work + %d * stage_cap, b_val, lo, hi, b_nnz, al, lane);\n"
-               "    cpa_commit(); cpa_wait1();\n",
-               j + 1, j + 1, len[j + 1], (j + 1) & 1, (j + 1) & 1);
-      s += buf;
-    } else {
-      s += "    cpa_wait0();\n";
-    }
-    snprintf(buf, sizeof(buf),
-             "    __syncwarp();\n"
-             "    const float *st = work + %d * stage_cap + (active ? rp[%d] - cb%d : 0);\n"
-             "    const float a = av[%d];\n",
-             j & 1, j, j & 1, j);
-    s += buf;
-    for (int e = 0; e < len[j]; ++e) {
-      const int q = slot[size_t(t0 + e)];
-      snprintf(buf, sizeof(buf), "    c%d = __fadd_rn(c%d, __fmul_rn(a, st[%d]));\n", q, q, e);
-      s += buf;
-    }
-    s += "    __syncwarp();\n  }\n";
-    t0 += len[j];
-  }
-  // output: chunks of 32 positions through shared memory, coalesced per row
-  for (int q0 = 0; q0 < m; q0 += 32) {
-    const int cl = m - q0 < 32 ? m - q0 : 32;
-    s += "  {\n";
-    for (int q = q0; q < q0 + cl; ++q) {
-      snprintf(buf, sizeof(buf), "    work[%d * 33 + lane] = c%d;\n", q - q0, q);
-      s += buf;
-    }
-    snprintf(buf, sizeof(buf),
-             "    __syncwarp();\n"
-             "    for (int r = 0; r < 32; ++r) {\n"
-             "      const int base = __shfl_sync(FULL, cs, r);\n"
-             "      if (((mask >> r) & 1u) && lane < %d) c_val[base + %d + lane] = work[lane * 33 + r];\n"
-             "    }\n"
-             "    __syncwarp();\n  }\n",
-             cl, q0);
-    s += buf;
-  }
-  s += "}\n";
+       "}\n";
   return s;
 }
 
-// Compiles (or finds) the kernel of `src`.  Returns nullptr on failure.
-cudaKernel_t kernel_for(const std::string &src) {
-  std::lock_guard<std::mutex> lock(g_mutex);
-  auto it = g_cache.find(src);
-  if (it != g_cache.end()) return it->second;
-  if (!open_nvrtc()) return nullptr;
+// NVRTC compile of `src` into a cubin for `arch` (empty on failure).  Makes
+// no CUDA call, so several run at once on their own threads.
+std::vector<char> compile_cubin(const std::string &src, const std::string &arch) {
+  std::vector<char> bin;
+  nvrtcProgram prog = nullptr;
+  if (g_nvrtc.create(&prog, src.c_str(), "rvsp_pattern.cu", 0, nullptr, nullptr) !=
+      NVRTC_SUCCESS)
+    return bin;
+  const char *opts[] = {arch.c_str(), "-fmad=false", "--std=c++17", "-default-device"};
+  size_t n = 0;
+  if (g_nvrtc.compile(prog, 4, opts) == NVRTC_SUCCESS &&
+      g_nvrtc.cubin_size(prog, &n) == NVRTC_SUCCESS && n > 0) {
+    bin.resize(n);
+    if (g_nvrtc.cubin(prog, bin.data()) != NVRTC_SUCCESS) bin.clear();
+  }
+  g_nvrtc.destroy(&prog);
+  return bin;
+}
+
+// The kernels of `srcs` (nullptr where a compile failed): cached ones at
+// once, the others compiled side by side, one thread each, then loaded on
+// the calling thread (whose device is the plan's).
+void kernels_for(const std::vector<std::string> &srcs, std::vector<cudaKernel_t> &out) {
+  out.assign(srcs.size(), nullptr);
+  std::vector<size_t> todo;
+  {
+    std::lock_guard<std::mutex> lock(g_mutex);
+    for (size_t i = 0; i < srcs.size(); ++i) {
+      auto it = g_cache.find(srcs[i]);
+      if (it != g_cache.end()) out[i] = it->second;
+      else todo.push_back(i);
+    }
+    if (todo.empty() || !open_nvrtc()) return;
+  }
   int dev = 0, major = 0, minor = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev);
   cudaDeviceGetAttribute(&minor, cudaDevAttrComputeCapabilityMinor, dev);
-  char arch[64];
-  snprintf(arch, sizeof(arch), "--gpu-architecture=sm_%d%da", major, minor);
+  const std::string arch =
+      "--gpu-architecture=sm_" + std::to_string(major) + std::to_string(minor) + "a";
   const auto t0 = std::chrono::steady_clock::now();
-  nvrtcProgram prog = nullptr;
-  cudaKernel_t k = nullptr;
-  if (g_nvrtc.create(&prog, src.c_str(), "rvsp_pattern.cu", 0, nullptr, nullptr) ==
-      NVRTC_SUCCESS) {
-    const char *opts[] = {arch, "-fmad=false", "--std=c++17", "-default-device"};
-    size_t n = 0;
-    if (g_nvrtc.compile(prog, 4, opts) == NVRTC_SUCCESS &&
-        g_nvrtc.cubin_size(prog, &n) == NVRTC_SUCCESS && n > 0) {
-      std::vector<char> bin(n);
-      cudaLibrary_t lib = nullptr;
-      if (g_nvrtc.cubin(prog, bin.data()) == NVRTC_SUCCESS &&
-          cudaLibraryLoadData(&lib, bin.data(), nullptr, nullptr, 0, nullptr, nullptr, 0) ==
-              cudaSuccess &&
-          cudaLibraryGetKernel(&k, lib, "rvsp_pattern_tiles") != cudaSuccess)
-        k = nullptr;
+  std::vector<std::vector<char>> bins(todo.size());
+  std::vector<std::thread> threads;
+  for (size_t k = 0; k < todo.size(); ++k) {
+    try {
+      threads.emplace_back([&bins, &srcs, &todo, &arch, k] {
+        bins[k] = compile_cubin(srcs[todo[k]], arch);
+      });
+    } catch (...) {  // no thread: compile here
+      bins[k] = compile_cubin(srcs[todo[k]], arch);
     }
-    g_nvrtc.destroy(&prog);
   }
-  cudaGetLastError();
+  for (auto &t : threads) t.join();
+  std::lock_guard<std::mutex> lock(g_mutex);
+  for (size_t k = 0; k < todo.size(); ++k) {
+    cudaKernel_t kern = nullptr;
+    cudaLibrary_t lib = nullptr;
+    if (!bins[k].empty() &&
+        (cudaLibraryLoadData(&lib, bins[k].data(), nullptr, nullptr, 0, nullptr, nullptr, 0) !=
+             cudaSuccess ||
+         cudaLibraryGetKernel(&kern, lib, "rvsp_pattern_tiles") != cudaSuccess))
+      kern = nullptr;
+    cudaGetLastError();
+    // a failure is remembered too: the table kernel keeps the pattern
+    g_cache[srcs[todo[k]]] = kern;
+    out[todo[k]] = kern;
+    ++g_compiles;
+  }
   g_compile_ms += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0)
                       .count();
-  ++g_compiles;
-  g_cache[src] = k;  // a failure is remembered too: the table kernel keeps the pattern
-  return k;
 }
 
 // tiles of pattern pid, in order (count at *n, zeroed by the caller)
@@ -273,6 +445,143 @@ tile_select_kernel(const int4 *__restrict__ tiles, int32_t ntiles, int32_t pid,
   if (take) out[base + __popc(b & lanemask_lt())] = tiles[i];
 }
 
+// Per lane and A nonzero j of a tile: the start of B row k_j, or -1 for an
+// inactive lane or an empty B row, into srp[j * 32 + lane].  Eight A
+// nonzeros at a time, so that their loads are in flight together.
+__device__ __forceinline__ void gather_b_starts(int32_t *srp, int32_t na,
+                                                const int32_t *slen, bool active, int32_t p,
+                                                const int32_t *__restrict__ a_col,
+                                                const int32_t *__restrict__ b_rp, int lane) {
+  for (int32_t j0 = 0; j0 < na; j0 += 8) {
+    int32_t col[8];
+#pragma unroll
+    for (int u = 0; u < 8; ++u)
+      col[u] = (active && j0 + u < na && slen[j0 + u] > 0) ? __ldg(a_col + p + j0 + u) : -1;
+#pragma unroll
+    for (int u = 0; u < 8; ++u)
+      if (j0 + u < na) srp[(j0 + u) * 32 + lane] = col[u] >= 0 ? __ldg(b_rp + col[u]) : -1;
+  }
+  __syncwarp();
+}
+
+// Union spans of a pattern's tiles (warp per tile, grid-stride): for every
+// A nonzero j0 and run length g in [1, kJitMaxGroup], span[j0 * kJitMaxGroup
+// + g - 1] = the largest, over the tiles, of (end of the last B value - first
+// B value) that the tile's rows read for A nonzeros j0 .. j0 + g - 1.  A
+// nonzero with an empty B row reads nothing.  span zeroed by the caller.
+__global__ void __launch_bounds__(256)
+span_kernel(const int4 *__restrict__ tiles, int32_t ntiles, int32_t na,
+            const uint16_t *__restrict__ lens, const int32_t *__restrict__ a_rp,
+            const int32_t *__restrict__ a_col, const int32_t *__restrict__ b_rp,
+            int32_t *__restrict__ span) {
+  __shared__ int32_t srp[8][32 * 32];
+  __shared__ int32_t slo[8][32], shi[8][32], slen[32];
+  const int wib = threadIdx.x >> 5, lane = lane_id();
+  if (threadIdx.x < 32) slen[threadIdx.x] = threadIdx.x < na ? lens[threadIdx.x] : 0;
+  __syncthreads();
+  int32_t um[kJitMaxGroup];
+#pragma unroll
+  for (int g = 0; g < kJitMaxGroup; ++g) um[g] = 0;
+  for (int64_t w = int64_t(blockIdx.x) * 8 + wib; w < ntiles; w += int64_t(gridDim.x) * 8) {
+    const int4 t = tiles[w];
+    const bool active = ((static_cast<uint32_t>(t.y) >> lane) & 1u) != 0u;
+    const int32_t p = active ? a_rp[t.x + lane] : 0;
+    gather_b_starts(srp[wib], na, slen, active, p, a_col, b_rp, lane);
+    for (int32_t j = 0; j < na; ++j) {
+      const int32_t r = srp[wib][j * 32 + lane];
+      const int32_t lo = __reduce_min_sync(kFull, r >= 0 ? r : INT_MAX);
+      const int32_t hi = __reduce_max_sync(kFull, r >= 0 ? r + slen[j] : INT_MIN);
+      if (lane == 0) {
+        slo[wib][j] = lo;
+        shi[wib][j] = hi;
+      }
+    }
+    __syncwarp();
+    if (lane < na) {
+      int32_t lo = INT_MAX, hi = INT_MIN;
+#pragma unroll
+      for (int g = 0; g < kJitMaxGroup; ++g) {
+        if (lane + g < na) {
+          lo = min(lo, slo[wib][lane + g]);
+          hi = max(hi, shi[wib][lane + g]);
+          if (hi > lo) um[g] = max(um[g], hi - lo);
+        }
+      }
+    }
+    __syncwarp();
+  }
+  if (lane < na) {
+#pragma unroll
+    for (int g = 0; g < kJitMaxGroup; ++g)
+      if (um[g] > 0) atomicMax(span + lane * kJitMaxGroup + g, um[g]);
+  }
+}
+
+// Tile records of one pattern (warp per tile, grid-stride), rw words each:
+//   [0] first row of the tile, [1] lane mask, [2] A index of the first active
+//   row's first nonzero, [3] A entries from there to the last active row's
+//   end;  [4 + 2g], [5 + 2g]: the B range [lo, hi) that group g stages;
+//   then 32 uint16 A offsets (lane's first nonzero - [2]) and, per A nonzero
+//   j and lane, the uint16 offset of the lane's B row k_j from its group's
+//   lo (0 for inactive lanes and empty B rows).
+// arange[tile] = ([2], [3]); maxima[0] = the largest [3].  Structure only:
+// built once per structure, read by every numeric-only repeat.
+__global__ void __launch_bounds__(256)
+program_kernel(const int4 *__restrict__ tiles, int32_t ntiles, int32_t na, int32_t ngroups,
+               const int2 *__restrict__ groups, const uint16_t *__restrict__ lens,
+               const int32_t *__restrict__ a_rp, const int32_t *__restrict__ a_col,
+               const int32_t *__restrict__ b_rp, int32_t rw, int32_t *__restrict__ prog,
+               int2 *__restrict__ arange, int32_t *__restrict__ maxima) {
+  __shared__ int32_t srp[8][32 * 32];
+  __shared__ int32_t slen[32];
+  const int wib = threadIdx.x >> 5, lane = lane_id();
+  if (threadIdx.x < 32) slen[threadIdx.x] = threadIdx.x < na ? lens[threadIdx.x] : 0;
+  __syncthreads();
+  for (int64_t w = int64_t(blockIdx.x) * 8 + wib; w < ntiles; w += int64_t(gridDim.x) * 8) {
+    const int4 t = tiles[w];
+    const uint32_t mask = static_cast<uint32_t>(t.y);
+    const bool active = ((mask >> lane) & 1u) != 0u;
+    const int first = __ffs(static_cast<int>(mask)) - 1, last = 31 - __clz(static_cast<int>(mask));
+    const int32_t aseg0 = a_rp[t.x + first], aend = a_rp[t.x + last + 1];
+    const int32_t p = active ? a_rp[t.x + lane] : 0;
+    gather_b_starts(srp[wib], na, slen, active, p, a_col, b_rp, lane);
+    int32_t *const rec = prog + w * rw;
+    if (lane == 0) {
+      rec[0] = t.x;
+      rec[1] = t.y;
+      rec[2] = aseg0;
+      rec[3] = aend - aseg0;
+      arange[w] = make_int2(aseg0, aend - aseg0);
+      atomicMax(maxima, aend - aseg0);
+    }
+    uint16_t *const aoff = reinterpret_cast<uint16_t *>(rec + 4 + 2 * ngroups);
+    uint16_t *const d = aoff + 32;
+    aoff[lane] = static_cast<uint16_t>(active ? p - aseg0 : 0);
+    for (int32_t g = 0; g < ngroups; ++g) {
+      const int2 gr = groups[g];
+      int32_t lo = INT_MAX, hi = INT_MIN;
+      for (int32_t j = gr.x; j < gr.y; ++j) {
+        const int32_t r = srp[wib][j * 32 + lane];
+        if (r >= 0) {
+          lo = min(lo, r);
+          hi = max(hi, r + slen[j]);
+        }
+      }
+      lo = __reduce_min_sync(kFull, lo);
+      hi = __reduce_max_sync(kFull, hi);
+      if (lane == 0) {
+        rec[4 + 2 * g] = lo;
+        rec[5 + 2 * g] = hi;
+      }
+      for (int32_t j = gr.x; j < gr.y; ++j) {
+        const int32_t r = srp[wib][j * 32 + lane];
+        d[j * 32 + lane] = static_cast<uint16_t>(r >= 0 ? r - lo : 0);
+      }
+    }
+    __syncwarp();
+  }
+}
+
 // desc[pid].w = 1: the table kernel leaves the pattern's tiles alone.
 __global__ void mark_pattern_kernel(int4 *desc, int32_t pid) { desc[pid].w = 1; }
 
@@ -284,12 +593,57 @@ void jit_stats(int32_t *compiles, double *ms) {
   if (ms) *ms = g_compile_ms;
 }
 
-int jit_pattern_kernel(int na, const int *len, const std::vector<int> &slot, int m,
-                       void **kernel_out) {
-  if (na <= 0 || m <= 0) return 0;
-  const cudaKernel_t k = kernel_for(pattern_source(na, len, slot, m));
-  *kernel_out = reinterpret_cast<void *>(k);
-  return k != nullptr;
+int jit_pattern_kernels(std::vector<JitRequest> &reqs) {
+  std::vector<std::string> srcs;
+  std::vector<size_t> idx;
+  for (size_t i = 0; i < reqs.size(); ++i) {
+    JitRequest &r = reqs[i];
+    r.kernel = nullptr;
+    if (r.na <= 0 || r.na > 32 || r.m <= 0 || r.groups.empty()) continue;
+    srcs.push_back(pattern_source(r.na, r.len, r.slot, r.m, r.groups));
+    idx.push_back(i);
+  }
+  std::vector<cudaKernel_t> ks;
+  kernels_for(srcs, ks);
+  int ok = 0;
+  for (size_t k = 0; k < idx.size(); ++k) {
+    reqs[idx[k]].kernel = reinterpret_cast<void *>(ks[k]);
+    ok += ks[k] != nullptr;
+  }
+  return ok;
+}
+
+std::vector<std::pair<int, int>> jit_groups(int na, const int *len, const int32_t *span,
+                                            int32_t max_span, int32_t *stage_need) {
+  std::vector<std::pair<int, int>> groups;
+  int32_t need = 0;
+  auto at = [&](int j0, int g) { return span[j0 * kJitMaxGroup + g - 1]; };
+  for (int j = 0; j < na;) {
+    if (len[j] == 0) {
+      ++j;
+      continue;
+    }
+    int g = 1;
+    // grow the group while the next nonempty A nonzero adds less than half
+    // of its own span to the union
+    while (g < kJitMaxGroup && j + g < na) {
+      if (len[j + g] == 0) {
+        ++g;
+        continue;
+      }
+      const int32_t cur = at(j, g), nxt = at(j, g + 1), own = at(j + g, 1);
+      if (nxt > max_span || 2 * (nxt - cur) > own) break;
+      ++g;
+    }
+    // trailing empty A nonzeros belong to no group
+    int end = j + g;
+    while (end > j + 1 && len[end - 1] == 0) --end;
+    groups.emplace_back(j, end);
+    need = need > at(j, end - j) ? need : at(j, end - j);
+    j = j + g;
+  }
+  *stage_need = need;
+  return groups;
 }
 
 void launch_tile_select(const int4 *tiles, int32_t ntiles, int32_t pid, int4 *out, int32_t *n,
@@ -298,15 +652,79 @@ void launch_tile_select(const int4 *tiles, int32_t ntiles, int32_t pid, int4 *ou
   tile_select_kernel<<<(ntiles + 255) / 256, 256, 0, s>>>(tiles, ntiles, pid, out, n);
 }
 
+void launch_jit_spans(const int4 *tiles, int32_t ntiles, int32_t na, const uint16_t *lens,
+                      const int32_t *a_rp, const int32_t *a_col, const int32_t *b_rp,
+                      int32_t *span, int num_sms, cudaStream_t s) {
+  if (ntiles <= 0 || na <= 0) return;
+  int64_t grid = (int64_t(ntiles) + 7) / 8;
+  const int64_t cap = int64_t(num_sms > 0 ? num_sms : 148) * 6;
+  if (grid > cap) grid = cap;
+  span_kernel<<<static_cast<unsigned>(grid), 256, 0, s>>>(tiles, ntiles, na, lens, a_rp, a_col,
+                                                          b_rp, span);
+}
+
 void launch_mark_pattern(int4 *desc, int32_t pid, cudaStream_t s) {
   mark_pattern_kernel<<<1, 1, 0, s>>>(desc, pid);
 }
 
-cudaError_t launch_pattern_kernel(void *kernel, const Operands &op, int32_t b_nnz,
-                                  const int4 *tiles, int32_t ntiles, const int32_t *c_rp,
-                                  float *c_val, int32_t stage_cap, int32_t work_floats,
+int32_t jit_record_words(int na, int ngroups) { return record_words(na, ngroups); }
+
+void launch_jit_programs(const int4 *tiles, int32_t ntiles, int32_t na,
+                         const std::vector<std::pair<int, int>> &groups, const int2 *groups_dev,
+                         const uint16_t *lens, const int32_t *a_rp, const int32_t *a_col,
+                         const int32_t *b_rp, int32_t *prog, int2 *arange, int32_t *maxima,
+                         int num_sms, cudaStream_t s) {
+  if (ntiles <= 0) return;
+  const int32_t rw = record_words(na, static_cast<int>(groups.size()));
+  cudaMemsetAsync(prog, 0, size_t(ntiles) * size_t(rw) * sizeof(int32_t), s);
+  int64_t grid = (int64_t(ntiles) + 7) / 8;
+  const int64_t cap = int64_t(num_sms > 0 ? num_sms : 148) * 6;
+  if (grid > cap) grid = cap;
+  program_kernel<<<static_cast<unsigned>(grid), 256, 0, s>>>(
+      tiles, ntiles, na, static_cast<int32_t>(groups.size()), groups_dev, lens, a_rp, a_col,
+      b_rp, rw, prog, arange, maxima);
+}
+
+void jit_layout(int32_t rw, int32_t seg_max, int32_t need, int32_t m, int32_t *stage_cap,
+                int32_t *abuf_floats, int32_t *work_floats) {
+  const int32_t ms = (m & 1) ? m : m + 1;
+  // a tile buffer: the record, then A values widened by up to 3 floats at
+  // each end; a stage buffer: a B range widened the same way
+  const int32_t ab = (rw + seg_max + 8 + 3) & ~3;
+  int32_t sc = (need + 8 + 3) & ~3;
+  // the output region (one tile buffer and both stage buffers) holds 16 rows
+  if (ab + 2 * sc < 16 * ms + 4) sc = ((16 * ms + 4 - ab + 1) / 2 + 3) & ~3;
+  *stage_cap = sc;
+  *abuf_floats = ab;
+  *work_floats = 2 * ab + 2 * sc;
+}
+
+int jit_grid(void *kernel, int32_t ntiles, int32_t work_floats, int32_t m, int num_sms) {
+  (void)kernel;
+  // registers: a quarter of the SM's file per scheduler, 256-register units
+  // per warp; shared memory: the SM's total with 1 KB reserved per block
+  const int warp_regs = ((pattern_regs(m) * 32) + 255) & ~255;
+  const int by_regs = (4 * (16384 / warp_regs)) / (kJitThreads / 32);
+  int dev = 0, sm_bytes = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sm_bytes, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
+  const size_t block_bytes =
+      size_t(kJitThreads / 32) * size_t(work_floats) * sizeof(float) + 64 + 1024;
+  int by_smem = sm_bytes > 0 ? static_cast<int>(size_t(sm_bytes) / block_bytes) : 1;
+  int per_sm = by_regs < by_smem ? by_regs : by_smem;
+  if (per_sm < 1) per_sm = 1;
+  if (per_sm > 16) per_sm = 16;
+  const int64_t want = (int64_t(ntiles) + 1) / 2;
+  const int64_t cap = int64_t(num_sms > 0 ? num_sms : 148) * per_sm;
+  return static_cast<int>(want < cap ? want : cap);
+}
+
+cudaError_t launch_pattern_kernel(void *kernel, const Operands &op, const int32_t *prog,
+                                  const int2 *arange, int32_t ntiles, const int32_t *c_rp,
+                                  float *c_val, int32_t stage_cap, int32_t abuf_floats,
+                                  int32_t work_floats, int grid, int32_t *status,
                                   cudaStream_t s) {
-  if (ntiles <= 0) return cudaSuccess;
+  if (ntiles <= 0 || grid <= 0) return cudaSuccess;
   const size_t smem = size_t(kJitThreads / 32) * size_t(work_floats) * sizeof(float);
   int dev = 0;
   cudaGetDevice(&dev);
@@ -315,16 +733,15 @@ cudaError_t launch_pattern_kernel(void *kernel, const Operands &op, int32_t b_nn
       k, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem), dev);
   if (e != cudaSuccess) return e;
   float zero = 0.0f;
-  const int4 *t = tiles;
+  const int32_t *pr = prog;
+  const int2 *ar = arange;
   int32_t nt = ntiles;
-  const int32_t *a_rp = op.a_rp, *a_col = op.a_col, *b_rp = op.b_rp;
   const float *a_val = op.a_val, *b_val = op.b_val;
-  int32_t bn = b_nnz, sc = stage_cap, wf = work_floats;
-  void *args[] = {&t, &nt, &a_rp, &a_col, &a_val, &b_rp, &b_val, &bn, &c_rp, &c_val, &sc,
-                  &wf, &zero};
-  const unsigned grid = static_cast<unsigned>((int64_t(ntiles) + 1) / 2);
-  return cudaLaunchKernel(reinterpret_cast<const void *>(k), dim3(grid), dim3(kJitThreads),
-                          args, smem, s);
+  int32_t sc = stage_cap, abf = abuf_floats, wf = work_floats;
+  int32_t *st = status;
+  void *args[] = {&pr, &ar, &nt, &a_val, &b_val, &c_rp, &c_val, &sc, &abf, &wf, &zero, &st};
+  return cudaLaunchKernel(reinterpret_cast<const void *>(k), dim3(static_cast<unsigned>(grid)),
+                          dim3(kJitThreads), args, smem, s);
 }
 
 }  // namespace rvsp

@@ -3,6 +3,7 @@
 
 #include <cstddef>
 #include <cstdint>
+#include <utility>
 #include <vector>
 #include <cuda_runtime.h>
 
@@ -360,23 +361,63 @@ void launch_persist_numeric(const Operands &op, const int64_t *ops, const Persis
                             cudaStream_t s);
 
 // ---- k_jit.cu --------------------------------------------------------------
-// Pattern kernels (see k_jit.cu): *kernel_out = a kernel compiled for one
-// pattern (na A nonzeros, B row lengths len[j], slot[t] = output position of
-// flattened product t, m outputs); returns 0 when NVRTC is missing or the
-// compile failed.  Kernels are cached for the process.
-int jit_pattern_kernel(int na, const int *len, const std::vector<int> &slot, int m,
-                       void **kernel_out);
+// A nonzeros staged together by a pattern kernel: runs of at most this many.
+constexpr int kJitMaxGroup = 8;
+// One pattern for a compiled kernel (see k_jit.cu): na A nonzeros, B row
+// lengths len[j], slot[t] = output position of flattened product t, m
+// outputs, groups = [first, end) runs of A nonzeros whose B values are
+// staged by one copy.
+struct JitRequest {
+  int na = 0, m = 0;
+  int len[32] = {};
+  std::vector<int> slot;
+  std::vector<std::pair<int, int>> groups;
+  void *kernel = nullptr;  // out: nullptr when NVRTC is missing or the compile failed
+};
+// Compiles the requests' kernels (side by side; cached for the process);
+// returns how many compiled.
+int jit_pattern_kernels(std::vector<JitRequest> &reqs);
 void jit_stats(int32_t *compiles, double *ms);
+// The groups of a pattern from its union spans (launch_jit_spans): runs of
+// A nonzeros grown while the next one adds less than half its own span and
+// the union stays within max_span floats.  *stage_need = the largest union.
+std::vector<std::pair<int, int>> jit_groups(int na, const int *len, const int32_t *span,
+                                            int32_t max_span, int32_t *stage_need);
+// span[j0 * kJitMaxGroup + g - 1] = the largest B range (floats) that one of
+// the tiles reads for A nonzeros j0 .. j0 + g - 1 (span zeroed by the caller).
+void launch_jit_spans(const int4 *tiles, int32_t ntiles, int32_t na, const uint16_t *lens,
+                      const int32_t *a_rp, const int32_t *a_col, const int32_t *b_rp,
+                      int32_t *span, int num_sms, cudaStream_t s);
 // out[*n] = the tiles of pattern pid (*n zeroed by the caller).
 void launch_tile_select(const int4 *tiles, int32_t ntiles, int32_t pid, int4 *out, int32_t *n,
                         cudaStream_t s);
 // Marks pattern pid's tiles for the table kernel to skip (desc[pid].w = 1).
 void launch_mark_pattern(int4 *desc, int32_t pid, cudaStream_t s);
-// One launch of a pattern kernel over its tiles; work_floats per warp holds
-// the A segment, two stage buffers of stage_cap floats, and 32 x 33 floats.
-cudaError_t launch_pattern_kernel(void *kernel, const Operands &op, int32_t b_nnz,
-                                  const int4 *tiles, int32_t ntiles, const int32_t *c_rp,
-                                  float *c_val, int32_t stage_cap, int32_t work_floats,
+// Words of one tile record of a pattern kernel (na A nonzeros, ngroups
+// staging groups).
+int32_t jit_record_words(int na, int ngroups);
+// The tile records of a pattern (see k_jit.cu): prog[ntiles * record words],
+// arange[ntiles] = the A range of each tile, maxima[0] = the longest (zeroed
+// by the caller); groups_dev = the groups as int2 on the device.
+void launch_jit_programs(const int4 *tiles, int32_t ntiles, int32_t na,
+                         const std::vector<std::pair<int, int>> &groups, const int2 *groups_dev,
+                         const uint16_t *lens, const int32_t *a_rp, const int32_t *a_col,
+                         const int32_t *b_rp, int32_t *prog, int2 *arange, int32_t *maxima,
+                         int num_sms, cudaStream_t s);
+// Shared memory of one warp of a pattern kernel, in floats: two tile buffers
+// (record + A values) of *abuf_floats and two B stage buffers of *stage_cap
+// (the largest B range `need` plus widening; room for 16 output rows).
+void jit_layout(int32_t rw, int32_t seg_max, int32_t need, int32_t m, int32_t *stage_cap,
+                int32_t *abuf_floats, int32_t *work_floats);
+// Blocks of a persistent pattern kernel launch: the tiles' pairs, at most
+// what fits the SMs at once.
+int jit_grid(void *kernel, int32_t ntiles, int32_t work_floats, int32_t m, int num_sms);
+// One launch of a pattern kernel over its tile records (status:
+// kDevWaitTimeout when a bounded wait ran out).
+cudaError_t launch_pattern_kernel(void *kernel, const Operands &op, const int32_t *prog,
+                                  const int2 *arange, int32_t ntiles, const int32_t *c_rp,
+                                  float *c_val, int32_t stage_cap, int32_t abuf_floats,
+                                  int32_t work_floats, int grid, int32_t *status,
                                   cudaStream_t s);
 
 // ---- k_shift.cu ------------------------------------------------------------

@@ -89,7 +89,15 @@ namespace rvsp {
 struct JitPattern {
   void *kernel = nullptr;
   DevArray<int4> tiles;
-  int32_t n = 0;
+  DevArray<int32_t> prog;  // tile records (k_jit.cu)
+  DevArray<int2> arange;   // per tile its A range
+  int32_t n = 0, m = 0, stage_cap = 0, abuf_floats = 0, work_floats = 0;
+  int grid = 0;
+  void release() {
+    tiles.release();
+    prog.release();
+    arange.release();
+  }
 };
 struct TileBuild {
   std::vector<JitPattern> jit;  // patterns with their own kernel (k_jit.cu)
@@ -97,7 +105,7 @@ struct TileBuild {
   int32_t n_tiles = 0, n_lo = 0, stage = 0, aseg = 0, max_out = 0, b_nnz = 0;
   DevArray<uint16_t> tab, lens;
   DevArray<int4> desc, tiles;
-  DevArray<int32_t> pid, lo_rows, lo_ids, counts, all_rows, all_ids;
+  DevArray<int32_t> pid, lo_rows, lo_ids, counts, all_rows, all_ids, spans;
   void release() {
     tab.release();
     lens.release();
@@ -109,7 +117,8 @@ struct TileBuild {
     counts.release();
     all_rows.release();
     all_ids.release();
-    for (auto &j : jit) j.tiles.release();
+    spans.release();
+    for (auto &j : jit) j.release();
     jit.clear();
     ready = 0;
   }
@@ -225,6 +234,12 @@ struct rvsp_cuda_plan {
   int rmap_state = 0;
   int64_t rmap_entries = 0;
 
+  // Side streams of the numeric-only pass (created on first use; state 0
+  // untried, 1 ready, -1 unavailable).
+  cudaStream_t side[2] = {nullptr, nullptr};
+  cudaEvent_t fork_ev = nullptr, join_ev[2] = {nullptr, nullptr};
+  int side_state = 0;
+
   bool profiling = false;
   struct Pending {
     cudaEvent_t a, b;
@@ -284,6 +299,59 @@ void resolve_pending(rvsp_cuda_plan *pl) {
   }
   pl->pending.clear();
 }
+
+// The plan's two side streams, created on first use (at the highest stream
+// priority, on the plan's device, never while `s` is being captured).
+bool side_streams(rvsp_cuda_plan *p, cudaStream_t s) {
+  if (p->side_state == 0) {
+    int dev = -1;
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev != p->device ||
+        cudaStreamIsCapturing(s, &cap) != cudaSuccess || cap != cudaStreamCaptureStatusNone) {
+      cudaGetLastError();
+      return false;
+    }
+    p->side_state = -1;
+    int least = 0, greatest = 0;
+    bool ok = cudaDeviceGetStreamPriorityRange(&least, &greatest) == cudaSuccess &&
+              cudaEventCreateWithFlags(&p->fork_ev, cudaEventDisableTiming) == cudaSuccess;
+    for (int i = 0; i < 2 && ok; ++i)
+      ok = cudaStreamCreateWithPriority(&p->side[i], cudaStreamNonBlocking, greatest) ==
+               cudaSuccess &&
+           cudaEventCreateWithFlags(&p->join_ev[i], cudaEventDisableTiming) == cudaSuccess;
+    if (ok) p->side_state = 1;
+    else cudaGetLastError();
+  }
+  return p->side_state == 1;
+}
+
+// Streams of one numeric-only pass.  Its row groups (pattern kernels, table
+// tiles, leftover rows, class kernels) write disjoint rows of C and only
+// read A, B and the plan's tables, so all but the largest go to the two side
+// streams, forked from the caller's stream and joined back into it: the
+// small launches, bound by the latency of a few long rows, run beside the
+// large one instead of after it.  Lane 0 is the caller's stream; without
+// side streams every lane is.
+struct Lanes {
+  rvsp_cuda_plan *pl;
+  cudaStream_t s;
+  bool forked = false;
+  Lanes(rvsp_cuda_plan *p, cudaStream_t st, bool want) : pl(p), s(st) {
+    if (want && side_streams(p, st) && cudaEventRecord(p->fork_ev, st) == cudaSuccess)
+      forked = cudaStreamWaitEvent(p->side[0], p->fork_ev, 0) == cudaSuccess &&
+               cudaStreamWaitEvent(p->side[1], p->fork_ev, 0) == cudaSuccess;
+  }
+  cudaStream_t operator[](int k) const { return forked && k > 0 ? pl->side[k - 1] : s; }
+  void join() {
+    if (!forked) return;
+    for (int i = 0; i < 2; ++i) {
+      cudaEventRecord(pl->join_ev[i], pl->side[i]);
+      cudaStreamWaitEvent(s, pl->join_ev[i], 0);
+    }
+    forked = false;
+  }
+  ~Lanes() { join(); }
+};
 
 rvsp_status_t device_status_to_rvsp(int32_t st) {
   return st == kDevOk ? RVSP_SUCCESS : RVSP_ERROR_DEVICE;
@@ -407,6 +475,11 @@ void rvsp_cuda_plan_destroy(rvsp_cuda_plan_t p) {
   if (!p) return;
   resolve_pending(p);
   for (cudaEvent_t e : p->pool) cudaEventDestroy(e);
+  for (int i = 0; i < 2; ++i) {
+    if (p->side[i]) cudaStreamDestroy(p->side[i]);
+    if (p->join_ev[i]) cudaEventDestroy(p->join_ev[i]);
+  }
+  if (p->fork_ev) cudaEventDestroy(p->fork_ev);
   p->rmap.release();
   p->rmap_off.release();
   p->rmap_ops.release();
@@ -1111,27 +1184,24 @@ constexpr size_t kReuseMapMaxBytes = size_t(24) << 30;
 // The tile tables may take at most this much device memory.
 constexpr size_t kTileTablesMaxBytes = size_t(256) << 20;
 // Patterns with at least this many tiles (of 32 rows) get a compiled kernel,
-// the kJitMaxPatterns largest of them.
+// the kJitMaxPatterns largest of them, when their rows have at most
+// kJitMaxOut outputs (one register each).
 constexpr int32_t kJitMinTiles = 128;
-constexpr int kJitMaxPatterns = 4;
-
-// Work area of one warp of a pattern kernel (k_jit.cu), in floats.
-int32_t pattern_work_floats(const TileBuild &tb) {
-  int32_t stage_cap = (tb.stage + 3) & ~3;
-  int32_t w = 2 * stage_cap;
-  if (2 * tb.aseg > w) w = 2 * tb.aseg;
-  if (32 * 33 > w) w = 32 * 33;
-  return (w + 3) & ~3;
-}
+constexpr int kJitMaxPatterns = 12;
+constexpr int32_t kJitMaxOut = 160;
+// Largest B range (floats) one stage buffer of a pattern kernel takes.
+constexpr int32_t kJitMaxSpan = 4096;
 
 // Compiled kernels for the patterns that cover the most tiles: the tile list
-// is read back once, each chosen pattern's table is turned into CUDA source
-// (k_jit.cu), and its tiles are listed for its kernel and marked so the
-// table kernel skips them.  A pattern whose compile fails stays on the table
-// kernel.  Synchronizes `s`.
-cudaError_t build_pattern_kernels(rvsp_cuda_plan *p, cudaStream_t s, int32_t npat,
-                                  TileBuild &tb) {
-  for (auto &j : tb.jit) j.tiles.release();
+// is read back once; for each chosen pattern its tiles are listed, the union
+// spans of runs of its A nonzeros measured over those tiles (the staging
+// groups and buffer size follow), its table turned into CUDA source
+// (k_jit.cu) and compiled, and its tiles marked so the table kernel skips
+// them.  A pattern whose compile fails stays on the table kernel.
+// Synchronizes `s`.
+cudaError_t build_pattern_kernels(rvsp_cuda_plan *p, cudaStream_t s, const Operands &op,
+                                  int32_t npat, TileBuild &tb) {
+  for (auto &j : tb.jit) j.release();
   tb.jit.clear();
   std::vector<int4> tiles(static_cast<size_t>(tb.n_tiles));
   cudaError_t e = cudaMemcpyAsync(tiles.data(), tb.tiles.p, tiles.size() * sizeof(int4),
@@ -1147,7 +1217,19 @@ cudaError_t build_pattern_kernels(rvsp_cuda_plan *p, cudaStream_t s, int32_t npa
   std::sort(order.begin(), order.end(),
             [&](int32_t a, int32_t b) { return count[size_t(a)] > count[size_t(b)]; });
   if (order.size() > size_t(kJitMaxPatterns)) order.resize(size_t(kJitMaxPatterns));
+  if (order.empty()) return cudaSuccess;
+  if (tb.spans.reserve(size_t(32 * kJitMaxGroup)) != cudaSuccess) {
+    cudaGetLastError();
+    return cudaSuccess;
+  }
   const int32_t stride = tile_tab_stride();
+  std::vector<JitRequest> reqs;
+  std::vector<JitPattern> cand;
+  std::vector<int32_t> cand_id;
+  auto drop = [&cand](cudaError_t err) {
+    for (auto &c : cand) c.release();
+    return err;
+  };
   for (int32_t id : order) {
     int4 d;
     uint16_t lens[32];
@@ -1160,26 +1242,91 @@ cudaError_t build_pattern_kernels(rvsp_cuda_plan *p, cudaStream_t s, int32_t npa
       e = cudaMemcpyAsync(tab.data(), tb.tab.p + size_t(id) * stride,
                           tab.size() * sizeof(uint16_t), cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
-    if (e != cudaSuccess) return e;
-    if (d.x <= 0 || d.x > 32 || d.y <= 0) continue;
-    int len[32];
-    std::vector<int> slot;
+    if (e != cudaSuccess) return drop(e);
+    if (d.x <= 0 || d.x > 32 || d.y <= 0 || d.y > kJitMaxOut) continue;
+    JitRequest rq;
+    rq.na = d.x;
+    rq.m = d.y;
     int32_t off = 0;
     for (int j = 0; j < d.x; ++j) {
-      len[j] = lens[j];
-      for (int ee = 0; ee < len[j]; ++ee) slot.push_back(tab[size_t(off + ee)] & 0x7fff);
-      off += (len[j] + 7) & ~7;
+      rq.len[j] = lens[j];
+      for (int ee = 0; ee < rq.len[j]; ++ee) rq.slot.push_back(tab[size_t(off + ee)] & 0x7fff);
+      off += (rq.len[j] + 7) & ~7;
     }
     JitPattern jp;
-    if (!jit_pattern_kernel(d.x, len, slot, d.y, &jp.kernel)) continue;
     if (jp.tiles.reserve(size_t(count[size_t(id)])) != cudaSuccess) {
       cudaGetLastError();
       continue;
     }
     cudaMemsetAsync(tb.counts.p + 6, 0, sizeof(int32_t), s);
+    cudaMemsetAsync(tb.spans.p, 0, size_t(32 * kJitMaxGroup) * sizeof(int32_t), s);
     launch_tile_select(tb.tiles.p, tb.n_tiles, id, jp.tiles.p, tb.counts.p + 6, s);
-    launch_mark_pattern(tb.desc.p, id, s);
+    launch_jit_spans(jp.tiles.p, count[size_t(id)], d.x, tb.lens.p + size_t(id) * 32, op.a_rp,
+                     op.a_col, op.b_rp, tb.spans.p, p->num_sms, s);
+    int32_t span[32 * kJitMaxGroup];
+    e = cudaMemcpyAsync(span, tb.spans.p, sizeof(span), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) {
+      jp.release();
+      return drop(e);
+    }
+    int32_t need = 0;
+    rq.groups = jit_groups(d.x, rq.len, span, kJitMaxSpan, &need);
+    if (rq.groups.empty() || need <= 0 || need > kJitMaxSpan) {
+      jp.release();
+      continue;
+    }
     jp.n = count[size_t(id)];
+    jp.m = d.y;
+    jp.stage_cap = need;  // the largest B range; the layout follows the records
+    reqs.push_back(std::move(rq));
+    cand.push_back(std::move(jp));
+    cand_id.push_back(id);
+  }
+  jit_pattern_kernels(reqs);
+  for (size_t i = 0; i < reqs.size(); ++i) {
+    JitPattern &jp = cand[i];
+    if (!reqs[i].kernel) {
+      jp.release();
+      continue;
+    }
+    const JitRequest &rq = reqs[i];
+    const int32_t rw = jit_record_words(rq.na, static_cast<int>(rq.groups.size()));
+    std::vector<int2> gh;
+    for (const auto &g : rq.groups) gh.push_back(make_int2(g.first, g.second));
+    DevArray<int2> gdev;
+    if (jp.prog.reserve(size_t(jp.n) * size_t(rw)) != cudaSuccess ||
+        jp.arange.reserve(size_t(jp.n)) != cudaSuccess || gdev.reserve(gh.size()) != cudaSuccess) {
+      cudaGetLastError();
+      jp.release();
+      gdev.release();
+      continue;
+    }
+    int32_t seg_max = 0;
+    cudaMemcpyAsync(gdev.p, gh.data(), gh.size() * sizeof(int2), cudaMemcpyHostToDevice, s);
+    cudaMemsetAsync(tb.spans.p, 0, sizeof(int32_t), s);
+    launch_jit_programs(jp.tiles.p, jp.n, rq.na, rq.groups, gdev.p,
+                        tb.lens.p + size_t(cand_id[i]) * 32, op.a_rp, op.a_col, op.b_rp,
+                        jp.prog.p, jp.arange.p, tb.spans.p, p->num_sms, s);
+    e = cudaMemcpyAsync(&seg_max, tb.spans.p, sizeof(int32_t), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    gdev.release();
+    if (e != cudaSuccess) {
+      for (size_t k = i; k < cand.size(); ++k) cand[k].release();
+      return e;
+    }
+    jit_layout(rw, seg_max, jp.stage_cap, jp.m, &jp.stage_cap, &jp.abuf_floats,
+               &jp.work_floats);
+    // two warps must fit one block's shared memory
+    int dev_max = 0;
+    cudaDeviceGetAttribute(&dev_max, cudaDevAttrMaxSharedMemoryPerBlockOptin, p->device);
+    if (size_t(2) * size_t(jp.work_floats) * sizeof(float) > size_t(dev_max)) {
+      jp.release();
+      continue;
+    }
+    jp.grid = jit_grid(rq.kernel, jp.n, jp.work_floats, jp.m, p->num_sms);
+    jp.kernel = rq.kernel;
+    launch_mark_pattern(tb.desc.p, cand_id[i], s);
     tb.jit.push_back(std::move(jp));
   }
   return cudaGetLastError();
@@ -1244,7 +1391,7 @@ cudaError_t build_row_tiles(rvsp_cuda_plan *p, cudaStream_t s, const Operands &o
   tb.max_out = h[4];
   tb.b_nnz = b_nnz;
   tb.ready = 1;
-  if (p->pattern_kernels) return build_pattern_kernels(p, s, npat, tb);
+  if (p->pattern_kernels) return build_pattern_kernels(p, s, op, npat, tb);
   return cudaSuccess;
 }
 
@@ -1386,36 +1533,40 @@ cudaError_t build_shift_tables(rvsp_cuda_plan *p, cudaStream_t s, const Operands
 }
 
 // The pattern kernels of a tile set (k_jit.cu); returns the launches.
+// The first (the pattern with the most tiles) goes to lane 0, the others
+// alternate between lanes 1 and 2.
 int launch_pattern_kernels(const TileBuild &tb, const Operands &op, const int32_t *c_rp,
-                           float *c_val, cudaStream_t s) {
-  const int32_t wf = pattern_work_floats(tb);
-  const int32_t stage_cap = (tb.stage + 3) & ~3;
-  for (const auto &j : tb.jit)
-    launch_pattern_kernel(j.kernel, op, tb.b_nnz, j.tiles.p, j.n, c_rp, c_val, stage_cap, wf, s);
+                           float *c_val, int32_t *status, const Lanes &ln) {
+  for (size_t i = 0; i < tb.jit.size(); ++i) {
+    const auto &j = tb.jit[i];
+    launch_pattern_kernel(j.kernel, op, j.prog.p, j.arange.p, j.n, c_rp, c_val, j.stage_cap,
+                          j.abuf_floats, j.work_floats, j.grid, status,
+                          ln[i == 0 ? 0 : 1 + int(i & 1)]);
+  }
   return static_cast<int>(tb.jit.size());
 }
 
 // Values of the shift-class member rows (tables built): row tiles, then the
 // members no tile took through the warp-per-row table kernel; every member
 // through that kernel when tiles are off.
-int launch_shift_numeric(rvsp_cuda_plan *p, cudaStream_t s, const Operands &op,
+int launch_shift_numeric(rvsp_cuda_plan *p, const Lanes &ln, const Operands &op,
                          const int32_t *c_rp, float *c_val) {
   int launches = 0;
   if (p->st.ready && p->tiles_enabled) {
     launch_tile_numeric(op, p->st.b_nnz, p->st.tiles.p, p->st.n_tiles, p->st.desc.p,
                         p->st.lens.p, p->st.tab.p, c_rp, c_val, p->st.stage, p->st.aseg,
-                        p->st.max_out, s);
-    launches += 1 + launch_pattern_kernels(p->st, op, c_rp, c_val, s);
+                        p->st.max_out, ln[1]);
+    launches += 1 + launch_pattern_kernels(p->st, op, c_rp, c_val, p->misc.p + kStatus, ln);
     if (p->st.n_lo > 0) {
       launch_pat_numeric(op, p->ops.p, p->st.lo_rows.p, p->st.lo_ids.p, p->st.n_lo, c_rp,
                          c_val, p->sh_pat_off.p, p->sh_steps.p, p->sh_rec.p, p->sh_max_ops,
-                         p->sh_max_out, s);
+                         p->sh_max_out, ln[2]);
       ++launches;
     }
   } else {
     launch_pat_numeric(op, p->ops.p, p->st.all_rows.p, p->st.all_ids.p, p->shift_members,
                        c_rp, c_val, p->sh_pat_off.p, p->sh_steps.p, p->sh_rec.p,
-                       p->sh_max_ops, p->sh_max_out, s);
+                       p->sh_max_ops, p->sh_max_out, ln[0]);
     ++launches;
   }
   return launches;
@@ -1612,24 +1763,27 @@ rvsp_status_t rvsp_cuda_numeric(rvsp_cuda_plan_t p, void *stream,
     }
   }
   const bool use_map = fill == 0 && p->rmap_state == 1 && p->rmap_col == c_col_idx;
+  // numeric-only with every table in place: the row groups run side by side
+  Lanes ln(p, s, use_map && (!p->shift_active || p->shift_tables == 1));
   {
     PhaseScope ph(p, s, RVSP_PHASE_NUMERIC);
     if (use_map && p->pat_ready && p->n_pat_rows > 0) {
       if (p->rt.ready && p->tiles_enabled) {
         launch_tile_numeric(op, p->rt.b_nnz, p->rt.tiles.p, p->rt.n_tiles, p->rt.desc.p,
                             p->rt.lens.p, p->rt.tab.p, c_row_ptr, c_values, p->rt.stage,
-                            p->rt.aseg, p->rt.max_out, s);
-        ph.launches += 1 + launch_pattern_kernels(p->rt, op, c_row_ptr, c_values, s);
+                            p->rt.aseg, p->rt.max_out, ln[1]);
+        ph.launches += 1 + launch_pattern_kernels(p->rt, op, c_row_ptr, c_values,
+                                                   p->misc.p + kStatus, ln);
         if (p->rt.n_lo > 0) {
           launch_pat_numeric(op, p->ops.p, p->rt.lo_rows.p, p->rt.lo_ids.p, p->rt.n_lo,
                              c_row_ptr, c_values, p->pat_off.p, p->pat_steps.p, p->pat_rec.p,
-                             p->pat_max_ops, p->pat_max_out, s);
+                             p->pat_max_ops, p->pat_max_out, ln[2]);
           ph.launches += 1;
         }
       } else {
         launch_pat_numeric(op, p->ops.p, p->pat_rows.p, p->pat_ids.p, p->n_pat_rows,
                            c_row_ptr, c_values, p->pat_off.p, p->pat_steps.p, p->pat_rec.p,
-                           p->pat_max_ops, p->pat_max_out, s);
+                           p->pat_max_ops, p->pat_max_out, ln[0]);
         ph.launches += 1;
       }
     }
@@ -1662,7 +1816,7 @@ rvsp_status_t rvsp_cuda_numeric(rvsp_cuda_plan_t p, void *stream,
       }
       launch_persist_numeric(op, p->ops.p, pp, p->persist_head.p, c_row_ptr, c_values,
                              p->rmap_off.p, p->rmap.p, p->misc.p + kStatus, max_out,
-                             p->persist_blocks, p->num_sms, s);
+                             p->persist_blocks, p->num_sms, ln[2]);
       ph.launches += 2;
     } else {
       cudaGetLastError();
@@ -1677,16 +1831,17 @@ rvsp_status_t rvsp_cuda_numeric(rvsp_cuda_plan_t p, void *stream,
         if (p->res_count[c] > 0)
           launch_map_numeric(c, op, p->ops.p, p->res_rows.p + p->res_off[c],
                              p->res_count[c], c_row_ptr, c_values, p->rmap_off.p,
-                             p->rmap.p, p->misc.p + kStatus, s);
+                             p->rmap.p, p->misc.p + kStatus, ln[2]);
       } else if (use_map && map_class(c))
         launch_map_numeric(c, op, p->ops.p, rows, nrows, c_row_ptr, c_values,
-                           p->rmap_off.p, p->rmap.p, p->misc.p + kStatus, s);
+                           p->rmap_off.p, p->rmap.p, p->misc.p + kStatus, ln[2]);
       else
         launch_numeric_class(c, op, p->ops.p, rows, nrows, c_row_ptr, c_col_idx, c_values,
                              fill != 0, dense_acc, dense_bits, p->dense_slots,
-                             p->misc.p + kStatus, p->num_sms, s);
+                             p->misc.p + kStatus, p->num_sms, ln[2]);
       ph.launches += 1;
     }
+    if (!p->shift_active) ln.join();
   }
   if (p->shift_active) {
     // Shift-class members: columns by translation of their canonical rows
@@ -1705,7 +1860,8 @@ rvsp_status_t rvsp_cuda_numeric(rvsp_cuda_plan_t p, void *stream,
     }
     if (p->shift_tables != 1) return RVSP_ERROR_DEVICE;
     PhaseScope ph(p, s, RVSP_PHASE_NUMERIC);
-    ph.launches = launch_shift_numeric(p, s, op, c_row_ptr, c_values);
+    ph.launches = launch_shift_numeric(p, ln, op, c_row_ptr, c_values);
+    ln.join();
   }
   return map_cuda(cudaGetLastError());
 }

@@ -5,8 +5,10 @@ per lane.  Bar: values bit-exact against the oracle (the reference's
 numeric-only compute, spgemm_descr.c:330-349, re-running
 gustavson_core_f32.inc:31-62 on new values) for stencils, a banded matrix
 with far off-diagonals, tiles whose lanes skip rows of another pattern, a B
-value array that is not 16-byte aligned (the 4-byte copy path) and with
-tiles switched off, which must give the same bits.
+value array that is not 16-byte aligned (the 4-byte copy path), with tiles
+switched off, which must give the same bits, and the compiled pattern
+kernels (bulk copies of B ranges, bulk stores of whole tiles) at every
+alignment of B's and C's value arrays.
 """
 import ctypes as C
 
@@ -45,15 +47,16 @@ class _Plan:
                                             rp.data_ptr(), C.byref(total)), "symbolic")
         return rp, total.value
 
-    def numeric(self, dA, dB, rp, ci, cv, fill, b_values_ptr=None):
+    def numeric(self, dA, dB, rp, ci, cv, fill, b_values_ptr=None, c_values_ptr=None):
         import torch
         ws_b = max(self.lib.rvsp_cuda_numeric_workspace_bytes(self.h), 256)
         ws = torch.zeros(ws_b, dtype=torch.uint8, device="cuda")
         bv = b_values_ptr if b_values_ptr is not None else dB.values.data_ptr()
+        cvp = c_values_ptr if c_values_ptr is not None else cv.data_ptr()
         L.check(self.lib.rvsp_cuda_numeric(
             self.h, _stream(), dA.row_ptr.data_ptr(), dA.col_idx.data_ptr(),
             dA.values.data_ptr(), dB.row_ptr.data_ptr(), dB.col_idx.data_ptr(), bv,
-            rp.data_ptr(), ci.data_ptr(), cv.data_ptr(), fill, ws.data_ptr(), ws_b), "numeric")
+            rp.data_ptr(), ci.data_ptr(), cvp, fill, ws.data_ptr(), ws_b), "numeric")
         torch.cuda.synchronize()
         L.check(self.lib.rvsp_cuda_plan_status(self.h, _stream()), "status")
 
@@ -248,3 +251,37 @@ def test_pattern_kernels_match_table_kernel(shift):
     compiles, ms = C.c_int32(), C.c_double()
     lib.rvsp_cuda_pattern_kernel_stats(C.byref(compiles), C.byref(ms))
     assert compiles.value >= 1
+
+
+@pytest.mark.parametrize("b_off,c_off", [(0, 0), (1, 3), (2, 1), (3, 2)])
+def test_pattern_kernels_any_alignment(b_off, c_off):
+    # a 40^3 stencil: interior runs of 36 rows, so whole tiles (32 rows of
+    # the pattern) exist and their C block goes out by one bulk store; B's
+    # and C's values are handed over b_off / c_off floats into larger buffers,
+    # so the bulk copies and stores start at every offset within 16 bytes
+    import torch
+    lib = L.load()
+    A = gen.stencil_3d_27(40)
+    dA = DeviceCSR.from_host(A)
+    plan = _Plan(lib)
+    try:
+        rp, n = plan.symbolic(dA, dA)
+        ci = torch.zeros(n, dtype=torch.int32, device="cuda")
+        cv = torch.zeros(n, dtype=torch.float32, device="cuda")
+        plan.numeric(dA, dA, rp, ci, cv, 1)
+        rng = np.random.default_rng(31 + b_off)
+        bvals = (A.values + rng.uniform(-0.01, 0.01, A.nnz)).astype(np.float32)
+        bbuf = torch.zeros(A.nnz + 4, dtype=torch.float32, device="cuda")
+        bbuf[b_off:b_off + A.nnz].copy_(torch.from_numpy(bvals))
+        cbuf = torch.full((n + 4,), float("nan"), dtype=torch.float32, device="cuda")
+        torch.cuda.synchronize()
+        plan.numeric(dA, dA, rp, ci, cv, 0, b_values_ptr=bbuf.data_ptr() + 4 * b_off,
+                     c_values_ptr=cbuf.data_ptr() + 4 * c_off)
+        assert lib.rvsp_cuda_plan_pattern_kernel_rows(plan.h) > 0
+        got = cbuf.cpu().numpy()
+        want = oracle.spgemm(A, A.with_values(bvals))[2]
+        assert np.array_equal(_bits(got[c_off:c_off + n]), _bits(want))
+        # nothing written outside C's values
+        assert np.isnan(got[:c_off]).all() and np.isnan(got[c_off + n:]).all()
+    finally:
+        plan.close()
