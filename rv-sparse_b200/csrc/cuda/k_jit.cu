@@ -46,8 +46,9 @@
 // NVRTC is opened at run time (dlopen of libnvrtc.so.12); without it, or if
 // a compile fails, the pattern stays on the table kernel.  The patterns of
 // one structure compile side by side, one host thread each.  Compiled
-// kernels are kept for the life of the process, keyed by their source text,
-// so a pattern is compiled once per process.
+// kernels are kept for the life of the process, keyed by the pattern's
+// numbers and the architecture: a pattern is compiled once per process, and
+// a cached one is not even turned into source again.
 #include <cuda_runtime.h>
 #include <dlfcn.h>
 #include <nvrtc.h>
@@ -83,7 +84,7 @@ struct Nvrtc {
 
 std::mutex g_mutex;
 Nvrtc g_nvrtc;
-std::map<std::string, cudaKernel_t> g_cache;  // source text -> kernel
+std::map<std::string, cudaKernel_t> g_cache;  // pattern key -> kernel
 int g_compiles = 0;
 double g_compile_ms = 0.0;
 
@@ -132,10 +133,22 @@ __device__ __forceinline__ bool bar_wait(u32 bar, u32 ph) {
     if (clock64() - t0 > (1ll << 31)) return false;
   return true;
 }
-__device__ __forceinline__ void bulk_load(void *dst, u64 src, u32 bytes, u32 bar) {
-  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes"
-               " [%0], [%1], %2, [%3];\n"
-               ::"r"(saddr(dst)), "l"(src), "r"(bytes), "r"(bar) : "memory");
+// L2 policies: B ranges are read by up to nine tiles (kept: evict_last);
+// tile records, A values and C blocks pass through once (evict_first).
+__device__ __forceinline__ u64 policy_keep() {
+  u64 p;
+  asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;\n" : "=l"(p));
+  return p;
+}
+__device__ __forceinline__ u64 policy_stream() {
+  u64 p;
+  asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;\n" : "=l"(p));
+  return p;
+}
+__device__ __forceinline__ void bulk_load(void *dst, u64 src, u32 bytes, u32 bar, u64 pol) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes.L2::cache_hint"
+               " [%0], [%1], %2, [%3], %4;\n"
+               ::"r"(saddr(dst)), "l"(src), "r"(bytes), "r"(bar), "l"(pol) : "memory");
 }
 __device__ __forceinline__ void expect(u32 bar, u32 bytes) {
   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n"
@@ -144,13 +157,13 @@ __device__ __forceinline__ void expect(u32 bar, u32 bytes) {
 // Lane 0 copies B values [lo, hi) (widened to whole 16-byte units) to dst,
 // completing on bar.  Returns the position in dst of B value lo.
 __device__ __forceinline__ int stage(float *dst, const float *b_val, int lo, int hi, u32 bar,
-                                     int lane) {
+                                     int lane, u64 pol) {
   const u64 g0 = (u64)(b_val + lo);
   if (lane == 0) {
     const u64 a0 = g0 & ~15ull;
     const u64 a1 = ((u64)(b_val + hi) + 15ull) & ~15ull;
     expect(bar, (u32)(a1 - a0));
-    bulk_load(dst, a0, (u32)(a1 - a0), bar);
+    bulk_load(dst, a0, (u32)(a1 - a0), bar, pol);
   }
   return (int)((g0 & 15ull) >> 2);
 }
@@ -158,19 +171,26 @@ __device__ __forceinline__ int stage(float *dst, const float *b_val, int lo, int
 // values a_val[r.x, r.x + r.y) (widened to 16-byte units) after it,
 // completing on bar.
 __device__ __forceinline__ void stage_tile(float *dst, const int *prog, int rwords, int2 r,
-                                           int tile, const float *a_val, u32 bar, int lane) {
+                                           int tile, const float *a_val, u32 bar, int lane,
+                                           u64 pol) {
   if (lane == 0) {
     const u64 a0 = (u64)(a_val + r.x) & ~15ull;
     const u64 a1 = ((u64)(a_val + r.x + r.y) + 15ull) & ~15ull;
     const u32 rb = (u32)rwords * 4u, ab = r.y > 0 ? (u32)(a1 - a0) : 0u;
     expect(bar, rb + ab);
-    bulk_load(dst, (u64)(prog + (size_t)tile * rwords), rb, bar);
-    if (ab) bulk_load(dst + rwords, a0, ab, bar);
+    bulk_load(dst, (u64)(prog + (size_t)tile * rwords), rb, bar, pol);
+    if (ab) bulk_load(dst + rwords, a0, ab, bar, pol);
   }
 }
-__device__ __forceinline__ void store_block(float *g, const float *s, int bytes) {
-  asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;\n"
-               ::"l"(g), "r"(saddr(s)), "r"(bytes) : "memory");
+// The next tile of the launch's queue (head zeroed before the launch).
+__device__ __forceinline__ int take(int *head, int lane) {
+  int t = 0;
+  if (lane == 0) t = atomicAdd(head, 1);
+  return __shfl_sync(FULL, t, 0);
+}
+__device__ __forceinline__ void store_block(float *g, const float *s, int bytes, u64 pol) {
+  asm volatile("cp.async.bulk.global.shared::cta.bulk_group.L2::cache_hint [%0], [%1], %2, %3;\n"
+               ::"l"(g), "r"(saddr(s)), "r"(bytes), "l"(pol) : "memory");
   asm volatile("cp.async.bulk.commit_group;\n" ::: "memory");
   asm volatile("cp.async.bulk.wait_group.read 0;\n" ::: "memory");
 }
@@ -196,7 +216,8 @@ int record_words(int na, int ngroups) { return (4 + 2 * ngroups + 16 + 16 * na +
 // order), m outputs, and the groups of A nonzeros staged together
 // ([first, end) ranges over j, in order, covering every j with len > 0).
 //
-// The kernel is persistent: warp w takes tiles w, w + 2 * gridDim.x, ...
+// The kernel is persistent: each warp takes tiles from the launch's queue
+// (an atomic counter), so warps that start late take fewer.
 // Per warp, shared memory holds two tile buffers (record + A values) around
 // two B stage buffers: [tile 0 | stage 0 | stage 1 | tile 1].  While a tile
 // is computed, the next tile's record and A values are copied into the other
@@ -210,7 +231,9 @@ std::string pattern_source(int na, const int *len, const std::vector<int> &slot,
   const int ng = static_cast<int>(groups.size());
   const int rw = record_words(na, ng);
   const int aoff_w = 4 + 2 * ng, d_w = aoff_w + 16;
-  const int mid = ng > 1 ? 1 : 0;  // the next tile's copies go out with group mid's
+  // the next tile's copies go out with group mid's, late enough that the
+  // next tile's number (an atomic on the queue head) and A range are in
+  const int mid = ng / 2;
   std::vector<int> t_of(size_t(na) + 1, 0);
   for (int j = 0; j < na; ++j) t_of[size_t(j) + 1] = t_of[size_t(j)] + len[j];
   snprintf(buf, sizeof(buf), "#define RW %d\n#define M %d\n#define MS %d\n", rw, m, ms);
@@ -220,7 +243,8 @@ std::string pattern_source(int na, const int *len, const std::vector<int> &slot,
   s += "rvsp_pattern_tiles(const int *__restrict__ prog, const int2 *__restrict__ arange,\n"
        "    int ntiles, const float *__restrict__ a_val, const float *__restrict__ b_val,\n"
        "    const int *__restrict__ c_rp, float *__restrict__ c_val, int stage_cap,\n"
-       "    int abuf_floats, int work_floats, float zero, int *__restrict__ status) {\n"
+       "    int abuf_floats, int work_floats, float zero, int *__restrict__ head,\n"
+       "    int *__restrict__ status) {\n"
        "  extern __shared__ __align__(16) float sm[];\n"
        "  __shared__ __align__(8) u64 bars[8];\n"
        "  const int wib = threadIdx.x >> 5, lane = threadIdx.x & 31;\n"
@@ -228,8 +252,7 @@ std::string pattern_source(int na, const int *len, const std::vector<int> &slot,
        "  float *const sb0 = work + abuf_floats;\n"
        "  float *const sb1 = sb0 + stage_cap;\n"
        "  float *const tb1 = sb1 + stage_cap;\n"
-       "  const int stride = gridDim.x * 2;\n"
-       "  int tile = blockIdx.x * 2 + wib;\n"
+       "  int tile = take(head, lane);\n"
        "  if (tile >= ntiles) return;\n"
        "  const u32 bar0 = saddr(&bars[4 * wib]), bar1 = bar0 + 8u;\n"
        "  const u32 bara0 = bar0 + 16u, bara1 = bar0 + 24u;\n"
@@ -239,15 +262,20 @@ std::string pattern_source(int na, const int *len, const std::vector<int> &slot,
        "  }\n"
        "  __syncwarp();\n"
        "  u32 pb0 = 0u, pb1 = 0u, pa0 = 0u, pa1 = 0u;\n"
-       "  stage_tile(work, prog, RW, __ldg(arange + tile), tile, a_val, bara0, lane);\n"
-       "  for (int it = 0; tile < ntiles; ++it, tile += stride) {\n"
+       "  const u64 keep = policy_keep(), once = policy_stream();\n"
+       "  // lane 0 holds the ticket of the tile after this one, requested a\n"
+       "  // tile ahead so that its atomic is back when the number is needed\n"
+       "  int ticket = lane == 0 ? atomicAdd(head, 1) : 0;\n"
+       "  stage_tile(work, prog, RW, __ldg(arange + tile), tile, a_val, bara0, lane, once);\n"
+       "  for (int it = 0; tile < ntiles; ++it) {\n"
        "    const bool odd = (it & 1) != 0;\n"
        "    float *const ab = odd ? tb1 : work;\n"
        "    float *const nb = odd ? work : tb1;\n"
        "    float *const region = odd ? sb0 : work;\n"
        "    const u32 bara = odd ? bara1 : bara0, barn = odd ? bara0 : bara1;\n"
        "    const u32 pa = odd ? pa1 : pa0, pn = odd ? pa0 : pa1;\n"
-       "    const int nxt = tile + stride;\n"
+       "    const int nxt = __shfl_sync(FULL, ticket, 0);\n"
+       "    if (lane == 0 && nxt < ntiles) ticket = atomicAdd(head, 1);\n"
        "    const int2 nr = nxt < ntiles ? __ldg(arange + nxt) : make_int2(0, 0);\n"
        "    if (!__all_sync(FULL, bar_wait(bara, pa))) {\n"
        "      bar_wait(bara, pa);\n"
@@ -269,16 +297,16 @@ std::string pattern_source(int na, const int *len, const std::vector<int> &slot,
     snprintf(buf, sizeof(buf), "    float c%d = zero;\n", q);
     s += buf;
   }
-  s += "    int cb0 = stage(sb0, b_val, rec[4], rec[5], bar0, lane), cb1 = 0;\n";
+  s += "    int cb0 = stage(sb0, b_val, rec[4], rec[5], bar0, lane, keep), cb1 = 0;\n";
   for (int g = 0; g < ng; ++g) {
     const int b = g & 1;
     if (g + 1 < ng) {
       snprintf(buf, sizeof(buf),
-               "    cb%d = stage(sb%d, b_val, rec[%d], rec[%d], bar%d, lane);\n",
+               "    cb%d = stage(sb%d, b_val, rec[%d], rec[%d], bar%d, lane, keep);\n",
                (g + 1) & 1, (g + 1) & 1, 4 + 2 * (g + 1), 5 + 2 * (g + 1), (g + 1) & 1);
       s += buf;
     }
-    if (g == mid) s += "    if (nxt < ntiles) stage_tile(nb, prog, RW, nr, nxt, a_val, barn, lane);\n";
+    if (g == mid) s += "    if (nxt < ntiles) stage_tile(nb, prog, RW, nr, nxt, a_val, barn, lane, once);\n";
     // bounded wait; on a timeout wait (bounded) for the copies still out
     snprintf(buf, sizeof(buf), "    if (!__all_sync(FULL, bar_wait(bar%d, pb%d))) {\n", b, b);
     s += buf;
@@ -340,7 +368,7 @@ std::string pattern_source(int na, const int *len, const std::vector<int> &slot,
        "        const int body = (total - head) & ~3;\n"
        "        if (lane < head) g[lane] = region[sh + lane];\n"
        "        if (head + body + lane < total) g[head + body + lane] = region[sh + head + body + lane];\n"
-       "        if (lane == 0 && body > 0) store_block(g + head, region + sh + head, body * 4);\n"
+       "        if (lane == 0 && body > 0) store_block(g + head, region + sh + head, body * 4, once);\n"
        "      } else {\n"
        "        __syncwarp();\n"
        "        int k = 0;\n"
@@ -354,6 +382,7 @@ std::string pattern_source(int na, const int *len, const std::vector<int> &slot,
        "      }\n"
        "      __syncwarp();\n"
        "    }\n"
+       "    tile = nxt;\n"
        "  }\n"
        "}\n";
   return s;
@@ -378,37 +407,46 @@ std::vector<char> compile_cubin(const std::string &src, const std::string &arch)
   return bin;
 }
 
-// The kernels of `srcs` (nullptr where a compile failed): cached ones at
-// once, the others compiled side by side, one thread each, then loaded on
-// the calling thread (whose device is the plan's).
-void kernels_for(const std::vector<std::string> &srcs, std::vector<cudaKernel_t> &out) {
-  out.assign(srcs.size(), nullptr);
+// The architecture string of the current device (`--gpu-architecture=sm_XYa`).
+std::string current_arch() {
+  int dev = 0, major = 0, minor = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev);
+  cudaDeviceGetAttribute(&minor, cudaDevAttrComputeCapabilityMinor, dev);
+  return "--gpu-architecture=sm_" + std::to_string(major) + std::to_string(minor) + "a";
+}
+
+// The kernels for `keys` (nullptr where a compile failed): cached ones at
+// once; for the others source(i) is generated and compiled side by side,
+// one thread each, then loaded on the calling thread (whose device is the
+// plan's).  A key names everything its source depends on, so a cached
+// pattern costs no source generation.
+template <class Source>
+void kernels_for(const std::vector<std::string> &keys, const Source &source,
+                 std::vector<cudaKernel_t> &out) {
+  out.assign(keys.size(), nullptr);
   std::vector<size_t> todo;
   {
     std::lock_guard<std::mutex> lock(g_mutex);
-    for (size_t i = 0; i < srcs.size(); ++i) {
-      auto it = g_cache.find(srcs[i]);
+    for (size_t i = 0; i < keys.size(); ++i) {
+      auto it = g_cache.find(keys[i]);
       if (it != g_cache.end()) out[i] = it->second;
       else todo.push_back(i);
     }
     if (todo.empty() || !open_nvrtc()) return;
   }
-  int dev = 0, major = 0, minor = 0;
-  cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev);
-  cudaDeviceGetAttribute(&minor, cudaDevAttrComputeCapabilityMinor, dev);
-  const std::string arch =
-      "--gpu-architecture=sm_" + std::to_string(major) + std::to_string(minor) + "a";
+  const std::string arch = current_arch();
   const auto t0 = std::chrono::steady_clock::now();
   std::vector<std::vector<char>> bins(todo.size());
   std::vector<std::thread> threads;
   for (size_t k = 0; k < todo.size(); ++k) {
+    auto work = [&bins, &source, &todo, &arch, k] {
+      bins[k] = compile_cubin(source(todo[k]), arch);
+    };
     try {
-      threads.emplace_back([&bins, &srcs, &todo, &arch, k] {
-        bins[k] = compile_cubin(srcs[todo[k]], arch);
-      });
+      threads.emplace_back(work);
     } catch (...) {  // no thread: compile here
-      bins[k] = compile_cubin(srcs[todo[k]], arch);
+      work();
     }
   }
   for (auto &t : threads) t.join();
@@ -423,7 +461,7 @@ void kernels_for(const std::vector<std::string> &srcs, std::vector<cudaKernel_t>
       kern = nullptr;
     cudaGetLastError();
     // a failure is remembered too: the table kernel keeps the pattern
-    g_cache[srcs[todo[k]]] = kern;
+    g_cache[keys[todo[k]]] = kern;
     out[todo[k]] = kern;
     ++g_compiles;
   }
@@ -431,37 +469,40 @@ void kernels_for(const std::vector<std::string> &srcs, std::vector<cudaKernel_t>
                       .count();
 }
 
-// tiles of pattern pid, in order (count at *n, zeroed by the caller)
-__global__ void __launch_bounds__(256)
-tile_select_kernel(const int4 *__restrict__ tiles, int32_t ntiles, int32_t pid,
-                   int4 *__restrict__ out, int32_t *__restrict__ n) {
-  const int32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  const bool take = i < ntiles && tiles[i].z == pid;
-  const unsigned b = __ballot_sync(kFull, take);
-  if (!b) return;
-  int32_t base = 0;
-  if (lane_id() == 0) base = atomicAdd(n, __popc(b));
-  base = __shfl_sync(kFull, base, 0);
-  if (take) out[base + __popc(b & lanemask_lt())] = tiles[i];
-}
+// Warps per block of the span and record kernels, and the A entries of one
+// tile's segment they stage (the tile builder keeps segments within this).
+constexpr int kBuildWarps = 4;
+constexpr int kBuildSeg = 2048;
 
-// Per lane and A nonzero j of a tile: the start of B row k_j, or -1 for an
-// inactive lane or an empty B row, into srp[j * 32 + lane].  Eight A
-// nonzeros at a time, so that their loads are in flight together.
-__device__ __forceinline__ void gather_b_starts(int32_t *srp, int32_t na,
-                                                const int32_t *slen, bool active, int32_t p,
-                                                const int32_t *__restrict__ a_col,
-                                                const int32_t *__restrict__ b_rp, int lane) {
-  for (int32_t j0 = 0; j0 < na; j0 += 8) {
-    int32_t col[8];
+// The start of B row a_col[seg0 + i], for every i < seg, into sb[i]: loads
+// of a_col coalesced across the lanes, eight of each kind in flight.
+__device__ __forceinline__ void stage_b_starts(int32_t *sb, int32_t seg0, int32_t seg,
+                                               const int32_t *__restrict__ a_col,
+                                               const int32_t *__restrict__ b_rp, int lane) {
+  for (int32_t i0 = 0; i0 < seg; i0 += 256) {
+    int32_t c[8];
 #pragma unroll
-    for (int u = 0; u < 8; ++u)
-      col[u] = (active && j0 + u < na && slen[j0 + u] > 0) ? __ldg(a_col + p + j0 + u) : -1;
+    for (int u = 0; u < 8; ++u) {
+      const int32_t i = i0 + u * 32 + lane;
+      c[u] = i < seg ? __ldg(a_col + seg0 + i) : 0;
+    }
 #pragma unroll
-    for (int u = 0; u < 8; ++u)
-      if (j0 + u < na) srp[(j0 + u) * 32 + lane] = col[u] >= 0 ? __ldg(b_rp + col[u]) : -1;
+    for (int u = 0; u < 8; ++u) {
+      const int32_t i = i0 + u * 32 + lane;
+      if (i < seg) sb[i] = __ldg(b_rp + c[u]);
+    }
   }
   __syncwarp();
+}
+
+// A tile's segment: from the first active row's first A nonzero to the last
+// active row's end.
+__device__ __forceinline__ void tile_segment(const int4 &t, const int32_t *__restrict__ a_rp,
+                                             int32_t *seg0, int32_t *seg) {
+  const uint32_t mask = static_cast<uint32_t>(t.y);
+  const int first = __ffs(static_cast<int>(mask)) - 1, last = 31 - __clz(static_cast<int>(mask));
+  *seg0 = a_rp[t.x + first];
+  *seg = a_rp[t.x + last + 1] - *seg0;
 }
 
 // Union spans of a pattern's tiles (warp per tile, grid-stride): for every
@@ -469,28 +510,35 @@ __device__ __forceinline__ void gather_b_starts(int32_t *srp, int32_t na,
 // + g - 1] = the largest, over the tiles, of (end of the last B value - first
 // B value) that the tile's rows read for A nonzeros j0 .. j0 + g - 1.  A
 // nonzero with an empty B row reads nothing.  span zeroed by the caller.
-__global__ void __launch_bounds__(256)
-span_kernel(const int4 *__restrict__ tiles, int32_t ntiles, int32_t na,
+__global__ void __launch_bounds__(kBuildWarps * 32)
+span_kernel(const int4 *__restrict__ tiles, int32_t ntiles, const int4 *__restrict__ desc,
             const uint16_t *__restrict__ lens, const int32_t *__restrict__ a_rp,
             const int32_t *__restrict__ a_col, const int32_t *__restrict__ b_rp,
             int32_t *__restrict__ span) {
-  __shared__ int32_t srp[8][32 * 32];
-  __shared__ int32_t slo[8][32], shi[8][32], slen[32];
+  __shared__ int32_t sseg[kBuildWarps][kBuildSeg];
+  __shared__ int32_t slo[kBuildWarps][32], shi[kBuildWarps][32], slen[32];
   const int wib = threadIdx.x >> 5, lane = lane_id();
+  const int32_t na = desc->x;  // A nonzeros of the pattern
+  if (na <= 0 || na > 32) return;
   if (threadIdx.x < 32) slen[threadIdx.x] = threadIdx.x < na ? lens[threadIdx.x] : 0;
   __syncthreads();
   int32_t um[kJitMaxGroup];
 #pragma unroll
   for (int g = 0; g < kJitMaxGroup; ++g) um[g] = 0;
-  for (int64_t w = int64_t(blockIdx.x) * 8 + wib; w < ntiles; w += int64_t(gridDim.x) * 8) {
+  for (int64_t w = int64_t(blockIdx.x) * kBuildWarps + wib; w < ntiles;
+       w += int64_t(gridDim.x) * kBuildWarps) {
     const int4 t = tiles[w];
     const bool active = ((static_cast<uint32_t>(t.y) >> lane) & 1u) != 0u;
-    const int32_t p = active ? a_rp[t.x + lane] : 0;
-    gather_b_starts(srp[wib], na, slen, active, p, a_col, b_rp, lane);
+    int32_t seg0 = 0, seg = 0;
+    tile_segment(t, a_rp, &seg0, &seg);
+    const int32_t p = active ? a_rp[t.x + lane] - seg0 : 0;
+    if (seg > kBuildSeg) seg = kBuildSeg;  // (never: the tile builder's bound)
+    stage_b_starts(sseg[wib], seg0, seg, a_col, b_rp, lane);
     for (int32_t j = 0; j < na; ++j) {
-      const int32_t r = srp[wib][j * 32 + lane];
-      const int32_t lo = __reduce_min_sync(kFull, r >= 0 ? r : INT_MAX);
-      const int32_t hi = __reduce_max_sync(kFull, r >= 0 ? r + slen[j] : INT_MIN);
+      const bool use = active && slen[j] > 0 && p + j < seg;
+      const int32_t r = use ? sseg[wib][p + j] : 0;
+      const int32_t lo = __reduce_min_sync(kFull, use ? r : INT_MAX);
+      const int32_t hi = __reduce_max_sync(kFull, use ? r + slen[j] : INT_MIN);
       if (lane == 0) {
         slo[wib][j] = lo;
         shi[wib][j] = hi;
@@ -526,43 +574,43 @@ span_kernel(const int4 *__restrict__ tiles, int32_t ntiles, int32_t na,
 //   lo (0 for inactive lanes and empty B rows).
 // arange[tile] = ([2], [3]); maxima[0] = the largest [3].  Structure only:
 // built once per structure, read by every numeric-only repeat.
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(kBuildWarps * 32)
 program_kernel(const int4 *__restrict__ tiles, int32_t ntiles, int32_t na, int32_t ngroups,
                const int2 *__restrict__ groups, const uint16_t *__restrict__ lens,
                const int32_t *__restrict__ a_rp, const int32_t *__restrict__ a_col,
                const int32_t *__restrict__ b_rp, int32_t rw, int32_t *__restrict__ prog,
                int2 *__restrict__ arange, int32_t *__restrict__ maxima) {
-  __shared__ int32_t srp[8][32 * 32];
+  __shared__ int32_t sseg[kBuildWarps][kBuildSeg];
   __shared__ int32_t slen[32];
   const int wib = threadIdx.x >> 5, lane = lane_id();
   if (threadIdx.x < 32) slen[threadIdx.x] = threadIdx.x < na ? lens[threadIdx.x] : 0;
   __syncthreads();
-  for (int64_t w = int64_t(blockIdx.x) * 8 + wib; w < ntiles; w += int64_t(gridDim.x) * 8) {
+  for (int64_t w = int64_t(blockIdx.x) * kBuildWarps + wib; w < ntiles;
+       w += int64_t(gridDim.x) * kBuildWarps) {
     const int4 t = tiles[w];
-    const uint32_t mask = static_cast<uint32_t>(t.y);
-    const bool active = ((mask >> lane) & 1u) != 0u;
-    const int first = __ffs(static_cast<int>(mask)) - 1, last = 31 - __clz(static_cast<int>(mask));
-    const int32_t aseg0 = a_rp[t.x + first], aend = a_rp[t.x + last + 1];
-    const int32_t p = active ? a_rp[t.x + lane] : 0;
-    gather_b_starts(srp[wib], na, slen, active, p, a_col, b_rp, lane);
+    const bool active = ((static_cast<uint32_t>(t.y) >> lane) & 1u) != 0u;
+    int32_t seg0 = 0, seg = 0;
+    tile_segment(t, a_rp, &seg0, &seg);
+    const int32_t p = active ? a_rp[t.x + lane] - seg0 : 0;
+    stage_b_starts(sseg[wib], seg0, seg < kBuildSeg ? seg : kBuildSeg, a_col, b_rp, lane);
     int32_t *const rec = prog + w * rw;
     if (lane == 0) {
       rec[0] = t.x;
       rec[1] = t.y;
-      rec[2] = aseg0;
-      rec[3] = aend - aseg0;
-      arange[w] = make_int2(aseg0, aend - aseg0);
-      atomicMax(maxima, aend - aseg0);
+      rec[2] = seg0;
+      rec[3] = seg;
+      arange[w] = make_int2(seg0, seg);
+      atomicMax(maxima, seg);
     }
     uint16_t *const aoff = reinterpret_cast<uint16_t *>(rec + 4 + 2 * ngroups);
     uint16_t *const d = aoff + 32;
-    aoff[lane] = static_cast<uint16_t>(active ? p - aseg0 : 0);
+    aoff[lane] = static_cast<uint16_t>(p);
     for (int32_t g = 0; g < ngroups; ++g) {
       const int2 gr = groups[g];
       int32_t lo = INT_MAX, hi = INT_MIN;
       for (int32_t j = gr.x; j < gr.y; ++j) {
-        const int32_t r = srp[wib][j * 32 + lane];
-        if (r >= 0) {
+        if (active && slen[j] > 0 && p + j < kBuildSeg) {
+          const int32_t r = sseg[wib][p + j];
           lo = min(lo, r);
           hi = max(hi, r + slen[j]);
         }
@@ -574,8 +622,8 @@ program_kernel(const int4 *__restrict__ tiles, int32_t ntiles, int32_t na, int32
         rec[5 + 2 * g] = hi;
       }
       for (int32_t j = gr.x; j < gr.y; ++j) {
-        const int32_t r = srp[wib][j * 32 + lane];
-        d[j * 32 + lane] = static_cast<uint16_t>(r >= 0 ? r - lo : 0);
+        const bool use = active && slen[j] > 0 && p + j < kBuildSeg;
+        d[j * 32 + lane] = static_cast<uint16_t>(use ? sseg[wib][p + j] - lo : 0);
       }
     }
     __syncwarp();
@@ -584,6 +632,27 @@ program_kernel(const int4 *__restrict__ tiles, int32_t ntiles, int32_t na, int32
 
 // desc[pid].w = 1: the table kernel leaves the pattern's tiles alone.
 __global__ void mark_pattern_kernel(int4 *desc, int32_t pid) { desc[pid].w = 1; }
+
+// The tiles the table kernel keeps (pattern not marked), in order of
+// arrival (count at *n, zeroed by the caller).
+__global__ void __launch_bounds__(256)
+table_tiles_kernel(const int4 *__restrict__ tiles, int32_t ntiles,
+                   const int4 *__restrict__ desc, int4 *__restrict__ out,
+                   int32_t *__restrict__ n) {
+  const int32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  int4 t = make_int4(0, 0, 0, 0);
+  bool take = false;
+  if (i < ntiles) {
+    t = tiles[i];
+    take = desc[t.z].w == 0;
+  }
+  const unsigned b = __ballot_sync(kFull, take);
+  if (!b) return;
+  int32_t base = 0;
+  if (lane_id() == 0) base = atomicAdd(n, __popc(b));
+  base = __shfl_sync(kFull, base, 0);
+  if (take) out[base + __popc(b & lanemask_lt())] = t;
+}
 
 }  // namespace
 
@@ -594,17 +663,33 @@ void jit_stats(int32_t *compiles, double *ms) {
 }
 
 int jit_pattern_kernels(std::vector<JitRequest> &reqs) {
-  std::vector<std::string> srcs;
+  std::vector<std::string> keys;
   std::vector<size_t> idx;
+  const std::string arch = current_arch();
   for (size_t i = 0; i < reqs.size(); ++i) {
     JitRequest &r = reqs[i];
     r.kernel = nullptr;
     if (r.na <= 0 || r.na > 32 || r.m <= 0 || r.groups.empty()) continue;
-    srcs.push_back(pattern_source(r.na, r.len, r.slot, r.m, r.groups));
+    // the key: architecture, generator version and the pattern's numbers
+    std::vector<int32_t> w = {4, r.na, r.m, static_cast<int32_t>(r.groups.size())};
+    w.insert(w.end(), r.len, r.len + r.na);
+    for (const auto &g : r.groups) {
+      w.push_back(g.first);
+      w.push_back(g.second);
+    }
+    w.insert(w.end(), r.slot.begin(), r.slot.end());
+    std::string key = arch;
+    key.append(reinterpret_cast<const char *>(w.data()), w.size() * sizeof(int32_t));
+    keys.push_back(std::move(key));
     idx.push_back(i);
   }
   std::vector<cudaKernel_t> ks;
-  kernels_for(srcs, ks);
+  kernels_for(keys,
+              [&reqs, &idx](size_t k) {
+                const JitRequest &r = reqs[idx[k]];
+                return pattern_source(r.na, r.len, r.slot, r.m, r.groups);
+              },
+              ks);
   int ok = 0;
   for (size_t k = 0; k < idx.size(); ++k) {
     reqs[idx[k]].kernel = reinterpret_cast<void *>(ks[k]);
@@ -646,25 +731,25 @@ std::vector<std::pair<int, int>> jit_groups(int na, const int *len, const int32_
   return groups;
 }
 
-void launch_tile_select(const int4 *tiles, int32_t ntiles, int32_t pid, int4 *out, int32_t *n,
-                        cudaStream_t s) {
-  if (ntiles <= 0) return;
-  tile_select_kernel<<<(ntiles + 255) / 256, 256, 0, s>>>(tiles, ntiles, pid, out, n);
-}
-
-void launch_jit_spans(const int4 *tiles, int32_t ntiles, int32_t na, const uint16_t *lens,
+void launch_jit_spans(const int4 *tiles, int32_t ntiles, const int4 *desc, const uint16_t *lens,
                       const int32_t *a_rp, const int32_t *a_col, const int32_t *b_rp,
                       int32_t *span, int num_sms, cudaStream_t s) {
-  if (ntiles <= 0 || na <= 0) return;
-  int64_t grid = (int64_t(ntiles) + 7) / 8;
+  if (ntiles <= 0) return;
+  int64_t grid = (int64_t(ntiles) + kBuildWarps - 1) / kBuildWarps;
   const int64_t cap = int64_t(num_sms > 0 ? num_sms : 148) * 6;
   if (grid > cap) grid = cap;
-  span_kernel<<<static_cast<unsigned>(grid), 256, 0, s>>>(tiles, ntiles, na, lens, a_rp, a_col,
+  span_kernel<<<static_cast<unsigned>(grid), kBuildWarps * 32, 0, s>>>(tiles, ntiles, desc, lens, a_rp, a_col,
                                                           b_rp, span);
 }
 
 void launch_mark_pattern(int4 *desc, int32_t pid, cudaStream_t s) {
   mark_pattern_kernel<<<1, 1, 0, s>>>(desc, pid);
+}
+
+void launch_table_tiles(const int4 *tiles, int32_t ntiles, const int4 *desc, int4 *out,
+                        int32_t *n, cudaStream_t s) {
+  if (ntiles <= 0) return;
+  table_tiles_kernel<<<(ntiles + 255) / 256, 256, 0, s>>>(tiles, ntiles, desc, out, n);
 }
 
 int32_t jit_record_words(int na, int ngroups) { return record_words(na, ngroups); }
@@ -677,10 +762,10 @@ void launch_jit_programs(const int4 *tiles, int32_t ntiles, int32_t na,
   if (ntiles <= 0) return;
   const int32_t rw = record_words(na, static_cast<int>(groups.size()));
   cudaMemsetAsync(prog, 0, size_t(ntiles) * size_t(rw) * sizeof(int32_t), s);
-  int64_t grid = (int64_t(ntiles) + 7) / 8;
+  int64_t grid = (int64_t(ntiles) + kBuildWarps - 1) / kBuildWarps;
   const int64_t cap = int64_t(num_sms > 0 ? num_sms : 148) * 6;
   if (grid > cap) grid = cap;
-  program_kernel<<<static_cast<unsigned>(grid), 256, 0, s>>>(
+  program_kernel<<<static_cast<unsigned>(grid), kBuildWarps * 32, 0, s>>>(
       tiles, ntiles, na, static_cast<int32_t>(groups.size()), groups_dev, lens, a_rp, a_col,
       b_rp, rw, prog, arange, maxima);
 }
@@ -722,14 +807,16 @@ int jit_grid(void *kernel, int32_t ntiles, int32_t work_floats, int32_t m, int n
 cudaError_t launch_pattern_kernel(void *kernel, const Operands &op, const int32_t *prog,
                                   const int2 *arange, int32_t ntiles, const int32_t *c_rp,
                                   float *c_val, int32_t stage_cap, int32_t abuf_floats,
-                                  int32_t work_floats, int grid, int32_t *status,
-                                  cudaStream_t s) {
+                                  int32_t work_floats, int grid, int32_t *head,
+                                  int32_t *status, cudaStream_t s) {
   if (ntiles <= 0 || grid <= 0) return cudaSuccess;
+  cudaError_t e = cudaMemsetAsync(head, 0, sizeof(int32_t), s);
+  if (e != cudaSuccess) return e;
   const size_t smem = size_t(kJitThreads / 32) * size_t(work_floats) * sizeof(float);
   int dev = 0;
   cudaGetDevice(&dev);
   cudaKernel_t k = reinterpret_cast<cudaKernel_t>(kernel);
-  cudaError_t e = cudaKernelSetAttributeForDevice(
+  e = cudaKernelSetAttributeForDevice(
       k, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem), dev);
   if (e != cudaSuccess) return e;
   float zero = 0.0f;
@@ -738,8 +825,8 @@ cudaError_t launch_pattern_kernel(void *kernel, const Operands &op, const int32_
   int32_t nt = ntiles;
   const float *a_val = op.a_val, *b_val = op.b_val;
   int32_t sc = stage_cap, abf = abuf_floats, wf = work_floats;
-  int32_t *st = status;
-  void *args[] = {&pr, &ar, &nt, &a_val, &b_val, &c_rp, &c_val, &sc, &abf, &wf, &zero, &st};
+  int32_t *hd = head, *st = status;
+  void *args[] = {&pr, &ar, &nt, &a_val, &b_val, &c_rp, &c_val, &sc, &abf, &wf, &zero, &hd, &st};
   return cudaLaunchKernel(reinterpret_cast<const void *>(k), dim3(static_cast<unsigned>(grid)),
                           dim3(kJitThreads), args, smem, s);
 }

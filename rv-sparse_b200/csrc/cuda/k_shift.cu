@@ -174,16 +174,47 @@ shift_fill32_kernel(const int32_t *__restrict__ on, int32_t *__restrict__ p, siz
     p[i] = v;
 }
 
-// B row keys: warp per B row.
+// Rows per warp in the key and resolve passes: a warp takes kShiftRows
+// consecutive rows and issues each step's loads for all of them before it
+// waits, so one warp keeps kShiftRows dependent load chains in flight.
+constexpr int kShiftRows = 4;
+
+// B row keys: kShiftRows B rows per warp, a lane per entry.
 __global__ void __launch_bounds__(kThreads)
 shift_bkey_kernel(const int32_t *__restrict__ on, int32_t b_rows,
                   const int32_t *__restrict__ b_rp, const int32_t *__restrict__ b_col,
                   unsigned long long *__restrict__ bkey) {
   if (!*on) return;
-  const int32_t k = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  if (k >= b_rows) return;
-  const unsigned long long key = brow_key(b_rp, b_col, k, lane_id());
-  if (lane_id() == 0) bkey[k] = key;
+  const int64_t k0 = ((int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5) * kShiftRows;
+  if (k0 >= b_rows) return;
+  const int lane = lane_id();
+  const int32_t v = (lane <= kShiftRows && k0 + lane <= b_rows) ? __ldg(b_rp + k0 + lane) : 0;
+  int32_t b0[kShiftRows], len[kShiftRows], col[kShiftRows];
+#pragma unroll
+  for (int u = 0; u < kShiftRows; ++u) {
+    b0[u] = __shfl_sync(kFull, v, u);
+    const int32_t b1 = __shfl_sync(kFull, v, u + 1);
+    len[u] = k0 + u < b_rows ? b1 - b0[u] : 0;
+  }
+#pragma unroll
+  for (int u = 0; u < kShiftRows; ++u) col[u] = lane < len[u] ? __ldg(b_col + b0[u] + lane) : 0;
+#pragma unroll
+  for (int u = 0; u < kShiftRows; ++u) {
+    if (k0 + u >= b_rows) break;
+    const int32_t k = static_cast<int32_t>(k0) + u;
+    // the key of brow_key: entry e contributes mix64(e, column - k)
+    unsigned long long h = 0;
+    if (lane < len[u])
+      h = mix64((static_cast<unsigned long long>(lane) << 32) |
+                static_cast<uint32_t>(col[u] - k));
+    for (int32_t e = lane + 32; e < len[u]; e += 32)
+      h ^= mix64((static_cast<unsigned long long>(e) << 32) |
+                 static_cast<uint32_t>(__ldg(b_col + b0[u] + e) - k));
+    h = warp_xor64(h);
+    if (lane == 0)
+      bkey[k] = mix64(h ^ (static_cast<unsigned long long>(len[u]) * 0x9E3779B97F4A7C15ull)) |
+                1ull;
+  }
 }
 
 // Inserts every nonzero key into the table (tkey zeroed, trow INT_MAX), the
@@ -237,7 +268,8 @@ __device__ __forceinline__ int32_t lookup(unsigned long long key,
 }
 
 // bcls[k]: the smallest B row with k's translated columns (checked entry by
-// entry), else k.  Warp per B row.
+// entry), else k.  kShiftRows B rows per warp: lane u < kShiftRows looks up
+// row k0 + u's key, then every lane compares one entry of each row.
 __global__ void __launch_bounds__(kThreads)
 shift_bresolve_kernel(const int32_t *__restrict__ on, int32_t b_rows,
                       const unsigned long long *__restrict__ bkey,
@@ -246,48 +278,95 @@ shift_bresolve_kernel(const int32_t *__restrict__ on, int32_t b_rows,
                       const int32_t *__restrict__ b_rp, const int32_t *__restrict__ b_col,
                       int32_t *__restrict__ bcls) {
   if (!*on) return;
-  const int32_t k = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  if (k >= b_rows) return;
+  const int64_t k0 = ((int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5) * kShiftRows;
+  if (k0 >= b_rows) return;
   const int lane = lane_id();
-  const int32_t c = lookup(bkey[k], tkey, trow, mask);
-  bool ok = c >= 0 && c < b_rows;
-  if (ok && c != k) {
-    const int32_t k0 = __ldg(b_rp + k), len = __ldg(b_rp + k + 1) - k0;
-    const int32_t c0 = __ldg(b_rp + c), lc = __ldg(b_rp + c + 1) - c0;
-    bool same = len == lc;
-    for (int32_t e = lane; same && e < len; e += 32)
-      same = (__ldg(b_col + k0 + e) - k) == (__ldg(b_col + c0 + e) - c);
-    ok = __all_sync(kFull, same);
+  // lane u: row k0 + u's canonical row and both rows' bounds
+  int32_t mc = -1, mk0 = 0, mk1 = 0, mc0 = 0, mc1 = 0;
+  if (lane < kShiftRows && k0 + lane < b_rows) {
+    const int32_t k = static_cast<int32_t>(k0) + lane;
+    mc = lookup(bkey[k], tkey, trow, mask);
+    mk0 = __ldg(b_rp + k);
+    mk1 = __ldg(b_rp + k + 1);
+    if (mc >= 0 && mc < b_rows && mc != k) {
+      mc0 = __ldg(b_rp + mc);
+      mc1 = __ldg(b_rp + mc + 1);
+    }
   }
-  if (lane == 0) bcls[k] = ok ? c : k;
+  int32_t c[kShiftRows], kb[kShiftRows], cb[kShiftRows], len[kShiftRows];
+  bool check[kShiftRows];
+#pragma unroll
+  for (int u = 0; u < kShiftRows; ++u) {
+    c[u] = __shfl_sync(kFull, mc, u);
+    kb[u] = __shfl_sync(kFull, mk0, u);
+    len[u] = __shfl_sync(kFull, mk1, u) - kb[u];
+    cb[u] = __shfl_sync(kFull, mc0, u);
+    const int32_t lc = __shfl_sync(kFull, mc1, u) - cb[u];
+    check[u] = c[u] >= 0 && c[u] < b_rows && c[u] != static_cast<int32_t>(k0) + u &&
+               len[u] == lc;
+  }
+  bool same[kShiftRows];
+#pragma unroll
+  for (int u = 0; u < kShiftRows; ++u) {
+    same[u] = true;
+    const int32_t k = static_cast<int32_t>(k0) + u;
+    if (check[u])
+      for (int32_t e = lane; e < len[u]; e += 32)
+        same[u] = same[u] && (__ldg(b_col + kb[u] + e) - k) == (__ldg(b_col + cb[u] + e) - c[u]);
+  }
+#pragma unroll
+  for (int u = 0; u < kShiftRows; ++u) {
+    if (k0 + u >= b_rows) break;
+    const int32_t k = static_cast<int32_t>(k0) + u;
+    const bool found = c[u] >= 0 && c[u] < b_rows;
+    const bool ok = found && (c[u] == k || (check[u] && __all_sync(kFull, same[u])));
+    if (lane == 0) bcls[k] = ok ? c[u] : k;
+  }
 }
 
-// Row keys: warp per row; 0 for a row that cannot join a pattern.
+// Row keys: kShiftRows rows per warp, a lane per A nonzero; 0 for a row
+// that cannot join a pattern.
 __global__ void __launch_bounds__(kThreads)
 shift_rkey_kernel(const int32_t *__restrict__ on, int32_t a_rows,
                   const int32_t *__restrict__ a_rp, const int32_t *__restrict__ a_col,
                   const int64_t *__restrict__ ops, const int32_t *__restrict__ bcls,
                   unsigned long long *__restrict__ rkey) {
   if (!*on) return;
-  const int32_t i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  if (i >= a_rows) return;
+  const int64_t i0 = ((int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5) * kShiftRows;
+  if (i0 >= a_rows) return;
   const int lane = lane_id();
-  const int32_t p0 = a_rp[i], na = a_rp[i + 1] - p0;
-  if (!shiftable(na, ops[i])) {
-    if (lane == 0) rkey[i] = 0ull;
-    return;
+  const int32_t v = (lane <= kShiftRows && i0 + lane <= a_rows) ? a_rp[i0 + lane] : 0;
+  const int64_t mops = (lane < kShiftRows && i0 + lane < a_rows) ? ops[i0 + lane] : 0;
+  int32_t p0[kShiftRows], na[kShiftRows], k[kShiftRows], bc[kShiftRows];
+  bool ok[kShiftRows];
+#pragma unroll
+  for (int u = 0; u < kShiftRows; ++u) {
+    p0[u] = __shfl_sync(kFull, v, u);
+    na[u] = i0 + u < a_rows ? __shfl_sync(kFull, v, u + 1) - p0[u] : 0;
+    const int64_t o = __shfl_sync(kFull, mops, u);
+    ok[u] = i0 + u < a_rows && shiftable(na[u], o);
   }
-  int32_t k = 0, bc = 0;
-  if (lane < na) {
-    k = __ldg(a_col + p0 + lane);
-    bc = __ldg(bcls + k);
+#pragma unroll
+  for (int u = 0; u < kShiftRows; ++u) k[u] = ok[u] && lane < na[u] ? __ldg(a_col + p0[u] + lane) : 0;
+#pragma unroll
+  for (int u = 0; u < kShiftRows; ++u) bc[u] = ok[u] && lane < na[u] ? __ldg(bcls + k[u]) : 0;
+#pragma unroll
+  for (int u = 0; u < kShiftRows; ++u) {
+    if (i0 + u >= a_rows) break;
+    const int32_t i = static_cast<int32_t>(i0) + u;
+    if (!ok[u]) {
+      if (lane == 0) rkey[i] = 0ull;
+      continue;
+    }
+    const unsigned long long key = row_key(na[u], lane, k[u] - i, static_cast<uint32_t>(bc[u]));
+    if (lane == 0) rkey[i] = key;
   }
-  const unsigned long long key = row_key(na, lane, k - i, static_cast<uint32_t>(bc));
-  if (lane == 0) rkey[i] = key;
 }
 
 // rcls[i]: the smallest row with i's translated A row over the same B
-// classes (checked entry by entry), else i.  Warp per row.
+// classes (checked entry by entry), else i.  kShiftRows rows per warp: lane
+// u < kShiftRows looks up row i0 + u's key, then every lane compares one A
+// nonzero of each row.
 __global__ void __launch_bounds__(kThreads)
 shift_rresolve_kernel(const int32_t *__restrict__ on, int32_t a_rows,
                       const unsigned long long *__restrict__ rkey,
@@ -296,23 +375,57 @@ shift_rresolve_kernel(const int32_t *__restrict__ on, int32_t a_rows,
                       const int32_t *__restrict__ a_rp, const int32_t *__restrict__ a_col,
                       const int32_t *__restrict__ bcls, int32_t *__restrict__ rcls) {
   if (!*on) return;
-  const int32_t i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  if (i >= a_rows) return;
+  const int64_t i0 = ((int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5) * kShiftRows;
+  if (i0 >= a_rows) return;
   const int lane = lane_id();
-  const unsigned long long key = rkey[i];
-  const int32_t c = key ? lookup(key, tkey, trow, mask) : -1;
-  bool ok = c >= 0 && c < a_rows && c != i;
-  if (ok) {
-    const int32_t pi = a_rp[i], na = a_rp[i + 1] - pi;
-    const int32_t pc = a_rp[c], nc = a_rp[c + 1] - pc;
-    bool same = na == nc && na <= kShiftMaxA;
-    if (same && lane < na) {
-      const int32_t ki = __ldg(a_col + pi + lane), kc = __ldg(a_col + pc + lane);
-      same = (ki - i) == (kc - c) && __ldg(bcls + ki) == __ldg(bcls + kc);
+  int32_t mc = -1, mi0 = 0, mi1 = 0, mc0 = 0, mc1 = 0;
+  if (lane < kShiftRows && i0 + lane < a_rows) {
+    const int32_t i = static_cast<int32_t>(i0) + lane;
+    const unsigned long long key = rkey[i];
+    mc = key ? lookup(key, tkey, trow, mask) : -1;
+    if (mc >= 0 && mc < a_rows && mc != i) {
+      mi0 = a_rp[i];
+      mi1 = a_rp[i + 1];
+      mc0 = a_rp[mc];
+      mc1 = a_rp[mc + 1];
+    } else {
+      mc = -1;
     }
-    ok = __all_sync(kFull, same);
   }
-  if (lane == 0) rcls[i] = ok ? c : i;
+  int32_t c[kShiftRows], pi[kShiftRows], pc[kShiftRows], na[kShiftRows];
+  bool check[kShiftRows];
+#pragma unroll
+  for (int u = 0; u < kShiftRows; ++u) {
+    c[u] = __shfl_sync(kFull, mc, u);
+    pi[u] = __shfl_sync(kFull, mi0, u);
+    na[u] = __shfl_sync(kFull, mi1, u) - pi[u];
+    pc[u] = __shfl_sync(kFull, mc0, u);
+    const int32_t nc = __shfl_sync(kFull, mc1, u) - pc[u];
+    check[u] = c[u] >= 0 && na[u] == nc && na[u] <= kShiftMaxA;
+  }
+  int32_t ki[kShiftRows], kc[kShiftRows];
+#pragma unroll
+  for (int u = 0; u < kShiftRows; ++u) {
+    const bool in = check[u] && lane < na[u];
+    ki[u] = in ? __ldg(a_col + pi[u] + lane) : 0;
+    kc[u] = in ? __ldg(a_col + pc[u] + lane) : 0;
+  }
+  bool same[kShiftRows];
+#pragma unroll
+  for (int u = 0; u < kShiftRows; ++u) {
+    same[u] = true;
+    if (check[u] && lane < na[u]) {
+      const int32_t i = static_cast<int32_t>(i0) + u;
+      same[u] = (ki[u] - i) == (kc[u] - c[u]) && __ldg(bcls + ki[u]) == __ldg(bcls + kc[u]);
+    }
+  }
+#pragma unroll
+  for (int u = 0; u < kShiftRows; ++u) {
+    if (i0 + u >= a_rows) break;
+    const int32_t i = static_cast<int32_t>(i0) + u;
+    const bool ok = check[u] && __all_sync(kFull, same[u]);
+    if (lane == 0) rcls[i] = ok ? c[u] : i;
+  }
 }
 
 // share[c] += rows whose class is c (other than c); warp-aggregated.
@@ -473,17 +586,45 @@ shift_copy_counts_kernel(const int32_t *__restrict__ on, int32_t n,
   counts[i] = counts[rcls[i]];
 }
 
-// Member rows' columns: the canonical row's, moved by i - c.  Warp per row.
+// Member rows' columns: the canonical row's, moved by i - c.  kShiftRows
+// rows per warp (lane u < kShiftRows finds row i0 + u's canonical row and
+// bounds), every lane copying one entry of each row per step.
 __global__ void __launch_bounds__(kThreads)
 shift_fill_kernel(int32_t n, const int32_t *__restrict__ pid_of_row,
                   const int32_t *__restrict__ rcls, const int32_t *__restrict__ c_rp,
                   int32_t *__restrict__ c_col) {
-  const int32_t i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  if (i >= n || pid_of_row[i] < 0) return;
-  const int32_t c = rcls[i];
-  const int32_t cs = c_rp[i], cc = c_rp[c], m = c_rp[i + 1] - cs;
-  const int32_t d = i - c;
-  for (int32_t e = lane_id(); e < m; e += 32) c_col[cs + e] = __ldg(c_col + cc + e) + d;
+  const int64_t i0 = ((int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5) * kShiftRows;
+  if (i0 >= n) return;
+  const int lane = lane_id();
+  int32_t mcs = 0, mcc = 0, mm = 0, md = 0;
+  if (lane < kShiftRows && i0 + lane < n) {
+    const int32_t i = static_cast<int32_t>(i0) + lane;
+    if (pid_of_row[i] >= 0) {
+      const int32_t c = rcls[i];
+      mcs = c_rp[i];
+      mm = c_rp[i + 1] - mcs;
+      mcc = c_rp[c];
+      md = i - c;
+    }
+  }
+  int32_t cs[kShiftRows], cc[kShiftRows], m[kShiftRows], d[kShiftRows];
+  int32_t longest = 0;
+#pragma unroll
+  for (int u = 0; u < kShiftRows; ++u) {
+    cs[u] = __shfl_sync(kFull, mcs, u);
+    cc[u] = __shfl_sync(kFull, mcc, u);
+    m[u] = __shfl_sync(kFull, mm, u);
+    d[u] = __shfl_sync(kFull, md, u);
+    longest = max(longest, m[u]);
+  }
+  for (int32_t e = lane; e < longest; e += 32) {
+    int32_t v[kShiftRows];
+#pragma unroll
+    for (int u = 0; u < kShiftRows; ++u) v[u] = e < m[u] ? __ldg(c_col + cc[u] + e) : 0;
+#pragma unroll
+    for (int u = 0; u < kShiftRows; ++u)
+      if (e < m[u]) c_col[cs[u] + e] = v[u] + d[u];
+  }
 }
 
 // Map of each pattern's canonical row: for product t in flattened order
@@ -566,20 +707,21 @@ void launch_shift_classes(const int32_t *on, const Operands &op, int32_t b_rows,
   // B classes
   shift_fill64_kernel<<<grid_fill(tcap), kThreads, 0, s>>>(on, tkey, tcap, 0ull);
   shift_fill32_kernel<<<grid_fill(tcap), kThreads, 0, s>>>(on, trow, tcap, INT_MAX);
-  shift_bkey_kernel<<<grid_warps(b_rows), kThreads, 0, s>>>(on, b_rows, op.b_rp, op.b_col,
-                                                            bkey);
+  const int64_t bw = (int64_t(b_rows) + kShiftRows - 1) / kShiftRows;
+  const int64_t aw = (int64_t(op.a_rows) + kShiftRows - 1) / kShiftRows;
+  shift_bkey_kernel<<<grid_warps(bw), kThreads, 0, s>>>(on, b_rows, op.b_rp, op.b_col, bkey);
   shift_insert_kernel<<<grid_threads(b_rows), kThreads, 0, s>>>(on, b_rows, bkey, tkey, trow,
                                                                 mask);
-  shift_bresolve_kernel<<<grid_warps(b_rows), kThreads, 0, s>>>(on, b_rows, bkey, tkey, trow,
-                                                                mask, op.b_rp, op.b_col, bcls);
+  shift_bresolve_kernel<<<grid_warps(bw), kThreads, 0, s>>>(on, b_rows, bkey, tkey, trow, mask,
+                                                            op.b_rp, op.b_col, bcls);
   // row classes
   shift_fill64_kernel<<<grid_fill(tcap), kThreads, 0, s>>>(on, tkey, tcap, 0ull);
   shift_fill32_kernel<<<grid_fill(tcap), kThreads, 0, s>>>(on, trow, tcap, INT_MAX);
-  shift_rkey_kernel<<<grid_warps(op.a_rows), kThreads, 0, s>>>(on, op.a_rows, op.a_rp,
-                                                               op.a_col, ops, bcls, rkey);
+  shift_rkey_kernel<<<grid_warps(aw), kThreads, 0, s>>>(on, op.a_rows, op.a_rp, op.a_col, ops,
+                                                        bcls, rkey);
   shift_insert_kernel<<<grid_threads(op.a_rows), kThreads, 0, s>>>(on, op.a_rows, rkey, tkey,
                                                                    trow, mask);
-  shift_rresolve_kernel<<<grid_warps(op.a_rows), kThreads, 0, s>>>(
+  shift_rresolve_kernel<<<grid_warps(aw), kThreads, 0, s>>>(
       on, op.a_rows, rkey, tkey, trow, mask, op.a_rp, op.a_col, bcls, rcls);
 }
 
@@ -611,7 +753,8 @@ void launch_shift_copy_counts(const int32_t *on, int32_t n, const int32_t *pid_o
 
 void launch_shift_fill(int32_t n, const int32_t *pid_of_row, const int32_t *rcls,
                        const int32_t *c_rp, int32_t *c_col, cudaStream_t s) {
-  shift_fill_kernel<<<grid_warps(n), kThreads, 0, s>>>(n, pid_of_row, rcls, c_rp, c_col);
+  shift_fill_kernel<<<grid_warps((int64_t(n) + kShiftRows - 1) / kShiftRows), kThreads, 0, s>>>(
+      n, pid_of_row, rcls, c_rp, c_col);
 }
 
 void launch_shift_canon_map(int32_t npat, const int32_t *pat_canon, const Operands &op,

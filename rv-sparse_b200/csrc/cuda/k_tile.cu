@@ -141,8 +141,12 @@ tile_tab_kernel(int32_t npat, const int32_t *__restrict__ pat_canon,
   if (lane == 0) desc[id] = make_int4(na, m, t0, 0);
 }
 
+// Warps per block of the tile builder (each stages its chunk's B row
+// starts: kTileASegMax ints of shared memory a warp).
+constexpr int kBuildWarps = 4;
+
 // Warp per chunk of 32 consecutive rows (see the file comment).
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(kBuildWarps * 32)
 tile_build_kernel(int32_t n, const int32_t *__restrict__ pid_of_row,
                   const int4 *__restrict__ desc, const uint16_t *__restrict__ lens,
                   const int32_t *__restrict__ a_rp, const int32_t *__restrict__ a_col,
@@ -178,10 +182,29 @@ tile_build_kernel(int32_t n, const int32_t *__restrict__ pid_of_row,
     ok = __all_sync(kFull, fits);
   }
   if (ok) {
-    const int32_t p = in ? a_rp[row] : 0;
+    // the chunk's B row starts, staged with coalesced loads of a_col (the
+    // chunk's A segment is at most kTileASegMax entries here)
+    __shared__ int32_t sseg[kBuildWarps][kTileASegMax];
+    int32_t *const sb = sseg[(threadIdx.x >> 5) % kBuildWarps];
+    const int32_t seg0 = a_rp[row0];
+    for (int32_t i0 = 0; i0 < seg; i0 += 256) {
+      int32_t c[8];
+#pragma unroll
+      for (int u = 0; u < 8; ++u) {
+        const int32_t i = i0 + u * 32 + lane;
+        c[u] = i < seg ? __ldg(a_col + seg0 + i) : 0;
+      }
+#pragma unroll
+      for (int u = 0; u < 8; ++u) {
+        const int32_t i = i0 + u * 32 + lane;
+        if (i < seg) sb[i] = __ldg(b_rp + c[u]);
+      }
+    }
+    __syncwarp();
+    const int32_t p = in ? a_rp[row] - seg0 : 0;
     for (int32_t j = 0; j < d.x; ++j) {
       const int32_t lj = lens[size_t(bpid) * 32 + j];
-      const int32_t rp = in ? __ldg(b_rp + __ldg(a_col + p + j)) : 0;
+      const int32_t rp = in ? sb[p + j] : 0;
       const int32_t lo = __reduce_min_sync(kFull, in ? rp : INT_MAX);
       const int32_t hi = __reduce_max_sync(kFull, in ? rp + lj : INT_MIN);
       need = max(need, hi - (lo & ~3) + 8);
@@ -416,8 +439,8 @@ void launch_tile_build(int32_t n, const int32_t *pid_of_row, const int4 *desc,
                        cudaStream_t s) {
   if (n <= 0) return;
   const int64_t chunks = (int64_t(n) + 31) / 32;
-  const int64_t grid = (chunks + 7) / 8;
-  tile_build_kernel<<<static_cast<unsigned>(grid), 256, 0, s>>>(
+  const int64_t grid = (chunks + kBuildWarps - 1) / kBuildWarps;
+  tile_build_kernel<<<static_cast<unsigned>(grid), kBuildWarps * 32, 0, s>>>(
       n, pid_of_row, desc, lens, a_rp, a_col, b_rp, c_rp, tiles, ntiles, lo_rows, lo_ids, lo_n,
       maxima);
 }

@@ -384,15 +384,16 @@ void jit_stats(int32_t *compiles, double *ms);
 std::vector<std::pair<int, int>> jit_groups(int na, const int *len, const int32_t *span,
                                             int32_t max_span, int32_t *stage_need);
 // span[j0 * kJitMaxGroup + g - 1] = the largest B range (floats) that one of
-// the tiles reads for A nonzeros j0 .. j0 + g - 1 (span zeroed by the caller).
-void launch_jit_spans(const int4 *tiles, int32_t ntiles, int32_t na, const uint16_t *lens,
+// the tiles reads for A nonzeros j0 .. j0 + g - 1 (span zeroed by the caller;
+// desc->x = the pattern's A nonzeros, nothing done unless in 1..32).
+void launch_jit_spans(const int4 *tiles, int32_t ntiles, const int4 *desc, const uint16_t *lens,
                       const int32_t *a_rp, const int32_t *a_col, const int32_t *b_rp,
                       int32_t *span, int num_sms, cudaStream_t s);
-// out[*n] = the tiles of pattern pid (*n zeroed by the caller).
-void launch_tile_select(const int4 *tiles, int32_t ntiles, int32_t pid, int4 *out, int32_t *n,
-                        cudaStream_t s);
 // Marks pattern pid's tiles for the table kernel to skip (desc[pid].w = 1).
 void launch_mark_pattern(int4 *desc, int32_t pid, cudaStream_t s);
+// out[*n] = the tiles whose pattern is not marked (*n zeroed by the caller).
+void launch_table_tiles(const int4 *tiles, int32_t ntiles, const int4 *desc, int4 *out,
+                        int32_t *n, cudaStream_t s);
 // Words of one tile record of a pattern kernel (na A nonzeros, ngroups
 // staging groups).
 int32_t jit_record_words(int na, int ngroups);
@@ -412,13 +413,14 @@ void jit_layout(int32_t rw, int32_t seg_max, int32_t need, int32_t m, int32_t *s
 // Blocks of a persistent pattern kernel launch: the tiles' pairs, at most
 // what fits the SMs at once.
 int jit_grid(void *kernel, int32_t ntiles, int32_t work_floats, int32_t m, int num_sms);
-// One launch of a pattern kernel over its tile records (status:
-// kDevWaitTimeout when a bounded wait ran out).
+// One launch of a pattern kernel over its tile records (head: one device
+// word for the launch's tile queue, zeroed here; status: kDevWaitTimeout
+// when a bounded wait ran out).
 cudaError_t launch_pattern_kernel(void *kernel, const Operands &op, const int32_t *prog,
                                   const int2 *arange, int32_t ntiles, const int32_t *c_rp,
                                   float *c_val, int32_t stage_cap, int32_t abuf_floats,
-                                  int32_t work_floats, int grid, int32_t *status,
-                                  cudaStream_t s);
+                                  int32_t work_floats, int grid, int32_t *head,
+                                  int32_t *status, cudaStream_t s);
 
 // ---- k_shift.cu ------------------------------------------------------------
 // Shift classes (see k_shift.cu).  Every pass but the probe is gated by the

@@ -91,35 +91,47 @@ struct JitPattern {
   DevArray<int4> tiles;
   DevArray<int32_t> prog;  // tile records (k_jit.cu)
   DevArray<int2> arange;   // per tile its A range
+  DevArray<int32_t> head;  // the launch's tile queue
   int32_t n = 0, m = 0, stage_cap = 0, abuf_floats = 0, work_floats = 0;
   int grid = 0;
   void release() {
     tiles.release();
     prog.release();
     arange.release();
+    head.release();
   }
 };
 struct TileBuild {
-  std::vector<JitPattern> jit;  // patterns with their own kernel (k_jit.cu)
+  std::vector<JitPattern> jit;   // patterns with their own kernel (k_jit.cu)
+  std::vector<JitPattern> pool;  // device arrays of earlier builds, for reuse
+  DevArray<int32_t> jwords;      // per chosen pattern: spans, record extent
+  DevArray<int2> jgroups;        // per chosen pattern: its staging groups
   int ready = 0;
   int32_t n_tiles = 0, n_lo = 0, stage = 0, aseg = 0, max_out = 0, b_nnz = 0;
   DevArray<uint16_t> tab, lens;
   DevArray<int4> desc, tiles;
-  DevArray<int32_t> pid, lo_rows, lo_ids, counts, all_rows, all_ids, spans;
+  DevArray<int4> table;  // the tiles left to the table kernel, when patterns are compiled
+  int32_t n_table = 0;
+  DevArray<int32_t> pid, lo_rows, lo_ids, counts, all_rows, all_ids;
   void release() {
     tab.release();
     lens.release();
     desc.release();
     tiles.release();
+    table.release();
+    n_table = 0;
     pid.release();
     lo_rows.release();
     lo_ids.release();
     counts.release();
     all_rows.release();
     all_ids.release();
-    spans.release();
     for (auto &j : jit) j.release();
+    for (auto &j : pool) j.release();
     jit.clear();
+    pool.clear();
+    jwords.release();
+    jgroups.release();
     ready = 0;
   }
 };
@@ -1192,16 +1204,19 @@ constexpr int32_t kJitMaxOut = 160;
 // Largest B range (floats) one stage buffer of a pattern kernel takes.
 constexpr int32_t kJitMaxSpan = 4096;
 
-// Compiled kernels for the patterns that cover the most tiles: the tile list
-// is read back once; for each chosen pattern its tiles are listed, the union
-// spans of runs of its A nonzeros measured over those tiles (the staging
-// groups and buffer size follow), its table turned into CUDA source
-// (k_jit.cu) and compiled, and its tiles marked so the table kernel skips
-// them.  A pattern whose compile fails stays on the table kernel.
+// Compiled kernels for the patterns that cover the most tiles.  The tile
+// list is read back once to count each pattern's tiles and list them in row
+// order; then, for all the chosen patterns at once, the union spans of
+// runs of their A nonzeros measured (one round trip with their tables), the
+// staging groups chosen and the kernels compiled side by side (k_jit.cu),
+// their tile records built (one round trip for the records' A extents), and
+// their tiles marked so the table kernel skips them (one round trip for the
+// table kernel's own list).  A pattern whose compile fails stays on the
+// table kernel.  The device arrays of earlier builds are kept and reused.
 // Synchronizes `s`.
 cudaError_t build_pattern_kernels(rvsp_cuda_plan *p, cudaStream_t s, const Operands &op,
                                   int32_t npat, TileBuild &tb) {
-  for (auto &j : tb.jit) j.release();
+  for (auto &j : tb.jit) tb.pool.push_back(j);
   tb.jit.clear();
   std::vector<int4> tiles(static_cast<size_t>(tb.n_tiles));
   cudaError_t e = cudaMemcpyAsync(tiles.data(), tb.tiles.p, tiles.size() * sizeof(int4),
@@ -1218,116 +1233,170 @@ cudaError_t build_pattern_kernels(rvsp_cuda_plan *p, cudaStream_t s, const Opera
             [&](int32_t a, int32_t b) { return count[size_t(a)] > count[size_t(b)]; });
   if (order.size() > size_t(kJitMaxPatterns)) order.resize(size_t(kJitMaxPatterns));
   if (order.empty()) return cudaSuccess;
-  if (tb.spans.reserve(size_t(32 * kJitMaxGroup)) != cudaSuccess) {
+  const size_t K = order.size();
+  // per chosen pattern: spans (32 x kJitMaxGroup words), its records' A
+  // extent
+  constexpr size_t W = size_t(32 * kJitMaxGroup) + 2;
+  if (tb.jwords.reserve(K * W) != cudaSuccess || tb.jgroups.reserve(K * 32) != cudaSuccess) {
     cudaGetLastError();
     return cudaSuccess;
   }
   const int32_t stride = tile_tab_stride();
-  std::vector<JitRequest> reqs;
-  std::vector<JitPattern> cand;
-  std::vector<int32_t> cand_id;
-  auto drop = [&cand](cudaError_t err) {
-    for (auto &c : cand) c.release();
-    return err;
-  };
-  for (int32_t id : order) {
-    int4 d;
-    uint16_t lens[32];
-    std::vector<uint16_t> tab(static_cast<size_t>(stride));
-    e = cudaMemcpyAsync(&d, tb.desc.p + id, sizeof(int4), cudaMemcpyDeviceToHost, s);
-    if (e == cudaSuccess)
-      e = cudaMemcpyAsync(lens, tb.lens.p + size_t(id) * 32, sizeof(lens),
-                          cudaMemcpyDeviceToHost, s);
-    if (e == cudaSuccess)
-      e = cudaMemcpyAsync(tab.data(), tb.tab.p + size_t(id) * stride,
-                          tab.size() * sizeof(uint16_t), cudaMemcpyDeviceToHost, s);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
-    if (e != cudaSuccess) return drop(e);
-    if (d.x <= 0 || d.x > 32 || d.y <= 0 || d.y > kJitMaxOut) continue;
-    JitRequest rq;
+  std::vector<int4> desc(static_cast<size_t>(npat));
+  std::vector<uint16_t> lens(size_t(npat) * 32);
+  std::vector<uint16_t> tabs(K * size_t(stride));
+  std::vector<int32_t> words(K * W, 0);
+  std::vector<JitPattern> cand(K);
+  auto give_back = [&tb](JitPattern &jp) { tb.pool.push_back(jp); jp = JitPattern(); };
+  // each chosen pattern's tiles in order of their first row (one tile per
+  // chunk of 32 rows: a counting pass over the chunks), so that the
+  // persistent warps, which take tiles in list order, work on neighbouring
+  // rows at any one time and their B ranges stay in L2 between tiles
+  std::vector<int32_t> kof(static_cast<size_t>(npat), -1);
+  for (size_t k = 0; k < K; ++k) kof[size_t(order[k])] = static_cast<int32_t>(k);
+  std::vector<std::vector<int4>> lists(K);
+  {
+    const int64_t nchunks = (int64_t(p->a_rows) + 31) / 32;
+    std::vector<int32_t> at(static_cast<size_t>(nchunks), -1);
+    for (size_t i = 0; i < tiles.size(); ++i) {
+      const int64_t c = int64_t(tiles[i].x) / 32;
+      if (c >= 0 && c < nchunks) at[size_t(c)] = static_cast<int32_t>(i);
+    }
+    for (size_t k = 0; k < K; ++k) lists[k].reserve(size_t(count[size_t(order[k])]));
+    for (const int32_t i : at) {
+      if (i < 0) continue;
+      const int4 &t = tiles[size_t(i)];
+      if (t.z >= 0 && t.z < npat && kof[size_t(t.z)] >= 0) lists[size_t(kof[size_t(t.z)])].push_back(t);
+    }
+  }
+  e = cudaMemcpyAsync(desc.data(), tb.desc.p, desc.size() * sizeof(int4), cudaMemcpyDeviceToHost,
+                      s);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(lens.data(), tb.lens.p, lens.size() * sizeof(uint16_t),
+                        cudaMemcpyDeviceToHost, s);
+  for (size_t k = 0; k < K && e == cudaSuccess; ++k)
+    e = cudaMemcpyAsync(tabs.data() + k * stride, tb.tab.p + size_t(order[k]) * stride,
+                        size_t(stride) * sizeof(uint16_t), cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaMemsetAsync(tb.jwords.p, 0, K * W * sizeof(int32_t), s);
+  for (size_t k = 0; k < K && e == cudaSuccess; ++k) {
+    const int32_t id = order[k];
+    JitPattern &jp = cand[k];
+    if (!tb.pool.empty()) {
+      jp = tb.pool.back();
+      tb.pool.pop_back();
+    }
+    jp.n = static_cast<int32_t>(lists[k].size());
+    if (jp.n <= 0 || jp.tiles.reserve(size_t(jp.n)) != cudaSuccess) {
+      cudaGetLastError();
+      give_back(jp);
+      continue;
+    }
+    int32_t *const wk = tb.jwords.p + k * W;
+    e = cudaMemcpyAsync(jp.tiles.p, lists[k].data(), lists[k].size() * sizeof(int4),
+                        cudaMemcpyHostToDevice, s);
+    if (e != cudaSuccess) break;
+    launch_jit_spans(jp.tiles.p, jp.n, tb.desc.p + id, tb.lens.p + size_t(id) * 32, op.a_rp,
+                     op.a_col, op.b_rp, wk, p->num_sms, s);
+  }
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(words.data(), tb.jwords.p, K * W * sizeof(int32_t),
+                        cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) {
+    for (auto &c : cand) give_back(c);
+    return e;
+  }
+  // requests for the patterns that can have a kernel
+  std::vector<JitRequest> reqs(K);
+  for (size_t k = 0; k < K; ++k) {
+    JitPattern &jp = cand[k];
+    const int4 d = desc[size_t(order[k])];
+    if (!jp.tiles.p || d.x <= 0 || d.x > 32 || d.y <= 0 || d.y > kJitMaxOut) {
+      give_back(jp);
+      continue;
+    }
+    JitRequest &rq = reqs[k];
     rq.na = d.x;
     rq.m = d.y;
+    const uint16_t *tab = tabs.data() + k * stride;
     int32_t off = 0;
     for (int j = 0; j < d.x; ++j) {
-      rq.len[j] = lens[j];
+      rq.len[j] = lens[size_t(order[k]) * 32 + j];
       for (int ee = 0; ee < rq.len[j]; ++ee) rq.slot.push_back(tab[size_t(off + ee)] & 0x7fff);
       off += (rq.len[j] + 7) & ~7;
     }
-    JitPattern jp;
-    if (jp.tiles.reserve(size_t(count[size_t(id)])) != cudaSuccess) {
-      cudaGetLastError();
-      continue;
-    }
-    cudaMemsetAsync(tb.counts.p + 6, 0, sizeof(int32_t), s);
-    cudaMemsetAsync(tb.spans.p, 0, size_t(32 * kJitMaxGroup) * sizeof(int32_t), s);
-    launch_tile_select(tb.tiles.p, tb.n_tiles, id, jp.tiles.p, tb.counts.p + 6, s);
-    launch_jit_spans(jp.tiles.p, count[size_t(id)], d.x, tb.lens.p + size_t(id) * 32, op.a_rp,
-                     op.a_col, op.b_rp, tb.spans.p, p->num_sms, s);
-    int32_t span[32 * kJitMaxGroup];
-    e = cudaMemcpyAsync(span, tb.spans.p, sizeof(span), cudaMemcpyDeviceToHost, s);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
-    if (e != cudaSuccess) {
-      jp.release();
-      return drop(e);
-    }
     int32_t need = 0;
-    rq.groups = jit_groups(d.x, rq.len, span, kJitMaxSpan, &need);
+    rq.groups = jit_groups(d.x, rq.len, words.data() + k * W, kJitMaxSpan, &need);
     if (rq.groups.empty() || need <= 0 || need > kJitMaxSpan) {
-      jp.release();
+      rq = JitRequest();
+      give_back(jp);
       continue;
     }
-    jp.n = count[size_t(id)];
     jp.m = d.y;
     jp.stage_cap = need;  // the largest B range; the layout follows the records
-    reqs.push_back(std::move(rq));
-    cand.push_back(std::move(jp));
-    cand_id.push_back(id);
   }
   jit_pattern_kernels(reqs);
-  for (size_t i = 0; i < reqs.size(); ++i) {
-    JitPattern &jp = cand[i];
-    if (!reqs[i].kernel) {
-      jp.release();
+  // tile records of the compiled patterns
+  std::vector<int2> gh(K * 32);
+  std::vector<int32_t> rws(K, 0);
+  for (size_t k = 0; k < K; ++k) {
+    JitPattern &jp = cand[k];
+    const JitRequest &rq = reqs[k];
+    if (!jp.tiles.p) continue;
+    if (!rq.kernel) {
+      give_back(jp);
       continue;
     }
-    const JitRequest &rq = reqs[i];
-    const int32_t rw = jit_record_words(rq.na, static_cast<int>(rq.groups.size()));
-    std::vector<int2> gh;
-    for (const auto &g : rq.groups) gh.push_back(make_int2(g.first, g.second));
-    DevArray<int2> gdev;
-    if (jp.prog.reserve(size_t(jp.n) * size_t(rw)) != cudaSuccess ||
-        jp.arange.reserve(size_t(jp.n)) != cudaSuccess || gdev.reserve(gh.size()) != cudaSuccess) {
+    rws[k] = jit_record_words(rq.na, static_cast<int>(rq.groups.size()));
+    if (jp.prog.reserve(size_t(jp.n) * size_t(rws[k])) != cudaSuccess ||
+        jp.arange.reserve(size_t(jp.n)) != cudaSuccess || jp.head.reserve(1) != cudaSuccess) {
       cudaGetLastError();
-      jp.release();
-      gdev.release();
+      give_back(jp);
       continue;
     }
-    int32_t seg_max = 0;
-    cudaMemcpyAsync(gdev.p, gh.data(), gh.size() * sizeof(int2), cudaMemcpyHostToDevice, s);
-    cudaMemsetAsync(tb.spans.p, 0, sizeof(int32_t), s);
-    launch_jit_programs(jp.tiles.p, jp.n, rq.na, rq.groups, gdev.p,
-                        tb.lens.p + size_t(cand_id[i]) * 32, op.a_rp, op.a_col, op.b_rp,
-                        jp.prog.p, jp.arange.p, tb.spans.p, p->num_sms, s);
-    e = cudaMemcpyAsync(&seg_max, tb.spans.p, sizeof(int32_t), cudaMemcpyDeviceToHost, s);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
-    gdev.release();
-    if (e != cudaSuccess) {
-      for (size_t k = i; k < cand.size(); ++k) cand[k].release();
-      return e;
-    }
-    jit_layout(rw, seg_max, jp.stage_cap, jp.m, &jp.stage_cap, &jp.abuf_floats,
+    for (size_t g = 0; g < rq.groups.size(); ++g)
+      gh[k * 32 + g] = make_int2(rq.groups[g].first, rq.groups[g].second);
+    cudaMemcpyAsync(tb.jgroups.p + k * 32, gh.data() + k * 32, rq.groups.size() * sizeof(int2),
+                    cudaMemcpyHostToDevice, s);
+    launch_jit_programs(jp.tiles.p, jp.n, rq.na, rq.groups, tb.jgroups.p + k * 32,
+                        tb.lens.p + size_t(order[k]) * 32, op.a_rp, op.a_col, op.b_rp,
+                        jp.prog.p, jp.arange.p, tb.jwords.p + k * W + W - 2, p->num_sms, s);
+  }
+  e = cudaMemcpyAsync(words.data(), tb.jwords.p, K * W * sizeof(int32_t),
+                      cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) {
+    for (auto &c : cand) if (c.tiles.p) give_back(c);
+    return e;
+  }
+  int dev_max = 0;
+  cudaDeviceGetAttribute(&dev_max, cudaDevAttrMaxSharedMemoryPerBlockOptin, p->device);
+  for (size_t k = 0; k < K; ++k) {
+    JitPattern &jp = cand[k];
+    if (!jp.tiles.p) continue;
+    jit_layout(rws[k], words[k * W + W - 2], jp.stage_cap, jp.m, &jp.stage_cap, &jp.abuf_floats,
                &jp.work_floats);
     // two warps must fit one block's shared memory
-    int dev_max = 0;
-    cudaDeviceGetAttribute(&dev_max, cudaDevAttrMaxSharedMemoryPerBlockOptin, p->device);
     if (size_t(2) * size_t(jp.work_floats) * sizeof(float) > size_t(dev_max)) {
-      jp.release();
+      give_back(jp);
       continue;
     }
-    jp.grid = jit_grid(rq.kernel, jp.n, jp.work_floats, jp.m, p->num_sms);
-    jp.kernel = rq.kernel;
-    launch_mark_pattern(tb.desc.p, cand_id[i], s);
-    tb.jit.push_back(std::move(jp));
+    jp.grid = jit_grid(reqs[k].kernel, jp.n, jp.work_floats, jp.m, p->num_sms);
+    jp.kernel = reqs[k].kernel;
+    launch_mark_pattern(tb.desc.p, order[k], s);
+    tb.jit.push_back(jp);
+  }
+  // the table kernel's own list: the tiles of the patterns left to it
+  if (!tb.jit.empty() && tb.table.reserve(size_t(tb.n_tiles)) == cudaSuccess) {
+    cudaMemsetAsync(tb.counts.p + 6, 0, sizeof(int32_t), s);
+    launch_table_tiles(tb.tiles.p, tb.n_tiles, tb.desc.p, tb.table.p, tb.counts.p + 6, s);
+    int32_t n = 0;
+    e = cudaMemcpyAsync(&n, tb.counts.p + 6, sizeof(int32_t), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return e;
+    tb.n_table = n;
+  } else {
+    cudaGetLastError();
   }
   return cudaGetLastError();
 }
@@ -1533,17 +1602,35 @@ cudaError_t build_shift_tables(rvsp_cuda_plan *p, cudaStream_t s, const Operands
 }
 
 // The pattern kernels of a tile set (k_jit.cu); returns the launches.
-// The first (the pattern with the most tiles) goes to lane 0, the others
-// alternate between lanes 1 and 2.
+// The table kernel over the tiles of the patterns without a compiled
+// kernel (every tile when none is compiled); returns the launches.
+int launch_table_tile_kernel(const TileBuild &tb, const Operands &op, const int32_t *c_rp,
+                             float *c_val, cudaStream_t s) {
+  const bool own = !tb.jit.empty() && tb.table.p;
+  const int32_t n = own ? tb.n_table : tb.n_tiles;
+  if (n <= 0) return 0;
+  launch_tile_numeric(op, tb.b_nnz, own ? tb.table.p : tb.tiles.p, n, tb.desc.p, tb.lens.p,
+                      tb.tab.p, c_rp, c_val, tb.stage, tb.aseg, tb.max_out, s);
+  return 1;
+}
+
+// Pattern kernels of a tile set.  The first (the pattern with the most
+// tiles, persistent over every SM) goes to lane 0, the others alternate
+// between lanes 1 and 2.  The caller launches the others (main = false)
+// before the first (main = true) and before its other small launches, so
+// that they reach the SMs before the persistent kernel fills them.
 int launch_pattern_kernels(const TileBuild &tb, const Operands &op, const int32_t *c_rp,
-                           float *c_val, int32_t *status, const Lanes &ln) {
-  for (size_t i = 0; i < tb.jit.size(); ++i) {
+                           float *c_val, int32_t *status, const Lanes &ln, bool main) {
+  int launches = 0;
+  for (size_t i = main ? 0 : 1; i < (main ? std::min<size_t>(1, tb.jit.size()) : tb.jit.size());
+       ++i) {
     const auto &j = tb.jit[i];
     launch_pattern_kernel(j.kernel, op, j.prog.p, j.arange.p, j.n, c_rp, c_val, j.stage_cap,
-                          j.abuf_floats, j.work_floats, j.grid, status,
+                          j.abuf_floats, j.work_floats, j.grid, j.head.p, status,
                           ln[i == 0 ? 0 : 1 + int(i & 1)]);
+    ++launches;
   }
-  return static_cast<int>(tb.jit.size());
+  return launches;
 }
 
 // Values of the shift-class member rows (tables built): row tiles, then the
@@ -1553,16 +1640,15 @@ int launch_shift_numeric(rvsp_cuda_plan *p, const Lanes &ln, const Operands &op,
                          const int32_t *c_rp, float *c_val) {
   int launches = 0;
   if (p->st.ready && p->tiles_enabled) {
-    launch_tile_numeric(op, p->st.b_nnz, p->st.tiles.p, p->st.n_tiles, p->st.desc.p,
-                        p->st.lens.p, p->st.tab.p, c_rp, c_val, p->st.stage, p->st.aseg,
-                        p->st.max_out, ln[1]);
-    launches += 1 + launch_pattern_kernels(p->st, op, c_rp, c_val, p->misc.p + kStatus, ln);
+    launches += launch_table_tile_kernel(p->st, op, c_rp, c_val, ln[1]);
     if (p->st.n_lo > 0) {
       launch_pat_numeric(op, p->ops.p, p->st.lo_rows.p, p->st.lo_ids.p, p->st.n_lo, c_rp,
                          c_val, p->sh_pat_off.p, p->sh_steps.p, p->sh_rec.p, p->sh_max_ops,
                          p->sh_max_out, ln[2]);
       ++launches;
     }
+    launches += launch_pattern_kernels(p->st, op, c_rp, c_val, p->misc.p + kStatus, ln, false);
+    launches += launch_pattern_kernels(p->st, op, c_rp, c_val, p->misc.p + kStatus, ln, true);
   } else {
     launch_pat_numeric(op, p->ops.p, p->st.all_rows.p, p->st.all_ids.p, p->shift_members,
                        c_rp, c_val, p->sh_pat_off.p, p->sh_steps.p, p->sh_rec.p,
@@ -1765,15 +1851,15 @@ rvsp_status_t rvsp_cuda_numeric(rvsp_cuda_plan_t p, void *stream,
   const bool use_map = fill == 0 && p->rmap_state == 1 && p->rmap_col == c_col_idx;
   // numeric-only with every table in place: the row groups run side by side
   Lanes ln(p, s, use_map && (!p->shift_active || p->shift_tables == 1));
+  bool rt_main = false;  // the largest shared-map pattern kernel, launched last
   {
     PhaseScope ph(p, s, RVSP_PHASE_NUMERIC);
     if (use_map && p->pat_ready && p->n_pat_rows > 0) {
       if (p->rt.ready && p->tiles_enabled) {
-        launch_tile_numeric(op, p->rt.b_nnz, p->rt.tiles.p, p->rt.n_tiles, p->rt.desc.p,
-                            p->rt.lens.p, p->rt.tab.p, c_row_ptr, c_values, p->rt.stage,
-                            p->rt.aseg, p->rt.max_out, ln[1]);
-        ph.launches += 1 + launch_pattern_kernels(p->rt, op, c_row_ptr, c_values,
-                                                   p->misc.p + kStatus, ln);
+        ph.launches += launch_table_tile_kernel(p->rt, op, c_row_ptr, c_values, ln[1]);
+        ph.launches += launch_pattern_kernels(p->rt, op, c_row_ptr, c_values,
+                                              p->misc.p + kStatus, ln, false);
+        rt_main = true;
         if (p->rt.n_lo > 0) {
           launch_pat_numeric(op, p->ops.p, p->rt.lo_rows.p, p->rt.lo_ids.p, p->rt.n_lo,
                              c_row_ptr, c_values, p->pat_off.p, p->pat_steps.p, p->pat_rec.p,
@@ -1841,6 +1927,9 @@ rvsp_status_t rvsp_cuda_numeric(rvsp_cuda_plan_t p, void *stream,
                              p->misc.p + kStatus, p->num_sms, ln[2]);
       ph.launches += 1;
     }
+    if (rt_main)
+      ph.launches += launch_pattern_kernels(p->rt, op, c_row_ptr, c_values, p->misc.p + kStatus,
+                                            ln, true);
     if (!p->shift_active) ln.join();
   }
   if (p->shift_active) {
