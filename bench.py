@@ -37,6 +37,7 @@ Multi-GPU (torchrun): every rank computes the full workload on its own GPU
 from __future__ import annotations
 
 import argparse
+import gc
 import json
 import os
 import statistics
@@ -124,9 +125,11 @@ def committed_traffic(workload: str, phase: str):
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled every 50 ms; start()
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms; start()
     returns once the first sample is written, so the timed region that
-    follows is covered."""
+    follows is covered.  Between start() and stop() Python's garbage
+    collector is off (collected once before), so no collection pause lands
+    in a timed step."""
 
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
@@ -138,11 +141,13 @@ class ClockSampler:
         self.path = Path(os.environ.get("TMPDIR", "/tmp")) / f"rvsp_clocks_{os.getpid()}.csv"
 
     def start(self):
+        gc.collect()
+        gc.disable()
         try:
             self.fh = open(self.path, "w")
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
-                 "--format=csv,noheader,nounits", "-lms", "50"],
+                 "--format=csv,noheader,nounits", "-lms", "200"],
                 stdout=self.fh, stderr=subprocess.DEVNULL)
         except Exception:
             self.proc = None
@@ -154,6 +159,7 @@ class ClockSampler:
             time.sleep(0.02)
 
     def stop(self):
+        gc.enable()
         if self.proc is None:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
         self.proc.terminate()
@@ -1245,14 +1251,18 @@ def run_job(args, world, rank, local):
                                  (float(np.mean(first_ms)) + prep_ms + R * repeat_ms)),
             "phase_ms_per_step": per_step,
             "roofline": {"bound": "hbm",
-                         "kernel": "numeric-only repeat (tile_numeric_kernel, with "
-                                   "pat_numeric_kernel and map_numeric for the rows no tile "
-                                   "takes)",
+                         "kernel": "numeric-only repeat: rvsp_pattern_tiles (kernels compiled "
+                                   "per term pattern, the interior one persistent over every "
+                                   "SM) on the caller's stream, the table tiles, leftover rows "
+                                   "and class kernels on two side streams joined back into it; "
+                                   "one launch = one numeric-only compute, timed by CUDA "
+                                   "events on the caller's stream",
                          "achieved": repeat_gbs, "peak": peak, "unit": "GB/s",
                          "frac": repeat_gbs / peak, "peak_source": peak_src,
                          "traffic": committed_traffic("stencil3d_job", "repeat"),
-                         "traffic_source": "committed: profiles/traffic.json (ncu capture "
-                                           "named there), not measured in this run",
+                         "traffic_source": "committed: profiles/traffic.json stencil3d_job "
+                                           "(DRAM bytes of every kernel of one repeat, one ncu "
+                                           "capture named there), not measured in this run",
                          "algorithmic_bytes_per_launch": alg_bytes},
             "clocks": clocks, "e2e": e2e, "gpu_launches": launches,
             "cpu_baseline": cpu,

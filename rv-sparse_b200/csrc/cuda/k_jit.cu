@@ -505,13 +505,16 @@ __device__ __forceinline__ void tile_segment(const int4 &t, const int32_t *__res
   *seg = a_rp[t.x + last + 1] - *seg0;
 }
 
-// Union spans of a pattern's tiles (warp per tile, grid-stride): for every
-// A nonzero j0 and run length g in [1, kJitMaxGroup], span[j0 * kJitMaxGroup
-// + g - 1] = the largest, over the tiles, of (end of the last B value - first
-// B value) that the tile's rows read for A nonzeros j0 .. j0 + g - 1.  A
-// nonzero with an empty B row reads nothing.  span zeroed by the caller.
+// Union spans of a sample of a pattern's tiles (every stride-th; warp per
+// tile, grid-stride): for every A nonzero j0 and run length g in
+// [1, kJitMaxGroup], span[j0 * kJitMaxGroup + g - 1] = the largest, over the
+// sample, of (end of the last B value - first B value) that the tile's rows
+// read for A nonzeros j0 .. j0 + g - 1.  A nonzero with an empty B row reads
+// nothing.  The grouping is chosen from these; the tile records then measure
+// every tile's ranges.  span zeroed by the caller.
 __global__ void __launch_bounds__(kBuildWarps * 32)
-span_kernel(const int4 *__restrict__ tiles, int32_t ntiles, const int4 *__restrict__ desc,
+span_kernel(const int4 *__restrict__ tiles, int32_t ntiles, int32_t stride,
+            const int4 *__restrict__ desc,
             const uint16_t *__restrict__ lens, const int32_t *__restrict__ a_rp,
             const int32_t *__restrict__ a_col, const int32_t *__restrict__ b_rp,
             int32_t *__restrict__ span) {
@@ -525,9 +528,9 @@ span_kernel(const int4 *__restrict__ tiles, int32_t ntiles, const int4 *__restri
   int32_t um[kJitMaxGroup];
 #pragma unroll
   for (int g = 0; g < kJitMaxGroup; ++g) um[g] = 0;
-  for (int64_t w = int64_t(blockIdx.x) * kBuildWarps + wib; w < ntiles;
+  for (int64_t w = int64_t(blockIdx.x) * kBuildWarps + wib; w * stride < ntiles;
        w += int64_t(gridDim.x) * kBuildWarps) {
-    const int4 t = tiles[w];
+    const int4 t = tiles[w * stride];
     const bool active = ((static_cast<uint32_t>(t.y) >> lane) & 1u) != 0u;
     int32_t seg0 = 0, seg = 0;
     tile_segment(t, a_rp, &seg0, &seg);
@@ -572,8 +575,9 @@ span_kernel(const int4 *__restrict__ tiles, int32_t ntiles, const int4 *__restri
 //   then 32 uint16 A offsets (lane's first nonzero - [2]) and, per A nonzero
 //   j and lane, the uint16 offset of the lane's B row k_j from its group's
 //   lo (0 for inactive lanes and empty B rows).
-// arange[tile] = ([2], [3]); maxima[0] = the largest [3].  Structure only:
-// built once per structure, read by every numeric-only repeat.
+// arange[tile] = ([2], [3]); maxima[0] = the largest [3], maxima[1 + g] =
+// the largest B range of group g.  Structure only: built once per
+// structure, read by every numeric-only repeat.
 __global__ void __launch_bounds__(kBuildWarps * 32)
 program_kernel(const int4 *__restrict__ tiles, int32_t ntiles, int32_t na, int32_t ngroups,
                const int2 *__restrict__ groups, const uint16_t *__restrict__ lens,
@@ -620,6 +624,7 @@ program_kernel(const int4 *__restrict__ tiles, int32_t ntiles, int32_t na, int32
       if (lane == 0) {
         rec[4 + 2 * g] = lo;
         rec[5 + 2 * g] = hi;
+        atomicMax(maxima + 1 + g, hi - lo);
       }
       for (int32_t j = gr.x; j < gr.y; ++j) {
         const bool use = active && slen[j] > 0 && p + j < kBuildSeg;
@@ -735,11 +740,14 @@ void launch_jit_spans(const int4 *tiles, int32_t ntiles, const int4 *desc, const
                       const int32_t *a_rp, const int32_t *a_col, const int32_t *b_rp,
                       int32_t *span, int num_sms, cudaStream_t s) {
   if (ntiles <= 0) return;
-  int64_t grid = (int64_t(ntiles) + kBuildWarps - 1) / kBuildWarps;
+  // a sample of at most about 1024 tiles spread over the list
+  const int32_t stride = ntiles > 1024 ? ntiles / 1024 : 1;
+  const int64_t sampled = (int64_t(ntiles) + stride - 1) / stride;
+  int64_t grid = (sampled + kBuildWarps - 1) / kBuildWarps;
   const int64_t cap = int64_t(num_sms > 0 ? num_sms : 148) * 6;
   if (grid > cap) grid = cap;
-  span_kernel<<<static_cast<unsigned>(grid), kBuildWarps * 32, 0, s>>>(tiles, ntiles, desc, lens, a_rp, a_col,
-                                                          b_rp, span);
+  span_kernel<<<static_cast<unsigned>(grid), kBuildWarps * 32, 0, s>>>(
+      tiles, ntiles, stride, desc, lens, a_rp, a_col, b_rp, span);
 }
 
 void launch_mark_pattern(int4 *desc, int32_t pid, cudaStream_t s) {

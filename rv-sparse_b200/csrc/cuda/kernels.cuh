@@ -384,8 +384,9 @@ void jit_stats(int32_t *compiles, double *ms);
 std::vector<std::pair<int, int>> jit_groups(int na, const int *len, const int32_t *span,
                                             int32_t max_span, int32_t *stage_need);
 // span[j0 * kJitMaxGroup + g - 1] = the largest B range (floats) that one of
-// the tiles reads for A nonzeros j0 .. j0 + g - 1 (span zeroed by the caller;
-// desc->x = the pattern's A nonzeros, nothing done unless in 1..32).
+// a sample of the tiles reads for A nonzeros j0 .. j0 + g - 1 (span zeroed by
+// the caller; desc->x = the pattern's A nonzeros, nothing done unless in
+// 1..32).
 void launch_jit_spans(const int4 *tiles, int32_t ntiles, const int4 *desc, const uint16_t *lens,
                       const int32_t *a_rp, const int32_t *a_col, const int32_t *b_rp,
                       int32_t *span, int num_sms, cudaStream_t s);
@@ -398,8 +399,9 @@ void launch_table_tiles(const int4 *tiles, int32_t ntiles, const int4 *desc, int
 // staging groups).
 int32_t jit_record_words(int na, int ngroups);
 // The tile records of a pattern (see k_jit.cu): prog[ntiles * record words],
-// arange[ntiles] = the A range of each tile, maxima[0] = the longest (zeroed
-// by the caller); groups_dev = the groups as int2 on the device.
+// arange[ntiles] = the A range of each tile, maxima[0] = the longest,
+// maxima[1 + g] = group g's largest B range (zeroed by the caller);
+// groups_dev = the groups as int2 on the device.
 void launch_jit_programs(const int4 *tiles, int32_t ntiles, int32_t na,
                          const std::vector<std::pair<int, int>> &groups, const int2 *groups_dev,
                          const uint16_t *lens, const int32_t *a_rp, const int32_t *a_col,

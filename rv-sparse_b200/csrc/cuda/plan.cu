@@ -248,8 +248,9 @@ struct rvsp_cuda_plan {
 
   // Side streams of the numeric-only pass (created on first use; state 0
   // untried, 1 ready, -1 unavailable).
-  cudaStream_t side[2] = {nullptr, nullptr};
-  cudaEvent_t fork_ev = nullptr, join_ev[2] = {nullptr, nullptr};
+  static constexpr int kSide = 6;
+  cudaStream_t side[kSide] = {};
+  cudaEvent_t fork_ev = nullptr, join_ev[kSide] = {};
   int side_state = 0;
 
   bool profiling = false;
@@ -327,7 +328,7 @@ bool side_streams(rvsp_cuda_plan *p, cudaStream_t s) {
     int least = 0, greatest = 0;
     bool ok = cudaDeviceGetStreamPriorityRange(&least, &greatest) == cudaSuccess &&
               cudaEventCreateWithFlags(&p->fork_ev, cudaEventDisableTiming) == cudaSuccess;
-    for (int i = 0; i < 2 && ok; ++i)
+    for (int i = 0; i < rvsp_cuda_plan::kSide && ok; ++i)
       ok = cudaStreamCreateWithPriority(&p->side[i], cudaStreamNonBlocking, greatest) ==
                cudaSuccess &&
            cudaEventCreateWithFlags(&p->join_ev[i], cudaEventDisableTiming) == cudaSuccess;
@@ -339,24 +340,34 @@ bool side_streams(rvsp_cuda_plan *p, cudaStream_t s) {
 
 // Streams of one numeric-only pass.  Its row groups (pattern kernels, table
 // tiles, leftover rows, class kernels) write disjoint rows of C and only
-// read A, B and the plan's tables, so all but the largest go to the two side
+// read A, B and the plan's tables, so all but the largest go to the side
 // streams, forked from the caller's stream and joined back into it: the
-// small launches, bound by the latency of a few long rows, run beside the
-// large one instead of after it.  Lane 0 is the caller's stream; without
-// side streams every lane is.
+// small launches, each bound by the latency of a few long rows, run beside
+// the large one and beside each other instead of after one another.  main()
+// is the caller's stream; next() hands out the side streams in turn
+// (without side streams, the caller's stream).
 struct Lanes {
   rvsp_cuda_plan *pl;
   cudaStream_t s;
   bool forked = false;
+  int turn = 0;
   Lanes(rvsp_cuda_plan *p, cudaStream_t st, bool want) : pl(p), s(st) {
-    if (want && side_streams(p, st) && cudaEventRecord(p->fork_ev, st) == cudaSuccess)
-      forked = cudaStreamWaitEvent(p->side[0], p->fork_ev, 0) == cudaSuccess &&
-               cudaStreamWaitEvent(p->side[1], p->fork_ev, 0) == cudaSuccess;
+    if (!(want && side_streams(p, st) && cudaEventRecord(p->fork_ev, st) == cudaSuccess)) return;
+    bool ok = true;
+    for (int i = 0; i < rvsp_cuda_plan::kSide; ++i)
+      ok = ok && cudaStreamWaitEvent(p->side[i], p->fork_ev, 0) == cudaSuccess;
+    forked = ok;
   }
-  cudaStream_t operator[](int k) const { return forked && k > 0 ? pl->side[k - 1] : s; }
+  cudaStream_t main() const { return s; }
+  cudaStream_t next() {
+    if (!forked) return s;
+    const cudaStream_t x = pl->side[turn];
+    turn = (turn + 1) % rvsp_cuda_plan::kSide;
+    return x;
+  }
   void join() {
     if (!forked) return;
-    for (int i = 0; i < 2; ++i) {
+    for (int i = 0; i < rvsp_cuda_plan::kSide; ++i) {
       cudaEventRecord(pl->join_ev[i], pl->side[i]);
       cudaStreamWaitEvent(s, pl->join_ev[i], 0);
     }
@@ -487,7 +498,7 @@ void rvsp_cuda_plan_destroy(rvsp_cuda_plan_t p) {
   if (!p) return;
   resolve_pending(p);
   for (cudaEvent_t e : p->pool) cudaEventDestroy(e);
-  for (int i = 0; i < 2; ++i) {
+  for (int i = 0; i < rvsp_cuda_plan::kSide; ++i) {
     if (p->side[i]) cudaStreamDestroy(p->side[i]);
     if (p->join_ev[i]) cudaEventDestroy(p->join_ev[i]);
   }
@@ -1281,9 +1292,19 @@ cudaError_t build_pattern_kernels(rvsp_cuda_plan *p, cudaStream_t s, const Opera
   for (size_t k = 0; k < K && e == cudaSuccess; ++k) {
     const int32_t id = order[k];
     JitPattern &jp = cand[k];
+    // the device arrays of an earlier build: the smallest whose tile
+    // capacity holds this pattern's tiles, else the largest (so that a
+    // repeated analysis of the same structure allocates nothing)
     if (!tb.pool.empty()) {
-      jp = tb.pool.back();
-      tb.pool.pop_back();
+      const size_t need = lists[k].size();
+      size_t best = 0;
+      for (size_t q = 1; q < tb.pool.size(); ++q) {
+        const size_t c = tb.pool[q].tiles.cap, bc = tb.pool[best].tiles.cap;
+        const bool f = c >= need, bf = bc >= need;
+        if ((f && (!bf || c < bc)) || (!f && !bf && c > bc)) best = q;
+      }
+      jp = tb.pool[best];
+      tb.pool.erase(tb.pool.begin() + static_cast<std::ptrdiff_t>(best));
     }
     jp.n = static_cast<int32_t>(lists[k].size());
     if (jp.n <= 0 || jp.tiles.reserve(size_t(jp.n)) != cudaSuccess) {
@@ -1336,7 +1357,9 @@ cudaError_t build_pattern_kernels(rvsp_cuda_plan *p, cudaStream_t s, const Opera
     jp.stage_cap = need;  // the largest B range; the layout follows the records
   }
   jit_pattern_kernels(reqs);
-  // tile records of the compiled patterns
+  // tile records of the compiled patterns (their maxima: the records' A
+  // extent, then each group's largest B range over every tile)
+  cudaMemsetAsync(tb.jwords.p, 0, K * W * sizeof(int32_t), s);
   std::vector<int2> gh(K * 32);
   std::vector<int32_t> rws(K, 0);
   for (size_t k = 0; k < K; ++k) {
@@ -1360,7 +1383,7 @@ cudaError_t build_pattern_kernels(rvsp_cuda_plan *p, cudaStream_t s, const Opera
                     cudaMemcpyHostToDevice, s);
     launch_jit_programs(jp.tiles.p, jp.n, rq.na, rq.groups, tb.jgroups.p + k * 32,
                         tb.lens.p + size_t(order[k]) * 32, op.a_rp, op.a_col, op.b_rp,
-                        jp.prog.p, jp.arange.p, tb.jwords.p + k * W + W - 2, p->num_sms, s);
+                        jp.prog.p, jp.arange.p, tb.jwords.p + k * W, p->num_sms, s);
   }
   e = cudaMemcpyAsync(words.data(), tb.jwords.p, K * W * sizeof(int32_t),
                       cudaMemcpyDeviceToHost, s);
@@ -1374,7 +1397,16 @@ cudaError_t build_pattern_kernels(rvsp_cuda_plan *p, cudaStream_t s, const Opera
   for (size_t k = 0; k < K; ++k) {
     JitPattern &jp = cand[k];
     if (!jp.tiles.p) continue;
-    jit_layout(rws[k], words[k * W + W - 2], jp.stage_cap, jp.m, &jp.stage_cap, &jp.abuf_floats,
+    // the largest B range any tile's group reads (the sample only chose
+    // the groups); past kJitMaxSpan the uint16 offsets would not hold
+    int32_t need = 0;
+    for (size_t g = 0; g < reqs[k].groups.size(); ++g)
+      need = std::max(need, words[k * W + 1 + g]);
+    if (need <= 0 || need > kJitMaxSpan) {
+      give_back(jp);
+      continue;
+    }
+    jit_layout(rws[k], words[k * W], need, jp.m, &jp.stage_cap, &jp.abuf_floats,
                &jp.work_floats);
     // two warps must fit one block's shared memory
     if (size_t(2) * size_t(jp.work_floats) * sizeof(float) > size_t(dev_max)) {
@@ -1601,7 +1633,6 @@ cudaError_t build_shift_tables(rvsp_cuda_plan *p, cudaStream_t s, const Operands
   return cudaSuccess;
 }
 
-// The pattern kernels of a tile set (k_jit.cu); returns the launches.
 // The table kernel over the tiles of the patterns without a compiled
 // kernel (every tile when none is compiled); returns the launches.
 int launch_table_tile_kernel(const TileBuild &tb, const Operands &op, const int32_t *c_rp,
@@ -1614,20 +1645,21 @@ int launch_table_tile_kernel(const TileBuild &tb, const Operands &op, const int3
   return 1;
 }
 
-// Pattern kernels of a tile set.  The first (the pattern with the most
-// tiles, persistent over every SM) goes to lane 0, the others alternate
-// between lanes 1 and 2.  The caller launches the others (main = false)
-// before the first (main = true) and before its other small launches, so
-// that they reach the SMs before the persistent kernel fills them.
+// Pattern kernels of a tile set (k_jit.cu); returns the launches.  The
+// first (the pattern with the most tiles, persistent over every SM) goes to
+// the caller's stream, the others to the side streams in turn.  The caller
+// launches the others (main = false) with its other small launches before
+// the first (main = true), so that they reach the SMs before the persistent
+// kernel fills them.
 int launch_pattern_kernels(const TileBuild &tb, const Operands &op, const int32_t *c_rp,
-                           float *c_val, int32_t *status, const Lanes &ln, bool main) {
+                           float *c_val, int32_t *status, Lanes &ln, bool main) {
   int launches = 0;
   for (size_t i = main ? 0 : 1; i < (main ? std::min<size_t>(1, tb.jit.size()) : tb.jit.size());
        ++i) {
     const auto &j = tb.jit[i];
     launch_pattern_kernel(j.kernel, op, j.prog.p, j.arange.p, j.n, c_rp, c_val, j.stage_cap,
                           j.abuf_floats, j.work_floats, j.grid, j.head.p, status,
-                          ln[i == 0 ? 0 : 1 + int(i & 1)]);
+                          i == 0 ? ln.main() : ln.next());
     ++launches;
   }
   return launches;
@@ -1636,15 +1668,15 @@ int launch_pattern_kernels(const TileBuild &tb, const Operands &op, const int32_
 // Values of the shift-class member rows (tables built): row tiles, then the
 // members no tile took through the warp-per-row table kernel; every member
 // through that kernel when tiles are off.
-int launch_shift_numeric(rvsp_cuda_plan *p, const Lanes &ln, const Operands &op,
+int launch_shift_numeric(rvsp_cuda_plan *p, Lanes &ln, const Operands &op,
                          const int32_t *c_rp, float *c_val) {
   int launches = 0;
   if (p->st.ready && p->tiles_enabled) {
-    launches += launch_table_tile_kernel(p->st, op, c_rp, c_val, ln[1]);
+    launches += launch_table_tile_kernel(p->st, op, c_rp, c_val, ln.next());
     if (p->st.n_lo > 0) {
       launch_pat_numeric(op, p->ops.p, p->st.lo_rows.p, p->st.lo_ids.p, p->st.n_lo, c_rp,
                          c_val, p->sh_pat_off.p, p->sh_steps.p, p->sh_rec.p, p->sh_max_ops,
-                         p->sh_max_out, ln[2]);
+                         p->sh_max_out, ln.next());
       ++launches;
     }
     launches += launch_pattern_kernels(p->st, op, c_rp, c_val, p->misc.p + kStatus, ln, false);
@@ -1652,7 +1684,7 @@ int launch_shift_numeric(rvsp_cuda_plan *p, const Lanes &ln, const Operands &op,
   } else {
     launch_pat_numeric(op, p->ops.p, p->st.all_rows.p, p->st.all_ids.p, p->shift_members,
                        c_rp, c_val, p->sh_pat_off.p, p->sh_steps.p, p->sh_rec.p,
-                       p->sh_max_ops, p->sh_max_out, ln[0]);
+                       p->sh_max_ops, p->sh_max_out, ln.main());
     ++launches;
   }
   return launches;
@@ -1686,11 +1718,16 @@ cudaError_t build_reuse_map(rvsp_cuda_plan *p, cudaStream_t s, const Operands &o
     e = cudaMemcpyAsync(&too_long, p->rmap_ops.p + n, sizeof(int32_t), cudaMemcpyDeviceToHost, s);
   if (e == cudaSuccess) e = cudaStreamSynchronize(s);
   if (e != cudaSuccess) return e;
-  size_t free_b = 0, total_b = 0;
-  if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) return cudaGetLastError();
   const size_t bytes = static_cast<size_t>(entries) * sizeof(uint16_t);
-  if (too_long || entries <= 0 || bytes > kReuseMapMaxBytes || bytes > free_b / 4)
-    return cudaSuccess;
+  if (too_long || entries <= 0 || bytes > kReuseMapMaxBytes) return cudaSuccess;
+  // the free-memory bound only matters when the map must grow (a repeated
+  // analysis of the same structure reuses its allocation without asking
+  // the driver)
+  if (static_cast<size_t>(entries) > p->rmap.cap) {
+    size_t free_b = 0, total_b = 0;
+    if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) return cudaGetLastError();
+    if (bytes > free_b / 4) return cudaSuccess;
+  }
   if (p->rmap.reserve(static_cast<size_t>(entries)) != cudaSuccess) {
     cudaGetLastError();  // out of memory: keep the hash path
     return cudaSuccess;
@@ -1856,20 +1893,20 @@ rvsp_status_t rvsp_cuda_numeric(rvsp_cuda_plan_t p, void *stream,
     PhaseScope ph(p, s, RVSP_PHASE_NUMERIC);
     if (use_map && p->pat_ready && p->n_pat_rows > 0) {
       if (p->rt.ready && p->tiles_enabled) {
-        ph.launches += launch_table_tile_kernel(p->rt, op, c_row_ptr, c_values, ln[1]);
+        ph.launches += launch_table_tile_kernel(p->rt, op, c_row_ptr, c_values, ln.next());
         ph.launches += launch_pattern_kernels(p->rt, op, c_row_ptr, c_values,
                                               p->misc.p + kStatus, ln, false);
         rt_main = true;
         if (p->rt.n_lo > 0) {
           launch_pat_numeric(op, p->ops.p, p->rt.lo_rows.p, p->rt.lo_ids.p, p->rt.n_lo,
                              c_row_ptr, c_values, p->pat_off.p, p->pat_steps.p, p->pat_rec.p,
-                             p->pat_max_ops, p->pat_max_out, ln[2]);
+                             p->pat_max_ops, p->pat_max_out, ln.next());
           ph.launches += 1;
         }
       } else {
         launch_pat_numeric(op, p->ops.p, p->pat_rows.p, p->pat_ids.p, p->n_pat_rows,
                            c_row_ptr, c_values, p->pat_off.p, p->pat_steps.p, p->pat_rec.p,
-                           p->pat_max_ops, p->pat_max_out, ln[0]);
+                           p->pat_max_ops, p->pat_max_out, ln.main());
         ph.launches += 1;
       }
     }
@@ -1902,7 +1939,7 @@ rvsp_status_t rvsp_cuda_numeric(rvsp_cuda_plan_t p, void *stream,
       }
       launch_persist_numeric(op, p->ops.p, pp, p->persist_head.p, c_row_ptr, c_values,
                              p->rmap_off.p, p->rmap.p, p->misc.p + kStatus, max_out,
-                             p->persist_blocks, p->num_sms, ln[2]);
+                             p->persist_blocks, p->num_sms, ln.next());
       ph.launches += 2;
     } else {
       cudaGetLastError();
@@ -1917,14 +1954,14 @@ rvsp_status_t rvsp_cuda_numeric(rvsp_cuda_plan_t p, void *stream,
         if (p->res_count[c] > 0)
           launch_map_numeric(c, op, p->ops.p, p->res_rows.p + p->res_off[c],
                              p->res_count[c], c_row_ptr, c_values, p->rmap_off.p,
-                             p->rmap.p, p->misc.p + kStatus, ln[2]);
+                             p->rmap.p, p->misc.p + kStatus, ln.next());
       } else if (use_map && map_class(c))
         launch_map_numeric(c, op, p->ops.p, rows, nrows, c_row_ptr, c_values,
-                           p->rmap_off.p, p->rmap.p, p->misc.p + kStatus, ln[2]);
+                           p->rmap_off.p, p->rmap.p, p->misc.p + kStatus, ln.next());
       else
         launch_numeric_class(c, op, p->ops.p, rows, nrows, c_row_ptr, c_col_idx, c_values,
                              fill != 0, dense_acc, dense_bits, p->dense_slots,
-                             p->misc.p + kStatus, p->num_sms, ln[2]);
+                             p->misc.p + kStatus, p->num_sms, ln.next());
       ph.launches += 1;
     }
     if (rt_main)
