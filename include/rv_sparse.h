@@ -214,7 +214,8 @@ rvsp_status_t rvsp_spgemm_get_tiled_rows(rvsp_spgemm_descr_t descr, int32_t *n_o
 rvsp_status_t rvsp_spgemm_set_pattern_kernels(rvsp_spgemm_descr_t descr, int32_t enable);
 
 /* Shift classes in work_estimation (see rvsp_cuda_plan_set_shift_classes):
- * 1 (default) or 0.  Results are identical either way. */
+ * 1 (default: where they pay), 2 (whenever rows are translates) or 0.
+ * Results are identical either way. */
 rvsp_status_t rvsp_spgemm_set_shift_classes(rvsp_spgemm_descr_t descr, int32_t enable);
 
 /* Rows of the last work_estimation that took their structure from a shift

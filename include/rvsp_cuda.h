@@ -234,14 +234,17 @@ rvsp_status_t rvsp_cuda_plan_set_persistent(rvsp_cuda_plan_t plan, int32_t merge
                                            int32_t blocks_per_sm);
 
 /* Pattern kernels (1, the default) or not (0).  When row tiles are built,
- * the (at most four) patterns with at least 128 tiles get a kernel written
- * for that pattern and compiled at run time with NVRTC (k_jit.cu): each lane
- * keeps its row's outputs in registers, so a product is a shared load, a
- * multiply and an add.  Values are identical to the table kernel's (same
- * order, separately rounded products and sums).  Without NVRTC in the
+ * the (at most twelve) patterns with at least 128 tiles and at most 160
+ * outputs a row get a kernel written for that pattern and compiled at run
+ * time with NVRTC (k_jit.cu): persistent warps over per-tile records, each
+ * lane keeping its row's outputs in registers, so a product is a shared
+ * load, a multiply and an add.  Values are identical to the table kernel's
+ * (same order, separately rounded products and sums).  Without NVRTC in the
  * process, or if a compile fails, the pattern stays on the table kernel.
  * Kernels are cached for the life of the process.  Changing the setting
- * rebuilds the tiles on the next numeric-only call. */
+ * rebuilds the tiles on the next numeric-only call.  A numeric-only call
+ * runs its independent row groups on six internal streams of the plan,
+ * forked from and joined back into the caller's stream. */
 rvsp_status_t rvsp_cuda_plan_set_pattern_kernels(rvsp_cuda_plan_t plan, int32_t enable);
 
 /* Rows (32 per tile, the tiles' masks not subtracted) the pattern kernels
@@ -252,18 +255,22 @@ int32_t rvsp_cuda_plan_pattern_kernel_rows(rvsp_cuda_plan_t plan);
  * compiles took (NULL outputs are skipped). */
 void rvsp_cuda_pattern_kernel_stats(int32_t *compiles, double *compile_ms);
 
-/* Shift classes in the analysis (1, the default) or not (0).  The GPU form of
+/* Shift classes in the analysis: 1 (the default) where they pay, 2 on any
+ * matrix whose rows are translates, 0 never.  The GPU form of
  * rvsp_symbolic_count + rvsp_symbolic_fill (rvsp_symbolic.c:13-137) for rows
  * that are exact translates of another row (banded and stencil matrices):
  * such a row's A nonzeros sit at the same offsets from it as the other row's,
  * over B rows whose columns sit at the same offsets from their own index
  * (checked entry by entry).  Its count, columns (moved by the row distance)
  * and term table come from the canonical row, so it skips the symbolic pass
- * and the fill (k_shift.cu).  Matrices of at least 4096 rows run a probe of
- * 2048 rows on the device, and the analysis only when at least half of them
- * have a translate among the others; the learned analysis hands such
- * matrices to it.  Values are identical either way.  Applies from the next
- * analysis. */
+ * and the fill (k_shift.cu).  With 1, matrices of at least 32768 rows run a
+ * probe of 2048 rows on the device, and the analysis only when at least half
+ * of them have a translate among the others and they average at least 64
+ * products (cheaper rows are left to the merge kernels: for them the
+ * analysis and its tile builds cost more than one product saves); with 2,
+ * any matrix of 64 rows or more whose sampled rows have translates.  The
+ * learned analysis hands such matrices to it.  Values are identical either
+ * way.  Applies from the next analysis. */
 rvsp_status_t rvsp_cuda_plan_set_shift_classes(rvsp_cuda_plan_t plan, int32_t enable);
 
 /* Rows of the last analysis that took their structure from a shift class (0

@@ -110,11 +110,18 @@ shift_probe_kernel(Operands op, int32_t samples, unsigned long long *__restrict_
   const int32_t i = static_cast<int32_t>((static_cast<int64_t>(w) * op.a_rows) / samples);
   const int32_t p0 = op.a_rp[i], na = op.a_rp[i + 1] - p0;
   if (na <= 0 || na > kShiftMaxA) {
-    if (lane == 0) keys[w] = 0;
+    // a row of more A nonzeros than a pattern takes counts as a costly row
+    if (lane == 0) {
+      keys[w] = 0;
+      keys[samples + w] = na > 0 ? kShiftMaxOps : 0;
+    }
     return;
   }
-  int32_t k = 0;
-  if (lane < na) k = __ldg(op.a_col + p0 + lane);
+  int32_t k = 0, len = 0;
+  if (lane < na) {
+    k = __ldg(op.a_col + p0 + lane);
+    len = __ldg(op.b_rp + k + 1) - __ldg(op.b_rp + k);
+  }
   unsigned long long mine = 0;
   for (int32_t j = 0; j < na; ++j) {
     const int32_t kj = __shfl_sync(kFull, k, j);
@@ -122,23 +129,39 @@ shift_probe_kernel(Operands op, int32_t samples, unsigned long long *__restrict_
     if (lane == j) mine = bk;
   }
   const unsigned long long key = row_key(na, lane, k - i, mine);
-  if (lane == 0) keys[w] = key;
+  const int32_t ops = warp_sum(len);
+  if (lane == 0) {
+    keys[w] = key;
+    keys[samples + w] = static_cast<unsigned long long>(ops);
+  }
 }
 
 // The decision: sorts the probe's keys (one block) and sets *on when at
-// least half of the sampled rows share their key with another sampled row.
-// *on stays 0 when the structure check failed.
+// least half of the sampled rows share their key with another sampled row
+// and the sampled rows average at least min_mean_ops products (the caller's
+// bar: rows of few products are cheap on the merge kernels, and the
+// analysis and the tile builds would cost more than they save in a single
+// product).  *on stays 0 when the structure check failed.
 __global__ void __launch_bounds__(1024)
 shift_decide_kernel(const unsigned long long *__restrict__ keys, int32_t samples,
-                    int32_t *__restrict__ on, CheckGuard guard) {
+                    int32_t min_mean_ops, int32_t *__restrict__ on, CheckGuard guard) {
   __shared__ unsigned long long sk[kShiftSamples];
   __shared__ int32_t dup;
+  __shared__ unsigned long long total_ops;
   const int tid = threadIdx.x;
   if (tid == 0) {
     *on = 0;
     dup = 0;
+    total_ops = 0;
   }
   if (guard.failed()) return;
+  {
+    unsigned long long o = 0;
+    for (int t = tid; t < samples; t += blockDim.x) o += keys[samples + t];
+    for (int d = 16; d; d >>= 1) o += __shfl_xor_sync(kFull, o, d);
+    __syncthreads();
+    if (lane_id() == 0 && o) atomicAdd(&total_ops, o);
+  }
   for (int t = tid; t < kShiftSamples; t += blockDim.x)
     sk[t] = t < samples ? keys[t] : ~0ull;
   __syncthreads();
@@ -153,7 +176,12 @@ shift_decide_kernel(const unsigned long long *__restrict__ keys, int32_t samples
   mine = warp_sum(mine);
   if (lane_id() == 0 && mine) atomicAdd(&dup, mine);
   __syncthreads();
-  if (tid == 0) *on = 2 * dup >= samples ? 1 : 0;
+  if (tid == 0)
+    *on = (2 * dup >= samples &&
+           total_ops >= static_cast<unsigned long long>(min_mean_ops) *
+                            static_cast<unsigned long long>(samples))
+              ? 1
+              : 0;
 }
 
 // Gated fills.
@@ -692,11 +720,11 @@ unsigned grid_fill(size_t n) {
 int32_t shift_max_ops() { return kShiftMaxOps; }
 int32_t shift_samples() { return kShiftSamples; }
 
-void launch_shift_decide(const Operands &op, unsigned long long *keys, int32_t *on,
-                         CheckGuard guard, cudaStream_t s) {
+void launch_shift_decide(const Operands &op, unsigned long long *keys, int32_t min_mean_ops,
+                         int32_t *on, CheckGuard guard, cudaStream_t s) {
   const int32_t samples = op.a_rows < kShiftSamples ? op.a_rows : kShiftSamples;
   shift_probe_kernel<<<grid_warps(samples), kThreads, 0, s>>>(op, samples, keys, guard);
-  shift_decide_kernel<<<1, 1024, 0, s>>>(keys, samples, on, guard);
+  shift_decide_kernel<<<1, 1024, 0, s>>>(keys, samples, min_mean_ops, on, guard);
 }
 
 void launch_shift_classes(const int32_t *on, const Operands &op, int32_t b_rows,

@@ -430,10 +430,11 @@ cudaError_t launch_pattern_kernel(void *kernel, const Operands &op, const int32_
 // without a host round trip.
 int32_t shift_max_ops();
 int32_t shift_samples();
-// Keys of up to shift_samples() rows spread over A (keys: that many words)
-// and the decision *on (1: at least half of them share their key).
-void launch_shift_decide(const Operands &op, unsigned long long *keys, int32_t *on,
-                         CheckGuard guard, cudaStream_t s);
+// Keys and product counts of up to shift_samples() rows spread over A (keys:
+// twice that many words) and the decision *on (1: at least half of them
+// share their key and they average at least min_mean_ops products).
+void launch_shift_decide(const Operands &op, unsigned long long *keys, int32_t min_mean_ops,
+                         int32_t *on, CheckGuard guard, cudaStream_t s);
 // bcls[b_rows], rcls[a_rows]: the class (smallest verified translate) of
 // every B row and row; bkey / rkey / tkey / trow scratch, tcap a power of two
 // >= 2 max(a_rows, b_rows).

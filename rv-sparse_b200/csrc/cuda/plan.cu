@@ -49,6 +49,29 @@ struct DevArray {
   }
 };
 
+// Page-locked host memory, grown on demand and kept: the tile builds'
+// transfers go through it (a copy from or to pageable memory is staged and
+// synchronous, tens of microseconds each).
+struct HostArray {
+  char *p = nullptr;
+  size_t cap = 0;
+  cudaError_t reserve(size_t n) {
+    if (n <= cap && p) return cudaSuccess;
+    release();
+    if (cudaMallocHost(reinterpret_cast<void **>(&p), n ? n : 1) != cudaSuccess) {
+      p = nullptr;
+      return cudaErrorMemoryAllocation;
+    }
+    cap = n;
+    return cudaSuccess;
+  }
+  void release() {
+    if (p) cudaFreeHost(p);
+    p = nullptr;
+    cap = 0;
+  }
+};
+
 rvsp_status_t map_cuda(cudaError_t e) {
   switch (e) {
     case cudaSuccess: return RVSP_SUCCESS;
@@ -106,6 +129,7 @@ struct TileBuild {
   std::vector<JitPattern> pool;  // device arrays of earlier builds, for reuse
   DevArray<int32_t> jwords;      // per chosen pattern: spans, record extent
   DevArray<int2> jgroups;        // per chosen pattern: its staging groups
+  HostArray staging;             // host side of the builds' transfers
   int ready = 0;
   int32_t n_tiles = 0, n_lo = 0, stage = 0, aseg = 0, max_out = 0, b_nnz = 0;
   DevArray<uint16_t> tab, lens;
@@ -132,6 +156,7 @@ struct TileBuild {
     pool.clear();
     jwords.release();
     jgroups.release();
+    staging.release();
     ready = 0;
   }
 };
@@ -567,7 +592,15 @@ void rvsp_cuda_plan_destroy(rvsp_cuda_plan_t p) {
 namespace {
 
 // Matrices of at least this many rows run the shift-class probe.
-constexpr int32_t kShiftMinRows = 4096;
+// The shift analysis runs by default (setting 1) on matrices of at least
+// kShiftMinRows rows whose sampled rows average kShiftMinMeanOps products;
+// setting 2 runs it on any matrix whose rows are translates.
+constexpr int32_t kShiftMinRows = 32768;
+constexpr int32_t kShiftMinMeanOps = 64;
+int32_t shift_bar(const rvsp_cuda_plan *p) { return p->shift_enabled == 2 ? 0 : kShiftMinMeanOps; }
+bool shift_size_ok(const rvsp_cuda_plan *p, int32_t a_rows) {
+  return p->shift_enabled == 2 ? a_rows >= 64 : a_rows >= kShiftMinRows;
+}
 
 // Scratch of the shift-class analysis (k_shift.cu).  The key table is a
 // power of two of at least twice the rows; a larger one kept from before is
@@ -579,7 +612,7 @@ cudaError_t reserve_shift(rvsp_cuda_plan *p, int32_t a_rows, int32_t b_rows) {
   p->shift_cap_pat = static_cast<int32_t>(n / kPatMinShare + 1);
   const size_t cp = static_cast<size_t>(p->shift_cap_pat);
   cudaError_t e = p->sh_on.reserve(1);
-  if (e == cudaSuccess) e = p->sh_probe.reserve(size_t(shift_samples()));
+  if (e == cudaSuccess) e = p->sh_probe.reserve(2 * size_t(shift_samples()));
   if (e == cudaSuccess) e = p->sh_bkey.reserve(nb);
   if (e == cudaSuccess) e = p->sh_rkey.reserve(n);
   if (e == cudaSuccess) e = p->sh_tkey.reserve(tcap);
@@ -711,7 +744,7 @@ rvsp_status_t symbolic_impl(rvsp_cuda_plan_t p, cudaStream_t s, int32_t a_rows,
   p->shift_tables = 0;
   p->shift_members = 0;
   p->shift_npat = 0;
-  const bool shift = p->shift_enabled && a_rows >= kShiftMinRows &&
+  const bool shift = p->shift_enabled && shift_size_ok(p, a_rows) &&
                      reserve_shift(p, a_rows, b_rows) == cudaSuccess;
   if (!shift) cudaGetLastError();
   {
@@ -725,7 +758,7 @@ rvsp_status_t symbolic_impl(rvsp_cuda_plan_t p, cudaStream_t s, int32_t a_rows,
       // Shift classes: the probe decides on the device; every pass after it
       // is gated by that decision, so no host round trip is added.  Member
       // rows leave the symbolic classes (census recounted).
-      launch_shift_decide(op, p->sh_probe.p, p->sh_on.p, guard, s);
+      launch_shift_decide(op, p->sh_probe.p, shift_bar(p), p->sh_on.p, guard, s);
       launch_shift_classes(p->sh_on.p, op, b_rows, p->ops.p, p->sh_bkey.p, p->sh_rkey.p,
                            p->sh_tkey.p, p->sh_trow.p, p->sh_tkey.cap, p->sh_bcls.p,
                            p->sh_rcls.p, s);
@@ -911,14 +944,14 @@ rvsp_status_t rvsp_cuda_learned_symbolic(
   p->shift_active = 0;
   p->shift_tables = 0;
   p->shift_members = 0;
-  if (p->shift_enabled && a_rows >= kShiftMinRows) {
+  if (p->shift_enabled && shift_size_ok(p, a_rows)) {
     // Rows that are translates of a few canonical rows need no prediction:
     // their structure comes from the canonical rows.  When the probe finds
     // them common, the analysis is the shift-class one (symbolic_impl).
     if (reserve_shift(p, a_rows, b_rows) == cudaSuccess) {
       const Operands pop{a_rows, b_cols, a_row_ptr, a_col_idx, nullptr,
                          b_row_ptr, b_col_idx, nullptr, false};
-      launch_shift_decide(pop, p->sh_probe.p, p->sh_on.p, CheckGuard(), s);
+      launch_shift_decide(pop, p->sh_probe.p, shift_bar(p), p->sh_on.p, CheckGuard(), s);
       cudaError_t e = cudaMemcpyAsync(p->h_misc, p->sh_on.p, sizeof(int32_t),
                                       cudaMemcpyDeviceToHost, s);
       if (e == cudaSuccess) e = cudaStreamSynchronize(s);
@@ -1172,7 +1205,7 @@ void rvsp_cuda_pattern_kernel_stats(int32_t *compiles, double *compile_ms) {
 
 rvsp_status_t rvsp_cuda_plan_set_shift_classes(rvsp_cuda_plan_t p, int32_t enable) {
   if (!p) return RVSP_ERROR_NULL_POINTER;
-  if (enable != 0 && enable != 1) return RVSP_ERROR_INVALID_ARGUMENT;
+  if (enable < 0 || enable > 2) return RVSP_ERROR_INVALID_ARGUMENT;
   p->shift_enabled = enable;
   return RVSP_SUCCESS;
 }
@@ -1217,76 +1250,95 @@ constexpr int32_t kJitMaxSpan = 4096;
 
 // Compiled kernels for the patterns that cover the most tiles.  The tile
 // list is read back once to count each pattern's tiles and list them in row
-// order; then, for all the chosen patterns at once, the union spans of
-// runs of their A nonzeros measured (one round trip with their tables), the
-// staging groups chosen and the kernels compiled side by side (k_jit.cu),
-// their tile records built (one round trip for the records' A extents), and
+// order; then, for all the chosen patterns at once, the union spans of runs
+// of their A nonzeros are measured on a sample of their tiles (one round
+// trip with their tables), the staging groups chosen and the kernels
+// compiled side by side (k_jit.cu), their tile records built (one round
+// trip for the records' A extents and every group's largest B range), and
 // their tiles marked so the table kernel skips them (one round trip for the
 // table kernel's own list).  A pattern whose compile fails stays on the
-// table kernel.  The device arrays of earlier builds are kept and reused.
-// Synchronizes `s`.
+// table kernel.  The device arrays of earlier builds are kept and reused;
+// every transfer goes through page-locked staging.  Synchronizes `s`.
 cudaError_t build_pattern_kernels(rvsp_cuda_plan *p, cudaStream_t s, const Operands &op,
                                   int32_t npat, TileBuild &tb) {
   for (auto &j : tb.jit) tb.pool.push_back(j);
   tb.jit.clear();
-  std::vector<int4> tiles(static_cast<size_t>(tb.n_tiles));
-  cudaError_t e = cudaMemcpyAsync(tiles.data(), tb.tiles.p, tiles.size() * sizeof(int4),
-                                  cudaMemcpyDeviceToHost, s);
+  // per chosen pattern: spans (32 x kJitMaxGroup words), its records' A
+  // extent and groups' B ranges
+  constexpr size_t W = size_t(32 * kJitMaxGroup) + 2;
+  const size_t KM = size_t(kJitMaxPatterns);
+  const int32_t stride = tile_tab_stride();
+  const size_t nt = static_cast<size_t>(tb.n_tiles), np = static_cast<size_t>(npat);
+  // the staging layout: tiles read back, desc, lens, tables, sorted tile
+  // lists, words, groups (16-byte aligned pieces)
+  auto up16 = [](size_t x) { return (x + 15) & ~size_t(15); };
+  const size_t o_tiles = 0, o_desc = o_tiles + up16(nt * sizeof(int4));
+  const size_t o_lens = o_desc + up16(np * sizeof(int4));
+  const size_t o_tabs = o_lens + up16(np * 32 * sizeof(uint16_t));
+  const size_t o_lists = o_tabs + up16(KM * size_t(stride) * sizeof(uint16_t));
+  const size_t o_words = o_lists + up16(nt * sizeof(int4));
+  const size_t o_groups = o_words + up16(KM * W * sizeof(int32_t));
+  const size_t total = o_groups + up16(KM * 32 * sizeof(int2));
+  if (tb.staging.reserve(total) != cudaSuccess) {
+    cudaGetLastError();
+    return cudaSuccess;
+  }
+  int4 *const tiles = reinterpret_cast<int4 *>(tb.staging.p + o_tiles);
+  int4 *const desc = reinterpret_cast<int4 *>(tb.staging.p + o_desc);
+  uint16_t *const lens = reinterpret_cast<uint16_t *>(tb.staging.p + o_lens);
+  uint16_t *const tabs = reinterpret_cast<uint16_t *>(tb.staging.p + o_tabs);
+  int4 *const lists = reinterpret_cast<int4 *>(tb.staging.p + o_lists);
+  int32_t *const words = reinterpret_cast<int32_t *>(tb.staging.p + o_words);
+  int2 *const gh = reinterpret_cast<int2 *>(tb.staging.p + o_groups);
+  cudaError_t e = cudaMemcpyAsync(tiles, tb.tiles.p, nt * sizeof(int4), cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(desc, tb.desc.p, np * sizeof(int4), cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(lens, tb.lens.p, np * 32 * sizeof(uint16_t), cudaMemcpyDeviceToHost, s);
   if (e == cudaSuccess) e = cudaStreamSynchronize(s);
   if (e != cudaSuccess) return e;
-  std::vector<int32_t> count(static_cast<size_t>(npat), 0);
-  for (const int4 &t : tiles)
-    if (t.z >= 0 && t.z < npat) ++count[size_t(t.z)];
+  std::vector<int32_t> count(np, 0);
+  for (size_t i = 0; i < nt; ++i)
+    if (tiles[i].z >= 0 && tiles[i].z < npat) ++count[size_t(tiles[i].z)];
   std::vector<int32_t> order;
   for (int32_t id = 0; id < npat; ++id)
     if (count[size_t(id)] >= kJitMinTiles) order.push_back(id);
   std::sort(order.begin(), order.end(),
             [&](int32_t a, int32_t b) { return count[size_t(a)] > count[size_t(b)]; });
-  if (order.size() > size_t(kJitMaxPatterns)) order.resize(size_t(kJitMaxPatterns));
+  if (order.size() > KM) order.resize(KM);
   if (order.empty()) return cudaSuccess;
   const size_t K = order.size();
-  // per chosen pattern: spans (32 x kJitMaxGroup words), its records' A
-  // extent
-  constexpr size_t W = size_t(32 * kJitMaxGroup) + 2;
   if (tb.jwords.reserve(K * W) != cudaSuccess || tb.jgroups.reserve(K * 32) != cudaSuccess) {
     cudaGetLastError();
     return cudaSuccess;
   }
-  const int32_t stride = tile_tab_stride();
-  std::vector<int4> desc(static_cast<size_t>(npat));
-  std::vector<uint16_t> lens(size_t(npat) * 32);
-  std::vector<uint16_t> tabs(K * size_t(stride));
-  std::vector<int32_t> words(K * W, 0);
   std::vector<JitPattern> cand(K);
   auto give_back = [&tb](JitPattern &jp) { tb.pool.push_back(jp); jp = JitPattern(); };
   // each chosen pattern's tiles in order of their first row (one tile per
   // chunk of 32 rows: a counting pass over the chunks), so that the
   // persistent warps, which take tiles in list order, work on neighbouring
   // rows at any one time and their B ranges stay in L2 between tiles
-  std::vector<int32_t> kof(static_cast<size_t>(npat), -1);
+  std::vector<int32_t> kof(np, -1);
   for (size_t k = 0; k < K; ++k) kof[size_t(order[k])] = static_cast<int32_t>(k);
-  std::vector<std::vector<int4>> lists(K);
+  std::vector<size_t> lbeg(K + 1, 0), lfill(K, 0);
+  for (size_t k = 0; k < K; ++k) lbeg[k + 1] = lbeg[k] + size_t(count[size_t(order[k])]);
   {
     const int64_t nchunks = (int64_t(p->a_rows) + 31) / 32;
     std::vector<int32_t> at(static_cast<size_t>(nchunks), -1);
-    for (size_t i = 0; i < tiles.size(); ++i) {
+    for (size_t i = 0; i < nt; ++i) {
       const int64_t c = int64_t(tiles[i].x) / 32;
       if (c >= 0 && c < nchunks) at[size_t(c)] = static_cast<int32_t>(i);
     }
-    for (size_t k = 0; k < K; ++k) lists[k].reserve(size_t(count[size_t(order[k])]));
     for (const int32_t i : at) {
       if (i < 0) continue;
       const int4 &t = tiles[size_t(i)];
-      if (t.z >= 0 && t.z < npat && kof[size_t(t.z)] >= 0) lists[size_t(kof[size_t(t.z)])].push_back(t);
+      if (t.z < 0 || t.z >= npat || kof[size_t(t.z)] < 0) continue;
+      const size_t k = size_t(kof[size_t(t.z)]);
+      lists[lbeg[k] + lfill[k]++] = t;
     }
   }
-  e = cudaMemcpyAsync(desc.data(), tb.desc.p, desc.size() * sizeof(int4), cudaMemcpyDeviceToHost,
-                      s);
-  if (e == cudaSuccess)
-    e = cudaMemcpyAsync(lens.data(), tb.lens.p, lens.size() * sizeof(uint16_t),
-                        cudaMemcpyDeviceToHost, s);
   for (size_t k = 0; k < K && e == cudaSuccess; ++k)
-    e = cudaMemcpyAsync(tabs.data() + k * stride, tb.tab.p + size_t(order[k]) * stride,
+    e = cudaMemcpyAsync(tabs + k * size_t(stride), tb.tab.p + size_t(order[k]) * stride,
                         size_t(stride) * sizeof(uint16_t), cudaMemcpyDeviceToHost, s);
   if (e == cudaSuccess) e = cudaMemsetAsync(tb.jwords.p, 0, K * W * sizeof(int32_t), s);
   for (size_t k = 0; k < K && e == cudaSuccess; ++k) {
@@ -1296,7 +1348,7 @@ cudaError_t build_pattern_kernels(rvsp_cuda_plan *p, cudaStream_t s, const Opera
     // capacity holds this pattern's tiles, else the largest (so that a
     // repeated analysis of the same structure allocates nothing)
     if (!tb.pool.empty()) {
-      const size_t need = lists[k].size();
+      const size_t need = lfill[k];
       size_t best = 0;
       for (size_t q = 1; q < tb.pool.size(); ++q) {
         const size_t c = tb.pool[q].tiles.cap, bc = tb.pool[best].tiles.cap;
@@ -1306,22 +1358,20 @@ cudaError_t build_pattern_kernels(rvsp_cuda_plan *p, cudaStream_t s, const Opera
       jp = tb.pool[best];
       tb.pool.erase(tb.pool.begin() + static_cast<std::ptrdiff_t>(best));
     }
-    jp.n = static_cast<int32_t>(lists[k].size());
+    jp.n = static_cast<int32_t>(lfill[k]);
     if (jp.n <= 0 || jp.tiles.reserve(size_t(jp.n)) != cudaSuccess) {
       cudaGetLastError();
       give_back(jp);
       continue;
     }
-    int32_t *const wk = tb.jwords.p + k * W;
-    e = cudaMemcpyAsync(jp.tiles.p, lists[k].data(), lists[k].size() * sizeof(int4),
+    e = cudaMemcpyAsync(jp.tiles.p, lists + lbeg[k], lfill[k] * sizeof(int4),
                         cudaMemcpyHostToDevice, s);
     if (e != cudaSuccess) break;
     launch_jit_spans(jp.tiles.p, jp.n, tb.desc.p + id, tb.lens.p + size_t(id) * 32, op.a_rp,
-                     op.a_col, op.b_rp, wk, p->num_sms, s);
+                     op.a_col, op.b_rp, tb.jwords.p + k * W, p->num_sms, s);
   }
   if (e == cudaSuccess)
-    e = cudaMemcpyAsync(words.data(), tb.jwords.p, K * W * sizeof(int32_t),
-                        cudaMemcpyDeviceToHost, s);
+    e = cudaMemcpyAsync(words, tb.jwords.p, K * W * sizeof(int32_t), cudaMemcpyDeviceToHost, s);
   if (e == cudaSuccess) e = cudaStreamSynchronize(s);
   if (e != cudaSuccess) {
     for (auto &c : cand) give_back(c);
@@ -1339,7 +1389,7 @@ cudaError_t build_pattern_kernels(rvsp_cuda_plan *p, cudaStream_t s, const Opera
     JitRequest &rq = reqs[k];
     rq.na = d.x;
     rq.m = d.y;
-    const uint16_t *tab = tabs.data() + k * stride;
+    const uint16_t *tab = tabs + k * size_t(stride);
     int32_t off = 0;
     for (int j = 0; j < d.x; ++j) {
       rq.len[j] = lens[size_t(order[k]) * 32 + j];
@@ -1347,20 +1397,18 @@ cudaError_t build_pattern_kernels(rvsp_cuda_plan *p, cudaStream_t s, const Opera
       off += (rq.len[j] + 7) & ~7;
     }
     int32_t need = 0;
-    rq.groups = jit_groups(d.x, rq.len, words.data() + k * W, kJitMaxSpan, &need);
+    rq.groups = jit_groups(d.x, rq.len, words + k * W, kJitMaxSpan, &need);
     if (rq.groups.empty() || need <= 0 || need > kJitMaxSpan) {
       rq = JitRequest();
       give_back(jp);
       continue;
     }
     jp.m = d.y;
-    jp.stage_cap = need;  // the largest B range; the layout follows the records
   }
   jit_pattern_kernels(reqs);
   // tile records of the compiled patterns (their maxima: the records' A
   // extent, then each group's largest B range over every tile)
   cudaMemsetAsync(tb.jwords.p, 0, K * W * sizeof(int32_t), s);
-  std::vector<int2> gh(K * 32);
   std::vector<int32_t> rws(K, 0);
   for (size_t k = 0; k < K; ++k) {
     JitPattern &jp = cand[k];
@@ -1379,14 +1427,13 @@ cudaError_t build_pattern_kernels(rvsp_cuda_plan *p, cudaStream_t s, const Opera
     }
     for (size_t g = 0; g < rq.groups.size(); ++g)
       gh[k * 32 + g] = make_int2(rq.groups[g].first, rq.groups[g].second);
-    cudaMemcpyAsync(tb.jgroups.p + k * 32, gh.data() + k * 32, rq.groups.size() * sizeof(int2),
+    cudaMemcpyAsync(tb.jgroups.p + k * 32, gh + k * 32, rq.groups.size() * sizeof(int2),
                     cudaMemcpyHostToDevice, s);
     launch_jit_programs(jp.tiles.p, jp.n, rq.na, rq.groups, tb.jgroups.p + k * 32,
                         tb.lens.p + size_t(order[k]) * 32, op.a_rp, op.a_col, op.b_rp,
                         jp.prog.p, jp.arange.p, tb.jwords.p + k * W, p->num_sms, s);
   }
-  e = cudaMemcpyAsync(words.data(), tb.jwords.p, K * W * sizeof(int32_t),
-                      cudaMemcpyDeviceToHost, s);
+  e = cudaMemcpyAsync(words, tb.jwords.p, K * W * sizeof(int32_t), cudaMemcpyDeviceToHost, s);
   if (e == cudaSuccess) e = cudaStreamSynchronize(s);
   if (e != cudaSuccess) {
     for (auto &c : cand) if (c.tiles.p) give_back(c);
@@ -1422,11 +1469,10 @@ cudaError_t build_pattern_kernels(rvsp_cuda_plan *p, cudaStream_t s, const Opera
   if (!tb.jit.empty() && tb.table.reserve(size_t(tb.n_tiles)) == cudaSuccess) {
     cudaMemsetAsync(tb.counts.p + 6, 0, sizeof(int32_t), s);
     launch_table_tiles(tb.tiles.p, tb.n_tiles, tb.desc.p, tb.table.p, tb.counts.p + 6, s);
-    int32_t n = 0;
-    e = cudaMemcpyAsync(&n, tb.counts.p + 6, sizeof(int32_t), cudaMemcpyDeviceToHost, s);
+    e = cudaMemcpyAsync(words, tb.counts.p + 6, sizeof(int32_t), cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) return e;
-    tb.n_table = n;
+    tb.n_table = words[0];
   } else {
     cudaGetLastError();
   }

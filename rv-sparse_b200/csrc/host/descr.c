@@ -123,7 +123,7 @@ rvsp_status_t rvsp_spgemm_set_shift_classes(rvsp_spgemm_descr_t d, int32_t enabl
 {
     if (d == NULL)
         return RVSP_ERROR_NULL_POINTER;
-    if (enable != 0 && enable != 1)
+    if (enable < 0 || enable > 2)
         return RVSP_ERROR_INVALID_ARGUMENT;
     d->shift_classes = enable;
     return d->plan ? rvsp_cuda_plan_set_shift_classes(d->plan, enable) : RVSP_SUCCESS;

@@ -304,10 +304,12 @@ class Descriptor:
         L.check(self.lib.rvsp_spgemm_set_pattern_kernels(self.h, int(bool(enable))),
                 "set_pattern_kernels")
 
-    def set_shift_classes(self, enable: bool):
-        """Shift classes in work_estimation (on by default)."""
-        L.check(self.lib.rvsp_spgemm_set_shift_classes(self.h, int(bool(enable))),
-                "set_shift_classes")
+    def set_shift_classes(self, enable):
+        """Shift classes in work_estimation: False/0 off, True/1 where they pay
+        (the default: large matrices of costly rows), 2 on any matrix whose
+        rows are translates."""
+        mode = 2 if enable == 2 else int(bool(enable))
+        L.check(self.lib.rvsp_spgemm_set_shift_classes(self.h, mode), "set_shift_classes")
 
     def shift_rows(self) -> int:
         n = C.c_int32()

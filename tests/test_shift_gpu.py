@@ -48,7 +48,9 @@ def _check(A, B, algo=L.ALGO_CUDA_PLAIN, shift=True, repeats=2, min_shift=1, mod
     with Descriptor(algo=algo, memory=memory) as d:
         if model is not None:
             d.set_model(model)
-        d.set_shift_classes(shift)
+        # 2: the analysis runs on these small matrices too (by default it
+        # waits for 32768 rows averaging 64 products)
+        d.set_shift_classes(2 if shift else 0)
         if memory == L.MEM_DEVICE:
             dA = DeviceCSR.from_host(A)
             dB = dA if B is A else DeviceCSR.from_host(B)
@@ -156,6 +158,7 @@ def test_tiles_off_uses_the_table_kernel_for_members():
     rp, ci, cv, _ = oracle.spgemm(A, A)
     dA = DeviceCSR.from_host(A)
     with Descriptor(memory=L.MEM_DEVICE) as d:
+        d.set_shift_classes(2)
         d.set_row_tiles(False)
         ws_b, n = d.work_estimation(dA, dA)
         dC = DeviceCSR.empty(A.rows, A.cols, n)
@@ -179,6 +182,7 @@ def test_c_abi_numeric_with_caller_structure():
     dA = DeviceCSR.from_host(A)
     plan = C.c_void_p()
     L.check(lib.rvsp_cuda_plan_create(C.byref(plan)), "plan_create")
+    L.check(lib.rvsp_cuda_plan_set_shift_classes(plan, 2), "set_shift_classes")
     try:
         stream = C.c_void_p(torch.cuda.current_stream().cuda_stream or 1)
         crp = torch.zeros(A.rows + 1, dtype=torch.int32, device="cuda")
@@ -203,3 +207,18 @@ def test_c_abi_numeric_with_caller_structure():
         assert np.array_equal(_bits(cvv.cpu().numpy()), _bits(cv))
     finally:
         lib.rvsp_cuda_plan_destroy(plan)
+
+
+def test_default_setting_leaves_cheap_rows_to_the_merge_kernels():
+    # a 2D 5-point Laplacian on 300^2 (90,000 rows of 25 products): its rows
+    # are translates, but at 25 products a row the default setting keeps the
+    # merge kernels (setting 2 takes the classes); both exact
+    A = gen.laplacian_2d(300)
+    rp, ci, cv, _ = oracle.spgemm(A, A)
+    for mode, expect in ((1, False), (2, True)):
+        with Descriptor(memory=L.MEM_HOST) as d:
+            d.set_shift_classes(mode)
+            got = d.multiply(A, A)
+            assert (d.shift_rows() > 0) == expect, (mode, d.shift_rows())
+        assert np.array_equal(got.col_idx, ci)
+        assert np.array_equal(_bits(got.values), _bits(cv))
