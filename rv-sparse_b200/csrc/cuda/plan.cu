@@ -744,8 +744,8 @@ rvsp_status_t symbolic_impl(rvsp_cuda_plan_t p, cudaStream_t s, int32_t a_rows,
   p->shift_tables = 0;
   p->shift_members = 0;
   p->shift_npat = 0;
-  const bool shift = p->shift_enabled && shift_size_ok(p, a_rows) &&
-                     reserve_shift(p, a_rows, b_rows) == cudaSuccess;
+  bool shift = p->shift_enabled && shift_size_ok(p, a_rows) &&
+               reserve_shift(p, a_rows, b_rows) == cudaSuccess;
   if (!shift) cudaGetLastError();
   {
     PhaseScope ph(p, s, RVSP_PHASE_ROWSTATS);
@@ -755,10 +755,19 @@ rvsp_status_t symbolic_impl(rvsp_cuda_plan_t p, cudaStream_t s, int32_t a_rows,
                          p->counts.p, misc + kSymCount, p->num_sms, s);
     ph.launches = 2;
     if (shift) {
-      // Shift classes: the probe decides on the device; every pass after it
-      // is gated by that decision, so no host round trip is added.  Member
-      // rows leave the symbolic classes (census recounted).
+      // Shift classes: the probe decides on the device and one small read
+      // brings the decision to the host, so a matrix without them queues
+      // none of the analysis's passes (each a full grid that would only
+      // read the flag and return).  Member rows leave the symbolic classes
+      // (census recounted).
       launch_shift_decide(op, p->sh_probe.p, shift_bar(p), p->sh_on.p, guard, s);
+      e = cudaMemcpyAsync(p->h_misc, p->sh_on.p, sizeof(int32_t), cudaMemcpyDeviceToHost, s);
+      if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+      if (e != cudaSuccess) return map_cuda(e);
+      shift = p->h_misc[0] != 0;
+      ph.launches += 2;
+    }
+    if (shift) {
       launch_shift_classes(p->sh_on.p, op, b_rows, p->ops.p, p->sh_bkey.p, p->sh_rkey.p,
                            p->sh_tkey.p, p->sh_trow.p, p->sh_tkey.cap, p->sh_bcls.p,
                            p->sh_rcls.p, s);
@@ -766,7 +775,7 @@ rvsp_status_t symbolic_impl(rvsp_cuda_plan_t p, cudaStream_t s, int32_t a_rows,
                             p->ops.p, p->sh_pat_of.p, p->sh_pat_canon.p, p->sh_pat_cap.p,
                             p->sh_pat_m.p, misc + kShiftNpat, p->shift_cap_pat, p->st.pid.p,
                             p->cls.p, misc + kShiftMembers, misc + kSymCount, p->num_sms, s);
-      ph.launches += 20;
+      ph.launches += 18;
     }
   }
   const int32_t *skip = shift ? p->st.pid.p : nullptr;
