@@ -43,6 +43,65 @@ constexpr int merge_class_of() {
   return K == 4 ? kM4 : K == 8 ? kM8 : kM16;
 }
 
+// The narrower list count a class's kernel switches to when all of a warp's
+// rows fit it (unused list slots still cost a compare and a select a step).
+template <int K>
+struct NarrowK {
+  static constexpr int value = K == 8 ? 6 : K == 16 ? 12 : K;
+};
+
+// The number of distinct columns of one row (the merge without values).
+template <int K>
+__device__ __forceinline__ int32_t count_row(const Operands &op, int32_t p0, int32_t k) {
+  Lists<K> L;
+  open_lists<K, false>(op, p0, k, L);
+  int32_t n = 0;
+  for (;;) {
+    const int32_t mn = min_head<K>(L);
+    if (mn == INT_MAX) break;
+#pragma unroll
+    for (int j = 0; j < K; ++j)
+      if (L.cur[j] == mn) advance<K, false>(op, L, j);
+    ++n;
+  }
+  return n;
+}
+
+// One row's merge with values, its outputs to shared memory (staged) or to
+// C; returns the outputs made.
+template <int K>
+__device__ __forceinline__ int32_t fill_row(const Operands &op, int32_t p0, int32_t k,
+                                            int32_t m, bool staged, int32_t *sc, float *sv,
+                                            int32_t base, int32_t *c_col, float *c_val,
+                                            int64_t out0, bool fill) {
+  Lists<K> L;
+  open_lists<K, true>(op, p0, k, L);
+  int32_t n = 0;
+  for (;;) {
+    const int32_t mn = min_head<K>(L);
+    if (mn == INT_MAX) break;
+    float acc = 0.0f;
+#pragma unroll
+    for (int j = 0; j < K; ++j) {
+      if (L.cur[j] == mn) {
+        acc = __fadd_rn(acc, __fmul_rn(L.a[j], L.curv[j]));
+        advance<K, true>(op, L, j);
+      }
+    }
+    if (n < m) {
+      if (staged) {
+        sc[base + n] = mn;
+        sv[base + n] = acc;
+      } else {
+        if (fill) c_col[out0 + n] = mn;
+        c_val[out0 + n] = acc;
+      }
+    }
+    ++n;
+  }
+  return n;
+}
+
 // Rows: rows[0..nrows) (rows == nullptr: rows 0..nrows).  With sel, rows
 // whose sel entry is not this kernel's class are skipped.
 template <int K>
@@ -57,18 +116,12 @@ merge_symbolic_kernel(Operands op, const int32_t *__restrict__ rows,
   if (guard.failed()) return;
   const int32_t p0 = op.a_rp[row];
   const int32_t k = op.a_rp[row + 1] - p0;
-  Lists<K> L;
-  open_lists<K, false>(op, p0, k, L);
-  int32_t n = 0;
-  for (;;) {
-    const int32_t mn = min_head<K>(L);
-    if (mn == INT_MAX) break;
-#pragma unroll
-    for (int j = 0; j < K; ++j)
-      if (L.cur[j] == mn) advance<K, false>(op, L, j);
-    ++n;
-  }
-  counts[row] = n;
+  // a warp whose rows all fit fewer lists runs the narrower merge
+  constexpr int KN = NarrowK<K>::value;
+  if (KN < K && __all_sync(__activemask(), k <= KN))
+    counts[row] = count_row<KN>(op, p0, k);
+  else
+    counts[row] = count_row<K>(op, p0, k);
 }
 
 // kFused: the row goes to its slab slot (fo.off[row], capacity fo.cap[row] =
@@ -143,34 +196,20 @@ merge_numeric_fill_kernel(Operands op, const int32_t *__restrict__ rows, int32_t
   const int32_t total = __shfl_sync(kFull, incl, 31);
   const int32_t base = incl - m;
   const bool staged = total <= kStageOut;  // the same in every lane
+  int32_t p0 = 0, k = 0;
   if (valid) {
-    const int32_t p0 = op.a_rp[row];
-    const int32_t k = op.a_rp[row + 1] - p0;
-    Lists<K> L;
-    open_lists<K, true>(op, p0, k, L);
-    int32_t n = 0;
-    for (;;) {
-      const int32_t mn = min_head<K>(L);
-      if (mn == INT_MAX) break;
-      float acc = 0.0f;
-#pragma unroll
-      for (int j = 0; j < K; ++j) {
-        if (L.cur[j] == mn) {
-          acc = __fadd_rn(acc, __fmul_rn(L.a[j], L.curv[j]));
-          advance<K, true>(op, L, j);
-        }
-      }
-      if (n < m) {
-        if (staged) {
-          s_col[wb][base + n] = mn;
-          s_val[wb][base + n] = acc;
-        } else {
-          if (fill) c_col[out0 + n] = mn;
-          c_val[out0 + n] = acc;
-        }
-      }
-      ++n;
-    }
+    p0 = op.a_rp[row];
+    k = op.a_rp[row + 1] - p0;
+  }
+  // a warp whose rows all fit fewer lists runs the narrower merge
+  constexpr int KN = NarrowK<K>::value;
+  const bool narrow = KN < K && __all_sync(kFull, k <= KN);
+  if (valid) {
+    const int32_t n =
+        narrow ? fill_row<KN>(op, p0, k, m, staged, s_col[wb], s_val[wb], base, c_col, c_val,
+                              out0, fill)
+               : fill_row<K>(op, p0, k, m, staged, s_col[wb], s_val[wb], base, c_col, c_val,
+                             out0, fill);
     if (n != m) report(status, kDevCountMismatch);
   }
   if (!staged) return;
