@@ -589,6 +589,9 @@ program_kernel(const int4 *__restrict__ tiles, int32_t ntiles, int32_t na, int32
   const int wib = threadIdx.x >> 5, lane = lane_id();
   if (threadIdx.x < 32) slen[threadIdx.x] = threadIdx.x < na ? lens[threadIdx.x] : 0;
   __syncthreads();
+  // the warp's maxima over its tiles (the A extent; lane g: group g's B
+  // range), merged into maxima once at the end
+  int32_t mine = 0, segmax = 0;
   for (int64_t w = int64_t(blockIdx.x) * kBuildWarps + wib; w < ntiles;
        w += int64_t(gridDim.x) * kBuildWarps) {
     const int4 t = tiles[w];
@@ -604,8 +607,8 @@ program_kernel(const int4 *__restrict__ tiles, int32_t ntiles, int32_t na, int32
       rec[2] = seg0;
       rec[3] = seg;
       arange[w] = make_int2(seg0, seg);
-      atomicMax(maxima, seg);
     }
+    segmax = max(segmax, seg);
     uint16_t *const aoff = reinterpret_cast<uint16_t *>(rec + 4 + 2 * ngroups);
     uint16_t *const d = aoff + 32;
     aoff[lane] = static_cast<uint16_t>(p);
@@ -624,8 +627,8 @@ program_kernel(const int4 *__restrict__ tiles, int32_t ntiles, int32_t na, int32
       if (lane == 0) {
         rec[4 + 2 * g] = lo;
         rec[5 + 2 * g] = hi;
-        atomicMax(maxima + 1 + g, hi - lo);
       }
+      if (lane == g) mine = max(mine, hi - lo);
       for (int32_t j = gr.x; j < gr.y; ++j) {
         const bool use = active && slen[j] > 0 && p + j < kBuildSeg;
         d[j * 32 + lane] = static_cast<uint16_t>(use ? sseg[wib][p + j] - lo : 0);
@@ -633,6 +636,8 @@ program_kernel(const int4 *__restrict__ tiles, int32_t ntiles, int32_t na, int32
     }
     __syncwarp();
   }
+  if (lane == 0 && segmax > 0) atomicMax(maxima, segmax);
+  if (lane < ngroups && mine > 0) atomicMax(maxima + 1 + lane, mine);
 }
 
 // desc[pid].w = 1: the table kernel leaves the pattern's tiles alone.

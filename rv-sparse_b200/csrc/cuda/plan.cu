@@ -1350,6 +1350,9 @@ cudaError_t build_pattern_kernels(rvsp_cuda_plan *p, cudaStream_t s, const Opera
     e = cudaMemcpyAsync(tabs + k * size_t(stride), tb.tab.p + size_t(order[k]) * stride,
                         size_t(stride) * sizeof(uint16_t), cudaMemcpyDeviceToHost, s);
   if (e == cudaSuccess) e = cudaMemsetAsync(tb.jwords.p, 0, K * W * sizeof(int32_t), s);
+  // the patterns' span and record kernels are small and bound by latency:
+  // they run side by side on the plan's side streams
+  Lanes ln(p, s, true);
   for (size_t k = 0; k < K && e == cudaSuccess; ++k) {
     const int32_t id = order[k];
     JitPattern &jp = cand[k];
@@ -1373,12 +1376,14 @@ cudaError_t build_pattern_kernels(rvsp_cuda_plan *p, cudaStream_t s, const Opera
       give_back(jp);
       continue;
     }
+    const cudaStream_t ks = k == 0 ? ln.main() : ln.next();
     e = cudaMemcpyAsync(jp.tiles.p, lists + lbeg[k], lfill[k] * sizeof(int4),
-                        cudaMemcpyHostToDevice, s);
+                        cudaMemcpyHostToDevice, ks);
     if (e != cudaSuccess) break;
     launch_jit_spans(jp.tiles.p, jp.n, tb.desc.p + id, tb.lens.p + size_t(id) * 32, op.a_rp,
-                     op.a_col, op.b_rp, tb.jwords.p + k * W, p->num_sms, s);
+                     op.a_col, op.b_rp, tb.jwords.p + k * W, p->num_sms, ks);
   }
+  ln.join();
   if (e == cudaSuccess)
     e = cudaMemcpyAsync(words, tb.jwords.p, K * W * sizeof(int32_t), cudaMemcpyDeviceToHost, s);
   if (e == cudaSuccess) e = cudaStreamSynchronize(s);
@@ -1419,6 +1424,7 @@ cudaError_t build_pattern_kernels(rvsp_cuda_plan *p, cudaStream_t s, const Opera
   // extent, then each group's largest B range over every tile)
   cudaMemsetAsync(tb.jwords.p, 0, K * W * sizeof(int32_t), s);
   std::vector<int32_t> rws(K, 0);
+  Lanes lr(p, s, true);
   for (size_t k = 0; k < K; ++k) {
     JitPattern &jp = cand[k];
     const JitRequest &rq = reqs[k];
@@ -1436,12 +1442,14 @@ cudaError_t build_pattern_kernels(rvsp_cuda_plan *p, cudaStream_t s, const Opera
     }
     for (size_t g = 0; g < rq.groups.size(); ++g)
       gh[k * 32 + g] = make_int2(rq.groups[g].first, rq.groups[g].second);
+    const cudaStream_t ks = k == 0 ? lr.main() : lr.next();
     cudaMemcpyAsync(tb.jgroups.p + k * 32, gh + k * 32, rq.groups.size() * sizeof(int2),
-                    cudaMemcpyHostToDevice, s);
+                    cudaMemcpyHostToDevice, ks);
     launch_jit_programs(jp.tiles.p, jp.n, rq.na, rq.groups, tb.jgroups.p + k * 32,
                         tb.lens.p + size_t(order[k]) * 32, op.a_rp, op.a_col, op.b_rp,
-                        jp.prog.p, jp.arange.p, tb.jwords.p + k * W, p->num_sms, s);
+                        jp.prog.p, jp.arange.p, tb.jwords.p + k * W, p->num_sms, ks);
   }
+  lr.join();
   e = cudaMemcpyAsync(words, tb.jwords.p, K * W * sizeof(int32_t), cudaMemcpyDeviceToHost, s);
   if (e == cudaSuccess) e = cudaStreamSynchronize(s);
   if (e != cudaSuccess) {
