@@ -202,46 +202,115 @@ shift_fill32_kernel(const int32_t *__restrict__ on, int32_t *__restrict__ p, siz
     p[i] = v;
 }
 
-// Rows per warp in the key and resolve passes: a warp takes kShiftRows
-// consecutive rows and issues each step's loads for all of them before it
-// waits, so one warp keeps kShiftRows dependent load chains in flight.
+// Rows per warp in the member fill: a warp takes kShiftRows consecutive
+// rows and issues each step's loads for all of them before it waits, so one
+// warp keeps kShiftRows dependent load chains in flight.
 constexpr int kShiftRows = 4;
 
-// B row keys: kShiftRows B rows per warp, a lane per entry.
-__global__ void __launch_bounds__(kThreads)
+// The key and resolve passes take 32 consecutive rows per warp, a lane per
+// row.  The warp first copies the rows' column indices (one contiguous
+// segment of the CSR column array) into its own shared memory with 16-byte
+// loads, so the column array leaves HBM once, in coalesced lines, and each
+// lane then walks its own row in shared memory.  A segment longer than
+// kSegCap entries is read from global memory by the lanes instead; B rows
+// longer than kLaneMax entries are keyed and checked afterwards by the whole
+// warp, one row at a time (A rows of more than kShiftMaxA nonzeros never
+// join a pattern).
+constexpr int kSegWarps = 4;
+constexpr int kSegThreads = kSegWarps * 32;
+constexpr int kSegCap = 2048;  // column indices one warp stages (8 KB)
+constexpr int kLaneMax = 64;   // longest B row one lane walks
+
+// Copies col[s0, s1) into the warp's seg and returns the column position
+// held in seg[0] (s0 rounded down to a multiple of four), or -1 when the
+// segment does not fit.  16-byte loads cover the whole four-entry groups
+// below s1, single loads the rest; every load stays inside [0, s1).
+__device__ __forceinline__ int64_t stage_segment(const int32_t *__restrict__ col, int64_t s0,
+                                                 int64_t s1, int32_t *seg, int lane) {
+  const int64_t base = s0 & ~int64_t(3);
+  if (s1 - base > kSegCap) return -1;
+  int64_t e = base;
+  if ((reinterpret_cast<uintptr_t>(col) & 15u) == 0) {
+    const int64_t g0 = base >> 2, g1 = s1 >> 2;
+    const int4 *v = reinterpret_cast<const int4 *>(col);
+    int4 *d = reinterpret_cast<int4 *>(seg);
+#pragma unroll 4
+    for (int64_t g = g0 + lane; g < g1; g += 32) d[g - g0] = __ldg(v + g);
+    e = g1 << 2;
+  }
+  for (int64_t t = e + lane; t < s1; t += 32) seg[t - base] = __ldg(col + t);
+  __syncwarp();
+  return base;
+}
+
+// brow_key's value, computed by one lane over its own row c[0, len).
+template <typename P>
+__device__ __forceinline__ unsigned long long brow_key_lane(P c, int32_t len, int32_t k) {
+  unsigned long long h = 0;
+  for (int32_t e = 0; e < len; ++e)
+    h ^= mix64((static_cast<unsigned long long>(e) << 32) | static_cast<uint32_t>(c[e] - k));
+  return mix64(h ^ (static_cast<unsigned long long>(len) * 0x9E3779B97F4A7C15ull)) | 1ull;
+}
+
+// Whether row a (at row index ka) is row b (at kb) moved by ka - kb, entry
+// by entry; both rows have len entries.
+template <typename P>
+__device__ __forceinline__ bool same_translate(P a, const int32_t *__restrict__ b, int32_t len,
+                                               int32_t ka, int32_t kb) {
+  for (int32_t e = 0; e < len; ++e)
+    if (a[e] - ka != __ldg(b + e) - kb) return false;
+  return true;
+}
+
+// A warp's 32 rows: this lane's row and its bounds, and the staged segment.
+struct SegRows {
+  int64_t r0;    // first row of the warp
+  int32_t r;     // this lane's row
+  bool live;     // r < rows
+  int32_t lo, len;
+  int64_t base;  // column position of seg[0], or -1 (rows read from global)
+};
+
+__device__ __forceinline__ SegRows seg_rows(int32_t rows, const int32_t *__restrict__ rp,
+                                            const int32_t *__restrict__ col, int32_t *seg,
+                                            int lane) {
+  SegRows s;
+  s.r0 = (int64_t(blockIdx.x) * kSegWarps + (threadIdx.x >> 5)) * 32;
+  s.r = static_cast<int32_t>(s.r0) + lane;
+  s.live = s.r0 + lane < rows;
+  s.lo = s.live ? __ldg(rp + s.r) : 0;
+  const int32_t hi = s.live ? __ldg(rp + s.r + 1) : 0;
+  s.len = hi - s.lo;
+  const int64_t left = rows - s.r0;
+  const int last = left < 32 ? static_cast<int>(left) - 1 : 31;
+  s.base = stage_segment(col, __shfl_sync(kFull, s.lo, 0), __shfl_sync(kFull, hi, last), seg,
+                         lane);
+  return s;
+}
+
+// B row keys, a lane per row.  A B row longer than kShiftMaxOps gets key 0:
+// every A row that reaches it has more products than a pattern takes.
+__global__ void __launch_bounds__(kSegThreads)
 shift_bkey_kernel(const int32_t *__restrict__ on, int32_t b_rows,
                   const int32_t *__restrict__ b_rp, const int32_t *__restrict__ b_col,
                   unsigned long long *__restrict__ bkey) {
+  __shared__ __align__(16) int32_t segs[kSegWarps][kSegCap];
   if (!*on) return;
-  const int64_t k0 = ((int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5) * kShiftRows;
-  if (k0 >= b_rows) return;
+  if ((int64_t(blockIdx.x) * kSegWarps + (threadIdx.x >> 5)) * 32 >= b_rows) return;
   const int lane = lane_id();
-  const int32_t v = (lane <= kShiftRows && k0 + lane <= b_rows) ? __ldg(b_rp + k0 + lane) : 0;
-  int32_t b0[kShiftRows], len[kShiftRows], col[kShiftRows];
-#pragma unroll
-  for (int u = 0; u < kShiftRows; ++u) {
-    b0[u] = __shfl_sync(kFull, v, u);
-    const int32_t b1 = __shfl_sync(kFull, v, u + 1);
-    len[u] = k0 + u < b_rows ? b1 - b0[u] : 0;
-  }
-#pragma unroll
-  for (int u = 0; u < kShiftRows; ++u) col[u] = lane < len[u] ? __ldg(b_col + b0[u] + lane) : 0;
-#pragma unroll
-  for (int u = 0; u < kShiftRows; ++u) {
-    if (k0 + u >= b_rows) break;
-    const int32_t k = static_cast<int32_t>(k0) + u;
-    // the key of brow_key: entry e contributes mix64(e, column - k)
-    unsigned long long h = 0;
-    if (lane < len[u])
-      h = mix64((static_cast<unsigned long long>(lane) << 32) |
-                static_cast<uint32_t>(col[u] - k));
-    for (int32_t e = lane + 32; e < len[u]; e += 32)
-      h ^= mix64((static_cast<unsigned long long>(e) << 32) |
-                 static_cast<uint32_t>(__ldg(b_col + b0[u] + e) - k));
-    h = warp_xor64(h);
-    if (lane == 0)
-      bkey[k] = mix64(h ^ (static_cast<unsigned long long>(len[u]) * 0x9E3779B97F4A7C15ull)) |
-                1ull;
+  int32_t *seg = segs[threadIdx.x >> 5];
+  const SegRows s = seg_rows(b_rows, b_rp, b_col, seg, lane);
+  if (s.live && s.len <= kLaneMax)
+    bkey[s.r] = s.base >= 0 ? brow_key_lane(seg + (s.lo - s.base), s.len, s.r)
+                            : brow_key_lane(b_col + s.lo, s.len, s.r);
+  else if (s.live && s.len > kShiftMaxOps)
+    bkey[s.r] = 0ull;
+  unsigned heavy = __ballot_sync(kFull, s.live && s.len > kLaneMax && s.len <= kShiftMaxOps);
+  while (heavy) {
+    const int32_t k = static_cast<int32_t>(s.r0) + (__ffs(heavy) - 1);
+    heavy &= heavy - 1;
+    const unsigned long long key = brow_key(b_rp, b_col, k, lane);
+    if (lane == 0) bkey[k] = key;
   }
 }
 
@@ -296,164 +365,121 @@ __device__ __forceinline__ int32_t lookup(unsigned long long key,
 }
 
 // bcls[k]: the smallest B row with k's translated columns (checked entry by
-// entry), else k.  kShiftRows B rows per warp: lane u < kShiftRows looks up
-// row k0 + u's key, then every lane compares one entry of each row.
-__global__ void __launch_bounds__(kThreads)
+// entry), else k.  A lane per row: it looks up the row's key and compares
+// the row (staged) with the canonical row; B rows longer than kLaneMax are
+// compared by the whole warp afterwards.
+__global__ void __launch_bounds__(kSegThreads)
 shift_bresolve_kernel(const int32_t *__restrict__ on, int32_t b_rows,
                       const unsigned long long *__restrict__ bkey,
                       const unsigned long long *__restrict__ tkey,
                       const int32_t *__restrict__ trow, unsigned long long mask,
                       const int32_t *__restrict__ b_rp, const int32_t *__restrict__ b_col,
                       int32_t *__restrict__ bcls) {
+  __shared__ __align__(16) int32_t segs[kSegWarps][kSegCap];
   if (!*on) return;
-  const int64_t k0 = ((int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5) * kShiftRows;
-  if (k0 >= b_rows) return;
+  if ((int64_t(blockIdx.x) * kSegWarps + (threadIdx.x >> 5)) * 32 >= b_rows) return;
   const int lane = lane_id();
-  // lane u: row k0 + u's canonical row and both rows' bounds
-  int32_t mc = -1, mk0 = 0, mk1 = 0, mc0 = 0, mc1 = 0;
-  if (lane < kShiftRows && k0 + lane < b_rows) {
-    const int32_t k = static_cast<int32_t>(k0) + lane;
-    mc = lookup(bkey[k], tkey, trow, mask);
-    mk0 = __ldg(b_rp + k);
-    mk1 = __ldg(b_rp + k + 1);
-    if (mc >= 0 && mc < b_rows && mc != k) {
-      mc0 = __ldg(b_rp + mc);
-      mc1 = __ldg(b_rp + mc + 1);
+  int32_t *seg = segs[threadIdx.x >> 5];
+  const SegRows s = seg_rows(b_rows, b_rp, b_col, seg, lane);
+  const unsigned long long key = s.live ? bkey[s.r] : 0ull;
+  int32_t c = -1, c0 = 0;
+  bool check = false;
+  if (key != 0ull) {
+    c = lookup(key, tkey, trow, mask);
+    if (c >= 0 && c < b_rows && c != s.r) {
+      c0 = __ldg(b_rp + c);
+      check = __ldg(b_rp + c + 1) - c0 == s.len;
     }
   }
-  int32_t c[kShiftRows], kb[kShiftRows], cb[kShiftRows], len[kShiftRows];
-  bool check[kShiftRows];
-#pragma unroll
-  for (int u = 0; u < kShiftRows; ++u) {
-    c[u] = __shfl_sync(kFull, mc, u);
-    kb[u] = __shfl_sync(kFull, mk0, u);
-    len[u] = __shfl_sync(kFull, mk1, u) - kb[u];
-    cb[u] = __shfl_sync(kFull, mc0, u);
-    const int32_t lc = __shfl_sync(kFull, mc1, u) - cb[u];
-    check[u] = c[u] >= 0 && c[u] < b_rows && c[u] != static_cast<int32_t>(k0) + u &&
-               len[u] == lc;
+  const bool found = c >= 0 && c < b_rows;
+  const bool wide = check && s.len > kLaneMax;
+  if (s.live && !wide) {
+    bool ok = found && c == s.r;
+    if (check)
+      ok = s.base >= 0 ? same_translate(seg + (s.lo - s.base), b_col + c0, s.len, s.r, c)
+                       : same_translate(b_col + s.lo, b_col + c0, s.len, s.r, c);
+    bcls[s.r] = ok ? c : s.r;
   }
-  bool same[kShiftRows];
-#pragma unroll
-  for (int u = 0; u < kShiftRows; ++u) {
-    same[u] = true;
-    const int32_t k = static_cast<int32_t>(k0) + u;
-    if (check[u])
-      for (int32_t e = lane; e < len[u]; e += 32)
-        same[u] = same[u] && (__ldg(b_col + kb[u] + e) - k) == (__ldg(b_col + cb[u] + e) - c[u]);
-  }
-#pragma unroll
-  for (int u = 0; u < kShiftRows; ++u) {
-    if (k0 + u >= b_rows) break;
-    const int32_t k = static_cast<int32_t>(k0) + u;
-    const bool found = c[u] >= 0 && c[u] < b_rows;
-    const bool ok = found && (c[u] == k || (check[u] && __all_sync(kFull, same[u])));
-    if (lane == 0) bcls[k] = ok ? c[u] : k;
+  unsigned todo = __ballot_sync(kFull, wide);
+  while (todo) {
+    const int u = __ffs(todo) - 1;
+    todo &= todo - 1;
+    const int32_t k = static_cast<int32_t>(s.r0) + u;
+    const int32_t cu = __shfl_sync(kFull, c, u), cb = __shfl_sync(kFull, c0, u);
+    const int32_t kb = __shfl_sync(kFull, s.lo, u), len = __shfl_sync(kFull, s.len, u);
+    bool same = true;
+    for (int32_t e = lane; e < len; e += 32)
+      same = same && (__ldg(b_col + kb + e) - k) == (__ldg(b_col + cb + e) - cu);
+    const bool ok = __all_sync(kFull, same);
+    if (lane == 0) bcls[k] = ok ? cu : k;
   }
 }
 
-// Row keys: kShiftRows rows per warp, a lane per A nonzero; 0 for a row
-// that cannot join a pattern.
-__global__ void __launch_bounds__(kThreads)
+// Row keys, a lane per row: key(nA, (A column - i, class of that B row) at
+// each position j) as row_key forms it; 0 for a row that cannot join a
+// pattern.
+__global__ void __launch_bounds__(kSegThreads)
 shift_rkey_kernel(const int32_t *__restrict__ on, int32_t a_rows,
                   const int32_t *__restrict__ a_rp, const int32_t *__restrict__ a_col,
                   const int64_t *__restrict__ ops, const int32_t *__restrict__ bcls,
                   unsigned long long *__restrict__ rkey) {
+  __shared__ __align__(16) int32_t segs[kSegWarps][kSegCap];
   if (!*on) return;
-  const int64_t i0 = ((int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5) * kShiftRows;
-  if (i0 >= a_rows) return;
+  if ((int64_t(blockIdx.x) * kSegWarps + (threadIdx.x >> 5)) * 32 >= a_rows) return;
   const int lane = lane_id();
-  const int32_t v = (lane <= kShiftRows && i0 + lane <= a_rows) ? a_rp[i0 + lane] : 0;
-  const int64_t mops = (lane < kShiftRows && i0 + lane < a_rows) ? ops[i0 + lane] : 0;
-  int32_t p0[kShiftRows], na[kShiftRows], k[kShiftRows], bc[kShiftRows];
-  bool ok[kShiftRows];
-#pragma unroll
-  for (int u = 0; u < kShiftRows; ++u) {
-    p0[u] = __shfl_sync(kFull, v, u);
-    na[u] = i0 + u < a_rows ? __shfl_sync(kFull, v, u + 1) - p0[u] : 0;
-    const int64_t o = __shfl_sync(kFull, mops, u);
-    ok[u] = i0 + u < a_rows && shiftable(na[u], o);
-  }
-#pragma unroll
-  for (int u = 0; u < kShiftRows; ++u) k[u] = ok[u] && lane < na[u] ? __ldg(a_col + p0[u] + lane) : 0;
-#pragma unroll
-  for (int u = 0; u < kShiftRows; ++u) bc[u] = ok[u] && lane < na[u] ? __ldg(bcls + k[u]) : 0;
-#pragma unroll
-  for (int u = 0; u < kShiftRows; ++u) {
-    if (i0 + u >= a_rows) break;
-    const int32_t i = static_cast<int32_t>(i0) + u;
-    if (!ok[u]) {
-      if (lane == 0) rkey[i] = 0ull;
-      continue;
+  int32_t *seg = segs[threadIdx.x >> 5];
+  const SegRows s = seg_rows(a_rows, a_rp, a_col, seg, lane);
+  if (!s.live) return;
+  unsigned long long key = 0ull;
+  if (shiftable(s.len, ops[s.r])) {
+    const int32_t *g = a_col + s.lo;
+    const int32_t *m = seg + (s.base >= 0 ? s.lo - s.base : 0);
+    unsigned long long h = 0;
+    for (int32_t j = 0; j < s.len; ++j) {
+      const int32_t k = s.base >= 0 ? m[j] : __ldg(g + j);
+      const unsigned long long cls = static_cast<uint32_t>(__ldg(bcls + k));
+      h ^= mix64((static_cast<unsigned long long>(j) << 32) | static_cast<uint32_t>(k - s.r)) ^
+           mix64(cls * 0xD6E8FEB86659FD93ull + static_cast<unsigned long long>(j));
     }
-    const unsigned long long key = row_key(na[u], lane, k[u] - i, static_cast<uint32_t>(bc[u]));
-    if (lane == 0) rkey[i] = key;
+    key = mix64(h ^ (static_cast<unsigned long long>(s.len) * 0xA0761D6478BD642Full)) | 1ull;
   }
+  rkey[s.r] = key;
 }
 
 // rcls[i]: the smallest row with i's translated A row over the same B
-// classes (checked entry by entry), else i.  kShiftRows rows per warp: lane
-// u < kShiftRows looks up row i0 + u's key, then every lane compares one A
-// nonzero of each row.
-__global__ void __launch_bounds__(kThreads)
+// classes (checked entry by entry), else i.  A lane per row.
+__global__ void __launch_bounds__(kSegThreads)
 shift_rresolve_kernel(const int32_t *__restrict__ on, int32_t a_rows,
                       const unsigned long long *__restrict__ rkey,
                       const unsigned long long *__restrict__ tkey,
                       const int32_t *__restrict__ trow, unsigned long long mask,
                       const int32_t *__restrict__ a_rp, const int32_t *__restrict__ a_col,
                       const int32_t *__restrict__ bcls, int32_t *__restrict__ rcls) {
+  __shared__ __align__(16) int32_t segs[kSegWarps][kSegCap];
   if (!*on) return;
-  const int64_t i0 = ((int64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5) * kShiftRows;
-  if (i0 >= a_rows) return;
+  if ((int64_t(blockIdx.x) * kSegWarps + (threadIdx.x >> 5)) * 32 >= a_rows) return;
   const int lane = lane_id();
-  int32_t mc = -1, mi0 = 0, mi1 = 0, mc0 = 0, mc1 = 0;
-  if (lane < kShiftRows && i0 + lane < a_rows) {
-    const int32_t i = static_cast<int32_t>(i0) + lane;
-    const unsigned long long key = rkey[i];
-    mc = key ? lookup(key, tkey, trow, mask) : -1;
-    if (mc >= 0 && mc < a_rows && mc != i) {
-      mi0 = a_rp[i];
-      mi1 = a_rp[i + 1];
-      mc0 = a_rp[mc];
-      mc1 = a_rp[mc + 1];
-    } else {
-      mc = -1;
+  int32_t *seg = segs[threadIdx.x >> 5];
+  const SegRows s = seg_rows(a_rows, a_rp, a_col, seg, lane);
+  if (!s.live) return;
+  const unsigned long long key = rkey[s.r];
+  int32_t cls = s.r;
+  const int32_t c = key ? lookup(key, tkey, trow, mask) : -1;
+  if (c >= 0 && c < a_rows && c != s.r && s.len <= kShiftMaxA) {
+    const int32_t c0 = __ldg(a_rp + c);
+    if (__ldg(a_rp + c + 1) - c0 == s.len) {
+      const int32_t *g = a_col + s.lo;
+      const int32_t *m = seg + (s.base >= 0 ? s.lo - s.base : 0);
+      bool same = true;
+      for (int32_t j = 0; j < s.len && same; ++j) {
+        const int32_t ki = s.base >= 0 ? m[j] : __ldg(g + j);
+        const int32_t kc = __ldg(a_col + c0 + j);
+        same = ki - s.r == kc - c && __ldg(bcls + ki) == __ldg(bcls + kc);
+      }
+      if (same) cls = c;
     }
   }
-  int32_t c[kShiftRows], pi[kShiftRows], pc[kShiftRows], na[kShiftRows];
-  bool check[kShiftRows];
-#pragma unroll
-  for (int u = 0; u < kShiftRows; ++u) {
-    c[u] = __shfl_sync(kFull, mc, u);
-    pi[u] = __shfl_sync(kFull, mi0, u);
-    na[u] = __shfl_sync(kFull, mi1, u) - pi[u];
-    pc[u] = __shfl_sync(kFull, mc0, u);
-    const int32_t nc = __shfl_sync(kFull, mc1, u) - pc[u];
-    check[u] = c[u] >= 0 && na[u] == nc && na[u] <= kShiftMaxA;
-  }
-  int32_t ki[kShiftRows], kc[kShiftRows];
-#pragma unroll
-  for (int u = 0; u < kShiftRows; ++u) {
-    const bool in = check[u] && lane < na[u];
-    ki[u] = in ? __ldg(a_col + pi[u] + lane) : 0;
-    kc[u] = in ? __ldg(a_col + pc[u] + lane) : 0;
-  }
-  bool same[kShiftRows];
-#pragma unroll
-  for (int u = 0; u < kShiftRows; ++u) {
-    same[u] = true;
-    if (check[u] && lane < na[u]) {
-      const int32_t i = static_cast<int32_t>(i0) + u;
-      same[u] = (ki[u] - i) == (kc[u] - c[u]) && __ldg(bcls + ki[u]) == __ldg(bcls + kc[u]);
-    }
-  }
-#pragma unroll
-  for (int u = 0; u < kShiftRows; ++u) {
-    if (i0 + u >= a_rows) break;
-    const int32_t i = static_cast<int32_t>(i0) + u;
-    const bool ok = check[u] && __all_sync(kFull, same[u]);
-    if (lane == 0) rcls[i] = ok ? c[u] : i;
-  }
+  rcls[s.r] = cls;
 }
 
 // share[c] += rows whose class is c (other than c); warp-aggregated.
@@ -710,6 +736,12 @@ unsigned grid_warps(int64_t warps) {
 unsigned grid_threads(int64_t n) {
   return static_cast<unsigned>((n + kThreads - 1) / kThreads);
 }
+// Blocks of the key and resolve passes: 32 rows a warp, kSegWarps warps.
+unsigned grid_segs(int32_t rows) {
+  const int64_t per = int64_t(32) * kSegWarps;
+  const int64_t b = (int64_t(rows) + per - 1) / per;
+  return static_cast<unsigned>(b ? b : 1);
+}
 unsigned grid_fill(size_t n) {
   const size_t b = (n + kThreads - 1) / kThreads;
   return static_cast<unsigned>(b < 4096 ? (b ? b : 1) : 4096);
@@ -735,22 +767,21 @@ void launch_shift_classes(const int32_t *on, const Operands &op, int32_t b_rows,
   // B classes
   shift_fill64_kernel<<<grid_fill(tcap), kThreads, 0, s>>>(on, tkey, tcap, 0ull);
   shift_fill32_kernel<<<grid_fill(tcap), kThreads, 0, s>>>(on, trow, tcap, INT_MAX);
-  const int64_t bw = (int64_t(b_rows) + kShiftRows - 1) / kShiftRows;
-  const int64_t aw = (int64_t(op.a_rows) + kShiftRows - 1) / kShiftRows;
-  shift_bkey_kernel<<<grid_warps(bw), kThreads, 0, s>>>(on, b_rows, op.b_rp, op.b_col, bkey);
+  const unsigned bg = grid_segs(b_rows), ag = grid_segs(op.a_rows);
+  shift_bkey_kernel<<<bg, kSegThreads, 0, s>>>(on, b_rows, op.b_rp, op.b_col, bkey);
   shift_insert_kernel<<<grid_threads(b_rows), kThreads, 0, s>>>(on, b_rows, bkey, tkey, trow,
                                                                 mask);
-  shift_bresolve_kernel<<<grid_warps(bw), kThreads, 0, s>>>(on, b_rows, bkey, tkey, trow, mask,
-                                                            op.b_rp, op.b_col, bcls);
+  shift_bresolve_kernel<<<bg, kSegThreads, 0, s>>>(on, b_rows, bkey, tkey, trow, mask, op.b_rp,
+                                                   op.b_col, bcls);
   // row classes
   shift_fill64_kernel<<<grid_fill(tcap), kThreads, 0, s>>>(on, tkey, tcap, 0ull);
   shift_fill32_kernel<<<grid_fill(tcap), kThreads, 0, s>>>(on, trow, tcap, INT_MAX);
-  shift_rkey_kernel<<<grid_warps(aw), kThreads, 0, s>>>(on, op.a_rows, op.a_rp, op.a_col, ops,
-                                                        bcls, rkey);
+  shift_rkey_kernel<<<ag, kSegThreads, 0, s>>>(on, op.a_rows, op.a_rp, op.a_col, ops, bcls,
+                                               rkey);
   shift_insert_kernel<<<grid_threads(op.a_rows), kThreads, 0, s>>>(on, op.a_rows, rkey, tkey,
                                                                    trow, mask);
-  shift_rresolve_kernel<<<grid_warps(aw), kThreads, 0, s>>>(
-      on, op.a_rows, rkey, tkey, trow, mask, op.a_rp, op.a_col, bcls, rcls);
+  shift_rresolve_kernel<<<ag, kSegThreads, 0, s>>>(on, op.a_rows, rkey, tkey, trow, mask,
+                                                   op.a_rp, op.a_col, bcls, rcls);
 }
 
 void launch_shift_patterns(const int32_t *on, const Operands &op, const int32_t *rcls,

@@ -126,6 +126,73 @@ def test_translates_mixed_with_random_rows():
     assert shifted <= 6000
 
 
+def test_wide_b_rows_take_the_warp_path():
+    # B rows of 80 entries: longer than one lane walks, so the whole warp
+    # keys them and checks them against their canonical row
+    A = _banded(6000, (-2, 0, 1, 3), 21)
+    B = _banded(6000, tuple(range(0, 160, 2)), 22, cols=6200)
+    _check(A, B, min_shift=5000, repeats=1)
+
+
+def test_b_rows_at_the_staging_limit():
+    # 64-entry B rows: 32 of them fill a warp's staged segment exactly, so
+    # the warps whose segment starts off a 16-byte boundary read their rows
+    # from global memory instead
+    A = _banded(6000, (-1, 0, 2), 23)
+    B = _banded(6000, tuple(range(0, 128, 2)), 24, cols=6200)
+    _check(A, B, min_shift=5000, repeats=1)
+
+
+def test_a_segments_too_long_to_stage():
+    # every third A row holds 200 random columns: 32 consecutive rows hold
+    # more column indices than a warp stages, so the banded rows between
+    # them are keyed and checked from global memory
+    n = 6000
+    band = _banded(n, (-3, 0, 4), 25)
+    rng = np.random.default_rng(26)
+    rows = []
+    for i in range(n):
+        if i % 3 == 1:
+            c = np.sort(rng.choice(n, 200, replace=False)).astype(np.int32)
+        else:
+            c = band.col_idx[band.row_ptr[i]:band.row_ptr[i + 1]]
+        rows.append(c)
+    rp = np.zeros(n + 1, np.int32)
+    rp[1:] = np.cumsum([len(c) for c in rows])
+    ci = np.concatenate(rows).astype(np.int32)
+    A = CSR(n, n, rp, ci, rng.uniform(-1, 1, ci.size).astype(np.float32))
+    B = _banded(n, (-2, 0, 1, 9), 27)
+    shifted = _check(A, B, min_shift=3500, repeats=1)
+    assert shifted <= 4000
+
+
+@pytest.mark.parametrize("off", [1, 2, 3])
+def test_column_arrays_off_16_byte_boundaries(off):
+    # A's column indices handed over `off` entries into a larger buffer: the
+    # key and resolve passes stage them with single loads instead of 16-byte
+    # ones
+    import torch
+    A = gen.stencil_3d_27(16)
+    rp, ci, cv, _ = oracle.spgemm(A, A)
+    buf = torch.zeros(A.nnz + 4, dtype=torch.int32, device="cuda")
+    buf[off:off + A.nnz].copy_(torch.from_numpy(A.col_idx))
+    dA = DeviceCSR(A.rows, A.cols, torch.from_numpy(A.row_ptr).cuda(), buf[off:off + A.nnz],
+                   torch.from_numpy(A.values).cuda())
+    torch.cuda.synchronize()
+    with Descriptor(algo=L.ALGO_CUDA_PLAIN, memory=L.MEM_DEVICE) as d:
+        d.set_shift_classes(2)
+        ws_b, n = d.work_estimation(dA, dA)
+        dC = DeviceCSR.empty(A.rows, A.cols, n)
+        ws = torch.zeros(max(ws_b, 1), dtype=torch.uint8, device="cuda")
+        d.compute(dA, dA, dC, ws)
+        d.synchronize()
+        got = dC.to_host(n)
+        assert d.shift_rows() > 2000
+    assert np.array_equal(got.row_ptr, rp)
+    assert np.array_equal(got.col_idx, ci)
+    assert np.array_equal(_bits(got.values), _bits(cv))
+
+
 def test_random_matrix_has_no_classes():
     A = gen.random_csr(8000, 7000, 12, mean_len=8.0, heavy_rows=3, heavy_len=900)
     B = gen.random_csr(7000, 9000, 13, mean_len=9.0)
