@@ -74,15 +74,22 @@ __device__ __forceinline__ unsigned long long brow_key(const int32_t *__restrict
   return mix64(h ^ (static_cast<unsigned long long>(len) * 0x9E3779B97F4A7C15ull)) | 1ull;
 }
 
+// A row key's term for A nonzero j at column offset d over a B row whose
+// class (or key) is cls_word; the key XORs the terms of all positions.
+__device__ __forceinline__ unsigned long long row_term(int32_t j, int32_t d,
+                                                       unsigned long long cls_word) {
+  return mix64(((static_cast<unsigned long long>(j) << 32) | static_cast<uint32_t>(d)) ^
+               (cls_word * 0xD6E8FEB86659FD93ull));
+}
+__device__ __forceinline__ unsigned long long row_key_of(unsigned long long h, int32_t na) {
+  return mix64(h ^ (static_cast<unsigned long long>(na) * 0xA0761D6478BD642Full)) | 1ull;
+}
+
 // Row key from per-position terms (lane j < na contributes its A nonzero j).
 __device__ __forceinline__ unsigned long long row_key(int32_t na, int lane, int32_t d,
                                                       unsigned long long cls_word) {
-  unsigned long long h = 0;
-  if (lane < na)
-    h = mix64((static_cast<unsigned long long>(lane) << 32) | static_cast<uint32_t>(d)) ^
-        mix64(cls_word * 0xD6E8FEB86659FD93ull + static_cast<unsigned long long>(lane));
-  h = warp_xor64(h);
-  return mix64(h ^ (static_cast<unsigned long long>(na) * 0xA0761D6478BD642Full)) | 1ull;
+  const unsigned long long h = lane < na ? row_term(lane, d, cls_word) : 0ull;
+  return row_key_of(warp_xor64(h), na);
 }
 
 __device__ __forceinline__ uint32_t key_slot(unsigned long long key, unsigned long long mask) {
@@ -210,37 +217,81 @@ constexpr int kShiftRows = 4;
 // The key and resolve passes take 32 consecutive rows per warp, a lane per
 // row.  The warp first copies the rows' column indices (one contiguous
 // segment of the CSR column array) into its own shared memory with 16-byte
-// loads, so the column array leaves HBM once, in coalesced lines, and each
-// lane then walks its own row in shared memory.  A segment longer than
-// kSegCap entries is read from global memory by the lanes instead; B rows
-// longer than kLaneMax entries are keyed and checked afterwards by the whole
-// warp, one row at a time (A rows of more than kShiftMaxA nonzeros never
-// join a pattern).
-constexpr int kSegWarps = 4;
-constexpr int kSegThreads = kSegWarps * 32;
-constexpr int kSegCap = 2048;  // column indices one warp stages (8 KB)
-constexpr int kLaneMax = 64;   // longest B row one lane walks
+// loads issued together, so the column array leaves HBM once, in coalesced
+// lines, and each lane then walks its own row in shared memory.  A segment
+// longer than kSegCap entries is read from global memory by the lanes
+// instead; B rows longer than kLaneMax entries are keyed and checked
+// afterwards by the whole warp, one row at a time (A rows of more than
+// kShiftMaxA nonzeros never join a pattern).
+constexpr int kSegCap = 1024;                // column indices one warp stages (4 KB)
+constexpr int kSegVec = kSegCap / 128;       // 16-byte loads a lane issues for it
+constexpr int kBWarps = 8, kAWarps = 4;      // warps per block: B passes, A passes
+constexpr int kLaneMax = 64;                 // longest B row one lane walks
 
-// Copies col[s0, s1) into the warp's seg and returns the column position
-// held in seg[0] (s0 rounded down to a multiple of four), or -1 when the
-// segment does not fit.  16-byte loads cover the whole four-entry groups
-// below s1, single loads the rest; every load stays inside [0, s1).
-__device__ __forceinline__ int64_t stage_segment(const int32_t *__restrict__ col, int64_t s0,
-                                                 int64_t s1, int32_t *seg, int lane) {
-  const int64_t base = s0 & ~int64_t(3);
-  if (s1 - base > kSegCap) return -1;
-  int64_t e = base;
+// A warp's 32 rows: this lane's row and bounds, and the staged segment.
+struct SegRows {
+  int64_t r0;    // first row of the warp
+  int32_t r;     // this lane's row
+  bool live;     // r < rows
+  int32_t lo, len;
+  int64_t base;  // column position held in seg[0], or -1 (rows read from global)
+  int32_t n;     // entries staged, seg[0, n)
+};
+
+// The warp's rows and their bounds; the segment's 16-byte loads are issued
+// into v (the caller may issue other loads before seg_land stores them).
+// base is s0 rounded down to a multiple of four; the whole four-entry groups
+// below the segment's end come by 16-byte loads when col is 16-byte aligned,
+// the rest by single loads in seg_land; every load stays inside [0, s1).
+__device__ __forceinline__ SegRows seg_issue(int32_t rows, int warps,
+                                             const int32_t *__restrict__ rp,
+                                             const int32_t *__restrict__ col, int lane,
+                                             int4 (&v)[kSegVec]) {
+  SegRows s;
+  s.r0 = (int64_t(blockIdx.x) * warps + (threadIdx.x >> 5)) * 32;
+  s.r = static_cast<int32_t>(s.r0) + lane;
+  s.live = s.r0 + lane < rows;
+  s.lo = s.live ? __ldg(rp + s.r) : 0;
+  const int32_t hi = s.live ? __ldg(rp + s.r + 1) : 0;
+  s.len = hi - s.lo;
+  const int64_t left = rows - s.r0;
+  const int last = left < 32 ? static_cast<int>(left) - 1 : 31;
+  const int64_t s0 = __shfl_sync(kFull, s.lo, 0), s1 = __shfl_sync(kFull, hi, last);
+  s.base = s0 & ~int64_t(3);
+  s.n = static_cast<int32_t>(s1 - s.base);
+  if (s1 - s.base > kSegCap) {
+    s.base = -1;
+    s.n = 0;
+  } else if ((reinterpret_cast<uintptr_t>(col) & 15u) == 0) {
+    const int64_t g0 = s.base >> 2, g1 = s1 >> 2;
+    const int4 *vec = reinterpret_cast<const int4 *>(col);
+#pragma unroll
+    for (int q = 0; q < kSegVec; ++q) {
+      const int64_t g = g0 + q * 32 + lane;
+      if (g < g1) v[q] = __ldg(vec + g);
+    }
+  }
+  return s;
+}
+
+// Stores the loads of seg_issue into seg and fetches the rest of the segment.
+__device__ __forceinline__ void seg_land(const SegRows &s, const int32_t *__restrict__ col,
+                                         int32_t *seg, int lane, const int4 (&v)[kSegVec]) {
+  if (s.base < 0) return;
+  const int64_t s1 = s.base + s.n;
+  int64_t e = s.base;
   if ((reinterpret_cast<uintptr_t>(col) & 15u) == 0) {
-    const int64_t g0 = base >> 2, g1 = s1 >> 2;
-    const int4 *v = reinterpret_cast<const int4 *>(col);
+    const int64_t g1 = s1 >> 2;
     int4 *d = reinterpret_cast<int4 *>(seg);
-#pragma unroll 4
-    for (int64_t g = g0 + lane; g < g1; g += 32) d[g - g0] = __ldg(v + g);
+#pragma unroll
+    for (int q = 0; q < kSegVec; ++q) {
+      const int64_t g = (s.base >> 2) + q * 32 + lane;
+      if (g < g1) d[q * 32 + lane] = v[q];
+    }
     e = g1 << 2;
   }
-  for (int64_t t = e + lane; t < s1; t += 32) seg[t - base] = __ldg(col + t);
+  for (int64_t t = e + lane; t < s1; t += 32) seg[t - s.base] = __ldg(col + t);
   __syncwarp();
-  return base;
 }
 
 // brow_key's value, computed by one lane over its own row c[0, len).
@@ -253,53 +304,31 @@ __device__ __forceinline__ unsigned long long brow_key_lane(P c, int32_t len, in
 }
 
 // Whether row a (at row index ka) is row b (at kb) moved by ka - kb, entry
-// by entry; both rows have len entries.
+// by entry; both rows have len entries.  No early exit, so the loads of
+// several entries are in flight together.
 template <typename P>
 __device__ __forceinline__ bool same_translate(P a, const int32_t *__restrict__ b, int32_t len,
                                                int32_t ka, int32_t kb) {
-  for (int32_t e = 0; e < len; ++e)
-    if (a[e] - ka != __ldg(b + e) - kb) return false;
-  return true;
-}
-
-// A warp's 32 rows: this lane's row and its bounds, and the staged segment.
-struct SegRows {
-  int64_t r0;    // first row of the warp
-  int32_t r;     // this lane's row
-  bool live;     // r < rows
-  int32_t lo, len;
-  int64_t base;  // column position of seg[0], or -1 (rows read from global)
-};
-
-__device__ __forceinline__ SegRows seg_rows(int32_t rows, const int32_t *__restrict__ rp,
-                                            const int32_t *__restrict__ col, int32_t *seg,
-                                            int lane) {
-  SegRows s;
-  s.r0 = (int64_t(blockIdx.x) * kSegWarps + (threadIdx.x >> 5)) * 32;
-  s.r = static_cast<int32_t>(s.r0) + lane;
-  s.live = s.r0 + lane < rows;
-  s.lo = s.live ? __ldg(rp + s.r) : 0;
-  const int32_t hi = s.live ? __ldg(rp + s.r + 1) : 0;
-  s.len = hi - s.lo;
-  const int64_t left = rows - s.r0;
-  const int last = left < 32 ? static_cast<int>(left) - 1 : 31;
-  s.base = stage_segment(col, __shfl_sync(kFull, s.lo, 0), __shfl_sync(kFull, hi, last), seg,
-                         lane);
-  return s;
+  bool same = true;
+#pragma unroll 4
+  for (int32_t e = 0; e < len; ++e) same &= (a[e] - ka == __ldg(b + e) - kb);
+  return same;
 }
 
 // B row keys, a lane per row.  A B row longer than kShiftMaxOps gets key 0:
 // every A row that reaches it has more products than a pattern takes.
-__global__ void __launch_bounds__(kSegThreads)
+__global__ void __launch_bounds__(kBWarps * 32)
 shift_bkey_kernel(const int32_t *__restrict__ on, int32_t b_rows,
                   const int32_t *__restrict__ b_rp, const int32_t *__restrict__ b_col,
                   unsigned long long *__restrict__ bkey) {
-  __shared__ __align__(16) int32_t segs[kSegWarps][kSegCap];
+  __shared__ __align__(16) int32_t segs[kBWarps][kSegCap];
   if (!*on) return;
-  if ((int64_t(blockIdx.x) * kSegWarps + (threadIdx.x >> 5)) * 32 >= b_rows) return;
+  if ((int64_t(blockIdx.x) * kBWarps + (threadIdx.x >> 5)) * 32 >= b_rows) return;
   const int lane = lane_id();
   int32_t *seg = segs[threadIdx.x >> 5];
-  const SegRows s = seg_rows(b_rows, b_rp, b_col, seg, lane);
+  int4 v[kSegVec];
+  const SegRows s = seg_issue(b_rows, kBWarps, b_rp, b_col, lane, v);
+  seg_land(s, b_col, seg, lane, v);
   if (s.live && s.len <= kLaneMax)
     bkey[s.r] = s.base >= 0 ? brow_key_lane(seg + (s.lo - s.base), s.len, s.r)
                             : brow_key_lane(b_col + s.lo, s.len, s.r);
@@ -365,22 +394,23 @@ __device__ __forceinline__ int32_t lookup(unsigned long long key,
 }
 
 // bcls[k]: the smallest B row with k's translated columns (checked entry by
-// entry), else k.  A lane per row: it looks up the row's key and compares
-// the row (staged) with the canonical row; B rows longer than kLaneMax are
-// compared by the whole warp afterwards.
-__global__ void __launch_bounds__(kSegThreads)
+// entry), else k.  A lane per row: it looks up the row's key (while the
+// segment's loads are in flight) and compares the row with the canonical
+// row; B rows longer than kLaneMax are compared by the whole warp.
+__global__ void __launch_bounds__(kBWarps * 32)
 shift_bresolve_kernel(const int32_t *__restrict__ on, int32_t b_rows,
                       const unsigned long long *__restrict__ bkey,
                       const unsigned long long *__restrict__ tkey,
                       const int32_t *__restrict__ trow, unsigned long long mask,
                       const int32_t *__restrict__ b_rp, const int32_t *__restrict__ b_col,
                       int32_t *__restrict__ bcls) {
-  __shared__ __align__(16) int32_t segs[kSegWarps][kSegCap];
+  __shared__ __align__(16) int32_t segs[kBWarps][kSegCap];
   if (!*on) return;
-  if ((int64_t(blockIdx.x) * kSegWarps + (threadIdx.x >> 5)) * 32 >= b_rows) return;
+  if ((int64_t(blockIdx.x) * kBWarps + (threadIdx.x >> 5)) * 32 >= b_rows) return;
   const int lane = lane_id();
   int32_t *seg = segs[threadIdx.x >> 5];
-  const SegRows s = seg_rows(b_rows, b_rp, b_col, seg, lane);
+  int4 v[kSegVec];
+  const SegRows s = seg_issue(b_rows, kBWarps, b_rp, b_col, lane, v);
   const unsigned long long key = s.live ? bkey[s.r] : 0ull;
   int32_t c = -1, c0 = 0;
   bool check = false;
@@ -391,6 +421,7 @@ shift_bresolve_kernel(const int32_t *__restrict__ on, int32_t b_rows,
       check = __ldg(b_rp + c + 1) - c0 == s.len;
     }
   }
+  seg_land(s, b_col, seg, lane, v);
   const bool found = c >= 0 && c < b_rows;
   const bool wide = check && s.len > kLaneMax;
   if (s.live && !wide) {
@@ -415,71 +446,112 @@ shift_bresolve_kernel(const int32_t *__restrict__ on, int32_t b_rows,
   }
 }
 
-// Row keys, a lane per row: key(nA, (A column - i, class of that B row) at
-// each position j) as row_key forms it; 0 for a row that cannot join a
-// pattern.
-__global__ void __launch_bounds__(kSegThreads)
+// The B class of every staged column, gathered by the whole warp (eight
+// loads a lane in flight at a time) into cls.
+__device__ __forceinline__ void gather_classes(const SegRows &s, const int32_t *seg,
+                                               const int32_t *__restrict__ bcls, int32_t *cls,
+                                               int lane) {
+  for (int32_t t0 = 0; t0 < s.n; t0 += 256) {
+    int32_t g[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      const int32_t t = t0 + q * 32 + lane;
+      g[q] = t < s.n ? __ldg(bcls + seg[t]) : 0;
+    }
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      const int32_t t = t0 + q * 32 + lane;
+      if (t < s.n) cls[t] = g[q];
+    }
+  }
+  __syncwarp();
+}
+
+// Row keys, a lane per row: the XOR of row_term(j, A column - i, class of
+// that B row) over the row's positions j, then row_key_of; 0 for a row that
+// cannot join a pattern.
+__global__ void __launch_bounds__(kAWarps * 32)
 shift_rkey_kernel(const int32_t *__restrict__ on, int32_t a_rows,
                   const int32_t *__restrict__ a_rp, const int32_t *__restrict__ a_col,
                   const int64_t *__restrict__ ops, const int32_t *__restrict__ bcls,
                   unsigned long long *__restrict__ rkey) {
-  __shared__ __align__(16) int32_t segs[kSegWarps][kSegCap];
+  __shared__ __align__(16) int32_t segs[kAWarps][kSegCap];
+  __shared__ int32_t clss[kAWarps][kSegCap];
   if (!*on) return;
-  if ((int64_t(blockIdx.x) * kSegWarps + (threadIdx.x >> 5)) * 32 >= a_rows) return;
+  if ((int64_t(blockIdx.x) * kAWarps + (threadIdx.x >> 5)) * 32 >= a_rows) return;
   const int lane = lane_id();
-  int32_t *seg = segs[threadIdx.x >> 5];
-  const SegRows s = seg_rows(a_rows, a_rp, a_col, seg, lane);
+  int32_t *seg = segs[threadIdx.x >> 5], *cls = clss[threadIdx.x >> 5];
+  int4 v[kSegVec];
+  const SegRows s = seg_issue(a_rows, kAWarps, a_rp, a_col, lane, v);
+  const int64_t o = s.live ? ops[s.r] : 0;
+  seg_land(s, a_col, seg, lane, v);
+  gather_classes(s, seg, bcls, cls, lane);
   if (!s.live) return;
   unsigned long long key = 0ull;
-  if (shiftable(s.len, ops[s.r])) {
-    const int32_t *g = a_col + s.lo;
-    const int32_t *m = seg + (s.base >= 0 ? s.lo - s.base : 0);
+  if (shiftable(s.len, o)) {
     unsigned long long h = 0;
-    for (int32_t j = 0; j < s.len; ++j) {
-      const int32_t k = s.base >= 0 ? m[j] : __ldg(g + j);
-      const unsigned long long cls = static_cast<uint32_t>(__ldg(bcls + k));
-      h ^= mix64((static_cast<unsigned long long>(j) << 32) | static_cast<uint32_t>(k - s.r)) ^
-           mix64(cls * 0xD6E8FEB86659FD93ull + static_cast<unsigned long long>(j));
+    if (s.base >= 0) {
+      const int32_t *m = seg + (s.lo - s.base), *mc = cls + (s.lo - s.base);
+      for (int32_t j = 0; j < s.len; ++j)
+        h ^= row_term(j, m[j] - s.r, static_cast<uint32_t>(mc[j]));
+    } else {
+      for (int32_t j = 0; j < s.len; ++j) {
+        const int32_t k = __ldg(a_col + s.lo + j);
+        h ^= row_term(j, k - s.r, static_cast<uint32_t>(__ldg(bcls + k)));
+      }
     }
-    key = mix64(h ^ (static_cast<unsigned long long>(s.len) * 0xA0761D6478BD642Full)) | 1ull;
+    key = row_key_of(h, s.len);
   }
   rkey[s.r] = key;
 }
 
 // rcls[i]: the smallest row with i's translated A row over the same B
-// classes (checked entry by entry), else i.  A lane per row.
-__global__ void __launch_bounds__(kSegThreads)
+// classes (checked entry by entry), else i.  A lane per row; its own row's
+// columns and classes staged, the canonical row's read from global memory
+// (a few rows, so cache hits).
+__global__ void __launch_bounds__(kAWarps * 32)
 shift_rresolve_kernel(const int32_t *__restrict__ on, int32_t a_rows,
                       const unsigned long long *__restrict__ rkey,
                       const unsigned long long *__restrict__ tkey,
                       const int32_t *__restrict__ trow, unsigned long long mask,
                       const int32_t *__restrict__ a_rp, const int32_t *__restrict__ a_col,
                       const int32_t *__restrict__ bcls, int32_t *__restrict__ rcls) {
-  __shared__ __align__(16) int32_t segs[kSegWarps][kSegCap];
+  __shared__ __align__(16) int32_t segs[kAWarps][kSegCap];
+  __shared__ int32_t clss[kAWarps][kSegCap];
   if (!*on) return;
-  if ((int64_t(blockIdx.x) * kSegWarps + (threadIdx.x >> 5)) * 32 >= a_rows) return;
+  if ((int64_t(blockIdx.x) * kAWarps + (threadIdx.x >> 5)) * 32 >= a_rows) return;
   const int lane = lane_id();
-  int32_t *seg = segs[threadIdx.x >> 5];
-  const SegRows s = seg_rows(a_rows, a_rp, a_col, seg, lane);
-  if (!s.live) return;
-  const unsigned long long key = rkey[s.r];
-  int32_t cls = s.r;
-  const int32_t c = key ? lookup(key, tkey, trow, mask) : -1;
+  int32_t *seg = segs[threadIdx.x >> 5], *cls = clss[threadIdx.x >> 5];
+  int4 v[kSegVec];
+  const SegRows s = seg_issue(a_rows, kAWarps, a_rp, a_col, lane, v);
+  const unsigned long long key = s.live ? rkey[s.r] : 0ull;
+  int32_t c = key ? lookup(key, tkey, trow, mask) : -1, c0 = 0;
+  bool check = false;
   if (c >= 0 && c < a_rows && c != s.r && s.len <= kShiftMaxA) {
-    const int32_t c0 = __ldg(a_rp + c);
-    if (__ldg(a_rp + c + 1) - c0 == s.len) {
-      const int32_t *g = a_col + s.lo;
-      const int32_t *m = seg + (s.base >= 0 ? s.lo - s.base : 0);
-      bool same = true;
-      for (int32_t j = 0; j < s.len && same; ++j) {
-        const int32_t ki = s.base >= 0 ? m[j] : __ldg(g + j);
+    c0 = __ldg(a_rp + c);
+    check = __ldg(a_rp + c + 1) - c0 == s.len;
+  }
+  seg_land(s, a_col, seg, lane, v);
+  gather_classes(s, seg, bcls, cls, lane);
+  if (!s.live) return;
+  bool same = check;
+  if (check) {
+    if (s.base >= 0) {
+      const int32_t *m = seg + (s.lo - s.base), *mc = cls + (s.lo - s.base);
+#pragma unroll 4
+      for (int32_t j = 0; j < s.len; ++j) {
         const int32_t kc = __ldg(a_col + c0 + j);
-        same = ki - s.r == kc - c && __ldg(bcls + ki) == __ldg(bcls + kc);
+        same &= m[j] - s.r == kc - c && mc[j] == __ldg(bcls + kc);
       }
-      if (same) cls = c;
+    } else {
+#pragma unroll 4
+      for (int32_t j = 0; j < s.len; ++j) {
+        const int32_t ki = __ldg(a_col + s.lo + j), kc = __ldg(a_col + c0 + j);
+        same &= ki - s.r == kc - c && __ldg(bcls + ki) == __ldg(bcls + kc);
+      }
     }
   }
-  rcls[s.r] = cls;
+  rcls[s.r] = same ? c : s.r;
 }
 
 // share[c] += rows whose class is c (other than c); warp-aggregated.
@@ -736,9 +808,9 @@ unsigned grid_warps(int64_t warps) {
 unsigned grid_threads(int64_t n) {
   return static_cast<unsigned>((n + kThreads - 1) / kThreads);
 }
-// Blocks of the key and resolve passes: 32 rows a warp, kSegWarps warps.
-unsigned grid_segs(int32_t rows) {
-  const int64_t per = int64_t(32) * kSegWarps;
+// Blocks of the key and resolve passes: 32 rows a warp.
+unsigned grid_segs(int32_t rows, int warps) {
+  const int64_t per = int64_t(32) * warps;
   const int64_t b = (int64_t(rows) + per - 1) / per;
   return static_cast<unsigned>(b ? b : 1);
 }
@@ -767,20 +839,20 @@ void launch_shift_classes(const int32_t *on, const Operands &op, int32_t b_rows,
   // B classes
   shift_fill64_kernel<<<grid_fill(tcap), kThreads, 0, s>>>(on, tkey, tcap, 0ull);
   shift_fill32_kernel<<<grid_fill(tcap), kThreads, 0, s>>>(on, trow, tcap, INT_MAX);
-  const unsigned bg = grid_segs(b_rows), ag = grid_segs(op.a_rows);
-  shift_bkey_kernel<<<bg, kSegThreads, 0, s>>>(on, b_rows, op.b_rp, op.b_col, bkey);
+  const unsigned bg = grid_segs(b_rows, kBWarps), ag = grid_segs(op.a_rows, kAWarps);
+  shift_bkey_kernel<<<bg, kBWarps * 32, 0, s>>>(on, b_rows, op.b_rp, op.b_col, bkey);
   shift_insert_kernel<<<grid_threads(b_rows), kThreads, 0, s>>>(on, b_rows, bkey, tkey, trow,
                                                                 mask);
-  shift_bresolve_kernel<<<bg, kSegThreads, 0, s>>>(on, b_rows, bkey, tkey, trow, mask, op.b_rp,
+  shift_bresolve_kernel<<<bg, kBWarps * 32, 0, s>>>(on, b_rows, bkey, tkey, trow, mask, op.b_rp,
                                                    op.b_col, bcls);
   // row classes
   shift_fill64_kernel<<<grid_fill(tcap), kThreads, 0, s>>>(on, tkey, tcap, 0ull);
   shift_fill32_kernel<<<grid_fill(tcap), kThreads, 0, s>>>(on, trow, tcap, INT_MAX);
-  shift_rkey_kernel<<<ag, kSegThreads, 0, s>>>(on, op.a_rows, op.a_rp, op.a_col, ops, bcls,
+  shift_rkey_kernel<<<ag, kAWarps * 32, 0, s>>>(on, op.a_rows, op.a_rp, op.a_col, ops, bcls,
                                                rkey);
   shift_insert_kernel<<<grid_threads(op.a_rows), kThreads, 0, s>>>(on, op.a_rows, rkey, tkey,
                                                                    trow, mask);
-  shift_rresolve_kernel<<<ag, kSegThreads, 0, s>>>(on, op.a_rows, rkey, tkey, trow, mask,
+  shift_rresolve_kernel<<<ag, kAWarps * 32, 0, s>>>(on, op.a_rows, rkey, tkey, trow, mask,
                                                    op.a_rp, op.a_col, bcls, rcls);
 }
 

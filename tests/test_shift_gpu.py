@@ -134,12 +134,14 @@ def test_wide_b_rows_take_the_warp_path():
     _check(A, B, min_shift=5000, repeats=1)
 
 
-def test_b_rows_at_the_staging_limit():
-    # 64-entry B rows: 32 of them fill a warp's staged segment exactly, so
-    # the warps whose segment starts off a 16-byte boundary read their rows
-    # from global memory instead
+@pytest.mark.parametrize("width", [32, 48])
+def test_b_rows_at_the_staging_limit(width):
+    # 32-entry B rows: 32 of them fill a warp's staged segment (1024 column
+    # indices) exactly, so the warps whose segment starts off a 16-byte
+    # boundary read their rows from global memory instead; 48-entry rows
+    # never fit, and are walked by one lane each from global memory
     A = _banded(6000, (-1, 0, 2), 23)
-    B = _banded(6000, tuple(range(0, 128, 2)), 24, cols=6200)
+    B = _banded(6000, tuple(range(0, 2 * width, 2)), 24, cols=6200)
     _check(A, B, min_shift=5000, repeats=1)
 
 
