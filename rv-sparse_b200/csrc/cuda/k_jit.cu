@@ -53,6 +53,7 @@
 #include <dlfcn.h>
 #include <nvrtc.h>
 
+#include <algorithm>
 #include <chrono>
 #include <climits>
 #include <cstdio>
@@ -115,6 +116,22 @@ typedef unsigned int u32;
 typedef unsigned long long u64;
 typedef unsigned short u16;
 #define FULL 0xffffffffu
+// Two products and sums in one f32x2 multiply and one f32x2 add, each half
+// rounded to nearest like __fmul_rn / __fadd_rn (never fused):
+// (c0, c1) = (c0 + a * b0, c1 + a * b1), a2 holding a in both halves.
+__device__ __forceinline__ u64 pk2(float a) {
+  u64 r;
+  asm("mov.b64 %0, {%1, %1};" : "=l"(r) : "f"(a));
+  return r;
+}
+__device__ __forceinline__ void muladd2(float &c0, float &c1, u64 a2, float b0, float b1) {
+  u64 acc, b, p;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(acc) : "f"(c0), "f"(c1));
+  asm("mov.b64 %0, {%1, %2};" : "=l"(b) : "f"(b0), "f"(b1));
+  asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(p) : "l"(a2), "l"(b));
+  asm("add.rn.f32x2 %0, %1, %2;" : "=l"(acc) : "l"(acc), "l"(p));
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(c0), "=f"(c1) : "l"(acc));
+}
 __device__ __forceinline__ u32 saddr(const void *p) { return (u32)__cvta_generic_to_shared(p); }
 __device__ __forceinline__ void bar_init(u32 bar) {
   asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(bar) : "memory");
@@ -208,6 +225,25 @@ int pattern_regs(int m) {
   return up > 255 ? 255 : up < r ? r : up;
 }
 
+// Accumulator pairs of a pattern kernel: outputs (2p + par, 2p + 1 + par),
+// for the parity par under which the most products of one A nonzero reach
+// both outputs of a pair (each such two products take one f32x2 multiply
+// and one f32x2 add).  Each output still sums its products in ascending
+// A-nonzero order.
+int pair_parity(int na, const int *len, const std::vector<int> &slot, int m) {
+  int count[2] = {0, 0};
+  std::vector<char> hit(size_t(m), 0);
+  size_t t = 0;
+  for (int j = 0; j < na; ++j) {
+    std::fill(hit.begin(), hit.end(), 0);
+    for (int e = 0; e < len[j]; ++e) hit[size_t(slot[t + size_t(e)])] = 1;
+    for (int q = 0; q + 1 < m; ++q)
+      if (hit[size_t(q)] && hit[size_t(q) + 1]) ++count[q & 1];
+    t += size_t(len[j]);
+  }
+  return count[1] > count[0] ? 1 : 0;
+}
+
 // Words of a tile record (see jit_record_words).
 int record_words(int na, int ngroups) { return (4 + 2 * ngroups + 16 + 16 * na + 3) & ~3; }
 
@@ -236,6 +272,7 @@ std::string pattern_source(int na, const int *len, const std::vector<int> &slot,
   const int mid = ng / 2;
   std::vector<int> t_of(size_t(na) + 1, 0);
   for (int j = 0; j < na; ++j) t_of[size_t(j) + 1] = t_of[size_t(j)] + len[j];
+  const int par = pair_parity(na, len, slot, m);
   snprintf(buf, sizeof(buf), "#define RW %d\n#define M %d\n#define MS %d\n", rw, m, ms);
   s += buf;
   snprintf(buf, sizeof(buf), "extern \"C\" __global__ void __maxnreg__(%d)\n", pattern_regs(m));
@@ -325,13 +362,26 @@ std::string pattern_source(int na, const int *len, const std::vector<int> &slot,
       if (len[j] == 0) continue;
       snprintf(buf, sizeof(buf),
                "      {\n        const float a = sa[%d];\n"
-               "        const float *const st = sbb + dd[%d];\n",
+               "        const float *const st = sbb + dd[%d];\n"
+               "        const u64 a2 = pk2(a);\n",
                j, j * 32);
       s += buf;
+      // e of each output this A nonzero reaches (its B row's columns are
+      // distinct, so at most one), then the pairs in one f32x2 step each
+      std::vector<int> e_of(size_t(m), -1);
+      for (int e = 0; e < len[j]; ++e) e_of[size_t(slot[size_t(t_of[size_t(j)] + e)])] = e;
       for (int e = 0; e < len[j]; ++e) {
         const int q = slot[size_t(t_of[size_t(j)] + e)];
-        snprintf(buf, sizeof(buf), "        c%d = __fadd_rn(c%d, __fmul_rn(a, st[%d]));\n", q,
-                 q, e);
+        const int mate = ((q - par) & 1) == 0 ? q + 1 : q - 1;
+        const int em = mate >= 0 && mate < m ? e_of[size_t(mate)] : -1;
+        if (em < 0)
+          snprintf(buf, sizeof(buf), "        c%d = __fadd_rn(c%d, __fmul_rn(a, st[%d]));\n", q,
+                   q, e);
+        else if (q < mate)
+          snprintf(buf, sizeof(buf), "        muladd2(c%d, c%d, a2, st[%d], st[%d]);\n", q, mate,
+                   e, em);
+        else
+          continue;
         s += buf;
       }
       s += "      }\n";
@@ -681,7 +731,7 @@ int jit_pattern_kernels(std::vector<JitRequest> &reqs) {
     r.kernel = nullptr;
     if (r.na <= 0 || r.na > 32 || r.m <= 0 || r.groups.empty()) continue;
     // the key: architecture, generator version and the pattern's numbers
-    std::vector<int32_t> w = {4, r.na, r.m, static_cast<int32_t>(r.groups.size())};
+    std::vector<int32_t> w = {5, r.na, r.m, static_cast<int32_t>(r.groups.size())};
     w.insert(w.end(), r.len, r.len + r.na);
     for (const auto &g : r.groups) {
       w.push_back(g.first);
