@@ -525,21 +525,27 @@ constexpr int kBuildWarps = 4;
 constexpr int kBuildSeg = 2048;
 
 // The start of B row a_col[seg0 + i], for every i < seg, into sb[i]: loads
-// of a_col coalesced across the lanes, eight of each kind in flight.
+// of a_col coalesced across the lanes, 1024 entries at a time (32 loads a
+// lane in flight, then their 32 gathers of b_rp).
 __device__ __forceinline__ void stage_b_starts(int32_t *sb, int32_t seg0, int32_t seg,
                                                const int32_t *__restrict__ a_col,
                                                const int32_t *__restrict__ b_rp, int lane) {
-  for (int32_t i0 = 0; i0 < seg; i0 += 256) {
-    int32_t c[8];
+  for (int32_t i0 = 0; i0 < seg; i0 += 1024) {
+    int32_t c[32];
 #pragma unroll
-    for (int u = 0; u < 8; ++u) {
+    for (int u = 0; u < 32; ++u) {
       const int32_t i = i0 + u * 32 + lane;
       c[u] = i < seg ? __ldg(a_col + seg0 + i) : 0;
     }
 #pragma unroll
-    for (int u = 0; u < 8; ++u) {
+    for (int u = 0; u < 32; ++u) {
       const int32_t i = i0 + u * 32 + lane;
-      if (i < seg) sb[i] = __ldg(b_rp + c[u]);
+      c[u] = i < seg ? __ldg(b_rp + c[u]) : 0;
+    }
+#pragma unroll
+    for (int u = 0; u < 32; ++u) {
+      const int32_t i = i0 + u * 32 + lane;
+      if (i < seg) sb[i] = c[u];
     }
   }
   __syncwarp();
