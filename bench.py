@@ -1254,7 +1254,7 @@ def run_job(args, world, rank, local):
                          "kernel": "numeric-only repeat: rvsp_pattern_tiles (kernels compiled "
                                    "per term pattern, the interior one persistent over every "
                                    "SM) on the caller's stream, the table tiles, leftover rows "
-                                   "and class kernels on two side streams joined back into it; "
+                                   "and class kernels on six side streams joined back into it; "
                                    "one launch = one numeric-only compute, timed by CUDA "
                                    "events on the caller's stream",
                          "achieved": repeat_gbs, "peak": peak, "unit": "GB/s",
