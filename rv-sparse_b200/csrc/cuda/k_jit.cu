@@ -520,35 +520,45 @@ void kernels_for(const std::vector<std::string> &keys, const Source &source,
 }
 
 // Warps per block of the span and record kernels, and the A entries of one
-// tile's segment they stage (the tile builder keeps segments within this).
+// tile's segment they stage in shared memory (a longer segment's B row
+// starts are read from global memory instead; 4 KB a warp and at most 64
+// registers keep 32 warps an SM resident, these kernels being bound by load
+// latency).
 constexpr int kBuildWarps = 4;
-constexpr int kBuildSeg = 2048;
+constexpr int kBuildSeg = 1024;
 
 // The start of B row a_col[seg0 + i], for every i < seg, into sb[i]: loads
-// of a_col coalesced across the lanes, 1024 entries at a time (32 loads a
-// lane in flight, then their 32 gathers of b_rp).
+// of a_col coalesced across the lanes, 512 entries at a time (16 loads a
+// lane in flight, then their 16 gathers of b_rp).
 __device__ __forceinline__ void stage_b_starts(int32_t *sb, int32_t seg0, int32_t seg,
                                                const int32_t *__restrict__ a_col,
                                                const int32_t *__restrict__ b_rp, int lane) {
-  for (int32_t i0 = 0; i0 < seg; i0 += 1024) {
-    int32_t c[32];
+  for (int32_t i0 = 0; i0 < seg; i0 += 512) {
+    int32_t c[16];
 #pragma unroll
-    for (int u = 0; u < 32; ++u) {
+    for (int u = 0; u < 16; ++u) {
       const int32_t i = i0 + u * 32 + lane;
       c[u] = i < seg ? __ldg(a_col + seg0 + i) : 0;
     }
 #pragma unroll
-    for (int u = 0; u < 32; ++u) {
+    for (int u = 0; u < 16; ++u) {
       const int32_t i = i0 + u * 32 + lane;
       c[u] = i < seg ? __ldg(b_rp + c[u]) : 0;
     }
 #pragma unroll
-    for (int u = 0; u < 32; ++u) {
+    for (int u = 0; u < 16; ++u) {
       const int32_t i = i0 + u * 32 + lane;
       if (i < seg) sb[i] = c[u];
     }
   }
   __syncwarp();
+}
+
+// The start of the B row of segment entry i: staged, or read through a_col.
+__device__ __forceinline__ int32_t b_start(const int32_t *sb, bool staged, int32_t seg0,
+                                           int32_t i, const int32_t *__restrict__ a_col,
+                                           const int32_t *__restrict__ b_rp) {
+  return staged ? sb[i] : __ldg(b_rp + __ldg(a_col + seg0 + i));
 }
 
 // A tile's segment: from the first active row's first A nonzero to the last
@@ -568,7 +578,7 @@ __device__ __forceinline__ void tile_segment(const int4 &t, const int32_t *__res
 // read for A nonzeros j0 .. j0 + g - 1.  A nonzero with an empty B row reads
 // nothing.  The grouping is chosen from these; the tile records then measure
 // every tile's ranges.  span zeroed by the caller.
-__global__ void __launch_bounds__(kBuildWarps * 32)
+__global__ void __launch_bounds__(kBuildWarps * 32, 8)
 span_kernel(const int4 *__restrict__ tiles, int32_t ntiles, int32_t stride,
             const int4 *__restrict__ desc,
             const uint16_t *__restrict__ lens, const int32_t *__restrict__ a_rp,
@@ -591,11 +601,11 @@ span_kernel(const int4 *__restrict__ tiles, int32_t ntiles, int32_t stride,
     int32_t seg0 = 0, seg = 0;
     tile_segment(t, a_rp, &seg0, &seg);
     const int32_t p = active ? a_rp[t.x + lane] - seg0 : 0;
-    if (seg > kBuildSeg) seg = kBuildSeg;  // (never: the tile builder's bound)
-    stage_b_starts(sseg[wib], seg0, seg, a_col, b_rp, lane);
+    const bool staged = seg <= kBuildSeg;
+    if (staged) stage_b_starts(sseg[wib], seg0, seg, a_col, b_rp, lane);
     for (int32_t j = 0; j < na; ++j) {
       const bool use = active && slen[j] > 0 && p + j < seg;
-      const int32_t r = use ? sseg[wib][p + j] : 0;
+      const int32_t r = use ? b_start(sseg[wib], staged, seg0, p + j, a_col, b_rp) : 0;
       const int32_t lo = __reduce_min_sync(kFull, use ? r : INT_MAX);
       const int32_t hi = __reduce_max_sync(kFull, use ? r + slen[j] : INT_MIN);
       if (lane == 0) {
@@ -634,7 +644,7 @@ span_kernel(const int4 *__restrict__ tiles, int32_t ntiles, int32_t stride,
 // arange[tile] = ([2], [3]); maxima[0] = the largest [3], maxima[1 + g] =
 // the largest B range of group g.  Structure only: built once per
 // structure, read by every numeric-only repeat.
-__global__ void __launch_bounds__(kBuildWarps * 32)
+__global__ void __launch_bounds__(kBuildWarps * 32, 8)
 program_kernel(const int4 *__restrict__ tiles, int32_t ntiles, int32_t na, int32_t ngroups,
                const int2 *__restrict__ groups, const uint16_t *__restrict__ lens,
                const int32_t *__restrict__ a_rp, const int32_t *__restrict__ a_col,
@@ -655,7 +665,8 @@ program_kernel(const int4 *__restrict__ tiles, int32_t ntiles, int32_t na, int32
     int32_t seg0 = 0, seg = 0;
     tile_segment(t, a_rp, &seg0, &seg);
     const int32_t p = active ? a_rp[t.x + lane] - seg0 : 0;
-    stage_b_starts(sseg[wib], seg0, seg < kBuildSeg ? seg : kBuildSeg, a_col, b_rp, lane);
+    const bool staged = seg <= kBuildSeg;
+    if (staged) stage_b_starts(sseg[wib], seg0, seg, a_col, b_rp, lane);
     int32_t *const rec = prog + w * rw;
     if (lane == 0) {
       rec[0] = t.x;
@@ -672,8 +683,8 @@ program_kernel(const int4 *__restrict__ tiles, int32_t ntiles, int32_t na, int32
       const int2 gr = groups[g];
       int32_t lo = INT_MAX, hi = INT_MIN;
       for (int32_t j = gr.x; j < gr.y; ++j) {
-        if (active && slen[j] > 0 && p + j < kBuildSeg) {
-          const int32_t r = sseg[wib][p + j];
+        if (active && slen[j] > 0 && p + j < seg) {
+          const int32_t r = b_start(sseg[wib], staged, seg0, p + j, a_col, b_rp);
           lo = min(lo, r);
           hi = max(hi, r + slen[j]);
         }
@@ -686,8 +697,9 @@ program_kernel(const int4 *__restrict__ tiles, int32_t ntiles, int32_t na, int32
       }
       if (lane == g) mine = max(mine, hi - lo);
       for (int32_t j = gr.x; j < gr.y; ++j) {
-        const bool use = active && slen[j] > 0 && p + j < kBuildSeg;
-        d[j * 32 + lane] = static_cast<uint16_t>(use ? sseg[wib][p + j] - lo : 0);
+        const bool use = active && slen[j] > 0 && p + j < seg;
+        d[j * 32 + lane] = static_cast<uint16_t>(
+            use ? b_start(sseg[wib], staged, seg0, p + j, a_col, b_rp) - lo : 0);
       }
     }
     __syncwarp();
@@ -805,7 +817,7 @@ void launch_jit_spans(const int4 *tiles, int32_t ntiles, const int4 *desc, const
   const int32_t stride = ntiles > 1024 ? ntiles / 1024 : 1;
   const int64_t sampled = (int64_t(ntiles) + stride - 1) / stride;
   int64_t grid = (sampled + kBuildWarps - 1) / kBuildWarps;
-  const int64_t cap = int64_t(num_sms > 0 ? num_sms : 148) * 6;
+  const int64_t cap = int64_t(num_sms > 0 ? num_sms : 148) * 8;
   if (grid > cap) grid = cap;
   span_kernel<<<static_cast<unsigned>(grid), kBuildWarps * 32, 0, s>>>(
       tiles, ntiles, stride, desc, lens, a_rp, a_col, b_rp, span);
@@ -832,7 +844,7 @@ void launch_jit_programs(const int4 *tiles, int32_t ntiles, int32_t na,
   const int32_t rw = record_words(na, static_cast<int>(groups.size()));
   cudaMemsetAsync(prog, 0, size_t(ntiles) * size_t(rw) * sizeof(int32_t), s);
   int64_t grid = (int64_t(ntiles) + kBuildWarps - 1) / kBuildWarps;
-  const int64_t cap = int64_t(num_sms > 0 ? num_sms : 148) * 6;
+  const int64_t cap = int64_t(num_sms > 0 ? num_sms : 148) * 8;
   if (grid > cap) grid = cap;
   program_kernel<<<static_cast<unsigned>(grid), kBuildWarps * 32, 0, s>>>(
       tiles, ntiles, na, static_cast<int32_t>(groups.size()), groups_dev, lens, a_rp, a_col,

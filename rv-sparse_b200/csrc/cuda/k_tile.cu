@@ -141,12 +141,13 @@ tile_tab_kernel(int32_t npat, const int32_t *__restrict__ pat_canon,
   if (lane == 0) desc[id] = make_int4(na, m, t0, 0);
 }
 
-// Warps per block of the tile builder (each stages its chunk's B row
-// starts: kTileASegMax ints of shared memory a warp).
+// Warps per block of the tile builder, and the A entries of a chunk whose B
+// row starts it stages in shared memory.
 constexpr int kBuildWarps = 4;
+constexpr int kBuildStage = 1024;
 
 // Warp per chunk of 32 consecutive rows (see the file comment).
-__global__ void __launch_bounds__(kBuildWarps * 32)
+__global__ void __launch_bounds__(kBuildWarps * 32, 8)
 tile_build_kernel(int32_t n, const int32_t *__restrict__ pid_of_row,
                   const int4 *__restrict__ desc, const uint16_t *__restrict__ lens,
                   const int32_t *__restrict__ a_rp, const int32_t *__restrict__ a_col,
@@ -182,29 +183,41 @@ tile_build_kernel(int32_t n, const int32_t *__restrict__ pid_of_row,
     ok = __all_sync(kFull, fits);
   }
   if (ok) {
-    // the chunk's B row starts, staged with coalesced loads of a_col (the
-    // chunk's A segment is at most kTileASegMax entries here)
-    __shared__ int32_t sseg[kBuildWarps][kTileASegMax];
+    // the chunk's B row starts: a segment of up to kBuildStage entries is
+    // staged in shared memory with coalesced loads of a_col (16 a lane in
+    // flight, then their gathers), a longer one read through a_col (4 KB a
+    // warp and at most 64 registers keep 32 warps an SM resident: this
+    // kernel is bound by load latency)
+    __shared__ int32_t sseg[kBuildWarps][kBuildStage];
     int32_t *const sb = sseg[(threadIdx.x >> 5) % kBuildWarps];
     const int32_t seg0 = a_rp[row0];
-    for (int32_t i0 = 0; i0 < seg; i0 += 256) {
-      int32_t c[8];
+    const bool staged = seg <= kBuildStage;
+    if (staged) {
+      for (int32_t i0 = 0; i0 < seg; i0 += 512) {
+        int32_t c[16];
 #pragma unroll
-      for (int u = 0; u < 8; ++u) {
-        const int32_t i = i0 + u * 32 + lane;
-        c[u] = i < seg ? __ldg(a_col + seg0 + i) : 0;
-      }
+        for (int u = 0; u < 16; ++u) {
+          const int32_t i = i0 + u * 32 + lane;
+          c[u] = i < seg ? __ldg(a_col + seg0 + i) : 0;
+        }
 #pragma unroll
-      for (int u = 0; u < 8; ++u) {
-        const int32_t i = i0 + u * 32 + lane;
-        if (i < seg) sb[i] = __ldg(b_rp + c[u]);
+        for (int u = 0; u < 16; ++u) {
+          const int32_t i = i0 + u * 32 + lane;
+          c[u] = i < seg ? __ldg(b_rp + c[u]) : 0;
+        }
+#pragma unroll
+        for (int u = 0; u < 16; ++u) {
+          const int32_t i = i0 + u * 32 + lane;
+          if (i < seg) sb[i] = c[u];
+        }
       }
     }
     __syncwarp();
     const int32_t p = in ? a_rp[row] - seg0 : 0;
     for (int32_t j = 0; j < d.x; ++j) {
       const int32_t lj = lens[size_t(bpid) * 32 + j];
-      const int32_t rp = in ? sb[p + j] : 0;
+      const int32_t rp =
+          in ? (staged ? sb[p + j] : __ldg(b_rp + __ldg(a_col + seg0 + p + j))) : 0;
       const int32_t lo = __reduce_min_sync(kFull, in ? rp : INT_MAX);
       const int32_t hi = __reduce_max_sync(kFull, in ? rp + lj : INT_MIN);
       need = max(need, hi - (lo & ~3) + 8);
