@@ -195,6 +195,30 @@ def test_column_arrays_off_16_byte_boundaries(off):
     assert np.array_equal(_bits(got.values), _bits(cv))
 
 
+def test_tiles_over_long_chunk_segments():
+    # every fourth A row holds 150 random columns, the others a band of 4: a
+    # run of 32 rows then holds about 1,300 A entries, more than the tile and
+    # record builders stage in shared memory (1,024), so they read those B
+    # row starts through the column array; the banded rows still form tiles
+    n = 6000
+    band = _banded(n, (-3, 0, 1, 4), 51)
+    rng = np.random.default_rng(52)
+    rows = []
+    for i in range(n):
+        if i % 4 == 2:
+            rows.append(np.sort(rng.choice(n, 150, replace=False)).astype(np.int32))
+        else:
+            rows.append(band.col_idx[band.row_ptr[i]:band.row_ptr[i + 1]])
+    rp = np.zeros(n + 1, np.int32)
+    rp[1:] = np.cumsum([len(c) for c in rows])
+    ci = np.concatenate(rows).astype(np.int32)
+    A = CSR(n, n, rp, ci, rng.uniform(-1, 1, ci.size).astype(np.float32))
+    assert int(rp[32] - rp[0]) > 1024
+    B = _banded(n, (-2, 0, 1, 9), 53)
+    shifted = _check(A, B, min_shift=4000, repeats=1)
+    assert shifted <= 4500
+
+
 def test_random_matrix_has_no_classes():
     A = gen.random_csr(8000, 7000, 12, mean_len=8.0, heavy_rows=3, heavy_len=900)
     B = gen.random_csr(7000, 9000, 13, mean_len=9.0)
