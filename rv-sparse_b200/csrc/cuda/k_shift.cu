@@ -30,9 +30,14 @@
 //
 // Whether to look at all is decided on the device: a probe keys rows spread
 // over A and one block sorts the keys; the analysis runs when at least half
-// of them have a translate among the others.  Every pass after the probe
-// reads that flag (*on) and returns at once when it is 0, so the plan queues
-// them without a host round trip.
+// of them have a translate among the others and they average enough
+// products.  The plan reads that flag (*on) back before it queues the
+// passes; every pass also reads it on the device and returns at once when it
+// is 0.
+//
+// The key and check passes give each warp 32 consecutive rows, a lane per
+// row, over the rows' column indices staged in the warp's shared memory
+// (see SegRows below).
 #include <climits>
 
 #include "device_common.cuh"
